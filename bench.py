@@ -1,0 +1,316 @@
+"""Benchmark of the B200 PDHG engine on the config-2 LP.
+
+Workload: the seeded random LP with m=40,000 rows, n=80,000 columns and
+512,025 nonzeros (6.4 per column, 1% of the rows hold 10% of the nonzeros),
+solved by restarted-Halpern PDHG to relative KKT 1e-6.  One step = one full
+solve from the cold start.
+
+Metric: time to relative KKT 1e-6, in seconds (lower is better).
+  value : device time of the PDHG loop (CUDA events on the engine's stream),
+          with the prepared problem already resident in HBM; L2 is flushed
+          (a 512 MiB write) before every step.
+  e2e   : the same solve through the public C ABI (b2p_solve_pdhg) from host
+          arrays: host preprocessing, host->device upload, the loop and the
+          device->host read of x and y, wall clock per step.
+N > 1 (torchrun): N independent replicas of the same solve, one per GPU
+("replicas only": a single LP is not partitioned); the reported time is the
+maximum over ranks.
+
+``--impl reference`` times the reference's own multithreaded CPU PDHG
+(oracle/_ref/libpramana_ref.so, built from the reference sources) on the
+host's cores, on a bounded sample of the same solve.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "optimized-gpu-accelerator_b200")]
+
+METRIC = "time-to-1e-6 rel KKT (s) & SpMV HBM GB/s: chosen form vs plain FP64 PDHG, B200"
+TOL = 1e-6
+SEED = 2
+CPU_SAMPLE_ITERS = 4096
+REF_ITERS_TO_TOL = 20288  # loop iterations of the reference CPU PDHG on this LP to 1e-6 (20,287 reported + 1)
+
+
+def workload_config(lp, extra=None):
+    cfg = {"workload": f"config-2 random LP m={lp.num_rows} n={lp.num_cols} nnz={lp.nnz} "
+                       f"(1% rows hold 10% nnz), seed {SEED}, to rel KKT {TOL:g}",
+           "form": "plain FP64 (iterate parity with the reference)", "check_every": 64,
+           "l2": "flushed before every step (512 MiB device write); the LP itself (~20 MB/iteration) is L2-resident "
+                 "within a solve"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_c2_traffic.txt")
+    try:
+        with open(p) as f:
+            for ln in f:
+                if ln.startswith("dram_bytes_per_launch:"):
+                    return float(ln.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_reference_sample(lp, iters: int, threads: int):
+    """Reference CPU PDHG (oracle/_ref) for a fixed number of iterations; returns s/iteration."""
+    from oracle import oracle as O
+    O.set_ref_threads(threads)
+    t0 = time.perf_counter()
+    O.solve(lp, "ref", tolerance=1e-30, max_iterations=iters)
+    wall = time.perf_counter() - t0
+    st = O.solve.last_stats
+    return st["solve_seconds"] / iters, wall, st
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's own CPU PDHG on this host's cores."""
+    if rank != 0:
+        return 0
+    from pramana_b200 import generators as G
+    from oracle import oracle as O
+    lp = G.config2(SEED)
+    threads = os.cpu_count() or 1
+    if not O.available("ref"):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libpramana_ref.so was not built"}))
+        return 0
+    per_iter = []
+    for s in range(args.warmup + args.steps):
+        spi, wall, st = cpu_reference_sample(lp, args.cpu_sample_iters, threads)
+        if s >= args.warmup:
+            per_iter.append(spi)
+    spi = statistics.mean(per_iter)
+    value = spi * REF_ITERS_TO_TOL
+    sample = (f"first {args.cpu_sample_iters} of the {REF_ITERS_TO_TOL} PDHG iterations the reference needs on this "
+              f"LP, per step; value = mean s/iteration x {REF_ITERS_TO_TOL}")
+    line = {"metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "config": workload_config(lp), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-sample-iters", type=int, default=CPU_SAMPLE_ITERS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-iters", type=int, default=0,
+                    help="small case for ncu: stop every solve after this many iterations, skip e2e and the CPU "
+                         "baseline; the printed line is not a benchmark result")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    from pramana_b200 import generators as G
+    from pramana_b200 import pdhg
+
+    lp = G.config2(SEED)
+    po = pdhg.PdhgOptions(tolerance=TOL, device=dev)
+    if args.profile_iters > 0:
+        po.maxIterations = args.profile_iters
+    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{dev}")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- value: device-timed loop, problem resident in HBM ----
+    eng = pdhg.Engine(lp, po)
+    for _ in range(args.warmup):
+        flush.zero_()
+        torch.cuda.synchronize()
+        eng.solve()
+    times, launches, iters = [], 0, None
+    barrier()
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            r = eng.solve()[0]
+            st = eng.last_stats
+            times.append(st.kernel_seconds)
+            launches += st.kernel_launches
+            iters = r.iterations
+            assert r.status == "Optimal" or args.profile_iters > 0, r.status
+        barrier()
+    t_dev = statistics.mean(times)
+
+    # ---- roofline of the dominant kernel: a profiled solve (events around every SpMV kernel) ----
+    eng.set_profiling(True)
+    flush.zero_()
+    torch.cuda.synchronize()
+    eng.solve()
+    eng.set_profiling(False)
+    prof = []
+    for cls, name in ((0, "k_primal"), (1, "k_dual")):
+        n_l, ms = eng.kernel_times(cls)
+        prof.append((ms, n_l, name, eng.kernel_bytes(cls)))
+    prof.sort(reverse=True)
+    ms, n_l, kname, kbytes = prof[0]
+    avg_s = ms / 1e3 / max(1, n_l)
+    achieved = kbytes / avg_s / 1e9
+    peak, peak_kind = measured_peak()
+    spmv_total_bytes = sum(p[3] * p[1] for p in prof)
+    spmv_total_s = sum(p[0] for p in prof) / 1e3
+    eng.close()
+
+    if args.profile_iters > 0:
+        print(json.dumps({"profile_run": True, "iterations": iters, "device_s_per_solve": t_dev,
+                          "dominant_kernel": kname, "avg_launch_us": avg_s * 1e6}))
+        return 0
+
+    # ---- e2e: public C ABI from host arrays ----
+    e2e_times, h2d, d2h = [], 0, 0
+    for s in range(args.warmup + args.steps):
+        flush.zero_()
+        barrier()
+        t0 = time.perf_counter()
+        r = pdhg.solvePdhg(lp, po)
+        t1 = time.perf_counter()
+        if s >= args.warmup:
+            e2e_times.append(t1 - t0)
+            h2d, d2h = r.stats.bytesUploaded, r.stats.bytesDownloaded
+    t_e2e = statistics.mean(e2e_times)
+
+    if dist is not None:
+        tt = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_dev, t_e2e = tt.tolist()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+        if O.available("ref"):
+            threads = os.cpu_count() or 1
+            spi, wall, _ = cpu_reference_sample(lp, args.cpu_sample_iters, threads)
+            cpu = {"value": spi * REF_ITERS_TO_TOL, "unit": "s", "cores": threads, "kind": "reference",
+                   "sample": f"first {args.cpu_sample_iters} of {REF_ITERS_TO_TOL} iterations of the same LP "
+                             f"({wall:.1f} s), scaled by iteration count"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": t_dev, "unit": "s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_dev * 1e3, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+                "config": workload_config(lp, {"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                                               "iterations": iters}),
+                "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "gpu_launches": launches,
+                "spmv_gbs": spmv_total_bytes / spmv_total_s / 1e9,
+                "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "peak_source": peak_kind,
+                             "traffic": ncu_traffic(kname), "algorithmic_bytes_per_launch": kbytes,
+                             "avg_launch_us": avg_s * 1e6, "launches_profiled": n_l},
+                "clocks": clk.summary(),
+                "cpu_baseline": cpu}
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

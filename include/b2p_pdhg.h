@@ -1,0 +1,190 @@
+/*
+ * b2p_pdhg.h -- C ABI of the B200 (sm_100a) restarted-Halpern PDHG engine.
+ *
+ * This is the drop-in boundary for PRAMANA's PDHG engine.  The reference
+ * exposes the path as C++ (src/pdhg/pdhg.h:73-80):
+ *
+ *   PdhgResult solvePdhg(const Model&, const PdhgOptions&, const Deadline*);
+ *   std::vector<PdhgResult> solvePdhgBatch(const Model&, const std::vector<LpCase>&,
+ *                                          const PdhgOptions&, const Deadline*, PdhgStats*);
+ *   bool gpuAvailable();
+ *   Json gpuInfoJson();
+ *
+ * and drives its GPU through gpu::CudaContext (src/gpu/cuda_driver.h:43-81)
+ * and the GpuBackend class (src/pdhg/pdhg.cpp:219-389).  The entry points
+ * below replace those: plain pointers and sizes, int return codes, no C++
+ * types and no exceptions across the boundary.  Results are in the original
+ * space of the (minimisation) model, exactly like PdhgResult.
+ *
+ * Errors: every function returns B2P_OK (0) or a B2P_ERR_* code, and
+ * b2p_last_error() gives a message for the calling thread.  There is no CPU
+ * fallback: without a usable sm_100 device the solve entry points return
+ * B2P_ERR_NO_DEVICE.
+ *
+ * Threading: one solve per calling thread; an engine object must not be used
+ * from two threads at once.
+ */
+#ifndef B2P_PDHG_H
+#define B2P_PDHG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Return codes. */
+enum {
+  B2P_OK = 0,
+  B2P_ERR_INVALID = 1,   /* bad argument or inconsistent model */
+  B2P_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+  B2P_ERR_NO_DEVICE = 3, /* no usable sm_100 GPU (or disabled by PRAMANA_DISABLE_GPU) */
+  B2P_ERR_OOM = 4,       /* device allocation failed */
+  B2P_ERR_TOO_LARGE = 5  /* size beyond a documented maximum */
+};
+
+/* Termination status; the numbering is pramana::Status (src/util/common.h:27-39). */
+enum {
+  B2P_STATUS_NOT_SOLVED = 0,
+  B2P_STATUS_OPTIMAL = 1,
+  B2P_STATUS_TIME_LIMIT = 5,
+  B2P_STATUS_ITERATION_LIMIT = 6
+};
+
+/* Arithmetic of the iterates. */
+enum {
+  B2P_PRECISION_FP64 = 0 /* plain form: FP64 everywhere, iterate parity with the reference */
+};
+
+/* A minimisation LP  min c'x + offset, L <= Ax <= U, l <= x <= u, with A in
+ * CSC form.  Replaces pramana::Model + SparseMatrix (src/core/model.h:24-64,
+ * src/core/sparse.h:11-16).  Bounds with |v| >= 1e20 are infinite. */
+typedef struct b2p_lp {
+  int32_t num_rows;
+  int32_t num_cols;
+  const int32_t* start; /* num_cols + 1 column pointers */
+  const int32_t* index; /* row index of each nonzero */
+  const double* value;
+  const double* col_cost;
+  const double* col_lower;
+  const double* col_upper;
+  const double* row_lower;
+  const double* row_upper;
+  double obj_offset;
+} b2p_lp;
+
+/* One case of a family sharing A; NULL means "same as the base model".
+ * Replaces pramana::LpCase (src/pdhg/pdhg.h:67-70). */
+typedef struct b2p_case {
+  const double* cost;
+  const double* col_lower;
+  const double* col_upper;
+  const double* row_lower;
+  const double* row_upper;
+} b2p_case;
+
+/* Replaces pramana::PdhgOptions (src/pdhg/pdhg.h:32-42) plus the Deadline
+ * (src/util/timer.h:22-42) and the device choice (PRAMANA_GPU_DEVICE,
+ * src/gpu/cuda_driver.cpp:223). */
+typedef struct b2p_options {
+  double tolerance;         /* relative KKT tolerance (default 1e-6) */
+  int64_t max_iterations;   /* default 1,000,000 */
+  int32_t check_every;      /* iterations between convergence checks (default 64) */
+  int32_t ruiz_iterations;  /* default 10 */
+  int32_t pock_chambolle;   /* default 1 */
+  int32_t rescale_objective_and_bounds; /* default 1 */
+  double reflection;        /* rho in [0,1] (default 1) */
+  int32_t log_interval;     /* progress line every N checks on stderr (0 = off) */
+  int32_t device;           /* CUDA ordinal; -1 = PRAMANA_GPU_DEVICE or 0 */
+  double time_limit;        /* seconds; <= 0 = none */
+  const volatile int32_t* cancel_flag; /* polled at every check when non-NULL; nonzero = stop */
+  int32_t precision;        /* B2P_PRECISION_* */
+  int32_t use_graphs;       /* capture each check interval as one CUDA graph (default 1) */
+} b2p_options;
+
+/* Replaces pramana::PdhgStats (src/pdhg/pdhg.h:44-56). */
+typedef struct b2p_stats {
+  int64_t iterations;
+  int32_t restarts;
+  int32_t pad0;
+  double primal_residual, dual_residual, gap;
+  double primal_weight;
+  double setup_seconds, solve_seconds;
+  double kernel_seconds;   /* device time of the iteration loop (CUDA events) */
+  double transfer_seconds; /* host<->device copies */
+  int64_t bytes_uploaded, bytes_downloaded, kernel_launches;
+  double spectral_norm;
+} b2p_stats;
+
+/* Replaces pramana::PdhgResult (src/pdhg/pdhg.h:58-65) minus the vectors,
+ * which go to caller-provided arrays. */
+typedef struct b2p_result {
+  int32_t status; /* B2P_STATUS_* */
+  int32_t pad0;
+  int64_t iterations;
+  double objective, dual_objective;
+  double relative_kkt;
+} b2p_result;
+
+/* Fills the reference defaults (src/pdhg/pdhg.h:32-42). */
+void b2p_default_options(b2p_options* opts);
+
+/* solvePdhg (src/pdhg/pdhg.cpp:712-717): x[num_cols], row_dual[num_rows]
+ * receive the solution in the original space; either may be NULL. */
+int b2p_solve_pdhg(const b2p_lp* lp, const b2p_options* opts, double* x, double* row_dual, b2p_result* result,
+                   b2p_stats* stats);
+
+/* solvePdhgBatch (src/pdhg/pdhg.cpp:719-728): num_cases LPs sharing A.
+ * x is num_cases x num_cols and row_dual num_cases x num_rows (row-major by
+ * case); results has num_cases entries. */
+int b2p_solve_pdhg_batch(const b2p_lp* base, const b2p_case* cases, int32_t num_cases, const b2p_options* opts,
+                         double* x, double* row_dual, b2p_result* results, b2p_stats* batch_stats);
+
+/* gpuAvailable (src/pdhg/pdhg.cpp:730): 1 if an sm_100 device is usable. */
+int b2p_gpu_available(void);
+
+/* gpuInfoJson (src/pdhg/pdhg.cpp:732-746): writes a NUL-terminated JSON
+ * object into buf (cap bytes) and returns the full length needed. */
+int b2p_gpu_info_json(char* buf, size_t cap);
+
+/* Message of the last error on this thread ("" if none). */
+const char* b2p_last_error(void);
+
+/* ---- Two-phase form of the same solve --------------------------------------
+ * b2p_engine_create does the work of runPdhg before its loop (prepare,
+ * GpuBackend::init uploads, case vectors; src/pdhg/pdhg.cpp:485-558);
+ * b2p_engine_solve runs the loop (pdhg.cpp:560-687) from the initial point,
+ * and may be called again to repeat the identical solve; b2p_engine_fetch
+ * copies the last solution back.  num_cases <= 0 means a single solve of the
+ * base model. */
+typedef struct b2p_engine b2p_engine;
+
+int b2p_engine_create(const b2p_lp* lp, const b2p_case* cases, int32_t num_cases, const b2p_options* opts,
+                      b2p_engine** out);
+int b2p_engine_solve(b2p_engine* e, b2p_result* results, b2p_stats* stats);
+int b2p_engine_fetch(b2p_engine* e, double* x, double* row_dual);
+int b2p_engine_destroy(b2p_engine* e);
+/* When on, every fused SpMV kernel launch of the next solve is bracketed by
+ * CUDA events; b2p_engine_kernel_times then returns, per kernel class
+ * (0 = A^T y + primal step, 1 = A x+ + dual step), the launch count and the
+ * summed device milliseconds. */
+int b2p_engine_set_profiling(b2p_engine* e, int32_t on);
+int b2p_engine_kernel_times(b2p_engine* e, int32_t kernel_class, int64_t* launches, double* total_ms);
+/* Algorithmic bytes of one launch of a kernel class (CSR values, indices and
+ * row pointers read once, gathered vector read once, every streamed vector
+ * read or written once). */
+int b2p_engine_kernel_bytes(b2p_engine* e, int32_t kernel_class, double* bytes);
+
+/* ---- Kernel-level entry -------------------------------------------------
+ * y(i,b) = sum_p val[p] * x(idx[p], b) for a CSR matrix (rows x cols) and k
+ * interleaved right-hand sides (element (i,b) at i*k+b), summed left to right
+ * like CpuBackend::mult (src/pdhg/pdhg.cpp:93-103).  Host arrays in and out. */
+int b2p_csr_spmv(int32_t rows, int32_t cols, int32_t k, const int32_t* ptr, const int32_t* idx, const double* val,
+                 const double* x, double* y);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B2P_PDHG_H */

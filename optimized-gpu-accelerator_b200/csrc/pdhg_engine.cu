@@ -1,0 +1,811 @@
+// PDHG engine for one B200: device state, the iteration loop, and the C ABI
+// declared in include/b2p_pdhg.h.
+//
+// The loop restates runPdhg (src/pdhg/pdhg.cpp:483-687).  What changes is
+// how it drives the GPU:
+//   - one check interval (check_every iterations, ending with the check) is
+//     enqueued as 2 fused kernels per iteration plus 4 check kernels and one
+//     small device->host copy, and captured once into a CUDA graph that is
+//     replayed for every interval (the reference issues ~8 launches per
+//     iteration and 2-4 blocking copies per check, pdhg.cpp:286-370);
+//   - the check reductions finish on the device: the host reads 10 doubles
+//     per case per check;
+//   - the host keeps exactly the reference's decisions (termination, restart,
+//     primal weight; pdhg.cpp:604-659) in FP64 with the C library's sqrt/exp/log.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/b2p_pdhg.h"
+#include "pdhg_kernels.cuh"
+#include "pdhg_prepare.h"
+
+namespace b2p {
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define B2P_CUDA(call)                                                                                     \
+  do {                                                                                                     \
+    cudaError_t e_ = (call);                                                                               \
+    if (e_ != cudaSuccess)                                                                                 \
+      throw Error(e_ == cudaErrorMemoryAllocation ? B2P_ERR_OOM : B2P_ERR_CUDA,                            \
+                  std::string("CUDA error in ") + #call + ": " + cudaGetErrorString(e_));                  \
+  } while (0)
+
+using Clock = std::chrono::steady_clock;
+double seconds_since(Clock::time_point t0) { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+
+// Device vector slots (the reference's enum V, src/pdhg/pdhg.cpp:45, minus
+// ATY/ATYP which the fused kernels never store, plus the initial point).
+enum Slot : int { X, XP, X0, C, LO, UP, XINIT, NCOLVEC, Y = NCOLVEC, YP, Y0, AX, AXP, AX0, RL, RU, AXINIT, NSLOT };
+inline bool row_slot(int s) { return s >= Y; }
+
+int pick_device(int requested) {
+  if (std::getenv("PRAMANA_DISABLE_GPU")) throw Error(B2P_ERR_NO_DEVICE, "disabled by PRAMANA_DISABLE_GPU");
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    throw Error(B2P_ERR_NO_DEVICE, "no CUDA device");
+  }
+  int dev = requested;
+  if (dev < 0) {
+    const char* env = std::getenv("PRAMANA_GPU_DEVICE");
+    dev = env ? std::atoi(env) : 0;
+  }
+  if (dev < 0 || dev >= count) throw Error(B2P_ERR_NO_DEVICE, "device ordinal out of range");
+  cudaDeviceProp p;
+  B2P_CUDA(cudaGetDeviceProperties(&p, dev));
+  if (p.major != 10) throw Error(B2P_ERR_NO_DEVICE, std::string("device is not sm_100: ") + p.name);
+  return dev;
+}
+
+void check_lp(const b2p_lp* lp) {
+  if (!lp) throw Error(B2P_ERR_INVALID, "lp is NULL");
+  if (lp->num_rows < 0 || lp->num_cols < 0) throw Error(B2P_ERR_INVALID, "negative dimension");
+  if (!lp->start) throw Error(B2P_ERR_INVALID, "start is NULL");
+  if (lp->start[0] != 0) throw Error(B2P_ERR_INVALID, "start[0] must be 0");
+  for (int32_t j = 0; j < lp->num_cols; ++j)
+    if (lp->start[j + 1] < lp->start[j]) throw Error(B2P_ERR_INVALID, "start must be non-decreasing");
+  const int32_t nnz = lp->start[lp->num_cols];
+  if (nnz > 0 && (!lp->index || !lp->value)) throw Error(B2P_ERR_INVALID, "index/value are NULL");
+  for (int32_t q = 0; q < nnz; ++q)
+    if (lp->index[q] < 0 || lp->index[q] >= lp->num_rows) throw Error(B2P_ERR_INVALID, "row index out of range");
+  if (lp->num_cols > 0 && (!lp->col_cost || !lp->col_lower || !lp->col_upper))
+    throw Error(B2P_ERR_INVALID, "column vectors are NULL");
+  if (lp->num_rows > 0 && (!lp->row_lower || !lp->row_upper)) throw Error(B2P_ERR_INVALID, "row vectors are NULL");
+}
+
+}  // namespace
+
+struct Engine {
+  // ---- problem ----
+  int device = 0;
+  int n = 0, m = 0, k = 1;
+  bool batch = false;
+  b2p_options opt{};
+  Prepared P;
+  std::vector<double> cNorm, rhsNorm, omega0;
+  double eta = 0;
+
+  // ---- device ----
+  cudaStream_t stream = nullptr;
+  std::vector<void*> allocs;
+  int32_t *dA_ptr = nullptr, *dA_idx = nullptr, *dT_ptr = nullptr, *dT_idx = nullptr;
+  double *dA_val = nullptr, *dT_val = nullptr, *d_rfac = nullptr, *d_cfac = nullptr;
+  double* v[NSLOT] = {};
+  double *d_tau = nullptr, *d_sigma = nullptr, *d_prow = nullptr, *d_pcol = nullptr, *d_sums = nullptr;
+  int64_t *d_it_base = nullptr, *d_restart_at = nullptr;
+  int32_t* d_mask = nullptr;
+  int g_rows = 1, g_cols = 1;
+
+  // ---- pinned host ----
+  double* h_sums = nullptr;   // k * kNumSums
+  double* h_steps = nullptr;  // tau[k], sigma[k]
+  int32_t* h_mask = nullptr;
+
+  // ---- graphs and profiling ----
+  std::map<int, cudaGraphExec_t> graphs;
+  std::map<int, cudaGraph_t> graph_defs;
+  bool profiling = false;
+  std::vector<cudaEvent_t> prof_ev;  // 4 per iteration of the longest interval
+  int64_t prof_launches[2] = {0, 0};
+  double prof_ms[2] = {0, 0};
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+
+  // ---- last solve ----
+  std::vector<double> x_out, y_out;  // num_cases x n / x m, original space
+  std::vector<b2p_result> results;
+  b2p_stats stats{};
+  int64_t launches = 0;
+  int64_t bytes_up = 0, bytes_down = 0;
+  double transfer_seconds = 0;
+
+  template <class T>
+  T* dalloc(size_t count) {
+    void* p = nullptr;
+    B2P_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    allocs.push_back(p);
+    return static_cast<T*>(p);
+  }
+  template <class T>
+  T* upload(const std::vector<T>& h) {
+    T* d = dalloc<T>(h.size());
+    if (!h.empty()) B2P_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+    bytes_up += static_cast<int64_t>(h.size() * sizeof(T));
+    return d;
+  }
+
+  ~Engine() {
+    for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+    for (auto& g : graph_defs) cudaGraphDestroy(g.second);
+    for (auto e : prof_ev) cudaEventDestroy(e);
+    if (ev_start) cudaEventDestroy(ev_start);
+    if (ev_stop) cudaEventDestroy(ev_stop);
+    for (void* p : allocs) cudaFree(p);
+    if (h_sums) cudaFreeHost(h_sums);
+    if (h_steps) cudaFreeHost(h_steps);
+    if (h_mask) cudaFreeHost(h_mask);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  CsrView viewA() const { return CsrView{dA_ptr, dA_idx, dA_val, m}; }
+  CsrView viewAT() const { return CsrView{dT_ptr, dT_idx, dT_val, n}; }
+  static unsigned blocks(int64_t len) { return static_cast<unsigned>(std::max<int64_t>(1, (len + kBlock - 1) / kBlock)); }
+  static int red_blocks(int64_t len) {
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(4 * 148, (len + kBlock - 1) / kBlock)));
+  }
+
+  void create(const b2p_lp* lp, const b2p_case* cases, int num_cases, const b2p_options* o) {
+    check_lp(lp);
+    if (o) opt = *o; else b2p_default_options(&opt);
+    if (opt.check_every <= 0) throw Error(B2P_ERR_INVALID, "check_every must be positive");
+    if (opt.precision != B2P_PRECISION_FP64) throw Error(B2P_ERR_INVALID, "unsupported precision");
+    device = pick_device(opt.device);
+    B2P_CUDA(cudaSetDevice(device));
+    B2P_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    B2P_CUDA(cudaEventCreate(&ev_start));
+    B2P_CUDA(cudaEventCreate(&ev_stop));
+    batch = num_cases > 0;
+    k = batch ? num_cases : 1;
+    n = lp->num_cols;
+    m = lp->num_rows;
+    const auto t0 = Clock::now();
+
+    PrepareOptions po;
+    po.ruiz_iterations = opt.ruiz_iterations;
+    po.pock_chambolle = opt.pock_chambolle != 0;
+    po.rescale = opt.rescale_objective_and_bounds != 0;
+    P = prepare(m, n, lp->start, lp->index, lp->value, lp->col_cost, lp->row_lower, lp->row_upper, lp->obj_offset,
+                po);
+
+    // Case data in scaled space, k-interleaved (src/pdhg/pdhg.cpp:466-481, 506-530).
+    const size_t nk = static_cast<size_t>(n) * k, mk = static_cast<size_t>(m) * k;
+    std::vector<double> c(nk), lo(nk), up(nk), rl(mk), ru(mk), x(nk);
+    cNorm.assign(k, 0.0);
+    rhsNorm.assign(k, 0.0);
+    omega0.assign(k, 1.0);
+    for (int b = 0; b < k; ++b) {
+      const b2p_case* cs = batch ? &cases[b] : nullptr;
+      const double* cc = (cs && cs->cost) ? cs->cost : lp->col_cost;
+      const double* cl = (cs && cs->col_lower) ? cs->col_lower : lp->col_lower;
+      const double* cu = (cs && cs->col_upper) ? cs->col_upper : lp->col_upper;
+      const double* rlo = (cs && cs->row_lower) ? cs->row_lower : lp->row_lower;
+      const double* rup = (cs && cs->row_upper) ? cs->row_upper : lp->row_upper;
+      double s = 0;
+      for (int j = 0; j < n; ++j) s += cc[j] * cc[j];
+      cNorm[b] = std::sqrt(s);
+      s = 0;
+      for (int i = 0; i < m; ++i) {
+        if (finite_bound(rlo[i])) s += rlo[i] * rlo[i];
+        if (finite_bound(rup[i]) && rup[i] != rlo[i]) s += rup[i] * rup[i];
+      }
+      rhsNorm[b] = std::sqrt(s);
+      double cn = 0, bn = 0;
+      for (int j = 0; j < n; ++j) {
+        const size_t t = static_cast<size_t>(j) * k + b;
+        c[t] = cc[j] * P.Cs[j] / P.gamma;
+        lo[t] = finite_bound(cl[j]) ? cl[j] / P.Cs[j] / P.beta : -HUGE_VAL;
+        up[t] = finite_bound(cu[j]) ? cu[j] / P.Cs[j] / P.beta : HUGE_VAL;
+        x[t] = smin(smax(0.0, lo[t]), up[t]);
+        cn += c[t] * c[t];
+      }
+      for (int i = 0; i < m; ++i) {
+        const size_t t = static_cast<size_t>(i) * k + b;
+        rl[t] = finite_bound(rlo[i]) ? rlo[i] * P.R[i] / P.beta : -HUGE_VAL;
+        ru[t] = finite_bound(rup[i]) ? rup[i] * P.R[i] / P.beta : HUGE_VAL;
+        if (finite_bound(rl[t])) bn += rl[t] * rl[t];
+        if (finite_bound(ru[t]) && ru[t] != rl[t]) bn += ru[t] * ru[t];
+      }
+      if (cn > 1e-20 && bn > 1e-20) omega0[b] = std::sqrt(cn) / std::sqrt(bn);
+    }
+    eta = 0.998 / P.normA;
+
+    // ---- device state (GpuBackend::init, src/pdhg/pdhg.cpp:238-277) ----
+    const auto tx = Clock::now();
+    dA_ptr = upload(P.A.ptr);
+    dA_idx = upload(P.A.idx);
+    dA_val = upload(P.A.val);
+    dT_ptr = upload(P.AT.ptr);
+    dT_idx = upload(P.AT.idx);
+    dT_val = upload(P.AT.val);
+    d_rfac = upload(P.rfac);
+    d_cfac = upload(P.cfac);
+    for (int s = 0; s < NSLOT; ++s) v[s] = dalloc<double>(row_slot(s) ? mk : nk);
+    auto put = [&](int s, const std::vector<double>& h) {
+      if (!h.empty())
+        B2P_CUDA(cudaMemcpyAsync(v[s], h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+      bytes_up += static_cast<int64_t>(h.size() * sizeof(double));
+    };
+    put(C, c);
+    put(LO, lo);
+    put(UP, up);
+    put(RL, rl);
+    put(RU, ru);
+    put(XINIT, x);
+    d_tau = dalloc<double>(k);
+    d_sigma = dalloc<double>(k);
+    d_it_base = dalloc<int64_t>(1);
+    d_restart_at = dalloc<int64_t>(k);
+    d_mask = dalloc<int32_t>(k);
+    g_rows = red_blocks(m);
+    g_cols = red_blocks(n);
+    d_prow = dalloc<double>(static_cast<size_t>(k) * g_rows * kRowSums);
+    d_pcol = dalloc<double>(static_cast<size_t>(k) * g_cols * kRowSums);
+    d_sums = dalloc<double>(static_cast<size_t>(k) * kNumSums);
+    B2P_CUDA(cudaMallocHost(&h_sums, sizeof(double) * k * kNumSums));
+    B2P_CUDA(cudaMallocHost(&h_steps, sizeof(double) * 2 * k));
+    B2P_CUDA(cudaMallocHost(&h_mask, sizeof(int32_t) * k));
+    // AX = A x0 on the device (pdhg.cpp:540-545), kept as the restart point of every solve.
+    if (m > 0) {
+      k_spmv<<<blocks(static_cast<int64_t>(m) * k), kBlock, 0, stream>>>(m, k, viewA(), v[XINIT], v[AXINIT]);
+      B2P_CUDA(cudaGetLastError());
+    }
+    B2P_CUDA(cudaStreamSynchronize(stream));
+    transfer_seconds = seconds_since(tx);
+    stats.setup_seconds = seconds_since(t0);
+    stats.spectral_norm = P.normA;
+  }
+
+  void reset_state(std::vector<double>& omega) {
+    const size_t nk = static_cast<size_t>(n) * k, mk = static_cast<size_t>(m) * k;
+    auto cp = [&](int dst, int src, size_t len) {
+      if (len) B2P_CUDA(cudaMemcpyAsync(v[dst], v[src], len * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    };
+    cp(X, XINIT, nk);
+    cp(X0, XINIT, nk);
+    cp(AX, AXINIT, mk);
+    cp(AX0, AXINIT, mk);
+    if (mk) {
+      B2P_CUDA(cudaMemsetAsync(v[Y], 0, mk * sizeof(double), stream));
+      B2P_CUDA(cudaMemsetAsync(v[Y0], 0, mk * sizeof(double), stream));
+      B2P_CUDA(cudaMemsetAsync(v[YP], 0, mk * sizeof(double), stream));
+      B2P_CUDA(cudaMemsetAsync(v[AXP], 0, mk * sizeof(double), stream));
+    }
+    if (nk) B2P_CUDA(cudaMemsetAsync(v[XP], 0, nk * sizeof(double), stream));
+    B2P_CUDA(cudaMemsetAsync(d_it_base, 0, sizeof(int64_t), stream));
+    B2P_CUDA(cudaMemsetAsync(d_restart_at, 0, sizeof(int64_t) * k, stream));
+    omega = omega0;
+    upload_steps(omega);
+  }
+
+  void upload_steps(const std::vector<double>& omega) {
+    for (int b = 0; b < k; ++b) {
+      h_steps[b] = eta / omega[b];
+      h_steps[k + b] = eta * omega[b];
+    }
+    B2P_CUDA(cudaMemcpyAsync(d_tau, h_steps, sizeof(double) * k, cudaMemcpyHostToDevice, stream));
+    B2P_CUDA(cudaMemcpyAsync(d_sigma, h_steps + k, sizeof(double) * k, cudaMemcpyHostToDevice, stream));
+    bytes_up += static_cast<int64_t>(2 * k * sizeof(double));
+  }
+
+  void ensure_prof_events(int L) {
+    const size_t need = static_cast<size_t>(4) * L;
+    while (prof_ev.size() < need) {
+      cudaEvent_t e;
+      B2P_CUDA(cudaEventCreate(&e));
+      prof_ev.push_back(e);
+    }
+  }
+
+  // Enqueues one check interval of L iterations on the stream (captured or not).
+  void enqueue_interval(int L) {
+    const double rho = opt.reflection;
+    const int64_t nk = static_cast<int64_t>(n) * k, mk = static_cast<int64_t>(m) * k;
+    const unsigned gp = blocks(nk), gd = blocks(mk);
+    const CsrView A = viewA(), AT = viewAT();
+    for (int l = 0; l < L; ++l) {
+      const bool last = l == L - 1;
+      const IterClock ck{d_it_base, d_restart_at, l};
+      if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 0], stream));
+      if (nk) {
+        if (last)
+          k_primal<false><<<gp, kBlock, 0, stream>>>(n, k, AT, v[Y], v[C], v[LO], v[UP], v[X], v[XP], v[X0], d_tau, ck, rho);
+        else
+          k_primal<true><<<gp, kBlock, 0, stream>>>(n, k, AT, v[Y], v[C], v[LO], v[UP], v[X], v[XP], v[X0], d_tau, ck, rho);
+      }
+      if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 1], stream));
+      if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 2], stream));
+      if (mk) {
+        if (last)
+          k_dual<false><<<gd, kBlock, 0, stream>>>(m, k, A, v[XP], v[RL], v[RU], v[Y], v[YP], v[Y0], v[AX], v[AXP],
+                                                  v[AX0], d_sigma, ck, rho);
+        else
+          k_dual<true><<<gd, kBlock, 0, stream>>>(m, k, A, v[XP], v[RL], v[RU], v[Y], v[YP], v[Y0], v[AX], v[AXP],
+                                                 v[AX0], d_sigma, ck, rho);
+      }
+      if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 3], stream));
+      B2P_CUDA(cudaGetLastError());
+    }
+    const IterClock ck{d_it_base, d_restart_at, L - 1};
+    k_check_rows<<<dim3(g_rows, k), kBlock, 0, stream>>>(m, k, v[AXP], v[RL], v[RU], v[YP], v[Y], v[Y0], d_rfac,
+                                                         d_prow);
+    k_check_cols<<<dim3(g_cols, k), kBlock, 0, stream>>>(n, k, viewAT(), v[YP], v[XP], v[X], v[X0], v[C], v[LO],
+                                                         v[UP], d_cfac, d_pcol);
+    k_halpern_all<<<blocks(nk + mk), kBlock, 0, stream>>>(n, m, k, v[X], v[XP], v[X0], v[Y], v[YP], v[Y0], v[AX],
+                                                         v[AXP], v[AX0], ck, rho);
+    k_check_finalize<<<k, kBlock, 0, stream>>>(k, g_rows, g_cols, d_prow, d_pcol, d_sums, d_it_base, L);
+    B2P_CUDA(cudaGetLastError());
+    B2P_CUDA(cudaMemcpyAsync(h_sums, d_sums, sizeof(double) * k * kNumSums, cudaMemcpyDeviceToHost, stream));
+  }
+
+  int64_t launches_per_interval(int L) const {
+    return static_cast<int64_t>(L) * ((n ? 1 : 0) + (m ? 1 : 0)) + 4;
+  }
+
+  void run_interval(int L) {
+    if (profiling) ensure_prof_events(L);
+    if (opt.use_graphs && !profiling) {
+      auto it = graphs.find(L);
+      if (it == graphs.end()) {
+        cudaGraph_t g;
+        B2P_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        try {
+          enqueue_interval(L);
+        } catch (...) {
+          cudaStreamEndCapture(stream, &g);
+          if (g) cudaGraphDestroy(g);
+          throw;
+        }
+        B2P_CUDA(cudaStreamEndCapture(stream, &g));
+        cudaGraphExec_t ge;
+        B2P_CUDA(cudaGraphInstantiate(&ge, g, 0));
+        graph_defs[L] = g;
+        it = graphs.emplace(L, ge).first;
+      }
+      B2P_CUDA(cudaGraphLaunch(it->second, stream));
+    } else {
+      enqueue_interval(L);
+    }
+    launches += launches_per_interval(L);
+    bytes_down += static_cast<int64_t>(sizeof(double) * k * kNumSums);
+  }
+
+  void collect_profile(int L) {
+    if (!profiling) return;
+    for (int l = 0; l < L; ++l) {
+      float ms = 0;
+      if (n) {
+        B2P_CUDA(cudaEventElapsedTime(&ms, prof_ev[4 * l], prof_ev[4 * l + 1]));
+        prof_ms[0] += ms;
+        prof_launches[0]++;
+      }
+      if (m) {
+        B2P_CUDA(cudaEventElapsedTime(&ms, prof_ev[4 * l + 2], prof_ev[4 * l + 3]));
+        prof_ms[1] += ms;
+        prof_launches[1]++;
+      }
+    }
+  }
+
+  void download_iterates(std::vector<double>& xs, std::vector<double>& ys) {
+    const auto t0 = Clock::now();
+    xs.resize(static_cast<size_t>(n) * k);
+    ys.resize(static_cast<size_t>(m) * k);
+    if (!xs.empty())
+      B2P_CUDA(cudaMemcpyAsync(xs.data(), v[XP], xs.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    if (!ys.empty())
+      B2P_CUDA(cudaMemcpyAsync(ys.data(), v[YP], ys.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    B2P_CUDA(cudaStreamSynchronize(stream));
+    bytes_down += static_cast<int64_t>((xs.size() + ys.size()) * sizeof(double));
+    transfer_seconds += seconds_since(t0);
+  }
+
+  // runPdhg's loop (src/pdhg/pdhg.cpp:560-687).
+  void solve(Clock::time_point deadline_start) {
+    B2P_CUDA(cudaSetDevice(device));
+    const auto t_solve = Clock::now();
+    std::vector<double> omega;
+    launches = 0;
+    prof_launches[0] = prof_launches[1] = 0;
+    prof_ms[0] = prof_ms[1] = 0;
+    reset_state(omega);
+    results.assign(k, b2p_result{});
+    x_out.assign(static_cast<size_t>(n) * k, 0.0);
+    y_out.assign(static_cast<size_t>(m) * k, 0.0);
+    stats.restarts = 0;
+    std::vector<char> done(k, 0);
+    std::vector<double> fpRestart(k, INFINITY), fpPrev(k, INFINITY);
+    std::vector<int64_t> sinceRestart(k, 0);
+    std::vector<double> xs, ys;
+    int remaining = k;
+    int checks = 0;
+    const double scaleObj = P.beta * P.gamma;
+    const int cE = opt.check_every;
+    auto expired = [&]() {
+      if (opt.cancel_flag && *opt.cancel_flag) return true;
+      return opt.time_limit > 0 && seconds_since(deadline_start) >= opt.time_limit;
+    };
+    auto extract = [&](int b, int status, double relKkt, double pobj, double dobj, int64_t it) {
+      for (int j = 0; j < n; ++j)
+        x_out[static_cast<size_t>(b) * n + j] = xs[static_cast<size_t>(j) * k + b] * P.Cs[j] * P.beta;
+      for (int i = 0; i < m; ++i)
+        y_out[static_cast<size_t>(b) * m + i] = ys[static_cast<size_t>(i) * k + b] * P.R[i] * P.gamma;
+      b2p_result& r = results[b];
+      r.status = status;
+      r.iterations = it;
+      r.relative_kkt = relKkt;
+      r.objective = pobj + P.offset;
+      r.dual_objective = dobj + P.offset;
+    };
+
+    B2P_CUDA(cudaEventRecord(ev_start, stream));
+    int64_t it = 0;
+    bool expiredStop = false;
+    while (it < opt.max_iterations) {
+      const int L = static_cast<int>(std::min<int64_t>(cE, opt.max_iterations - it));
+      run_interval(L);
+      B2P_CUDA(cudaStreamSynchronize(stream));
+      collect_profile(L);
+      it += L - 1;  // index of the check iteration
+      ++checks;
+      bool anyRestart = false, fetched = false;
+      for (int b = 0; b < k; ++b) h_mask[b] = 0;
+      for (int b = 0; b < k; ++b) {
+        if (done[b]) continue;
+        const double* s = h_sums + static_cast<size_t>(b) * kNumSums;
+        const double pobj = s[CS_POBJ] * scaleObj;
+        const double dobj = (s[CS_ROW_DOBJ] + s[CS_COL_DOBJ]) * scaleObj;
+        const double relP = std::sqrt(s[CS_ROW_RES2]) / (1.0 + rhsNorm[b]);
+        const double relD = std::sqrt(s[CS_COL_RES2]) / (1.0 + cNorm[b]);
+        const double gap = std::fabs(pobj - dobj) / (1.0 + std::fabs(pobj) + std::fabs(dobj));
+        const double kktErr = smax(relP, smax(relD, gap));
+        if (k == 1) {
+          stats.primal_residual = relP;
+          stats.dual_residual = relD;
+          stats.gap = gap;
+        }
+        if (opt.log_interval > 0 && k == 1 && checks % opt.log_interval == 0)
+          std::fprintf(stderr,
+                       "  pdhg %8lld  pobj % .8e  dobj % .8e  relP %.2e  relD %.2e  gap %.2e  w %.2e  restarts %d  %.2fs\n",
+                       static_cast<long long>(it + 1), pobj + P.offset, dobj + P.offset, relP, relD, gap, omega[b],
+                       stats.restarts, seconds_since(t_solve));
+        if (relP <= opt.tolerance && relD <= opt.tolerance && gap <= opt.tolerance) {
+          if (!fetched) {
+            download_iterates(xs, ys);
+            fetched = true;
+          }
+          extract(b, B2P_STATUS_OPTIMAL, kktErr, pobj, dobj, it);
+          done[b] = 1;
+          --remaining;
+          continue;
+        }
+        sinceRestart[b] += cE;
+        const double fp = std::sqrt(omega[b] * s[CS_DX2] + s[CS_DY2] / omega[b]);
+        if (fpRestart[b] == INFINITY) fpRestart[b] = fp;
+        const bool restart = fp <= 0.2 * fpRestart[b] || (fp <= 0.8 * fpRestart[b] && fp > fpPrev[b]) ||
+                             sinceRestart[b] >= static_cast<int64_t>(0.36 * static_cast<double>(it + 1));
+        fpPrev[b] = fp;
+        if (restart) {
+          h_mask[b] = 1;
+          anyRestart = true;
+        }
+      }
+      if (anyRestart) {
+        // Primal weight from the movement since the last restart (pdhg.cpp:642-656).
+        for (int b = 0; b < k; ++b) {
+          if (!h_mask[b]) continue;
+          const double* s = h_sums + static_cast<size_t>(b) * kNumSums;
+          const double dxn = std::sqrt(s[CS_AX2]), dyn = std::sqrt(s[CS_AY2]);
+          if (dxn > 1e-10 && dyn > 1e-10) omega[b] = std::exp(0.5 * std::log(dyn / dxn) + 0.5 * std::log(omega[b]));
+          fpRestart[b] = std::sqrt(omega[b] * s[CS_DX2] + s[CS_DY2] / omega[b]);
+          fpPrev[b] = INFINITY;
+          sinceRestart[b] = 0;
+          stats.restarts++;
+        }
+        upload_steps(omega);
+      }
+      if (remaining == 0) break;
+      if (expired()) {
+        expiredStop = true;
+        break;
+      }
+      if (anyRestart) {
+        const int64_t nk = static_cast<int64_t>(n) * k, mk = static_cast<int64_t>(m) * k;
+        B2P_CUDA(cudaMemcpyAsync(d_mask, h_mask, sizeof(int32_t) * k, cudaMemcpyHostToDevice, stream));
+        bytes_up += static_cast<int64_t>(sizeof(int32_t) * k);
+        k_restart<<<blocks(std::max<int64_t>(nk + mk, k)), kBlock, 0, stream>>>(
+            n, m, k, d_mask, v[X], v[X0], v[XP], v[Y], v[Y0], v[YP], v[AX], v[AX0], v[AXP], d_it_base, d_restart_at);
+        B2P_CUDA(cudaGetLastError());
+        ++launches;
+      }
+      ++it;
+    }
+    B2P_CUDA(cudaEventRecord(ev_stop, stream));
+    B2P_CUDA(cudaEventSynchronize(ev_stop));
+    float ms = 0;
+    B2P_CUDA(cudaEventElapsedTime(&ms, ev_start, ev_stop));
+    stats.kernel_seconds = ms / 1000.0;
+    stats.solve_seconds = seconds_since(t_solve);
+    stats.iterations = it + (remaining == 0 ? 1 : 0);
+    stats.primal_weight = omega.empty() ? 1 : omega[0];
+    if (remaining > 0) {
+      // Unconverged cases: the last check's sums are the KKT of (x+, y+)
+      // (the reference recomputes the same quantities, pdhg.cpp:668-680).
+      download_iterates(xs, ys);
+      for (int b = 0; b < k; ++b) {
+        if (done[b]) continue;
+        const double* s = h_sums + static_cast<size_t>(b) * kNumSums;
+        const double pobj = s[CS_POBJ] * scaleObj, dobj = (s[CS_ROW_DOBJ] + s[CS_COL_DOBJ]) * scaleObj;
+        const double relP = std::sqrt(s[CS_ROW_RES2]) / (1 + rhsNorm[b]);
+        const double relD = std::sqrt(s[CS_COL_RES2]) / (1 + cNorm[b]);
+        const double gap = std::fabs(pobj - dobj) / (1 + std::fabs(pobj) + std::fabs(dobj));
+        extract(b, (expiredStop || expired()) ? B2P_STATUS_TIME_LIMIT : B2P_STATUS_ITERATION_LIMIT,
+                smax(relP, smax(relD, gap)), pobj, dobj, it);
+      }
+    }
+    stats.kernel_launches = launches;
+    stats.bytes_uploaded = bytes_up;
+    stats.bytes_downloaded = bytes_down;
+    stats.transfer_seconds = transfer_seconds;
+  }
+
+  double kernel_bytes(int cls) const {
+    // Algorithmic bytes of one launch per case-batch: the CSR operator
+    // (12 nnz + 4 (rows+1)), the gathered vector once (8 cols k), and the
+    // streamed vectors (primal: x, c, lo, up, x0 read + x, x+ written = 7;
+    // dual: y, ax, rl, ru, y0, ax0 read + y, y+, ax, ax+ written = 10).
+    const double nnz = static_cast<double>(P.A.val.size());
+    if (cls == 0) return 12.0 * nnz + 4.0 * (n + 1) + 8.0 * m * k + 8.0 * 7 * n * k;
+    return 12.0 * nnz + 4.0 * (m + 1) + 8.0 * n * k + 8.0 * 10 * m * k;
+  }
+};
+
+}  // namespace b2p
+
+using b2p::Engine;
+using b2p::Error;
+
+namespace {
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    b2p::g_last_error.clear();
+    f();
+    return B2P_OK;
+  } catch (Error& e) {
+    b2p::g_last_error = e.what();
+    return e.code;
+  } catch (std::bad_alloc&) {
+    b2p::g_last_error = "host out of memory";
+    return B2P_ERR_OOM;
+  } catch (std::exception& e) {
+    b2p::g_last_error = e.what();
+    return B2P_ERR_CUDA;
+  }
+}
+
+void copy_results(Engine& e, double* x, double* y, b2p_result* results, b2p_stats* stats) {
+  if (x && !e.x_out.empty()) std::memcpy(x, e.x_out.data(), e.x_out.size() * sizeof(double));
+  if (y && !e.y_out.empty()) std::memcpy(y, e.y_out.data(), e.y_out.size() * sizeof(double));
+  if (results) std::memcpy(results, e.results.data(), e.results.size() * sizeof(b2p_result));
+  if (stats) *stats = e.stats;
+}
+
+}  // namespace
+
+extern "C" {
+
+void b2p_default_options(b2p_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->tolerance = 1e-6;
+  o->max_iterations = 1000000;
+  o->check_every = 64;
+  o->ruiz_iterations = 10;
+  o->pock_chambolle = 1;
+  o->rescale_objective_and_bounds = 1;
+  o->reflection = 1.0;
+  o->log_interval = 0;
+  o->device = -1;
+  o->time_limit = 0;
+  o->cancel_flag = nullptr;
+  o->precision = B2P_PRECISION_FP64;
+  o->use_graphs = 1;
+}
+
+const char* b2p_last_error(void) { return b2p::g_last_error.c_str(); }
+
+int b2p_engine_create(const b2p_lp* lp, const b2p_case* cases, int32_t num_cases, const b2p_options* opts,
+                      b2p_engine** out) {
+  return guarded([&] {
+    if (!out) throw Error(B2P_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (num_cases > 0 && !cases) throw Error(B2P_ERR_INVALID, "cases is NULL");
+    auto e = std::make_unique<Engine>();
+    e->create(lp, cases, num_cases, opts);
+    *out = reinterpret_cast<b2p_engine*>(e.release());
+  });
+}
+
+int b2p_engine_solve(b2p_engine* h, b2p_result* results, b2p_stats* stats) {
+  return guarded([&] {
+    if (!h) throw Error(B2P_ERR_INVALID, "engine is NULL");
+    Engine& e = *reinterpret_cast<Engine*>(h);
+    e.solve(b2p::Clock::now());
+    copy_results(e, nullptr, nullptr, results, stats);
+  });
+}
+
+int b2p_engine_fetch(b2p_engine* h, double* x, double* y) {
+  return guarded([&] {
+    if (!h) throw Error(B2P_ERR_INVALID, "engine is NULL");
+    copy_results(*reinterpret_cast<Engine*>(h), x, y, nullptr, nullptr);
+  });
+}
+
+int b2p_engine_destroy(b2p_engine* h) {
+  return guarded([&] { delete reinterpret_cast<Engine*>(h); });
+}
+
+int b2p_engine_set_profiling(b2p_engine* h, int32_t on) {
+  return guarded([&] {
+    if (!h) throw Error(B2P_ERR_INVALID, "engine is NULL");
+    reinterpret_cast<Engine*>(h)->profiling = on != 0;
+  });
+}
+
+int b2p_engine_kernel_times(b2p_engine* h, int32_t cls, int64_t* launches, double* total_ms) {
+  return guarded([&] {
+    if (!h || cls < 0 || cls > 1) throw Error(B2P_ERR_INVALID, "bad engine or kernel class");
+    Engine& e = *reinterpret_cast<Engine*>(h);
+    if (launches) *launches = e.prof_launches[cls];
+    if (total_ms) *total_ms = e.prof_ms[cls];
+  });
+}
+
+int b2p_engine_kernel_bytes(b2p_engine* h, int32_t cls, double* bytes) {
+  return guarded([&] {
+    if (!h || cls < 0 || cls > 1 || !bytes) throw Error(B2P_ERR_INVALID, "bad engine, class or output");
+    *bytes = reinterpret_cast<Engine*>(h)->kernel_bytes(cls);
+  });
+}
+
+int b2p_solve_pdhg(const b2p_lp* lp, const b2p_options* opts, double* x, double* row_dual, b2p_result* result,
+                   b2p_stats* stats) {
+  return guarded([&] {
+    const auto t0 = b2p::Clock::now();
+    Engine e;
+    e.create(lp, nullptr, 0, opts);
+    e.solve(t0);
+    copy_results(e, x, row_dual, result, stats);
+  });
+}
+
+int b2p_solve_pdhg_batch(const b2p_lp* base, const b2p_case* cases, int32_t num_cases, const b2p_options* opts,
+                         double* x, double* row_dual, b2p_result* results, b2p_stats* batch_stats) {
+  return guarded([&] {
+    if (num_cases <= 0) return;  // solvePdhgBatch returns {} for no cases
+    if (!cases) throw Error(B2P_ERR_INVALID, "cases is NULL");
+    const auto t0 = b2p::Clock::now();
+    Engine e;
+    e.create(base, cases, num_cases, opts);
+    e.solve(t0);
+    copy_results(e, x, row_dual, results, batch_stats);
+  });
+}
+
+int b2p_gpu_available(void) {
+  try {
+    const int dev = b2p::pick_device(-1);
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, b2p::k_spmv) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    (void)dev;
+    return 1;
+  } catch (...) {
+    return 0;
+  }
+}
+
+int b2p_gpu_info_json(char* buf, size_t cap) {
+  std::string name, reason;
+  bool avail = false;
+  int major = 0, minor = 0, sms = 0, drv = 0, rt = 0, binver = 0;
+  double mem = 0, bw = 0;
+  try {
+    const int dev = b2p::pick_device(-1);
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, dev) == cudaSuccess) {
+      name = p.name;
+      major = p.major;
+      minor = p.minor;
+      sms = p.multiProcessorCount;
+      mem = static_cast<double>(p.totalGlobalMem);
+      int clk = 0, bus = 0;
+      cudaDeviceGetAttribute(&clk, cudaDevAttrMemoryClockRate, dev);
+      cudaDeviceGetAttribute(&bus, cudaDevAttrGlobalMemoryBusWidth, dev);
+      bw = 2.0 * clk * 1e3 * (bus / 8.0) / 1e9;
+    }
+    cudaDriverGetVersion(&drv);
+    cudaRuntimeGetVersion(&rt);
+    avail = b2p_gpu_available() != 0;
+    if (!avail) reason = "kernels not loadable on this device";
+    cudaFuncAttributes fa;
+    if (avail && cudaFuncGetAttributes(&fa, b2p::k_spmv) == cudaSuccess) binver = fa.binaryVersion;
+  } catch (std::exception& e) {
+    reason = e.what();
+  }
+  char tmp[1024];
+  int len = std::snprintf(tmp, sizeof(tmp),
+                          "{\"available\": %s, \"name\": \"%s\", \"reason\": \"%s\", \"compute_capability\": \"%d.%d\", "
+                          "\"multiprocessors\": %d, \"memory_bytes\": %.0f, \"peak_bandwidth_GBs\": %.1f, "
+                          "\"driver_version\": %d, \"runtime_version\": %d, \"kernel_binary_version\": %d, "
+                          "\"kernels\": \"ahead-of-time sm_100a\"}",
+                          avail ? "true" : "false", name.c_str(), reason.c_str(), major, minor, sms, mem, bw, drv, rt,
+                          binver);
+  if (buf && cap > 0) {
+    std::strncpy(buf, tmp, cap - 1);
+    buf[cap - 1] = '\0';
+  }
+  return len;
+}
+
+int b2p_csr_spmv(int32_t rows, int32_t cols, int32_t k, const int32_t* ptr, const int32_t* idx, const double* val,
+                 const double* x, double* y) {
+  return guarded([&] {
+    if (rows < 0 || cols < 0 || k <= 0 || !ptr || (rows > 0 && !y)) throw Error(B2P_ERR_INVALID, "bad arguments");
+    const int32_t nnz = ptr[rows];
+    for (int32_t i = 0; i < rows; ++i)
+      if (ptr[i + 1] < ptr[i]) throw Error(B2P_ERR_INVALID, "ptr must be non-decreasing");
+    for (int32_t q = 0; q < nnz; ++q)
+      if (idx[q] < 0 || idx[q] >= cols) throw Error(B2P_ERR_INVALID, "column index out of range");
+    const int dev = b2p::pick_device(-1);
+    B2P_CUDA(cudaSetDevice(dev));
+    Engine tmp;  // owns the allocations and the stream
+    B2P_CUDA(cudaStreamCreateWithFlags(&tmp.stream, cudaStreamNonBlocking));
+    int32_t* dp = tmp.upload(std::vector<int32_t>(ptr, ptr + rows + 1));
+    int32_t* di = tmp.upload(std::vector<int32_t>(idx, idx + nnz));
+    double* dv = tmp.upload(std::vector<double>(val, val + nnz));
+    double* dx = tmp.upload(std::vector<double>(x, x + static_cast<size_t>(cols) * k));
+    double* dy = tmp.dalloc<double>(static_cast<size_t>(rows) * k);
+    if (rows > 0) {
+      b2p::k_spmv<<<Engine::blocks(static_cast<int64_t>(rows) * k), b2p::kBlock, 0, tmp.stream>>>(
+          rows, k, b2p::CsrView{dp, di, dv, rows}, dx, dy);
+      B2P_CUDA(cudaGetLastError());
+      B2P_CUDA(cudaMemcpyAsync(y, dy, sizeof(double) * rows * k, cudaMemcpyDeviceToHost, tmp.stream));
+    }
+    B2P_CUDA(cudaStreamSynchronize(tmp.stream));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,342 @@
+// Device kernels of the PDHG engine (sm_100a, FP64 plain form).
+//
+// One PDHG iteration is two fused kernels instead of the reference's eight
+// launches (src/pdhg/pdhg.cpp:588-662, kernels.cpp:19-85):
+//   k_primal : aty = A^T y (row j of A^T), x+ = proj(x - tau (c - aty)),
+//              Halpern step of x                          (spmvT + primalStep + halpern x)
+//   k_dual   : ax+ = A x+ (row i of A), y+ = v + sigma proj(-v/sigma),
+//              Halpern steps of y and Ax                  (spmv + dualStep + halpern y, Ax)
+// At a check iteration the Halpern steps are deferred to k_halpern_all so
+// that the check reductions see the pre-Halpern x and y, as in the reference.
+//
+// Numerics: every row sum runs left to right from s = 0 with separately
+// rounded products and sums (__dmul_rn/__dadd_rn, no FMA contraction), which
+// is exactly CpuBackend::mult (src/pdhg/pdhg.cpp:93-103); the element-wise
+// updates use the reference's operation order.  The iterates are therefore
+// bit-identical to the reference CPU run as long as the host takes the same
+// restart decisions.  The check reductions are deterministic trees.
+//
+// Vectors of k cases sharing A are k-interleaved: element (i, b) at i*k + b
+// (src/pdhg/kernels.cpp:1-4).
+#pragma once
+
+#include <cstdint>
+
+namespace b2p {
+
+constexpr int kBlock = 256;
+constexpr int kRowSums = 5;  // per case, per block: see CheckSum
+constexpr int kNumSums = 10;
+
+// Per-case results of one check (device -> host once per check interval).
+enum CheckSum : int {
+  CS_ROW_RES2 = 0,  // sum (unscaled primal residual)^2          (kkt_rows [0])
+  CS_ROW_DOBJ = 1,  // row part of the dual objective            (kkt_rows [1])
+  CS_Y2 = 2,        // sum y+^2                                  (kkt_rows [2])
+  CS_DY2 = 3,       // sum (y - y+)^2                            (diff2(Y, YP))
+  CS_AY2 = 4,       // sum (y+ - y0)^2                           (diff2(YP, Y0))
+  CS_COL_RES2 = 5,  // sum (unscaled dual residual)^2            (kkt_cols [0])
+  CS_POBJ = 6,      // c' x+                                     (kkt_cols [1])
+  CS_COL_DOBJ = 7,  // column part of the dual objective         (kkt_cols [2])
+  CS_DX2 = 8,       // sum (x - x+)^2                            (diff2(X, XP))
+  CS_AX2 = 9        // sum (x+ - x0)^2                           (diff2(XP, X0))
+};
+
+struct CsrView {
+  const int32_t* __restrict__ ptr;
+  const int32_t* __restrict__ idx;
+  const double* __restrict__ val;
+  int32_t rows;
+};
+
+// Iteration counter of case b at the current iteration: the reference keeps
+// iter[b] (reset to 0 at a restart, +1 after each Halpern step); here it is
+// (it_base + local) - restart_at[b], so a captured interval can be replayed.
+struct IterClock {
+  const int64_t* __restrict__ it_base;
+  const int64_t* __restrict__ restart_at;
+  int32_t local;
+};
+
+__device__ __forceinline__ double halpern_lambda(const IterClock& ck, int b) {
+  const double j = static_cast<double>(*ck.it_base + ck.local - ck.restart_at[b]);
+  return __ddiv_rn(__dadd_rn(j, 1.0), __dadd_rn(j, 2.0));
+}
+
+// z = lam((1+rho) z+ - rho z) + (1-lam) z0          (src/pdhg/pdhg.cpp:138-146)
+__device__ __forceinline__ double halpern_step(double z, double zp, double z0, double lam, double rho) {
+  const double a = __dsub_rn(__dmul_rn(__dadd_rn(1.0, rho), zp), __dmul_rn(rho, z));
+  return __dadd_rn(__dmul_rn(lam, a), __dmul_rn(__dsub_rn(1.0, lam), z0));
+}
+
+// Left-to-right row sum  s = (((0 + v0 x0) + v1 x1) + ...)
+__device__ __forceinline__ double row_dot(const CsrView& M, const double* __restrict__ x, int64_t row, int k, int b) {
+  int p = __ldg(M.ptr + row);
+  const int e = __ldg(M.ptr + row + 1);
+  double s = 0.0;
+  if (k == 1) {
+#pragma unroll 4
+    for (; p < e; ++p) s = __dadd_rn(s, __dmul_rn(__ldg(M.val + p), __ldg(x + __ldg(M.idx + p))));
+  } else {
+#pragma unroll 4
+    for (; p < e; ++p)
+      s = __dadd_rn(s, __dmul_rn(__ldg(M.val + p), __ldg(x + static_cast<int64_t>(__ldg(M.idx + p)) * k + b)));
+  }
+  return s;
+}
+
+__device__ __forceinline__ void split(int64_t t, int k, int64_t& row, int& b) {
+  if (k == 1) {
+    row = t;
+    b = 0;
+  } else {
+    row = t / k;
+    b = static_cast<int>(t - row * k);
+  }
+}
+
+// ---- per-iteration kernels ------------------------------------------------
+
+template <bool HALPERN>
+__global__ void __launch_bounds__(kBlock) k_primal(int32_t n, int32_t k, CsrView AT, const double* __restrict__ y,
+                                                   const double* __restrict__ c, const double* __restrict__ lo,
+                                                   const double* __restrict__ up, double* __restrict__ x,
+                                                   double* __restrict__ xp, const double* __restrict__ x0,
+                                                   const double* __restrict__ tau, IterClock ck, double rho) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= static_cast<int64_t>(n) * k) return;
+  int64_t j;
+  int b;
+  split(t, k, j, b);
+  const double aty = row_dot(AT, y, j, k, b);
+  const double xv = x[t];
+  // x+ = proj_[lo,up](x - tau (c - A^T y))          (src/pdhg/pdhg.cpp:116-125)
+  double v = __dsub_rn(xv, __dmul_rn(tau[b], __dsub_rn(c[t], aty)));
+  const double l = lo[t], u = up[t];
+  v = (v < l) ? l : v;
+  v = (u < v) ? u : v;
+  xp[t] = v;
+  if (HALPERN) x[t] = halpern_step(xv, v, x0[t], halpern_lambda(ck, b), rho);
+}
+
+template <bool HALPERN>
+__global__ void __launch_bounds__(kBlock) k_dual(int32_t m, int32_t k, CsrView A, const double* __restrict__ xp,
+                                                 const double* __restrict__ rl, const double* __restrict__ ru,
+                                                 double* __restrict__ y, double* __restrict__ yp,
+                                                 const double* __restrict__ y0, double* __restrict__ ax,
+                                                 double* __restrict__ axp, const double* __restrict__ ax0,
+                                                 const double* __restrict__ sigma, IterClock ck, double rho) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= static_cast<int64_t>(m) * k) return;
+  int64_t i;
+  int b;
+  split(t, k, i, b);
+  const double axpv = row_dot(A, xp, i, k, b);
+  const double axv = ax[t], yv = y[t];
+  // v = y - sigma (2 A x+ - A x);  y+ = v + sigma proj_[L,U](-v / sigma)   (src/pdhg/pdhg.cpp:126-137)
+  const double s = sigma[b];
+  const double v = __dsub_rn(yv, __dmul_rn(s, __dsub_rn(__dmul_rn(2.0, axpv), axv)));
+  double w = __ddiv_rn(-v, s);
+  const double l = rl[t], u = ru[t];
+  w = (w < l) ? l : w;
+  w = (u < w) ? u : w;
+  const double ypv = __dadd_rn(v, __dmul_rn(s, w));
+  axp[t] = axpv;
+  yp[t] = ypv;
+  if (HALPERN) {
+    const double lam = halpern_lambda(ck, b);
+    y[t] = halpern_step(yv, ypv, y0[t], lam, rho);
+    ax[t] = halpern_step(axv, axpv, ax0[t], lam, rho);
+  }
+}
+
+// Halpern steps of x, y and Ax at a check iteration (after the reductions).
+__global__ void __launch_bounds__(kBlock) k_halpern_all(int32_t n, int32_t m, int32_t k, double* __restrict__ x,
+                                                        const double* __restrict__ xp, const double* __restrict__ x0,
+                                                        double* __restrict__ y, const double* __restrict__ yp,
+                                                        const double* __restrict__ y0, double* __restrict__ ax,
+                                                        const double* __restrict__ axp,
+                                                        const double* __restrict__ ax0, IterClock ck, double rho) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t nx = static_cast<int64_t>(n) * k, ny = static_cast<int64_t>(m) * k;
+  if (t < nx) {
+    const int b = static_cast<int>(k == 1 ? 0 : t % k);
+    x[t] = halpern_step(x[t], xp[t], x0[t], halpern_lambda(ck, b), rho);
+  } else if (t < nx + ny) {
+    const int64_t u = t - nx;
+    const int b = static_cast<int>(k == 1 ? 0 : u % k);
+    const double lam = halpern_lambda(ck, b);
+    y[u] = halpern_step(y[u], yp[u], y0[u], lam, rho);
+    ax[u] = halpern_step(ax[u], axp[u], ax0[u], lam, rho);
+  }
+}
+
+// Masked restart z = z0 = z+ for x, y, Ax and iteration counter reset
+// (src/pdhg/pdhg.cpp:153-165).  Runs after the interval's clock advanced, so
+// the next iteration (index *it_base) has counter 0.
+__global__ void __launch_bounds__(kBlock) k_restart(int32_t n, int32_t m, int32_t k, const int32_t* __restrict__ mask,
+                                                    double* __restrict__ x, double* __restrict__ x0,
+                                                    const double* __restrict__ xp, double* __restrict__ y,
+                                                    double* __restrict__ y0, const double* __restrict__ yp,
+                                                    double* __restrict__ ax, double* __restrict__ ax0,
+                                                    const double* __restrict__ axp, const int64_t* __restrict__ it_base,
+                                                    int64_t* __restrict__ restart_at) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t nx = static_cast<int64_t>(n) * k, ny = static_cast<int64_t>(m) * k;
+  if (t < k && mask[t]) restart_at[t] = *it_base;
+  if (t < nx) {
+    if (mask[k == 1 ? 0 : t % k]) x[t] = x0[t] = xp[t];
+  } else if (t < nx + ny) {
+    const int64_t u = t - nx;
+    if (mask[k == 1 ? 0 : u % k]) {
+      y[u] = y0[u] = yp[u];
+      ax[u] = ax0[u] = axp[u];
+    }
+  }
+}
+
+// ---- check reductions --------------------------------------------------------
+
+template <int NQ>
+__device__ __forceinline__ void block_reduce(double (&s)[NQ], double* sh /* [NQ][kBlock/32] */) {
+#pragma unroll
+  for (int q = 0; q < NQ; ++q)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s[q] += __shfl_xor_sync(0xffffffffu, s[q], off);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) sh[q * (kBlock / 32) + warp] = s[q];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      double v = lane < kBlock / 32 ? sh[q * (kBlock / 32) + lane] : 0.0;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      s[q] = v;
+    }
+  }
+}
+
+// Row part of the check at (x+, y+): kkt_rows (src/pdhg/pdhg.cpp:166-180) +
+// diff2(Y, YP) + diff2(YP, Y0).  grid = (G, k); partial[(b*G + g)*5 + q].
+__global__ void __launch_bounds__(kBlock) k_check_rows(int32_t m, int32_t k, const double* __restrict__ axp,
+                                                       const double* __restrict__ rl, const double* __restrict__ ru,
+                                                       const double* __restrict__ yp, const double* __restrict__ y,
+                                                       const double* __restrict__ y0,
+                                                       const double* __restrict__ rfac,
+                                                       double* __restrict__ partial) {
+  __shared__ double sh[kRowSums * (kBlock / 32)];
+  const int b = blockIdx.y;
+  double s[kRowSums] = {0, 0, 0, 0, 0};
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < m;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t t = i * k + b;
+    const double a = axp[t], l = rl[t], u = ru[t];
+    double e1 = l - a, e2 = a - u;
+    e1 = (e1 < 0.0) ? 0.0 : e1;
+    e2 = (e2 < 0.0) ? 0.0 : e2;
+    const double res = (e1 + e2) * rfac[i];
+    s[0] += res * res;
+    const double yv = yp[t];
+    if (yv > 0.0 && l > -1e300)
+      s[1] += yv * l;
+    else if (yv < 0.0 && u < 1e300)
+      s[1] += yv * u;
+    s[2] += yv * yv;
+    const double d1 = y[t] - yv, d2 = yv - y0[t];
+    s[3] += d1 * d1;
+    s[4] += d2 * d2;
+  }
+  block_reduce<kRowSums>(s, sh);
+  if (threadIdx.x == 0) {
+    double* o = partial + (static_cast<int64_t>(b) * gridDim.x + blockIdx.x) * kRowSums;
+#pragma unroll
+    for (int q = 0; q < kRowSums; ++q) o[q] = s[q];
+  }
+}
+
+// Column part: A^T y+ (spmvT(YP, ATYP)) fused with kkt_cols
+// (src/pdhg/pdhg.cpp:181-196) + diff2(X, XP) + diff2(XP, X0).
+__global__ void __launch_bounds__(kBlock) k_check_cols(int32_t n, int32_t k, CsrView AT, const double* __restrict__ yp,
+                                                       const double* __restrict__ xp, const double* __restrict__ x,
+                                                       const double* __restrict__ x0, const double* __restrict__ c,
+                                                       const double* __restrict__ lo, const double* __restrict__ up,
+                                                       const double* __restrict__ cfac,
+                                                       double* __restrict__ partial) {
+  __shared__ double sh[kRowSums * (kBlock / 32)];
+  const int b = blockIdx.y;
+  double s[kRowSums] = {0, 0, 0, 0, 0};
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t t = j * k + b;
+    const double atyp = row_dot(AT, yp, j, k, b);
+    const double cv = c[t], l = lo[t], u = up[t], xpv = xp[t];
+    const double d = cv - atyp;
+    const bool hl = l > -1e300, hu = u < 1e300;
+    double res = 0.0;
+    if (!hl && !hu)
+      res = fabs(d);
+    else if (!hl)
+      res = (d < 0.0) ? 0.0 : d;
+    else if (!hu)
+      res = (-d < 0.0) ? 0.0 : -d;
+    res *= cfac[j];
+    s[0] += res * res;
+    s[1] += cv * xpv;
+    if (d > 0.0 && hl)
+      s[2] += d * l;
+    else if (d < 0.0 && hu)
+      s[2] += d * u;
+    const double d1 = x[t] - xpv, d2 = xpv - x0[t];
+    s[3] += d1 * d1;
+    s[4] += d2 * d2;
+  }
+  block_reduce<kRowSums>(s, sh);
+  if (threadIdx.x == 0) {
+    double* o = partial + (static_cast<int64_t>(b) * gridDim.x + blockIdx.x) * kRowSums;
+#pragma unroll
+    for (int q = 0; q < kRowSums; ++q) o[q] = s[q];
+  }
+}
+
+// Sums the block partials of case b (grid = k) into out[b*10 + CheckSum] and
+// advances the interval clock by L iterations.
+__global__ void __launch_bounds__(kBlock) k_check_finalize(int32_t k, int32_t g_rows, int32_t g_cols,
+                                                           const double* __restrict__ prow,
+                                                           const double* __restrict__ pcol, double* __restrict__ out,
+                                                           int64_t* __restrict__ it_base, int32_t L) {
+  __shared__ double sh[kNumSums * (kBlock / 32)];
+  const int b = blockIdx.x;
+  double s[kNumSums] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int g = threadIdx.x; g < g_rows; g += blockDim.x) {
+    const double* p = prow + (static_cast<int64_t>(b) * g_rows + g) * kRowSums;
+#pragma unroll
+    for (int q = 0; q < kRowSums; ++q) s[q] += p[q];
+  }
+  for (int g = threadIdx.x; g < g_cols; g += blockDim.x) {
+    const double* p = pcol + (static_cast<int64_t>(b) * g_cols + g) * kRowSums;
+#pragma unroll
+    for (int q = 0; q < kRowSums; ++q) s[kRowSums + q] += p[q];
+  }
+  block_reduce<kNumSums>(s, sh);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < kNumSums; ++q) out[static_cast<int64_t>(b) * kNumSums + q] = s[q];
+    if (b == 0) *it_base += L;
+  }
+}
+
+// Plain k-interleaved CSR SpMV y = M x (CpuBackend::mult order).
+__global__ void __launch_bounds__(kBlock) k_spmv(int32_t rows, int32_t k, CsrView M, const double* __restrict__ x,
+                                                 double* __restrict__ y) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= static_cast<int64_t>(rows) * k) return;
+  int64_t i;
+  int b;
+  split(t, k, i, b);
+  y[t] = row_dot(M, x, i, k, b);
+}
+
+}  // namespace b2p

@@ -1,0 +1,165 @@
+#include "pdhg_prepare.h"
+
+#include <cmath>
+
+namespace b2p {
+
+namespace {
+
+// Power-of-two rounding of a scale factor (src/lp/scaling.cpp:9-14): the
+// nearest 2^e with |e| <= 60, so that scaling and unscaling are exact.
+double pow2_round(double v) {
+  if (!(v > 0) || !std::isfinite(v)) return 1.0;
+  int e = static_cast<int>(std::lround(std::log2(v)));
+  e = e < -60 ? -60 : (e > 60 ? 60 : e);
+  return std::ldexp(1.0, e);
+}
+
+// Row-major copy of a CSC matrix: rows list their entries by increasing
+// column, which is the order SparseMatrix::transpose produces
+// (src/core/sparse.cpp:49-65) and hence the order of every row sum.
+HostCsr csr_from_csc(int32_t m, int32_t n, const int32_t* start, const int32_t* index, const double* value) {
+  HostCsr c;
+  c.rows = m;
+  c.cols = n;
+  const int32_t nnz = start[n];
+  c.ptr.assign(static_cast<size_t>(m) + 1, 0);
+  c.idx.resize(nnz);
+  c.val.resize(nnz);
+  for (int32_t q = 0; q < nnz; ++q) c.ptr[index[q] + 1]++;
+  for (int32_t i = 0; i < m; ++i) c.ptr[i + 1] += c.ptr[i];
+  std::vector<int32_t> pos(c.ptr.begin(), c.ptr.end() - 1);
+  for (int32_t j = 0; j < n; ++j)
+    for (int32_t q = start[j]; q < start[j + 1]; ++q) {
+      int32_t p = pos[index[q]]++;
+      c.idx[p] = j;
+      c.val[p] = value[q];
+    }
+  return c;
+}
+
+}  // namespace
+
+void ruiz_scaling(int32_t m, int32_t n, const int32_t* start, const int32_t* index, const double* value,
+                  int iterations, bool pock_chambolle, std::vector<double>& rs, std::vector<double>& cs) {
+  rs.assign(m, 1.0);
+  cs.assign(n, 1.0);
+  std::vector<double> rmax(m), cmax(n);
+  // Infinity-norm equilibration passes.
+  for (int it = 0; it < iterations; ++it) {
+    std::fill(rmax.begin(), rmax.end(), 0.0);
+    for (int32_t j = 0; j < n; ++j) {
+      double c = 0;
+      for (int32_t q = start[j]; q < start[j + 1]; ++q) {
+        const double a = std::fabs(value[q]) * cs[j] * rs[index[q]];
+        c = smax(c, a);
+        rmax[index[q]] = smax(rmax[index[q]], a);
+      }
+      cmax[j] = c;
+    }
+    for (int32_t i = 0; i < m; ++i)
+      if (rmax[i] > 0) rs[i] /= std::sqrt(rmax[i]);
+    for (int32_t j = 0; j < n; ++j)
+      if (cmax[j] > 0) cs[j] /= std::sqrt(cmax[j]);
+  }
+  // Pock-Chambolle step with alpha = 1 (row / column 1-norms).
+  if (pock_chambolle) {
+    std::vector<double> rsum(m, 0.0), csum(n, 0.0);
+    for (int32_t j = 0; j < n; ++j)
+      for (int32_t q = start[j]; q < start[j + 1]; ++q) {
+        const double a = std::fabs(value[q]) * cs[j] * rs[index[q]];
+        csum[j] += a;
+        rsum[index[q]] += a;
+      }
+    for (int32_t i = 0; i < m; ++i)
+      if (rsum[i] > 0) rs[i] /= std::sqrt(rsum[i]);
+    for (int32_t j = 0; j < n; ++j)
+      if (csum[j] > 0) cs[j] /= std::sqrt(csum[j]);
+  }
+  for (auto& v : rs) v = pow2_round(v);
+  for (auto& v : cs) v = pow2_round(v);
+}
+
+// ||A||_2 estimate: 40 steps of x <- A^T A x / ||A^T A x|| and sqrt of the
+// last norm (src/pdhg/pdhg.cpp:404-422), with the scatter-order products of
+// SparseMatrix::multiply / multiplyTranspose (src/core/sparse.cpp:67-82).
+double power_iteration(int32_t m, int32_t n, const int32_t* start, const int32_t* index, const double* value,
+                       int iters) {
+  if (start[n] == 0) return 1.0;
+  std::vector<double> x(n, 1.0 / std::sqrt(static_cast<double>(n > 1 ? n : 1))), y(m), z(n);
+  double s = 1;
+  for (int it = 0; it < iters; ++it) {
+    std::fill(y.begin(), y.end(), 0.0);
+    for (int32_t j = 0; j < n; ++j) {
+      const double xj = x[j];
+      if (xj == 0.0) continue;
+      for (int32_t q = start[j]; q < start[j + 1]; ++q) y[index[q]] += value[q] * xj;
+    }
+    for (int32_t j = 0; j < n; ++j) {
+      double t = 0;
+      for (int32_t q = start[j]; q < start[j + 1]; ++q) t += value[q] * y[index[q]];
+      z[j] = t;
+    }
+    double nz = 0;
+    for (int32_t j = 0; j < n; ++j) nz += z[j] * z[j];
+    nz = std::sqrt(nz);
+    if (nz == 0) return 1.0;
+    s = std::sqrt(nz);
+    for (int32_t j = 0; j < n; ++j) x[j] = z[j] / nz;
+  }
+  return s;
+}
+
+Prepared prepare(int32_t m, int32_t n, const int32_t* start, const int32_t* index, const double* value,
+                 const double* cost, const double* row_lower, const double* row_upper, double offset,
+                 const PrepareOptions& opt) {
+  Prepared P;
+  P.n = n;
+  P.m = m;
+  P.offset = offset;
+  const int32_t nnz = start[n];
+  if (opt.ruiz_iterations > 0 && nnz > 0) {
+    ruiz_scaling(m, n, start, index, value, opt.ruiz_iterations, opt.pock_chambolle, P.R, P.Cs);
+  } else {
+    P.R.assign(m, 1.0);
+    P.Cs.assign(n, 1.0);
+  }
+  // A <- diag(R) A diag(Cs) (src/lp/scaling.cpp:28-32); exact, the factors are powers of two.
+  std::vector<double> sval(nnz);
+  for (int32_t j = 0; j < n; ++j)
+    for (int32_t q = start[j]; q < start[j + 1]; ++q) sval[q] = value[q] * (P.R[index[q]] * P.Cs[j]);
+  if (opt.rescale) {
+    double cn = 0, bn = 0;
+    for (int32_t j = 0; j < n; ++j) {
+      const double t = cost[j] * P.Cs[j];
+      cn += t * t;
+    }
+    for (int32_t i = 0; i < m; ++i) {
+      if (finite_bound(row_lower[i])) {
+        const double t = row_lower[i] * P.R[i];
+        bn += t * t;
+      }
+      if (finite_bound(row_upper[i]) && row_upper[i] != row_lower[i]) {
+        const double t = row_upper[i] * P.R[i];
+        bn += t * t;
+      }
+    }
+    P.gamma = 1.0 + std::sqrt(cn);
+    P.beta = 1.0 + std::sqrt(bn);
+  }
+  P.A = csr_from_csc(m, n, start, index, sval.data());
+  // CSR of A^T is the (scaled) CSC of A.
+  P.AT.rows = n;
+  P.AT.cols = m;
+  P.AT.ptr.assign(start, start + n + 1);
+  P.AT.idx.assign(index, index + nnz);
+  P.AT.val = sval;
+  P.rfac.resize(m);
+  P.cfac.resize(n);
+  for (int32_t i = 0; i < m; ++i) P.rfac[i] = P.beta / P.R[i];
+  for (int32_t j = 0; j < n; ++j) P.cfac[j] = P.gamma / P.Cs[j];
+  P.normA = power_iteration(m, n, start, index, sval.data(), 40) * 1.01;
+  return P;
+}
+
+}  // namespace b2p

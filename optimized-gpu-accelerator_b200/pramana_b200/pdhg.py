@@ -1,0 +1,309 @@
+"""Python mirror of PRAMANA's PDHG engine interface (src/pdhg/pdhg.h:32-80),
+backed by the sm_100a engine through the C ABI of include/b2p_pdhg.h.
+
+Names follow the reference so that code and tests read alike::
+
+    po = PdhgOptions(); po.tolerance = 1e-7
+    r = solvePdhg(model, po)            # pramana::solvePdhg
+    rb = solvePdhgBatch(model, cases, po)
+    gpuAvailable(); gpuInfoJson()
+
+Every solve runs on the GPU.  There is no CPU backend behind this module:
+``useGpu=False`` is rejected and a machine without a usable sm_100 device
+raises ``B2pError`` (code 3).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from .model import LpCase, Model
+
+Status = _lib.STATUS_NAMES
+
+
+@dataclass
+class PdhgOptions:
+    """pramana::PdhgOptions (src/pdhg/pdhg.h:32-42) + deadline and device."""
+    tolerance: float = 1e-6
+    maxIterations: int = 1000000
+    checkEvery: int = 64
+    useGpu: bool = True
+    ruizIterations: int = 10
+    pockChambolle: bool = True
+    rescaleObjectiveAndBounds: bool = True
+    reflection: float = 1.0
+    logInterval: int = 0
+    timeLimit: float = 0.0        # seconds (pramana::Deadline); <= 0 = none
+    device: int = -1
+    useGraphs: bool = True
+    precision: int = _lib.PRECISION_FP64
+
+    def to_c(self, cancel_flag=None) -> _lib.B2pOptions:
+        if not self.useGpu:
+            raise ValueError("this PDHG engine has no CPU backend (useGpu=False)")
+        o = _lib.B2pOptions()
+        _lib.load().b2p_default_options(C.byref(o))
+        o.tolerance = float(self.tolerance)
+        o.max_iterations = int(self.maxIterations)
+        o.check_every = int(self.checkEvery)
+        o.ruiz_iterations = int(self.ruizIterations)
+        o.pock_chambolle = int(bool(self.pockChambolle))
+        o.rescale_objective_and_bounds = int(bool(self.rescaleObjectiveAndBounds))
+        o.reflection = float(self.reflection)
+        o.log_interval = int(self.logInterval)
+        o.device = int(self.device)
+        o.time_limit = float(self.timeLimit)
+        o.precision = int(self.precision)
+        o.use_graphs = int(bool(self.useGraphs))
+        if cancel_flag is not None:
+            o.cancel_flag = C.cast(cancel_flag, C.POINTER(C.c_int32))
+        return o
+
+
+@dataclass
+class PdhgStats:
+    """pramana::PdhgStats (src/pdhg/pdhg.h:44-56)."""
+    iterations: int = 0
+    restarts: int = 0
+    primalResidual: float = 0.0
+    dualResidual: float = 0.0
+    gap: float = 0.0
+    primalWeight: float = 1.0
+    setupSeconds: float = 0.0
+    solveSeconds: float = 0.0
+    kernelSeconds: float = 0.0
+    transferSeconds: float = 0.0
+    bytesUploaded: int = 0
+    bytesDownloaded: int = 0
+    kernelLaunches: int = 0
+    spectralNorm: float = 0.0
+    backend: str = "gpu"
+    device: str = ""
+
+    @classmethod
+    def from_c(cls, s: _lib.B2pStats, device: str = "") -> "PdhgStats":
+        return cls(iterations=s.iterations, restarts=s.restarts, primalResidual=s.primal_residual,
+                   dualResidual=s.dual_residual, gap=s.gap, primalWeight=s.primal_weight,
+                   setupSeconds=s.setup_seconds, solveSeconds=s.solve_seconds, kernelSeconds=s.kernel_seconds,
+                   transferSeconds=s.transfer_seconds, bytesUploaded=s.bytes_uploaded,
+                   bytesDownloaded=s.bytes_downloaded, kernelLaunches=s.kernel_launches,
+                   spectralNorm=s.spectral_norm, device=device)
+
+    def toJson(self) -> dict:
+        """Keys of PdhgStats::toJson (src/pdhg/pdhg.cpp:691-710)."""
+        return {"backend": self.backend, "device": self.device, "iterations": self.iterations,
+                "restarts": self.restarts, "relative_primal_residual": self.primalResidual,
+                "relative_dual_residual": self.dualResidual, "relative_gap": self.gap,
+                "primal_weight": self.primalWeight, "spectral_norm_estimate": self.spectralNorm,
+                "setup_seconds": self.setupSeconds, "solve_seconds": self.solveSeconds,
+                "kernel_seconds": self.kernelSeconds, "transfer_seconds": self.transferSeconds,
+                "bytes_uploaded": self.bytesUploaded, "bytes_downloaded": self.bytesDownloaded,
+                "kernel_launches": self.kernelLaunches}
+
+
+@dataclass
+class PdhgResult:
+    """pramana::PdhgResult (src/pdhg/pdhg.h:58-65)."""
+    status: str
+    objective: float
+    dualObjective: float
+    x: np.ndarray
+    rowDual: np.ndarray
+    iterations: int
+    relativeKkt: float
+    stats: PdhgStats = field(default_factory=PdhgStats)
+
+
+def _lp_struct(lp: Model):
+    keep = []
+
+    def p(a, ctype):
+        a = np.ascontiguousarray(a)
+        keep.append(a)
+        return a.ctypes.data_as(C.POINTER(ctype))
+
+    s = _lib.B2pLp(num_rows=lp.num_rows, num_cols=lp.num_cols, start=p(lp.start, C.c_int32),
+                   index=p(lp.index, C.c_int32), value=p(lp.value, C.c_double), col_cost=p(lp.col_cost, C.c_double),
+                   col_lower=p(lp.col_lower, C.c_double), col_upper=p(lp.col_upper, C.c_double),
+                   row_lower=p(lp.row_lower, C.c_double), row_upper=p(lp.row_upper, C.c_double),
+                   obj_offset=float(lp.obj_offset))
+    return s, keep
+
+
+def _cases_struct(cases, n, m):
+    keep = []
+    arr = (_lib.B2pCase * len(cases))()
+
+    def p(v, ln):
+        if v is None:
+            return None
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        if len(v) != ln:
+            raise ValueError("case vector has the wrong length")
+        keep.append(v)
+        return v.ctypes.data_as(_lib.dptr)
+
+    for b, cs in enumerate(cases):
+        arr[b] = _lib.B2pCase(cost=p(cs.cost, n), col_lower=p(cs.col_lower, n), col_upper=p(cs.col_upper, n),
+                              row_lower=p(cs.row_lower, m), row_upper=p(cs.row_upper, m))
+    return arr, keep
+
+
+def _device_name() -> str:
+    try:
+        return gpuInfoJson().get("name", "")
+    except Exception:  # noqa: BLE001 - informational only
+        return ""
+
+
+def _results(lp: Model, res, x, y, k, stats) -> list[PdhgResult]:
+    n, m = lp.num_cols, lp.num_rows
+    return [PdhgResult(status=Status.get(res[b].status, str(res[b].status)), objective=res[b].objective,
+                       dualObjective=res[b].dual_objective, x=x[b * n:(b + 1) * n].copy(),
+                       rowDual=y[b * m:(b + 1) * m].copy(), iterations=res[b].iterations,
+                       relativeKkt=res[b].relative_kkt, stats=stats) for b in range(k)]
+
+
+def solvePdhg(lp: Model, opts: PdhgOptions | None = None, cancel_flag=None) -> PdhgResult:
+    """pramana::solvePdhg (src/pdhg/pdhg.cpp:712-717); ``lp`` must be a minimisation LP."""
+    opts = opts or PdhgOptions()
+    lib = _lib.load()
+    s, keep = _lp_struct(lp)
+    o = opts.to_c(cancel_flag)
+    x = np.zeros(lp.num_cols)
+    y = np.zeros(lp.num_rows)
+    res = (_lib.B2pResult * 1)()
+    st = _lib.B2pStats()
+    _lib.check(lib.b2p_solve_pdhg(C.byref(s), C.byref(o), x.ctypes.data_as(_lib.dptr), y.ctypes.data_as(_lib.dptr),
+                                  res, C.byref(st)))
+    del keep
+    return _results(lp, res, x, y, 1, PdhgStats.from_c(st, _device_name()))[0]
+
+
+def solvePdhgBatch(base: Model, cases: list[LpCase], opts: PdhgOptions | None = None,
+                   batchStats: PdhgStats | None = None) -> list[PdhgResult]:
+    """pramana::solvePdhgBatch (src/pdhg/pdhg.cpp:719-728): cases share A."""
+    if not cases:
+        return []
+    opts = opts or PdhgOptions()
+    lib = _lib.load()
+    s, keep = _lp_struct(base)
+    arr, keep2 = _cases_struct(cases, base.num_cols, base.num_rows)
+    o = opts.to_c()
+    k = len(cases)
+    x = np.zeros(k * base.num_cols)
+    y = np.zeros(k * base.num_rows)
+    res = (_lib.B2pResult * k)()
+    st = _lib.B2pStats()
+    _lib.check(lib.b2p_solve_pdhg_batch(C.byref(s), arr, k, C.byref(o), x.ctypes.data_as(_lib.dptr),
+                                        y.ctypes.data_as(_lib.dptr), res, C.byref(st)))
+    del keep, keep2
+    stats = PdhgStats.from_c(st, _device_name())
+    if batchStats is not None:
+        batchStats.__dict__.update(stats.__dict__)
+    return _results(base, res, x, y, k, stats)
+
+
+def gpuAvailable() -> bool:
+    """pramana::gpuAvailable (src/pdhg/pdhg.cpp:730)."""
+    return bool(_lib.load().b2p_gpu_available())
+
+
+def gpuInfoJson() -> dict:
+    """pramana::gpuInfoJson (src/pdhg/pdhg.cpp:732-746)."""
+    lib = _lib.load()
+    need = lib.b2p_gpu_info_json(None, 0)
+    buf = C.create_string_buffer(need + 1)
+    lib.b2p_gpu_info_json(buf, need + 1)
+    return json.loads(buf.value.decode())
+
+
+class Engine:
+    """Two-phase solve: ``Engine(lp)`` prepares and uploads (inputs resident in
+    HBM afterwards), ``solve()`` runs the PDHG loop from the initial point and
+    can be repeated, ``fetch()`` returns the last solution."""
+
+    def __init__(self, lp: Model, opts: PdhgOptions | None = None, cases: list[LpCase] | None = None):
+        self.lp = lp
+        self.opts = opts or PdhgOptions()
+        self.k = len(cases) if cases else 1
+        self._lib = _lib.load()
+        s, keep = _lp_struct(lp)
+        arr, keep2 = (_cases_struct(cases, lp.num_cols, lp.num_rows) if cases else (None, []))
+        o = self.opts.to_c()
+        h = C.c_void_p()
+        t0 = time.perf_counter()
+        _lib.check(self._lib.b2p_engine_create(C.byref(s), arr, len(cases) if cases else 0, C.byref(o), C.byref(h)))
+        self.create_seconds = time.perf_counter() - t0
+        del keep, keep2
+        self._h = h
+        self.last_stats: _lib.B2pStats | None = None
+
+    def solve(self) -> list[PdhgResult]:
+        res = (_lib.B2pResult * self.k)()
+        st = _lib.B2pStats()
+        _lib.check(self._lib.b2p_engine_solve(self._h, res, C.byref(st)))
+        self.last_stats = st
+        x, y = self.fetch()
+        return _results(self.lp, res, x, y, self.k, PdhgStats.from_c(st))
+
+    def fetch(self):
+        x = np.zeros(self.k * self.lp.num_cols)
+        y = np.zeros(self.k * self.lp.num_rows)
+        _lib.check(self._lib.b2p_engine_fetch(self._h, x.ctypes.data_as(_lib.dptr), y.ctypes.data_as(_lib.dptr)))
+        return x, y
+
+    def set_profiling(self, on: bool) -> None:
+        _lib.check(self._lib.b2p_engine_set_profiling(self._h, int(on)))
+
+    def kernel_times(self, cls: int):
+        n = C.c_int64()
+        ms = C.c_double()
+        _lib.check(self._lib.b2p_engine_kernel_times(self._h, cls, C.byref(n), C.byref(ms)))
+        return n.value, ms.value
+
+    def kernel_bytes(self, cls: int) -> float:
+        b = C.c_double()
+        _lib.check(self._lib.b2p_engine_kernel_bytes(self._h, cls, C.byref(b)))
+        return b.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.b2p_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def csr_spmv(ptr, idx, val, x, rows: int, cols: int, k: int = 1) -> np.ndarray:
+    """Device CSR SpMV with k interleaved right-hand sides (CpuBackend::mult order)."""
+    lib = _lib.load()
+    ptr = np.ascontiguousarray(ptr, dtype=np.int32)
+    idx = np.ascontiguousarray(idx, dtype=np.int32)
+    val = np.ascontiguousarray(val, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.zeros(rows * k)
+    _lib.check(lib.b2p_csr_spmv(rows, cols, k, ptr.ctypes.data_as(_lib.iptr), idx.ctypes.data_as(_lib.iptr),
+                                val.ctypes.data_as(_lib.dptr), x.ctypes.data_as(_lib.dptr),
+                                y.ctypes.data_as(_lib.dptr)))
+    return y
+
+
+# snake_case aliases
+solve_pdhg = solvePdhg
+solve_pdhg_batch = solvePdhgBatch
+gpu_available = gpuAvailable
+gpu_info_json = gpuInfoJson

@@ -1,0 +1,198 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes front end of the two CPU checkers.
+
+* ``lib="oracle"`` -> oracle/liboracle_pdhg.so, this project's single-threaded
+  C restatement of the reference PDHG (pdhg_oracle.c);
+* ``lib="ref"``    -> oracle/_ref/libpramana_ref.so, the reference's own CPU
+  PDHG (src/pdhg/pdhg.cpp CpuBackend) compiled from its sources.
+
+Both export the same ``*_pdhg_solve`` signature, so every parity test can run
+against either.  Only tests, ``__graft_entry__.smoke()`` and the CPU-baseline
+leg of ``bench.py`` may import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle_pdhg.so")
+REF_SO = os.path.join(HERE, "_ref", "libpramana_ref.so")
+REFERENCE_SRC = "/root/reference"
+
+STATUS_NAMES = {0: "NotSolved", 1: "Optimal", 5: "TimeLimit", 6: "IterationLimit"}
+
+
+class Options(C.Structure):
+    _fields_ = [("tolerance", C.c_double), ("max_iterations", C.c_int64), ("check_every", C.c_int32),
+                ("ruiz_iterations", C.c_int32), ("pock_chambolle", C.c_int32), ("rescale", C.c_int32),
+                ("reflection", C.c_double), ("time_limit", C.c_double)]
+
+
+class CaseResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("pad", C.c_int32), ("iterations", C.c_int64), ("objective", C.c_double),
+                ("dual_objective", C.c_double), ("relative_kkt", C.c_double)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("iterations", C.c_int64), ("restarts", C.c_int32), ("threads", C.c_int32),
+                ("primal_weight", C.c_double), ("spectral_norm", C.c_double), ("setup_seconds", C.c_double),
+                ("solve_seconds", C.c_double), ("primal_residual", C.c_double), ("dual_residual", C.c_double),
+                ("gap", C.c_double)]
+
+
+@dataclass
+class OracleResult:
+    status: int
+    iterations: int
+    objective: float
+    dual_objective: float
+    relative_kkt: float
+    x: np.ndarray
+    y: np.ndarray
+
+
+def build(reference: bool = True) -> None:
+    """Compile the C restatement (and, when the reference tree is present, the reference)."""
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    if reference and os.path.isdir(REFERENCE_SRC):
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF={REFERENCE_SRC}"], check=True)
+
+
+_libs: dict = {}
+
+
+def _load(lib: str):
+    if lib in _libs:
+        return _libs[lib]
+    path = ORACLE_SO if lib == "oracle" else REF_SO
+    if not os.path.exists(path):
+        build(reference=(lib == "ref"))
+    if not os.path.exists(path):
+        raise FileNotFoundError(path)
+    h = C.CDLL(path)
+    fn = getattr(h, "oracle_pdhg_solve" if lib == "oracle" else "ref_pdhg_solve")
+    fn.restype = C.c_int
+    _libs[lib] = h
+    if lib == "ref":
+        h.ref_set_threads.argtypes = [C.c_int]
+        h.ref_threads.restype = C.c_int
+    return h
+
+
+def available(lib: str) -> bool:
+    try:
+        _load(lib)
+        return True
+    except (FileNotFoundError, OSError, subprocess.CalledProcessError):
+        return False
+
+
+def set_ref_threads(n: int) -> int:
+    """Size the reference ThreadPool; only effective before its first solve."""
+    h = _load("ref")
+    h.ref_set_threads(int(n))
+    return h.ref_threads()
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def default_options(**kw) -> Options:
+    o = Options(tolerance=1e-6, max_iterations=1000000, check_every=64, ruiz_iterations=10, pock_chambolle=1,
+                rescale=1, reflection=1.0, time_limit=0.0)
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def solve(lp, lib: str = "oracle", cases=None, **opts) -> list[OracleResult] | OracleResult:
+    """Run solvePdhg (cases is None) or solvePdhgBatch (list of LpCase-like objects)."""
+    h = _load(lib)
+    fn = h.oracle_pdhg_solve if lib == "oracle" else h.ref_pdhg_solve
+    m, n = lp.num_rows, lp.num_cols
+    o = default_options(**opts)
+    k = 0 if cases is None else len(cases)
+    kk = max(k, 1)
+    keep = []
+
+    def arr(field, ln):
+        if cases is None:
+            return None
+        p = (C.POINTER(C.c_double) * k)()
+        for b, cs in enumerate(cases):
+            v = getattr(cs, field)
+            if v is None:
+                p[b] = None
+            else:
+                v = np.ascontiguousarray(v, dtype=np.float64)
+                assert len(v) == ln
+                keep.append(v)
+                p[b] = _dp(v)
+        return p
+
+    cc, cl, cu, rl, ru = arr("cost", n), arr("col_lower", n), arr("col_upper", n), arr("row_lower", m), \
+        arr("row_upper", m)
+    x = np.zeros(kk * n)
+    y = np.zeros(kk * m)
+    res = (CaseResult * kk)()
+    st = Stats()
+    rc = fn(C.c_int(m), C.c_int(n), _ip(lp.start), _ip(lp.index), _dp(lp.value), _dp(lp.col_cost),
+            _dp(lp.col_lower), _dp(lp.col_upper), _dp(lp.row_lower), _dp(lp.row_upper), C.c_double(lp.obj_offset),
+            C.c_int(k), cc, cl, cu, rl, ru, C.byref(o), _dp(x), _dp(y), res, C.byref(st))
+    if rc != 0:
+        raise RuntimeError(f"{lib} solve failed")
+    out = [OracleResult(res[b].status, res[b].iterations, res[b].objective, res[b].dual_objective,
+                        res[b].relative_kkt, x[b * n:(b + 1) * n].copy(), y[b * m:(b + 1) * m].copy())
+           for b in range(kk)]
+    solve.last_stats = {f: getattr(st, f) for f, _ in Stats._fields_}
+    return out if cases is not None else out[0]
+
+
+def safe_dual_bound(lp, y, col_lower=None, col_upper=None) -> float:
+    """The reference's outward-rounded Neumaier-Shcherbina bound (needs the ref build)."""
+    h = _load("ref")
+    lo = np.ascontiguousarray(lp.col_lower if col_lower is None else col_lower, dtype=np.float64)
+    up = np.ascontiguousarray(lp.col_upper if col_upper is None else col_upper, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    bound = C.c_double()
+    inf_terms = C.c_int()
+    rc = h.ref_safe_dual_bound(C.c_int(lp.num_rows), C.c_int(lp.num_cols), _ip(lp.start), _ip(lp.index),
+                               _dp(lp.value), _dp(lp.col_cost), _dp(lo), _dp(up), _dp(lp.row_lower),
+                               _dp(lp.row_upper), _dp(y), C.byref(bound), C.byref(inf_terms))
+    if rc != 0:
+        raise RuntimeError("safe bound failed")
+    return bound.value + lp.obj_offset
+
+
+def ruiz(lp, lib: str = "oracle", iterations: int = 10, pock_chambolle: bool = True):
+    h = _load(lib)
+    fn = h.oracle_ruiz_scaling if lib == "oracle" else h.ref_ruiz_scaling
+    rs = np.zeros(lp.num_rows)
+    cs = np.zeros(lp.num_cols)
+    rc = fn(C.c_int(lp.num_rows), C.c_int(lp.num_cols), _ip(lp.start), _ip(lp.index), _dp(lp.value),
+            C.c_int(iterations), C.c_int(int(pock_chambolle)), _dp(rs), _dp(cs))
+    if rc != 0:
+        raise RuntimeError("ruiz failed")
+    return rs, cs
+
+
+def power_norm(m, n, start, index, value, iters=40) -> float:
+    h = _load("oracle")
+    h.oracle_power_iteration.restype = C.c_double
+    return h.oracle_power_iteration(C.c_int(m), C.c_int(n), _ip(start), _ip(index), _dp(value), C.c_int(iters))
+
+
+def csr_mult(ptr, idx, val, x, rows, k=1):
+    h = _load("oracle")
+    out = np.zeros(rows * k)
+    h.oracle_csr_mult(C.c_int(rows), C.c_int(k), _ip(ptr), _ip(idx), _dp(val), _dp(x), _dp(out))
+    return out

@@ -1,0 +1,207 @@
+// TEST INFRASTRUCTURE ONLY (the oracle). Never linked into the product.
+//
+// C-ABI shim over the reference's own CPU PDHG, compiled together with the
+// reference's unmodified sources (see oracle/Makefile) into
+// oracle/_ref/libpramana_ref.so.  It lets the parity tests and the CPU
+// baseline call, through ctypes:
+//   - pramana::solvePdhg / solvePdhgBatch with useGpu=false, i.e. the
+//     multithreaded CpuBackend            (src/pdhg/pdhg.cpp:712-728, 75-214)
+//   - pramana::safeDualBound, the outward-rounded Neumaier-Shcherbina bound
+//                                          (src/cert/certifier.h:93)
+//   - pramana::ruizScaling                 (src/lp/scaling.cpp:97-139)
+// The GPU path of the reference is switched off (PRAMANA_DISABLE_GPU) so that
+// loading this library never brings up a CUDA context or NVRTC.
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <exception>
+#include <string>
+#include <vector>
+
+#include "cert/certifier.h"
+#include "core/model.h"
+#include "lp/scaling.h"
+#include "pdhg/pdhg.h"
+#include "util/log.h"
+#include "util/parallel.h"
+#include "util/timer.h"
+
+using namespace pramana;
+
+namespace {
+std::string gErr;
+
+Model buildModel(int m, int n, const int* start, const int* index, const double* value, const double* cost,
+                 const double* colLower, const double* colUpper, const double* rowLower, const double* rowUpper,
+                 double offset) {
+  Model lp;
+  lp.objOffset = offset;
+  lp.A.numRows = m;
+  lp.A.numCols = n;
+  lp.A.start.assign(start, start + n + 1);
+  const int nnz = start[n];
+  lp.A.index.assign(index, index + nnz);
+  lp.A.value.assign(value, value + nnz);
+  lp.colCost.assign(cost, cost + n);
+  lp.colLower.assign(colLower, colLower + n);
+  lp.colUpper.assign(colUpper, colUpper + n);
+  lp.rowLower.assign(rowLower, rowLower + m);
+  lp.rowUpper.assign(rowUpper, rowUpper + m);
+  lp.colType.assign(n, VarType::Continuous);
+  return lp;
+}
+
+std::vector<double> vecOrEmpty(const double* p, int len) {
+  return p ? std::vector<double>(p, p + len) : std::vector<double>();
+}
+}  // namespace
+
+extern "C" {
+
+struct ref_options {
+  double tolerance;
+  int64_t max_iterations;
+  int32_t check_every;
+  int32_t ruiz_iterations;
+  int32_t pock_chambolle;
+  int32_t rescale;
+  double reflection;
+  double time_limit;  // <= 0: no limit
+};
+
+struct ref_case_result {
+  int32_t status;  // pramana::Status numbering (src/util/common.h:27-39)
+  int32_t pad;
+  int64_t iterations;
+  double objective;
+  double dual_objective;
+  double relative_kkt;
+};
+
+struct ref_stats {
+  int64_t iterations;
+  int32_t restarts;
+  int32_t threads;
+  double primal_weight;
+  double spectral_norm;
+  double setup_seconds;
+  double solve_seconds;
+  double primal_residual, dual_residual, gap;
+};
+
+const char* ref_last_error() { return gErr.c_str(); }
+
+void ref_set_threads(int n) {
+  ThreadPool::setThreads(n);
+  Log::setLevel(LogLevel::Error);
+}
+
+int ref_threads() { return ThreadPool::instance().threads(); }
+
+// cost/colLower/... of case b: cases_x[b] (NULL = base model's vector).
+int ref_pdhg_solve(int m, int n, const int* start, const int* index, const double* value, const double* cost,
+                   const double* colLower, const double* colUpper, const double* rowLower, const double* rowUpper,
+                   double offset, int k, const double* const* caseCost, const double* const* caseColLower,
+                   const double* const* caseColUpper, const double* const* caseRowLower,
+                   const double* const* caseRowUpper, const ref_options* o, double* xOut, double* yOut,
+                   ref_case_result* res, ref_stats* st) {
+  try {
+    setenv("PRAMANA_DISABLE_GPU", "1", 1);
+    Log::setLevel(LogLevel::Error);
+    Model lp = buildModel(m, n, start, index, value, cost, colLower, colUpper, rowLower, rowUpper, offset);
+    PdhgOptions po;
+    po.tolerance = o->tolerance;
+    po.maxIterations = o->max_iterations;
+    po.checkEvery = o->check_every;
+    po.ruizIterations = o->ruiz_iterations;
+    po.pockChambolle = o->pock_chambolle != 0;
+    po.rescaleObjectiveAndBounds = o->rescale != 0;
+    po.reflection = o->reflection;
+    po.useGpu = false;
+    Deadline dl(o->time_limit);
+    std::vector<PdhgResult> rr;
+    PdhgStats bst;
+    if (k <= 0) {
+      rr.push_back(solvePdhg(lp, po, o->time_limit > 0 ? &dl : nullptr));
+      bst = rr[0].stats;
+    } else {
+      std::vector<LpCase> cases(k);
+      for (int b = 0; b < k; ++b) {
+        cases[b].cost = vecOrEmpty(caseCost ? caseCost[b] : nullptr, n);
+        cases[b].colLower = vecOrEmpty(caseColLower ? caseColLower[b] : nullptr, n);
+        cases[b].colUpper = vecOrEmpty(caseColUpper ? caseColUpper[b] : nullptr, n);
+        cases[b].rowLower = vecOrEmpty(caseRowLower ? caseRowLower[b] : nullptr, m);
+        cases[b].rowUpper = vecOrEmpty(caseRowUpper ? caseRowUpper[b] : nullptr, m);
+      }
+      rr = solvePdhgBatch(lp, cases, po, o->time_limit > 0 ? &dl : nullptr, &bst);
+    }
+    for (size_t b = 0; b < rr.size(); ++b) {
+      const PdhgResult& r = rr[b];
+      res[b].status = static_cast<int32_t>(r.status);
+      res[b].iterations = r.iterations;
+      res[b].objective = r.objective;
+      res[b].dual_objective = r.dualObjective;
+      res[b].relative_kkt = r.relativeKkt;
+      if (xOut) std::memcpy(xOut + b * static_cast<size_t>(n), r.x.data(), sizeof(double) * n);
+      if (yOut) std::memcpy(yOut + b * static_cast<size_t>(m), r.rowDual.data(), sizeof(double) * m);
+    }
+    if (st) {
+      st->iterations = bst.iterations;
+      st->restarts = bst.restarts;
+      st->threads = ThreadPool::instance().threads();
+      st->primal_weight = bst.primalWeight;
+      st->spectral_norm = bst.spectralNorm;
+      st->setup_seconds = bst.setupSeconds;
+      st->solve_seconds = bst.solveSeconds;
+      st->primal_residual = bst.primalResidual;
+      st->dual_residual = bst.dualResidual;
+      st->gap = bst.gap;
+    }
+    return 0;
+  } catch (std::exception& e) {
+    gErr = e.what();
+    return 1;
+  }
+}
+
+// Outward-rounded lower bound on min c^T x over the given boxes, valid for any y.
+int ref_safe_dual_bound(int m, int n, const int* start, const int* index, const double* value, const double* cost,
+                        const double* colLower, const double* colUpper, const double* rowLower,
+                        const double* rowUpper, const double* y, double* bound, int* infiniteTerms) {
+  try {
+    SparseMatrix A(m, n);
+    A.start.assign(start, start + n + 1);
+    A.index.assign(index, index + start[n]);
+    A.value.assign(value, value + start[n]);
+    SafeBoundResult sb = safeDualBound(A, std::vector<double>(cost, cost + n),
+                                       std::vector<double>(colLower, colLower + n),
+                                       std::vector<double>(colUpper, colUpper + n),
+                                       std::vector<double>(rowLower, rowLower + m),
+                                       std::vector<double>(rowUpper, rowUpper + m), std::vector<double>(y, y + m));
+    *bound = sb.bound;
+    if (infiniteTerms) *infiniteTerms = sb.infiniteTerms;
+    return 0;
+  } catch (std::exception& e) {
+    gErr = e.what();
+    return 1;
+  }
+}
+
+int ref_ruiz_scaling(int m, int n, const int* start, const int* index, const double* value, int iterations,
+                     int pockChambolle, double* rowScale, double* colScale) {
+  try {
+    SparseMatrix A(m, n);
+    A.start.assign(start, start + n + 1);
+    A.index.assign(index, index + start[n]);
+    A.value.assign(value, value + start[n]);
+    ScalingResult s = ruizScaling(A, iterations, pockChambolle != 0);
+    std::memcpy(rowScale, s.rowScale.data(), sizeof(double) * m);
+    std::memcpy(colScale, s.colScale.data(), sizeof(double) * n);
+    return 0;
+  } catch (std::exception& e) {
+    gErr = e.what();
+    return 1;
+  }
+}
+
+}  // extern "C"
