@@ -29,6 +29,7 @@
 #include "../../include/b2p_pdhg.h"
 #include "pdhg_kernels.cuh"
 #include "pdhg_prepare.h"
+#include "pdhg_spmv.cuh"
 
 namespace b2p {
 
@@ -54,7 +55,7 @@ double seconds_since(Clock::time_point t0) { return std::chrono::duration<double
 
 // Device vector slots (the reference's enum V, src/pdhg/pdhg.cpp:45, minus
 // ATY/ATYP which the fused kernels never store, plus the initial point).
-enum Slot : int { X, XP, X0, C, LO, UP, XINIT, NCOLVEC, Y = NCOLVEC, YP, Y0, AX, AXP, AX0, RL, RU, AXINIT, NSLOT };
+enum Slot : int { X, XP, X0, C, LO, UP, XINIT, ATYP, NCOLVEC, Y = NCOLVEC, YP, Y0, AX, AXP, AX0, RL, RU, AXINIT, NSLOT };
 inline bool row_slot(int s) { return s >= Y; }
 
 int pick_device(int requested) {
@@ -92,6 +93,56 @@ void check_lp(const b2p_lp* lp) {
   if (lp->num_rows > 0 && (!lp->row_lower || !lp->row_upper)) throw Error(B2P_ERR_INVALID, "row vectors are NULL");
 }
 
+// Row-length bins of one CSR operator (see pdhg_spmv.cuh).
+struct HostBins {
+  std::vector<int32_t> long_rows, vlong_rows;
+  int g = 1;
+  int long_thr = 8;
+};
+
+constexpr int kVeryLongRow = 2048;  // rows longer than this get a 256-thread block
+
+HostBins make_bins(const HostCsr& M) {
+  HostBins hb;
+  const int64_t nnz = M.rows ? M.ptr[M.rows] : 0;
+  const double avg = M.rows ? static_cast<double>(nnz) / M.rows : 0.0;
+  while (hb.g < 32 && 2.0 * hb.g <= avg) hb.g *= 2;
+  hb.long_thr = std::max(4 * hb.g, 8);
+  for (int32_t i = 0; i < M.rows; ++i) {
+    const int32_t len = M.ptr[i + 1] - M.ptr[i];
+    if (len > kVeryLongRow)
+      hb.vlong_rows.push_back(i);
+    else if (len > hb.long_thr)
+      hb.long_rows.push_back(i);
+  }
+  return hb;
+}
+
+template <typename... KArgs, typename... Args>
+void launch(void (*kern)(KArgs...), unsigned grid, cudaStream_t stream, bool pdl, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kBlock);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = pdl ? attr : nullptr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  B2P_CUDA(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
+}
+
+#define B2P_G_SWITCH(g, F)                           \
+  switch (g) {                                       \
+    case 1: F(1); break;                             \
+    case 2: F(2); break;                             \
+    case 4: F(4); break;                             \
+    case 8: F(8); break;                             \
+    case 16: F(16); break;                           \
+    default: F(32); break;                           \
+  }
+
 }  // namespace
 
 struct Engine {
@@ -114,6 +165,7 @@ struct Engine {
   int64_t *d_it_base = nullptr, *d_restart_at = nullptr;
   int32_t* d_mask = nullptr;
   int g_rows = 1, g_cols = 1;
+  RowBins binsA{}, binsT{};  // k == 1 schedules of A and A^T
 
   // ---- pinned host ----
   double* h_sums = nullptr;   // k * kNumSums
@@ -247,6 +299,10 @@ struct Engine {
     dT_val = upload(P.AT.val);
     d_rfac = upload(P.rfac);
     d_cfac = upload(P.cfac);
+    if (k == 1) {
+      binsA = device_bins(P.A);
+      binsT = device_bins(P.AT);
+    }
     for (int s = 0; s < NSLOT; ++s) v[s] = dalloc<double>(row_slot(s) ? mk : nk);
     auto put = [&](int s, const std::vector<double>& h) {
       if (!h.empty())
@@ -281,6 +337,24 @@ struct Engine {
     transfer_seconds = seconds_since(tx);
     stats.setup_seconds = seconds_since(t0);
     stats.spectral_norm = P.normA;
+  }
+
+  RowBins device_bins(const HostCsr& M) {
+    HostBins hb = make_bins(M);
+    RowBins b{};
+    b.long_rows = upload(hb.long_rows);
+    b.vlong_rows = upload(hb.vlong_rows);
+    b.n_long = static_cast<int32_t>(hb.long_rows.size());
+    b.n_vlong = static_cast<int32_t>(hb.vlong_rows.size());
+    b.long_thr = hb.long_thr;
+    b.vlong_blocks = b.n_vlong;
+    b.long_blocks = (b.n_long + kBlock / 32 - 1) / (kBlock / 32);
+    b.short_blocks = static_cast<int32_t>((static_cast<int64_t>(M.rows) * hb.g + kBlock - 1) / kBlock);
+    b.g = hb.g;
+    return b;
+  }
+  static unsigned bin_grid(const RowBins& b) {
+    return static_cast<unsigned>(std::max(1, b.vlong_blocks + b.long_blocks + b.short_blocks));
   }
 
   void reset_state(std::vector<double>& omega) {
@@ -324,8 +398,71 @@ struct Engine {
     }
   }
 
+  // One LP: binned fused kernels with programmatic dependent launch.
+  void enqueue_interval_single(int L) {
+    const double rho = opt.reflection;
+    const CsrView A = viewA(), AT = viewAT();
+    const unsigned gp = bin_grid(binsT), gd = bin_grid(binsA);
+    for (int l = 0; l < L; ++l) {
+      const bool last = l == L - 1;
+      const IterClock ck{d_it_base, d_restart_at, l};
+      if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 0], stream));
+      if (n) {
+#define B2P_PRIMAL(G)                                                                                     \
+  if (last)                                                                                               \
+    launch(k_primal_binned<G, false>, gp, stream, true, AT, binsT, v[Y], v[C], v[LO], v[UP], v[X], v[XP], v[X0], \
+           d_tau, ck, rho);                                                                               \
+  else                                                                                                    \
+    launch(k_primal_binned<G, true>, gp, stream, true, AT, binsT, v[Y], v[C], v[LO], v[UP], v[X], v[XP], v[X0],  \
+           d_tau, ck, rho);
+        B2P_G_SWITCH(binsT.g, B2P_PRIMAL)
+#undef B2P_PRIMAL
+      }
+      if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 1], stream));
+      if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 2], stream));
+      if (m) {
+#define B2P_DUAL(G)                                                                                        \
+  if (last)                                                                                                \
+    launch(k_dual_binned<G, false>, gd, stream, true, A, binsA, v[XP], v[RL], v[RU], v[Y], v[YP], v[Y0], v[AX], \
+           v[AXP], v[AX0], d_sigma, ck, rho);                                                              \
+  else                                                                                                     \
+    launch(k_dual_binned<G, true>, gd, stream, true, A, binsA, v[XP], v[RL], v[RU], v[Y], v[YP], v[Y0], v[AX],  \
+           v[AXP], v[AX0], d_sigma, ck, rho);
+        B2P_G_SWITCH(binsA.g, B2P_DUAL)
+#undef B2P_DUAL
+      }
+      if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 3], stream));
+    }
+    // A^T y+ for the dual residual, then the check reductions.
+    if (n) {
+#define B2P_ATY(G) launch(k_spmv_binned<G>, gp, stream, false, AT, binsT, v[YP], v[ATYP]);
+      B2P_G_SWITCH(binsT.g, B2P_ATY)
+#undef B2P_ATY
+    }
+    enqueue_check_tail(L, v[ATYP]);
+  }
+
+  void enqueue_check_tail(int L, const double* atyp) {
+    const double rho = opt.reflection;
+    const int64_t nk = static_cast<int64_t>(n) * k, mk = static_cast<int64_t>(m) * k;
+    const IterClock ck{d_it_base, d_restart_at, L - 1};
+    k_check_rows<<<dim3(g_rows, k), kBlock, 0, stream>>>(m, k, v[AXP], v[RL], v[RU], v[YP], v[Y], v[Y0], d_rfac,
+                                                         d_prow);
+    k_check_cols<<<dim3(g_cols, k), kBlock, 0, stream>>>(n, k, viewAT(), v[YP], atyp, v[XP], v[X], v[X0], v[C],
+                                                         v[LO], v[UP], d_cfac, d_pcol);
+    k_halpern_all<<<blocks(nk + mk), kBlock, 0, stream>>>(n, m, k, v[X], v[XP], v[X0], v[Y], v[YP], v[Y0], v[AX],
+                                                         v[AXP], v[AX0], ck, rho);
+    k_check_finalize<<<k, kBlock, 0, stream>>>(k, g_rows, g_cols, d_prow, d_pcol, d_sums, d_it_base, L);
+    B2P_CUDA(cudaGetLastError());
+    B2P_CUDA(cudaMemcpyAsync(h_sums, d_sums, sizeof(double) * k * kNumSums, cudaMemcpyDeviceToHost, stream));
+  }
+
   // Enqueues one check interval of L iterations on the stream (captured or not).
   void enqueue_interval(int L) {
+    if (k == 1) {
+      enqueue_interval_single(L);
+      return;
+    }
     const double rho = opt.reflection;
     const int64_t nk = static_cast<int64_t>(n) * k, mk = static_cast<int64_t>(m) * k;
     const unsigned gp = blocks(nk), gd = blocks(mk);
@@ -353,20 +490,11 @@ struct Engine {
       if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 3], stream));
       B2P_CUDA(cudaGetLastError());
     }
-    const IterClock ck{d_it_base, d_restart_at, L - 1};
-    k_check_rows<<<dim3(g_rows, k), kBlock, 0, stream>>>(m, k, v[AXP], v[RL], v[RU], v[YP], v[Y], v[Y0], d_rfac,
-                                                         d_prow);
-    k_check_cols<<<dim3(g_cols, k), kBlock, 0, stream>>>(n, k, viewAT(), v[YP], v[XP], v[X], v[X0], v[C], v[LO],
-                                                         v[UP], d_cfac, d_pcol);
-    k_halpern_all<<<blocks(nk + mk), kBlock, 0, stream>>>(n, m, k, v[X], v[XP], v[X0], v[Y], v[YP], v[Y0], v[AX],
-                                                         v[AXP], v[AX0], ck, rho);
-    k_check_finalize<<<k, kBlock, 0, stream>>>(k, g_rows, g_cols, d_prow, d_pcol, d_sums, d_it_base, L);
-    B2P_CUDA(cudaGetLastError());
-    B2P_CUDA(cudaMemcpyAsync(h_sums, d_sums, sizeof(double) * k * kNumSums, cudaMemcpyDeviceToHost, stream));
+    enqueue_check_tail(L, nullptr);
   }
 
   int64_t launches_per_interval(int L) const {
-    return static_cast<int64_t>(L) * ((n ? 1 : 0) + (m ? 1 : 0)) + 4;
+    return static_cast<int64_t>(L) * ((n ? 1 : 0) + (m ? 1 : 0)) + 4 + (k == 1 && n ? 1 : 0);
   }
 
   void run_interval(int L) {

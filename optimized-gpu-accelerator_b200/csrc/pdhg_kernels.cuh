@@ -259,7 +259,10 @@ __global__ void __launch_bounds__(kBlock) k_check_rows(int32_t m, int32_t k, con
 
 // Column part: A^T y+ (spmvT(YP, ATYP)) fused with kkt_cols
 // (src/pdhg/pdhg.cpp:181-196) + diff2(X, XP) + diff2(XP, X0).
+// `atyp` (k = 1 only) is A^T y+ computed by the binned SpMV; when NULL the
+// row sums are computed here.
 __global__ void __launch_bounds__(kBlock) k_check_cols(int32_t n, int32_t k, CsrView AT, const double* __restrict__ yp,
+                                                       const double* __restrict__ atyp_in,
                                                        const double* __restrict__ xp, const double* __restrict__ x,
                                                        const double* __restrict__ x0, const double* __restrict__ c,
                                                        const double* __restrict__ lo, const double* __restrict__ up,
@@ -271,7 +274,7 @@ __global__ void __launch_bounds__(kBlock) k_check_cols(int32_t n, int32_t k, Csr
   for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
        j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int64_t t = j * k + b;
-    const double atyp = row_dot(AT, yp, j, k, b);
+    const double atyp = atyp_in ? atyp_in[t] : row_dot(AT, yp, j, k, b);
     const double cv = c[t], l = lo[t], u = up[t], xpv = xp[t];
     const double d = cv - atyp;
     const bool hl = l > -1e300, hu = u < 1e300;

