@@ -245,16 +245,19 @@ def main():
     eng.solve()
     eng.set_profiling(False)
     prof = []
-    for cls, name in ((0, "k_primal"), (1, "k_dual")):
+    for cls, name in ((0, "k_primal_binned"), (1, "k_dual_binned"), (2, "k_resident")):
         n_l, ms = eng.kernel_times(cls)
-        prof.append((ms, n_l, name, eng.kernel_bytes(cls)))
+        if n_l > 0:
+            prof.append((ms, n_l, name, eng.kernel_bytes(cls)))
     prof.sort(reverse=True)
     ms, n_l, kname, kbytes = prof[0]
+    # per launch for the per-iteration kernels; per iteration for the resident interval kernel
     avg_s = ms / 1e3 / max(1, n_l)
     achieved = kbytes / avg_s / 1e9
     peak, peak_kind = measured_peak()
     spmv_total_bytes = sum(p[3] * p[1] for p in prof)
     spmv_total_s = sum(p[0] for p in prof) / 1e3
+    form = {1: "fused", 2: "resident"}.get(eng.last_stats.kernel_mode, "?")
     eng.close()
 
     if args.profile_iters > 0:
@@ -295,14 +298,15 @@ def main():
                 "warmup": args.warmup, "ms_per_step": t_dev * 1e3, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
                 "config": workload_config(lp, {"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                                               "iterations": iters}),
+                                               "iterations": iters, "kernel_form": form}),
                 "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches,
                 "spmv_gbs": spmv_total_bytes / spmv_total_s / 1e9,
                 "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_source": peak_kind,
                              "traffic": ncu_traffic(kname), "algorithmic_bytes_per_launch": kbytes,
-                             "avg_launch_us": avg_s * 1e6, "launches_profiled": n_l},
+                             "avg_launch_us": avg_s * 1e6, "launches_profiled": n_l,
+                             "unit_of_work": "one PDHG iteration" if kname == "k_resident" else "one launch"},
                 "clocks": clk.summary(),
                 "cpu_baseline": cpu}
         print(json.dumps(line))

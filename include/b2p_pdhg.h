@@ -52,6 +52,13 @@ enum {
   B2P_STATUS_ITERATION_LIMIT = 6
 };
 
+/* Kernel form of a single-LP solve. */
+enum {
+  B2P_KERNELS_AUTO = 0,
+  B2P_KERNELS_FUSED = 1,    /* two fused SpMV kernels per iteration, CUDA graph per check interval */
+  B2P_KERNELS_RESIDENT = 2  /* one persistent cooperative kernel per check interval, operators in shared memory */
+};
+
 /* Arithmetic of the iterates. */
 enum {
   B2P_PRECISION_FP64 = 0 /* plain form: FP64 everywhere, iterate parity with the reference */
@@ -101,6 +108,16 @@ typedef struct b2p_options {
   const volatile int32_t* cancel_flag; /* polled at every check when non-NULL; nonzero = stop */
   int32_t precision;        /* B2P_PRECISION_* */
   int32_t use_graphs;       /* capture each check interval as one CUDA graph (default 1) */
+  /* SpMV schedule of the single-LP kernels (0 = automatic): lanes per short
+   * row of A and of A^T (a power of two, 1..32), and how many rounds of 4
+   * entries per lane a short row may take before it moves to the one-warp-
+   * per-row path. */
+  int32_t lanes_per_row_a;
+  int32_t lanes_per_row_at;
+  int32_t short_row_rounds;
+  /* Single-LP kernel form: B2P_KERNELS_AUTO picks the resident form when the
+   * LP's operators fit in the SMs' shared memory. */
+  int32_t kernel_mode;
 } b2p_options;
 
 /* Replaces pramana::PdhgStats (src/pdhg/pdhg.h:44-56). */
@@ -115,6 +132,14 @@ typedef struct b2p_stats {
   double transfer_seconds; /* host<->device copies */
   int64_t bytes_uploaded, bytes_downloaded, kernel_launches;
   double spectral_norm;
+  /* setup breakdown: host preparation (scaling, CSR, ||A||), allocations and
+   * uploads, and kernel set-up (schedules, resident-form set-up, capture and
+   * instantiation of the CUDA graphs) */
+  double prepare_seconds, upload_seconds, graph_seconds;
+  int32_t lanes_per_row_a, lanes_per_row_at; /* schedule used */
+  int32_t kernel_mode;                        /* B2P_KERNELS_FUSED or B2P_KERNELS_RESIDENT (batches: FUSED) */
+  int32_t resident_blocks;                    /* cooperative grid size in resident form */
+  int64_t resident_smem_bytes;                /* largest block's shared memory in resident form */
 } b2p_stats;
 
 /* Replaces pramana::PdhgResult (src/pdhg/pdhg.h:58-65) minus the vectors,
@@ -165,15 +190,16 @@ int b2p_engine_create(const b2p_lp* lp, const b2p_case* cases, int32_t num_cases
 int b2p_engine_solve(b2p_engine* e, b2p_result* results, b2p_stats* stats);
 int b2p_engine_fetch(b2p_engine* e, double* x, double* row_dual);
 int b2p_engine_destroy(b2p_engine* e);
-/* When on, every fused SpMV kernel launch of the next solve is bracketed by
- * CUDA events; b2p_engine_kernel_times then returns, per kernel class
- * (0 = A^T y + primal step, 1 = A x+ + dual step), the launch count and the
- * summed device milliseconds. */
+/* When on, every fused SpMV kernel launch (and, in resident form, every
+ * interval launch) of the next solve is bracketed by CUDA events;
+ * b2p_engine_kernel_times then returns, per kernel class (0 = A^T y + primal
+ * step, 1 = A x+ + dual step, 2 = resident interval kernel), the count and the
+ * summed device milliseconds; for class 2 the count is in iterations. */
 int b2p_engine_set_profiling(b2p_engine* e, int32_t on);
 int b2p_engine_kernel_times(b2p_engine* e, int32_t kernel_class, int64_t* launches, double* total_ms);
 /* Algorithmic bytes of one launch of a kernel class (CSR values, indices and
  * row pointers read once, gathered vector read once, every streamed vector
- * read or written once). */
+ * read or written once); class 2: bytes of one iteration (classes 0 + 1). */
 int b2p_engine_kernel_bytes(b2p_engine* e, int32_t kernel_class, double* bytes);
 
 /* ---- Kernel-level entry -------------------------------------------------

@@ -29,6 +29,7 @@
 #include "../../include/b2p_pdhg.h"
 #include "pdhg_kernels.cuh"
 #include "pdhg_prepare.h"
+#include "pdhg_resident.cuh"
 #include "pdhg_spmv.cuh"
 
 namespace b2p {
@@ -71,9 +72,13 @@ int pick_device(int requested) {
     dev = env ? std::atoi(env) : 0;
   }
   if (dev < 0 || dev >= count) throw Error(B2P_ERR_NO_DEVICE, "device ordinal out of range");
-  cudaDeviceProp p;
-  B2P_CUDA(cudaGetDeviceProperties(&p, dev));
-  if (p.major != 10) throw Error(B2P_ERR_NO_DEVICE, std::string("device is not sm_100: ") + p.name);
+  int major = 0;
+  B2P_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+  if (major != 10) {
+    cudaDeviceProp p;
+    B2P_CUDA(cudaGetDeviceProperties(&p, dev));
+    throw Error(B2P_ERR_NO_DEVICE, std::string("device is not sm_100: ") + p.name);
+  }
   return dev;
 }
 
@@ -97,22 +102,31 @@ void check_lp(const b2p_lp* lp) {
 struct HostBins {
   std::vector<int32_t> long_rows, vlong_rows;
   int g = 1;
-  int long_thr = 8;
+  int long_thr = kUnroll;
 };
 
-constexpr int kVeryLongRow = 2048;  // rows longer than this get a 256-thread block
-
-HostBins make_bins(const HostCsr& M) {
+// Lanes per short row: enough that 90% of the rows finish in one round of
+// kUnroll entries per lane, but no more than fit the grid in one wave of
+// `wave_threads`; `rounds` rounds of kUnroll entries stay on the short path.
+HostBins make_bins(const HostCsr& M, int64_t wave_threads, int g_override, int rounds) {
   HostBins hb;
-  const int64_t nnz = M.rows ? M.ptr[M.rows] : 0;
-  const double avg = M.rows ? static_cast<double>(nnz) / M.rows : 0.0;
-  while (hb.g < 32 && 2.0 * hb.g <= avg) hb.g *= 2;
-  hb.long_thr = std::max(4 * hb.g, 8);
+  std::vector<int32_t> len(M.rows);
+  for (int32_t i = 0; i < M.rows; ++i) len[i] = M.ptr[i + 1] - M.ptr[i];
+  if (g_override > 0) {
+    while (hb.g < 32 && hb.g * 2 <= g_override) hb.g *= 2;
+  } else if (M.rows > 0) {
+    std::vector<int32_t> sorted(len);
+    const size_t q = static_cast<size_t>(0.9 * (sorted.size() - 1));
+    std::nth_element(sorted.begin(), sorted.begin() + q, sorted.end());
+    const int p90 = sorted[q];
+    while (hb.g < 32 && hb.g * kUnroll < p90) hb.g *= 2;
+    while (hb.g > 1 && static_cast<int64_t>(M.rows) * hb.g > wave_threads) hb.g /= 2;
+  }
+  hb.long_thr = std::max(1, rounds) * kUnroll * hb.g;
   for (int32_t i = 0; i < M.rows; ++i) {
-    const int32_t len = M.ptr[i + 1] - M.ptr[i];
-    if (len > kVeryLongRow)
+    if (len[i] > kVeryLongRow)
       hb.vlong_rows.push_back(i);
-    else if (len > hb.long_thr)
+    else if (len[i] > hb.long_thr)
       hb.long_rows.push_back(i);
   }
   return hb;
@@ -143,6 +157,62 @@ void launch(void (*kern)(KArgs...), unsigned grid, cudaStream_t stream, bool pdl
     default: F(32); break;                           \
   }
 
+using ResidentFn = void (*)(ResidentArgs);
+
+template <int GC>
+ResidentFn resident_fn_rows(int gr) {
+  switch (gr) {
+    case 1: return k_resident<GC, 1>;
+    case 2: return k_resident<GC, 2>;
+    case 4: return k_resident<GC, 4>;
+    default: return k_resident<GC, 8>;
+  }
+}
+
+ResidentFn resident_fn(int gc, int gr) {
+  switch (gc) {
+    case 1: return resident_fn_rows<1>(gr);
+    case 2: return resident_fn_rows<2>(gr);
+    case 4: return resident_fn_rows<4>(gr);
+    default: return resident_fn_rows<8>(gr);
+  }
+}
+
+// Contiguous split of M's rows into nb parts of near-equal (nnz + 4 rows).
+std::vector<int32_t> balanced_split(const HostCsr& M, int nb) {
+  std::vector<int32_t> b(nb + 1, M.rows);
+  b[0] = 0;
+  const double total = static_cast<double>(M.ptr[M.rows]) + 4.0 * M.rows;
+  int part = 1;
+  double acc = 0;
+  for (int32_t i = 0; i < M.rows && part < nb; ++i) {
+    acc += (M.ptr[i + 1] - M.ptr[i]) + 4.0;
+    while (part < nb && acc >= total * part / nb) b[part++] = i + 1;
+  }
+  for (; part < nb; ++part) b[part] = M.rows;
+  return b;
+}
+
+// Lanes per short row in the resident kernel: at most 1024/G groups must
+// cover the block's rows in one pass; no more lanes than 90% of rows need.
+int resident_lanes(const HostCsr& M, const std::vector<int32_t>& bounds) {
+  int max_rows = 1;
+  for (size_t b = 0; b + 1 < bounds.size(); ++b) max_rows = std::max(max_rows, bounds[b + 1] - bounds[b]);
+  int cap = 1;
+  while (cap < 8 && (kResidentThreads / (cap * 2)) >= max_rows) cap *= 2;
+  std::vector<int32_t> len(M.rows);
+  for (int32_t i = 0; i < M.rows; ++i) len[i] = M.ptr[i + 1] - M.ptr[i];
+  int p90 = 0;
+  if (!len.empty()) {
+    const size_t q = static_cast<size_t>(0.9 * (len.size() - 1));
+    std::nth_element(len.begin(), len.begin() + q, len.end());
+    p90 = len[q];
+  }
+  int need = 1;
+  while (need < 8 && need * kResUnroll < p90) need *= 2;
+  return std::min(cap, need);
+}
+
 }  // namespace
 
 struct Engine {
@@ -166,6 +236,15 @@ struct Engine {
   int32_t* d_mask = nullptr;
   int g_rows = 1, g_cols = 1;
   RowBins binsA{}, binsT{};  // k == 1 schedules of A and A^T
+  // resident form
+  bool resident = false;
+  int res_blocks = 0, res_gc = 1, res_gr = 1;
+  size_t res_smem = 0;
+  int32_t *d_cb = nullptr, *d_rb = nullptr;
+  unsigned* d_sync = nullptr;  // arrive, generation, error flag
+  double* d_rpartial = nullptr;
+  int32_t* h_error = nullptr;
+  ResidentFn res_fn = nullptr;
 
   // ---- pinned host ----
   double* h_sums = nullptr;   // k * kNumSums
@@ -177,8 +256,8 @@ struct Engine {
   std::map<int, cudaGraph_t> graph_defs;
   bool profiling = false;
   std::vector<cudaEvent_t> prof_ev;  // 4 per iteration of the longest interval
-  int64_t prof_launches[2] = {0, 0};
-  double prof_ms[2] = {0, 0};
+  int64_t prof_launches[3] = {0, 0, 0};
+  double prof_ms[3] = {0, 0, 0};
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
 
   // ---- last solve ----
@@ -214,6 +293,7 @@ struct Engine {
     if (h_sums) cudaFreeHost(h_sums);
     if (h_steps) cudaFreeHost(h_steps);
     if (h_mask) cudaFreeHost(h_mask);
+    if (h_error) cudaFreeHost(h_error);
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -246,6 +326,7 @@ struct Engine {
     po.rescale = opt.rescale_objective_and_bounds != 0;
     P = prepare(m, n, lp->start, lp->index, lp->value, lp->col_cost, lp->row_lower, lp->row_upper, lp->obj_offset,
                 po);
+    stats.prepare_seconds = seconds_since(t0);
 
     // Case data in scaled space, k-interleaved (src/pdhg/pdhg.cpp:466-481, 506-530).
     const size_t nk = static_cast<size_t>(n) * k, mk = static_cast<size_t>(m) * k;
@@ -300,9 +381,21 @@ struct Engine {
     d_rfac = upload(P.rfac);
     d_cfac = upload(P.cfac);
     if (k == 1) {
-      binsA = device_bins(P.A);
-      binsT = device_bins(P.AT);
+      const auto tk = Clock::now();
+      int per_sm = 0;
+      B2P_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dual_binned<4, true>, kBlock, 0));
+      int sms = 0;
+      B2P_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+      const int64_t wave = static_cast<int64_t>(std::max(1, per_sm)) * sms * kBlock;
+      const int rounds = opt.short_row_rounds > 0 ? opt.short_row_rounds : 2;
+      binsA = device_bins(P.A, wave, opt.lanes_per_row_a, rounds);
+      binsT = device_bins(P.AT, wave, opt.lanes_per_row_at, rounds);
+      stats.lanes_per_row_a = binsA.g;
+      stats.lanes_per_row_at = binsT.g;
+      setup_resident(sms);
+      stats.graph_seconds += seconds_since(tk);
     }
+    stats.kernel_mode = resident ? B2P_KERNELS_RESIDENT : B2P_KERNELS_FUSED;
     for (int s = 0; s < NSLOT; ++s) v[s] = dalloc<double>(row_slot(s) ? mk : nk);
     auto put = [&](int s, const std::vector<double>& h) {
       if (!h.empty())
@@ -335,12 +428,102 @@ struct Engine {
     }
     B2P_CUDA(cudaStreamSynchronize(stream));
     transfer_seconds = seconds_since(tx);
+    stats.upload_seconds = transfer_seconds;
     stats.setup_seconds = seconds_since(t0);
     stats.spectral_norm = P.normA;
   }
 
-  RowBins device_bins(const HostCsr& M) {
-    HostBins hb = make_bins(M);
+  // Resident form if the LP's slices fit in shared memory, one block per SM.
+  void setup_resident(int sms) {
+    if (opt.kernel_mode == B2P_KERNELS_FUSED || n == 0 || m == 0) return;
+    int optin = 0;
+    B2P_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    const int nb = sms;
+    std::vector<int32_t> cb = balanced_split(P.AT, nb), rb = balanced_split(P.A, nb);
+    size_t need = 0;
+    for (int b = 0; b < nb; ++b) {
+      const int nc = cb[b + 1] - cb[b], nr = rb[b + 1] - rb[b];
+      const int tn = P.AT.ptr[cb[b + 1]] - P.AT.ptr[cb[b]], an = P.A.ptr[rb[b + 1]] - P.A.ptr[rb[b]];
+      need = std::max(need, resident_smem_bytes(nc, nr, tn, an));
+    }
+    const size_t reserve = 1024;  // static shared memory of the kernel
+    if (need + reserve > static_cast<size_t>(optin)) {
+      if (opt.kernel_mode == B2P_KERNELS_RESIDENT)
+        throw Error(B2P_ERR_TOO_LARGE, "LP does not fit the resident form (shared memory)");
+      return;
+    }
+    res_gc = resident_lanes(P.AT, cb);
+    res_gr = resident_lanes(P.A, rb);
+    res_fn = resident_fn(res_gc, res_gr);
+    B2P_CUDA(cudaFuncSetAttribute(res_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(need)));
+    int per_sm = 0;
+    B2P_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, res_fn, kResidentThreads, need));
+    if (per_sm < 1) {
+      if (opt.kernel_mode == B2P_KERNELS_RESIDENT)
+        throw Error(B2P_ERR_TOO_LARGE, "resident kernel cannot be resident on an SM");
+      return;
+    }
+    d_cb = upload(cb);
+    d_rb = upload(rb);
+    d_sync = dalloc<unsigned>(4);
+    d_rpartial = dalloc<double>(static_cast<size_t>(nb) * kNumSums);
+    B2P_CUDA(cudaMallocHost(&h_error, sizeof(int32_t)));
+    res_blocks = nb;
+    res_smem = need;
+    resident = true;
+    stats.resident_blocks = nb;
+    stats.resident_smem_bytes = static_cast<int64_t>(need);
+  }
+
+  void launch_resident(int L) {
+    B2P_CUDA(cudaMemsetAsync(d_sync, 0, 4 * sizeof(unsigned), stream));
+    ResidentArgs ra{};
+    ra.cb = d_cb;
+    ra.rb = d_rb;
+    ra.A = viewA();
+    ra.AT = viewAT();
+    ra.x = v[X];
+    ra.x0 = v[X0];
+    ra.xp = v[XP];
+    ra.y = v[Y];
+    ra.y0 = v[Y0];
+    ra.yp = v[YP];
+    ra.ax = v[AX];
+    ra.ax0 = v[AX0];
+    ra.axp = v[AXP];
+    ra.c = v[C];
+    ra.lo = v[LO];
+    ra.up = v[UP];
+    ra.rl = v[RL];
+    ra.ru = v[RU];
+    ra.rfac = d_rfac;
+    ra.cfac = d_cfac;
+    ra.tau = d_tau;
+    ra.sigma = d_sigma;
+    ra.ck = IterClock{d_it_base, d_restart_at, 0};
+    ra.rho = opt.reflection;
+    ra.L = L;
+    ra.g_cols = res_gc;
+    ra.g_rows = res_gr;
+    ra.lt_cols = 2 * kResUnroll * res_gc;
+    ra.lt_rows = 2 * kResUnroll * res_gr;
+    ra.arrive = d_sync;
+    ra.gen = d_sync + 1;
+    ra.error = reinterpret_cast<int32_t*>(d_sync + 2);
+    ra.partial = d_rpartial;
+    ra.sums = d_sums;
+    ra.it_base = d_it_base;
+    void* args[] = {&ra};
+    if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[0], stream));
+    B2P_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(res_fn), dim3(res_blocks), dim3(kResidentThreads),
+                                         args, res_smem, stream));
+    if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[1], stream));
+    B2P_CUDA(cudaMemcpyAsync(h_sums, d_sums, sizeof(double) * kNumSums, cudaMemcpyDeviceToHost, stream));
+    B2P_CUDA(cudaMemcpyAsync(h_error, ra.error, sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+  }
+
+  RowBins device_bins(const HostCsr& M, int64_t wave, int g_override, int rounds) {
+    HostBins hb = make_bins(M, wave, g_override, rounds);
     RowBins b{};
     b.long_rows = upload(hb.long_rows);
     b.vlong_rows = upload(hb.vlong_rows);
@@ -499,9 +682,16 @@ struct Engine {
 
   void run_interval(int L) {
     if (profiling) ensure_prof_events(L);
+    if (resident) {
+      launch_resident(L);
+      launches += 1;
+      bytes_down += static_cast<int64_t>(sizeof(double) * kNumSums + sizeof(int32_t));
+      return;
+    }
     if (opt.use_graphs && !profiling) {
       auto it = graphs.find(L);
       if (it == graphs.end()) {
+        const auto tg = Clock::now();
         cudaGraph_t g;
         B2P_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         try {
@@ -516,6 +706,7 @@ struct Engine {
         B2P_CUDA(cudaGraphInstantiate(&ge, g, 0));
         graph_defs[L] = g;
         it = graphs.emplace(L, ge).first;
+        stats.graph_seconds += seconds_since(tg);
       }
       B2P_CUDA(cudaGraphLaunch(it->second, stream));
     } else {
@@ -527,6 +718,13 @@ struct Engine {
 
   void collect_profile(int L) {
     if (!profiling) return;
+    if (resident) {
+      float ms = 0;
+      B2P_CUDA(cudaEventElapsedTime(&ms, prof_ev[0], prof_ev[1]));
+      prof_ms[2] += ms;
+      prof_launches[2] += L;
+      return;
+    }
     for (int l = 0; l < L; ++l) {
       float ms = 0;
       if (n) {
@@ -561,8 +759,8 @@ struct Engine {
     const auto t_solve = Clock::now();
     std::vector<double> omega;
     launches = 0;
-    prof_launches[0] = prof_launches[1] = 0;
-    prof_ms[0] = prof_ms[1] = 0;
+    prof_launches[0] = prof_launches[1] = prof_launches[2] = 0;
+    prof_ms[0] = prof_ms[1] = prof_ms[2] = 0;
     reset_state(omega);
     results.assign(k, b2p_result{});
     x_out.assign(static_cast<size_t>(n) * k, 0.0);
@@ -600,6 +798,8 @@ struct Engine {
       const int L = static_cast<int>(std::min<int64_t>(cE, opt.max_iterations - it));
       run_interval(L);
       B2P_CUDA(cudaStreamSynchronize(stream));
+      if (resident && *h_error)
+        throw Error(B2P_ERR_CUDA, "resident kernel: grid barrier timed out (kernel left the interval)");
       collect_profile(L);
       it += L - 1;  // index of the check iteration
       ++checks;
@@ -705,6 +905,7 @@ struct Engine {
   }
 
   double kernel_bytes(int cls) const {
+    if (cls == 2) return kernel_bytes(0) + kernel_bytes(1);
     // Algorithmic bytes of one launch per case-batch: the CSR operator
     // (12 nnz + 4 (rows+1)), the gathered vector once (8 cols k), and the
     // streamed vectors (primal: x, c, lo, up, x0 read + x, x+ written = 7;
@@ -767,6 +968,7 @@ void b2p_default_options(b2p_options* o) {
   o->cancel_flag = nullptr;
   o->precision = B2P_PRECISION_FP64;
   o->use_graphs = 1;
+  o->kernel_mode = B2P_KERNELS_AUTO;
 }
 
 const char* b2p_last_error(void) { return b2p::g_last_error.c_str(); }
@@ -812,7 +1014,7 @@ int b2p_engine_set_profiling(b2p_engine* h, int32_t on) {
 
 int b2p_engine_kernel_times(b2p_engine* h, int32_t cls, int64_t* launches, double* total_ms) {
   return guarded([&] {
-    if (!h || cls < 0 || cls > 1) throw Error(B2P_ERR_INVALID, "bad engine or kernel class");
+    if (!h || cls < 0 || cls > 2) throw Error(B2P_ERR_INVALID, "bad engine or kernel class");
     Engine& e = *reinterpret_cast<Engine*>(h);
     if (launches) *launches = e.prof_launches[cls];
     if (total_ms) *total_ms = e.prof_ms[cls];
@@ -821,7 +1023,7 @@ int b2p_engine_kernel_times(b2p_engine* h, int32_t cls, int64_t* launches, doubl
 
 int b2p_engine_kernel_bytes(b2p_engine* h, int32_t cls, double* bytes) {
   return guarded([&] {
-    if (!h || cls < 0 || cls > 1 || !bytes) throw Error(B2P_ERR_INVALID, "bad engine, class or output");
+    if (!h || cls < 0 || cls > 2 || !bytes) throw Error(B2P_ERR_INVALID, "bad engine, class or output");
     *bytes = reinterpret_cast<Engine*>(h)->kernel_bytes(cls);
   });
 }

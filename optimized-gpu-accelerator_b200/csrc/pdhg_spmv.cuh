@@ -2,20 +2,22 @@
 // iteration kernels.
 //
 // Rows are split by length on the host (RowBins):
-//   short rows (len <= long_thr): a group of G lanes per row (G = 1..32, a
-//       power of two picked from the average row length), 32/G rows per warp,
-//       in the original row order;
-//   long rows  (long_thr < len <= vlong_thr): one warp per row;
-//   very long rows (len > vlong_thr): one 256-thread block per row.
-// Each lane accumulates the products of the entries p = lane, lane+G, ...
+//   short rows (len <= long_thr = kUnroll * G): a group of G lanes per row
+//       (G = 1..32, a power of two chosen so that the grid fits in one wave),
+//       32/G rows per warp, in the original row order;
+//   long rows  (long_thr < len <= kVeryLongRow): one warp per row;
+//   very long rows: one 256-thread block per row.
+// Each lane accumulates the products of entries p = lane, lane+S, lane+2S, ...
 // left to right; the lanes are then combined by a fixed xor-shuffle tree, so
 // the sum is deterministic (it differs from the reference's strictly
 // sequential row sum only in rounding order).
 //
-// Programmatic dependent launch: the row pointers and the first chunk of
-// column indices and values (constant during a solve) are loaded before
-// griddepcontrol.wait, i.e. while the previous kernel is still draining;
-// everything that kernel wrote is read after the wait.
+// Latency hiding: a lane loads the column indices and values of its first
+// kUnroll chunks before anything else (these are constant during a solve, so
+// this happens before griddepcontrol.wait, while the previous kernel is still
+// draining under programmatic dependent launch); after the wait the kernel
+// issues its epilogue loads and all kUnroll gathers of x together, so a short
+// row costs three dependent memory round trips (pointers, indices, x).
 #pragma once
 
 #include <cstdint>
@@ -23,6 +25,9 @@
 #include "pdhg_kernels.cuh"
 
 namespace b2p {
+
+constexpr int kUnroll = 4;
+constexpr int kVeryLongRow = 2048;  // rows longer than this get a 256-thread block
 
 struct RowBins {
   const int32_t* __restrict__ long_rows;   // rows for the warp path
@@ -38,95 +43,114 @@ struct RowBins {
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" :::); }
 
-// Result of the calling thread: `row` >= 0 and `leader` set on exactly one
-// thread per row, which then runs the row's epilogue.
-struct RowSum {
-  int32_t row;
-  bool leader;
-  double value;
+// What one thread does for its row: entries beg+lane0, +stride, ... < end.
+struct RowPlan {
+  int32_t row;     // -1: no row
+  int32_t p;       // first entry of this lane
+  int32_t end;
+  int32_t stride;
+  int32_t path;    // 0 short, 1 warp, 2 block
+  bool leader;     // runs the row's epilogue
+  int32_t ci[kUnroll];
+  double cv[kUnroll];
 };
 
+// Pre-wait part: row assignment and the first kUnroll (index, value) pairs.
 template <int G>
-__device__ __forceinline__ double group_sum(double s) {
-#pragma unroll
-  for (int off = G / 2; off > 0; off >>= 1) s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, off));
-  return s;
-}
-
-// Sum of the row's entries p = beg+lane0, +stride, ... with the first entry
-// prefetched before the dependency wait.
-template <int STRIDE>
-__device__ __forceinline__ double strided_dot(const CsrView& M, const double* __restrict__ x, int beg, int end,
-                                              int lane0) {
-  int p = beg + lane0;
-  int ci = 0;
-  double cv = 0.0;
-  if (p < end) {
-    ci = __ldg(M.idx + p);
-    cv = __ldg(M.val + p);
-  }
-  pdl_wait();
-  double s = 0.0;
-  if (p < end) s = __dmul_rn(cv, __ldcg(x + ci));
-  for (p += STRIDE; p < end; p += STRIDE) s = __dadd_rn(s, __dmul_rn(__ldg(M.val + p), __ldcg(x + __ldg(M.idx + p))));
-  return s;
-}
-
-// Dispatch of one thread of a binned row-sum grid.  Every thread of the
-// block calls this (it contains warp shuffles and, on the block path, a
-// __syncthreads); it performs griddepcontrol.wait exactly once.
-template <int G>
-__device__ __forceinline__ RowSum binned_row_sum(const CsrView& M, const RowBins& bins, const double* __restrict__ x,
-                                                 double* sh /* kBlock/32 doubles */) {
-  RowSum r{-1, false, 0.0};
+__device__ __forceinline__ RowPlan plan_row(const CsrView& M, const RowBins& bins) {
+  RowPlan pl;
+  pl.row = -1;
+  pl.p = 0;
+  pl.end = 0;
+  pl.leader = false;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int blk = blockIdx.x;
   if (blk < bins.vlong_blocks) {
-    // one block per very long row
-    const int row = __ldg(bins.vlong_rows + blk);
-    const int beg = __ldg(M.ptr + row), end = __ldg(M.ptr + row + 1);
-    double s = strided_dot<kBlock>(M, x, beg, end, threadIdx.x);
-    s = group_sum<32>(s);
-    if (lane == 0) sh[warp] = s;
-    __syncthreads();
-    if (warp == 0) {
-      double v = lane < kBlock / 32 ? sh[lane] : 0.0;
-      v = group_sum<32>(v);
-      if (lane == 0) r = RowSum{row, true, v};
-    }
-    return r;
-  }
-  blk -= bins.vlong_blocks;
-  if (blk < bins.long_blocks) {
-    // one warp per long row
+    pl.path = 2;
+    pl.stride = kBlock;
+    pl.row = __ldg(bins.vlong_rows + blk);
+    pl.p = __ldg(M.ptr + pl.row) + threadIdx.x;
+    pl.end = __ldg(M.ptr + pl.row + 1);
+    pl.leader = threadIdx.x == 0;
+  } else if ((blk -= bins.vlong_blocks) < bins.long_blocks) {
+    pl.path = 1;
+    pl.stride = 32;
     const int q = blk * (kBlock / 32) + warp;
-    int beg = 0, end = 0, row = -1;
     if (q < bins.n_long) {
-      row = __ldg(bins.long_rows + q);
-      beg = __ldg(M.ptr + row);
-      end = __ldg(M.ptr + row + 1);
+      pl.row = __ldg(bins.long_rows + q);
+      pl.p = __ldg(M.ptr + pl.row) + lane;
+      pl.end = __ldg(M.ptr + pl.row + 1);
+      pl.leader = lane == 0;
     }
-    double s = strided_dot<32>(M, x, beg, end, lane);
-    s = group_sum<32>(s);
-    if (row >= 0 && lane == 0) r = RowSum{row, true, s};
-    return r;
+  } else {
+    blk -= bins.long_blocks;
+    pl.path = 0;
+    pl.stride = G;
+    const int row = (blk * kBlock + threadIdx.x) / G;
+    if (row < M.rows) {
+      const int beg = __ldg(M.ptr + row), end = __ldg(M.ptr + row + 1);
+      if (end - beg <= bins.long_thr) {
+        pl.row = row;
+        pl.p = beg + (threadIdx.x & (G - 1));
+        pl.end = end;
+        pl.leader = (threadIdx.x & (G - 1)) == 0;
+      }
+    }
   }
-  blk -= bins.long_blocks;
-  // G lanes per short row
-  const int row = (blk * kBlock + threadIdx.x) / G;
-  const int gl = threadIdx.x & (G - 1);
-  int beg = 0, end = 0;
-  bool mine = false;
-  if (row < M.rows) {
-    beg = __ldg(M.ptr + row);
-    end = __ldg(M.ptr + row + 1);
-    mine = end - beg <= bins.long_thr;
-    if (!mine) end = beg;  // handled by the warp or block path
+#pragma unroll
+  for (int u = 0; u < kUnroll; ++u) {
+    const int q = pl.p + u * pl.stride;
+    const bool ok = q < pl.end;
+    pl.ci[u] = ok ? __ldg(M.idx + q) : 0;
+    pl.cv[u] = ok ? __ldg(M.val + q) : 0.0;
   }
-  double s = strided_dot<G>(M, x, beg, end, gl);
-  s = group_sum<G>(s);
-  if (mine && gl == 0) r = RowSum{row, true, s};
-  return r;
+  return pl;
+}
+
+template <int W>
+__device__ __forceinline__ double lane_tree(double s) {
+#pragma unroll
+  for (int off = W / 2; off > 0; off >>= 1) s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, off));
+  return s;
+}
+
+// Post-wait part: the gathers, the lane sums and the tree.  Called by every
+// thread of the block (warp shuffles; __syncthreads on the block path, which
+// is block-uniform).  The result is valid on the leader thread.
+template <int G>
+__device__ __forceinline__ double finish_row(const RowPlan& pl, const CsrView& M, const double* __restrict__ x,
+                                             double* sh /* kBlock/32 doubles */) {
+  double xv[kUnroll];
+#pragma unroll
+  for (int u = 0; u < kUnroll; ++u) xv[u] = (pl.p + u * pl.stride < pl.end) ? __ldcg(x + pl.ci[u]) : 0.0;
+  double s = 0.0;
+#pragma unroll
+  for (int u = 0; u < kUnroll; ++u)
+    if (pl.p + u * pl.stride < pl.end) s = (u == 0) ? __dmul_rn(pl.cv[0], xv[0]) : __dadd_rn(s, __dmul_rn(pl.cv[u], xv[u]));
+  // Rows longer than kUnroll chunks (warp and block paths): further rounds.
+  for (int p = pl.p + kUnroll * pl.stride; p < pl.end; p += kUnroll * pl.stride) {
+    int ci[kUnroll];
+    double cv[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int q = p + u * pl.stride;
+      ci[u] = q < pl.end ? __ldg(M.idx + q) : 0;
+      cv[u] = q < pl.end ? __ldg(M.val + q) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) xv[u] = (p + u * pl.stride < pl.end) ? __ldcg(x + ci[u]) : 0.0;
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u)
+      if (p + u * pl.stride < pl.end) s = __dadd_rn(s, __dmul_rn(cv[u], xv[u]));
+  }
+  if (pl.path == 0) return lane_tree<G>(s);
+  s = lane_tree<32>(s);
+  if (pl.path == 1) return s;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) sh[warp] = s;
+  __syncthreads();
+  double v = lane < kBlock / 32 ? sh[lane] : 0.0;
+  return lane_tree<32>(v);
 }
 
 // x+ = proj(x - tau (c - A^T y)), Halpern step of x (skipped at a check
@@ -138,17 +162,32 @@ __global__ void __launch_bounds__(kBlock) k_primal_binned(CsrView AT, RowBins bi
                                                           double* __restrict__ xp, const double* __restrict__ x0,
                                                           const double* __restrict__ tau, IterClock ck, double rho) {
   __shared__ double sh[kBlock / 32];
-  const RowSum r = binned_row_sum<G>(AT, bins, y, sh);
+  const RowPlan pl = plan_row<G>(AT, bins);
+  const int j = pl.row;
+  double cj = 0, l = 0, u = 0;
+  if (pl.leader) {
+    cj = __ldg(c + j);
+    l = __ldg(lo + j);
+    u = __ldg(up + j);
+  }
+  pdl_wait();
+  double xv = 0, x0v = 0, t = 0, lam = 0;
+  if (pl.leader) {
+    xv = __ldcg(x + j);
+    t = __ldcg(tau);
+    if (HALPERN) {
+      x0v = __ldcg(x0 + j);
+      lam = halpern_lambda(ck, 0);
+    }
+  }
+  const double aty = finish_row<G>(pl, AT, y, sh);
   pdl_launch_dependents();
-  if (!r.leader) return;
-  const int j = r.row;
-  const double xv = __ldcg(x + j);
-  double v = __dsub_rn(xv, __dmul_rn(__ldcg(tau), __dsub_rn(__ldg(c + j), r.value)));
-  const double l = __ldg(lo + j), u = __ldg(up + j);
+  if (!pl.leader) return;
+  double v = __dsub_rn(xv, __dmul_rn(t, __dsub_rn(cj, aty)));
   v = (v < l) ? l : v;
   v = (u < v) ? u : v;
   xp[j] = v;
-  if (HALPERN) x[j] = halpern_step(xv, v, __ldcg(x0 + j), halpern_lambda(ck, 0), rho);
+  if (HALPERN) x[j] = halpern_step(xv, v, x0v, lam, rho);
 }
 
 // y+ = v + sigma proj(-v/sigma), v = y - sigma (2 A x+ - A x); Halpern steps of y and Ax.
@@ -160,24 +199,38 @@ __global__ void __launch_bounds__(kBlock) k_dual_binned(CsrView A, RowBins bins,
                                                         double* __restrict__ axp, const double* __restrict__ ax0,
                                                         const double* __restrict__ sigma, IterClock ck, double rho) {
   __shared__ double sh[kBlock / 32];
-  const RowSum r = binned_row_sum<G>(A, bins, xp, sh);
+  const RowPlan pl = plan_row<G>(A, bins);
+  const int i = pl.row;
+  double l = 0, u = 0;
+  if (pl.leader) {
+    l = __ldg(rl + i);
+    u = __ldg(ru + i);
+  }
+  pdl_wait();
+  double axv = 0, yv = 0, s = 0, y0v = 0, ax0v = 0, lam = 0;
+  if (pl.leader) {
+    axv = __ldcg(ax + i);
+    yv = __ldcg(y + i);
+    s = __ldcg(sigma);
+    if (HALPERN) {
+      y0v = __ldcg(y0 + i);
+      ax0v = __ldcg(ax0 + i);
+      lam = halpern_lambda(ck, 0);
+    }
+  }
+  const double axpv = finish_row<G>(pl, A, xp, sh);
   pdl_launch_dependents();
-  if (!r.leader) return;
-  const int i = r.row;
-  const double axpv = r.value, axv = __ldcg(ax + i), yv = __ldcg(y + i);
-  const double s = __ldcg(sigma);
+  if (!pl.leader) return;
   const double v = __dsub_rn(yv, __dmul_rn(s, __dsub_rn(__dmul_rn(2.0, axpv), axv)));
   double w = __ddiv_rn(-v, s);
-  const double l = __ldg(rl + i), u = __ldg(ru + i);
   w = (w < l) ? l : w;
   w = (u < w) ? u : w;
   const double ypv = __dadd_rn(v, __dmul_rn(s, w));
   axp[i] = axpv;
   yp[i] = ypv;
   if (HALPERN) {
-    const double lam = halpern_lambda(ck, 0);
-    y[i] = halpern_step(yv, ypv, __ldcg(y0 + i), lam, rho);
-    ax[i] = halpern_step(axv, axpv, __ldcg(ax0 + i), lam, rho);
+    y[i] = halpern_step(yv, ypv, y0v, lam, rho);
+    ax[i] = halpern_step(axv, axpv, ax0v, lam, rho);
   }
 }
 
@@ -186,9 +239,11 @@ template <int G>
 __global__ void __launch_bounds__(kBlock) k_spmv_binned(CsrView M, RowBins bins, const double* __restrict__ x,
                                                         double* __restrict__ out) {
   __shared__ double sh[kBlock / 32];
-  const RowSum r = binned_row_sum<G>(M, bins, x, sh);
+  const RowPlan pl = plan_row<G>(M, bins);
+  pdl_wait();
+  const double s = finish_row<G>(pl, M, x, sh);
   pdl_launch_dependents();
-  if (r.leader) out[r.row] = r.value;
+  if (pl.leader) out[pl.row] = s;
 }
 
 }  // namespace b2p

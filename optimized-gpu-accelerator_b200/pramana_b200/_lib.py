@@ -17,6 +17,7 @@ ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "no usable sm_100 device", 
           5: "size beyond maximum"}
 STATUS_NAMES = {0: "NotSolved", 1: "Optimal", 5: "TimeLimit", 6: "IterationLimit"}
 PRECISION_FP64 = 0
+KERNELS_AUTO, KERNELS_FUSED, KERNELS_RESIDENT = 0, 1, 2
 
 dptr = C.POINTER(C.c_double)
 iptr = C.POINTER(C.c_int32)
@@ -38,7 +39,9 @@ class B2pOptions(C.Structure):
                 ("ruiz_iterations", C.c_int32), ("pock_chambolle", C.c_int32),
                 ("rescale_objective_and_bounds", C.c_int32), ("reflection", C.c_double),
                 ("log_interval", C.c_int32), ("device", C.c_int32), ("time_limit", C.c_double),
-                ("cancel_flag", C.POINTER(C.c_int32)), ("precision", C.c_int32), ("use_graphs", C.c_int32)]
+                ("cancel_flag", C.POINTER(C.c_int32)), ("precision", C.c_int32), ("use_graphs", C.c_int32),
+                ("lanes_per_row_a", C.c_int32), ("lanes_per_row_at", C.c_int32), ("short_row_rounds", C.c_int32),
+                ("kernel_mode", C.c_int32)]
 
 
 class B2pStats(C.Structure):
@@ -46,7 +49,10 @@ class B2pStats(C.Structure):
                 ("primal_residual", C.c_double), ("dual_residual", C.c_double), ("gap", C.c_double),
                 ("primal_weight", C.c_double), ("setup_seconds", C.c_double), ("solve_seconds", C.c_double),
                 ("kernel_seconds", C.c_double), ("transfer_seconds", C.c_double), ("bytes_uploaded", C.c_int64),
-                ("bytes_downloaded", C.c_int64), ("kernel_launches", C.c_int64), ("spectral_norm", C.c_double)]
+                ("bytes_downloaded", C.c_int64), ("kernel_launches", C.c_int64), ("spectral_norm", C.c_double),
+                ("prepare_seconds", C.c_double), ("upload_seconds", C.c_double), ("graph_seconds", C.c_double),
+                ("lanes_per_row_a", C.c_int32), ("lanes_per_row_at", C.c_int32), ("kernel_mode", C.c_int32),
+                ("resident_blocks", C.c_int32), ("resident_smem_bytes", C.c_int64)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_ if not f.startswith("pad")}

@@ -43,6 +43,10 @@ class PdhgOptions:
     device: int = -1
     useGraphs: bool = True
     precision: int = _lib.PRECISION_FP64
+    lanesPerRowA: int = 0        # SpMV schedule overrides (0 = automatic)
+    lanesPerRowAT: int = 0
+    shortRowRounds: int = 0
+    kernelMode: int = _lib.KERNELS_AUTO   # KERNELS_FUSED / KERNELS_RESIDENT to force a form
 
     def to_c(self, cancel_flag=None) -> _lib.B2pOptions:
         if not self.useGpu:
@@ -61,6 +65,10 @@ class PdhgOptions:
         o.time_limit = float(self.timeLimit)
         o.precision = int(self.precision)
         o.use_graphs = int(bool(self.useGraphs))
+        o.lanes_per_row_a = int(self.lanesPerRowA)
+        o.lanes_per_row_at = int(self.lanesPerRowAT)
+        o.short_row_rounds = int(self.shortRowRounds)
+        o.kernel_mode = int(self.kernelMode)
         if cancel_flag is not None:
             o.cancel_flag = C.cast(cancel_flag, C.POINTER(C.c_int32))
         return o

@@ -44,6 +44,9 @@ def assert_close(g, o, exact_iters=True, window=0):
     assert abs(g.objective - o.objective) <= REL_TOL * (1 + abs(o.objective))
 
 
+FORMS = [1, 2]  # B2P_KERNELS_FUSED, B2P_KERNELS_RESIDENT
+
+
 def opts(**kw):
     po = pdhg.PdhgOptions()
     for k, v in kw.items():
@@ -76,29 +79,43 @@ def test_spmv_bitexact(oracle_mod, k):
     assert np.array_equal(y, oracle_mod.csr_mult(ptr, idx, val, x, rows, k))
 
 
+@pytest.mark.parametrize("mode", FORMS)
 @pytest.mark.parametrize("iters", [1, 2, 63, 64, 65, 1000])
-def test_fixed_iterations_c1(oracle_mod, iters):
+def test_fixed_iterations_c1(oracle_mod, iters, mode):
     lp = G.config1(1)
-    g = pdhg.solvePdhg(lp, opts(tolerance=1e-30, maxIterations=iters))
+    g = pdhg.solvePdhg(lp, opts(tolerance=1e-30, maxIterations=iters, kernelMode=mode))
     assert_close(g, oracle_mod.solve(lp, "oracle", tolerance=1e-30, max_iterations=iters))
 
 
-def test_before_first_restart_rounding_level(oracle_mod):
+@pytest.mark.parametrize("mode", FORMS)
+def test_before_first_restart_rounding_level(oracle_mod, mode):
     """Before the first restart the iterates differ from the reference only by
     the rounding order of the row sums: far inside the 1e-9 bar."""
     lp = G.config2(2)
-    g = pdhg.solvePdhg(lp, opts(tolerance=1e-30, maxIterations=64))
+    g = pdhg.solvePdhg(lp, opts(tolerance=1e-30, maxIterations=64, kernelMode=mode))
     o = oracle_mod.solve(lp, "oracle", tolerance=1e-30, max_iterations=64)
     assert rel_err(g.x, o.x) <= 1e-13 and rel_err(g.rowDual, o.y) <= 1e-13
 
 
+@pytest.mark.parametrize("mode", FORMS)
+def test_kernel_form_reported(mode):
+    lp = G.config1(1)
+    with pdhg.Engine(lp, opts(tolerance=1e-30, maxIterations=10, kernelMode=mode)) as e:
+        e.solve()
+        st = e.last_stats
+    assert st.kernel_mode == mode
+    if mode == 2:
+        assert st.resident_blocks > 0 and 0 < st.resident_smem_bytes <= 232448
+
+
+@pytest.mark.parametrize("mode", FORMS)
 @pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "*.npz"))))
-def test_golden_fixtures(path):
+def test_golden_fixtures(path, mode):
     d = np.load(path)
     lp = Model(num_rows=int(d["num_rows"]), num_cols=int(d["num_cols"]), start=d["start"], index=d["index"],
                value=d["value"], col_cost=d["col_cost"], col_lower=d["col_lower"], col_upper=d["col_upper"],
                row_lower=d["row_lower"], row_upper=d["row_upper"], obj_offset=float(d["obj_offset"]))
-    po = opts(tolerance=float(d["tolerance"]), maxIterations=int(d["max_iterations"]))
+    po = opts(tolerance=float(d["tolerance"]), maxIterations=int(d["max_iterations"]), kernelMode=mode)
     if bool(d["batch"]):
         rs = pdhg.solvePdhgBatch(lp, [LpCase(cost=c) for c in d["case_cost"]], po)
     else:
@@ -115,17 +132,20 @@ def test_golden_fixtures(path):
         assert_close(g, o)
 
 
+@pytest.mark.parametrize("mode", FORMS)
 @pytest.mark.parametrize("seed", [5, 6, 7])
-def test_edge_bounds(oracle_mod, seed):
+def test_edge_bounds(oracle_mod, seed, mode):
     lp = lp_cases.edge_lp(seed)
     for kw in (dict(tolerance=1e-30, max_iterations=500), dict(tolerance=1e-6, max_iterations=50000)):
-        g = pdhg.solvePdhg(lp, opts(tolerance=kw["tolerance"], maxIterations=kw["max_iterations"]))
+        g = pdhg.solvePdhg(lp, opts(tolerance=kw["tolerance"], maxIterations=kw["max_iterations"], kernelMode=mode))
         assert_close(g, oracle_mod.solve(lp, "oracle", **kw))
 
 
 @pytest.mark.parametrize("kw", [dict(ruizIterations=0), dict(pockChambolle=False),
                                 dict(rescaleObjectiveAndBounds=False), dict(reflection=0.5), dict(checkEvery=17),
-                                dict(maxIterations=1001), dict(useGraphs=False)])
+                                dict(maxIterations=1001), dict(useGraphs=False, kernelMode=1),
+                                dict(checkEvery=17, kernelMode=2), dict(maxIterations=1001, kernelMode=2),
+                                dict(reflection=0.5, kernelMode=2), dict(lanesPerRowA=8, lanesPerRowAT=4, kernelMode=1)])
 def test_options(oracle_mod, kw):
     lp = G.random_lp(200, 400, 4.0, 120, 9)
     ok = dict(tolerance=1e-5, max_iterations=20000)
@@ -171,9 +191,10 @@ def test_batch_equals_individual_solves():
         assert abs(r.objective - s.objective) <= 1e-5 * (1 + abs(s.objective))
 
 
-def test_resolve_is_deterministic():
+@pytest.mark.parametrize("mode", FORMS)
+def test_resolve_is_deterministic(mode):
     lp = G.config1(2)
-    with pdhg.Engine(lp, opts(tolerance=1e-4)) as e:
+    with pdhg.Engine(lp, opts(tolerance=1e-4, kernelMode=mode)) as e:
         a = e.solve()[0]
         b = e.solve()[0]
     assert a.iterations == b.iterations and np.array_equal(a.x, b.x) and np.array_equal(a.rowDual, b.rowDual)
@@ -234,14 +255,15 @@ def _host_kkt(lp: Model, x, y):
     return relP, relD, gap
 
 
-def test_c2_full_size_properties(oracle_mod):
+@pytest.mark.parametrize("mode", FORMS)
+def test_c2_full_size_properties(oracle_mod, mode):
     """m=40k, n=80k, 512k nnz (skewed rows) to 1e-6: too long for the oracle at
     this size, so check size-independent properties: the returned point's KKT
     recomputed on the host meets the tolerance, the iteration count matches
     the reference run of the same LP (20,287 +- 4 checks), and the
     reference's outward-rounded dual bound is valid and tight."""
     lp = G.config2(2)
-    g = pdhg.solvePdhg(lp, opts(tolerance=1e-6))
+    g = pdhg.solvePdhg(lp, opts(tolerance=1e-6, kernelMode=mode))
     assert g.status == "Optimal"
     assert abs(g.iterations - 20287) <= 4 * 64
     relP, relD, gap = _host_kkt(lp, g.x, g.rowDual)
