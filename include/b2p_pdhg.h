@@ -202,6 +202,18 @@ int b2p_engine_kernel_times(b2p_engine* e, int32_t kernel_class, int64_t* launch
  * read or written once); class 2: bytes of one iteration (classes 0 + 1). */
 int b2p_engine_kernel_bytes(b2p_engine* e, int32_t kernel_class, double* bytes);
 
+/* ---- KKT evaluation ---------------------------------------------------------
+ * Relative KKT error of caller-given points, as runPdhg measures it at every
+ * check (src/pdhg/pdhg.cpp:166-197, 608-615), in the original space: for case
+ * b, out[4b..4b+3] = relative primal residual, relative dual residual,
+ * relative gap, and their maximum.  x is num_cases x num_cols, row_dual
+ * num_cases x num_rows (case-major); num_cases <= 0 means one point of the
+ * base model.  Host arrays in and out.  (The reference computes this only
+ * inside its loop; this entry judges points from elsewhere, e.g. warm
+ * starts.) */
+int b2p_kkt_residual(const b2p_lp* lp, const b2p_case* cases, int32_t num_cases, const double* x,
+                     const double* row_dual, double* out);
+
 /* ---- Kernel-level entry -------------------------------------------------
  * y(i,b) = sum_p val[p] * x(idx[p], b) for a CSR matrix (rows x cols) and k
  * interleaved right-hand sides (element (i,b) at i*k+b), summed left to right

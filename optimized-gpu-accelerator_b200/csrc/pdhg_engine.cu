@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "../../include/b2p_pdhg.h"
+#include "pdhg_host_common.h"
 #include "pdhg_kernels.cuh"
 #include "pdhg_prepare.h"
 #include "pdhg_resident.cuh"
@@ -36,51 +37,10 @@ namespace b2p {
 
 namespace {
 
-thread_local std::string g_last_error;
-
-struct Error : std::runtime_error {
-  int code;
-  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
-};
-
-#define B2P_CUDA(call)                                                                                     \
-  do {                                                                                                     \
-    cudaError_t e_ = (call);                                                                               \
-    if (e_ != cudaSuccess)                                                                                 \
-      throw Error(e_ == cudaErrorMemoryAllocation ? B2P_ERR_OOM : B2P_ERR_CUDA,                            \
-                  std::string("CUDA error in ") + #call + ": " + cudaGetErrorString(e_));                  \
-  } while (0)
-
-using Clock = std::chrono::steady_clock;
-double seconds_since(Clock::time_point t0) { return std::chrono::duration<double>(Clock::now() - t0).count(); }
-
 // Device vector slots (the reference's enum V, src/pdhg/pdhg.cpp:45, minus
 // ATY/ATYP which the fused kernels never store, plus the initial point).
 enum Slot : int { X, XP, X0, C, LO, UP, XINIT, ATYP, NCOLVEC, Y = NCOLVEC, YP, Y0, AX, AXP, AX0, RL, RU, AXINIT, NSLOT };
 inline bool row_slot(int s) { return s >= Y; }
-
-int pick_device(int requested) {
-  if (std::getenv("PRAMANA_DISABLE_GPU")) throw Error(B2P_ERR_NO_DEVICE, "disabled by PRAMANA_DISABLE_GPU");
-  int count = 0;
-  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
-    cudaGetLastError();
-    throw Error(B2P_ERR_NO_DEVICE, "no CUDA device");
-  }
-  int dev = requested;
-  if (dev < 0) {
-    const char* env = std::getenv("PRAMANA_GPU_DEVICE");
-    dev = env ? std::atoi(env) : 0;
-  }
-  if (dev < 0 || dev >= count) throw Error(B2P_ERR_NO_DEVICE, "device ordinal out of range");
-  int major = 0;
-  B2P_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
-  if (major != 10) {
-    cudaDeviceProp p;
-    B2P_CUDA(cudaGetDeviceProperties(&p, dev));
-    throw Error(B2P_ERR_NO_DEVICE, std::string("device is not sm_100: ") + p.name);
-  }
-  return dev;
-}
 
 void check_lp(const b2p_lp* lp) {
   if (!lp) throw Error(B2P_ERR_INVALID, "lp is NULL");
@@ -920,26 +880,9 @@ struct Engine {
 
 using b2p::Engine;
 using b2p::Error;
+using b2p::guarded;
 
 namespace {
-
-template <class F>
-int guarded(F&& f) {
-  try {
-    b2p::g_last_error.clear();
-    f();
-    return B2P_OK;
-  } catch (Error& e) {
-    b2p::g_last_error = e.what();
-    return e.code;
-  } catch (std::bad_alloc&) {
-    b2p::g_last_error = "host out of memory";
-    return B2P_ERR_OOM;
-  } catch (std::exception& e) {
-    b2p::g_last_error = e.what();
-    return B2P_ERR_CUDA;
-  }
-}
 
 void copy_results(Engine& e, double* x, double* y, b2p_result* results, b2p_stats* stats) {
   if (x && !e.x_out.empty()) std::memcpy(x, e.x_out.data(), e.x_out.size() * sizeof(double));
@@ -971,7 +914,7 @@ void b2p_default_options(b2p_options* o) {
   o->kernel_mode = B2P_KERNELS_AUTO;
 }
 
-const char* b2p_last_error(void) { return b2p::g_last_error.c_str(); }
+const char* b2p_last_error(void) { return b2p::last_error().c_str(); }
 
 int b2p_engine_create(const b2p_lp* lp, const b2p_case* cases, int32_t num_cases, const b2p_options* opts,
                       b2p_engine** out) {

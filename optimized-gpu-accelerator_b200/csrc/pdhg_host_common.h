@@ -1,0 +1,86 @@
+// Host-side helpers shared by the engine's translation units: error type and
+// CUDA-call check, the per-thread last-error message behind b2p_last_error,
+// the ABI guard that turns exceptions into return codes, and device choice.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdlib>
+#include <new>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/b2p_pdhg.h"
+
+namespace b2p {
+
+inline std::string& last_error() {
+  thread_local std::string msg;
+  return msg;
+}
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define B2P_CUDA(call)                                                                                     \
+  do {                                                                                                     \
+    cudaError_t e_ = (call);                                                                               \
+    if (e_ != cudaSuccess)                                                                                 \
+      throw ::b2p::Error(e_ == cudaErrorMemoryAllocation ? B2P_ERR_OOM : B2P_ERR_CUDA,                     \
+                         std::string("CUDA error in ") + #call + ": " + cudaGetErrorString(e_));           \
+  } while (0)
+
+using Clock = std::chrono::steady_clock;
+inline double seconds_since(Clock::time_point t0) {
+  return std::chrono::duration<double>(Clock::now() - t0).count();
+}
+
+// Runs f and maps exceptions to B2P_ERR_* codes (no exception crosses the C ABI).
+template <class F>
+int guarded(F&& f) {
+  try {
+    last_error().clear();
+    f();
+    return B2P_OK;
+  } catch (Error& e) {
+    last_error() = e.what();
+    return e.code;
+  } catch (std::bad_alloc&) {
+    last_error() = "host out of memory";
+    return B2P_ERR_OOM;
+  } catch (std::exception& e) {
+    last_error() = e.what();
+    return B2P_ERR_CUDA;
+  }
+}
+
+// Ordinal of the sm_100 device to use: `requested`, else PRAMANA_GPU_DEVICE,
+// else 0 (src/gpu/cuda_driver.cpp:223); PRAMANA_DISABLE_GPU disables the
+// engine (cuda_driver.cpp:149).
+inline int pick_device(int requested) {
+  if (std::getenv("PRAMANA_DISABLE_GPU")) throw Error(B2P_ERR_NO_DEVICE, "disabled by PRAMANA_DISABLE_GPU");
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    throw Error(B2P_ERR_NO_DEVICE, "no CUDA device");
+  }
+  int dev = requested;
+  if (dev < 0) {
+    const char* env = std::getenv("PRAMANA_GPU_DEVICE");
+    dev = env ? std::atoi(env) : 0;
+  }
+  if (dev < 0 || dev >= count) throw Error(B2P_ERR_NO_DEVICE, "device ordinal out of range");
+  int major = 0;
+  B2P_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+  if (major != 10) {
+    cudaDeviceProp p;
+    B2P_CUDA(cudaGetDeviceProperties(&p, dev));
+    throw Error(B2P_ERR_NO_DEVICE, std::string("device is not sm_100: ") + p.name);
+  }
+  return dev;
+}
+
+}  // namespace b2p

@@ -98,7 +98,7 @@ __device__ __forceinline__ void split(int64_t t, int k, int64_t& row, int& b) {
 // ---- per-iteration kernels ------------------------------------------------
 
 template <bool HALPERN>
-__global__ void __launch_bounds__(kBlock) k_primal(int32_t n, int32_t k, CsrView AT, const double* __restrict__ y,
+static __global__ void __launch_bounds__(kBlock) k_primal(int32_t n, int32_t k, CsrView AT, const double* __restrict__ y,
                                                    const double* __restrict__ c, const double* __restrict__ lo,
                                                    const double* __restrict__ up, double* __restrict__ x,
                                                    double* __restrict__ xp, const double* __restrict__ x0,
@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(kBlock) k_primal(int32_t n, int32_t k, CsrView
 }
 
 template <bool HALPERN>
-__global__ void __launch_bounds__(kBlock) k_dual(int32_t m, int32_t k, CsrView A, const double* __restrict__ xp,
+static __global__ void __launch_bounds__(kBlock) k_dual(int32_t m, int32_t k, CsrView A, const double* __restrict__ xp,
                                                  const double* __restrict__ rl, const double* __restrict__ ru,
                                                  double* __restrict__ y, double* __restrict__ yp,
                                                  const double* __restrict__ y0, double* __restrict__ ax,
@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(kBlock) k_dual(int32_t m, int32_t k, CsrView A
 }
 
 // Halpern steps of x, y and Ax at a check iteration (after the reductions).
-__global__ void __launch_bounds__(kBlock) k_halpern_all(int32_t n, int32_t m, int32_t k, double* __restrict__ x,
+static __global__ void __launch_bounds__(kBlock) k_halpern_all(int32_t n, int32_t m, int32_t k, double* __restrict__ x,
                                                         const double* __restrict__ xp, const double* __restrict__ x0,
                                                         double* __restrict__ y, const double* __restrict__ yp,
                                                         const double* __restrict__ y0, double* __restrict__ ax,
@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(kBlock) k_halpern_all(int32_t n, int32_t m, in
 // Masked restart z = z0 = z+ for x, y, Ax and iteration counter reset
 // (src/pdhg/pdhg.cpp:153-165).  Runs after the interval's clock advanced, so
 // the next iteration (index *it_base) has counter 0.
-__global__ void __launch_bounds__(kBlock) k_restart(int32_t n, int32_t m, int32_t k, const int32_t* __restrict__ mask,
+static __global__ void __launch_bounds__(kBlock) k_restart(int32_t n, int32_t m, int32_t k, const int32_t* __restrict__ mask,
                                                     double* __restrict__ x, double* __restrict__ x0,
                                                     const double* __restrict__ xp, double* __restrict__ y,
                                                     double* __restrict__ y0, const double* __restrict__ yp,
@@ -221,7 +221,7 @@ __device__ __forceinline__ void block_reduce(double (&s)[NQ], double* sh /* [NQ]
 
 // Row part of the check at (x+, y+): kkt_rows (src/pdhg/pdhg.cpp:166-180) +
 // diff2(Y, YP) + diff2(YP, Y0).  grid = (G, k); partial[(b*G + g)*5 + q].
-__global__ void __launch_bounds__(kBlock) k_check_rows(int32_t m, int32_t k, const double* __restrict__ axp,
+static __global__ void __launch_bounds__(kBlock) k_check_rows(int32_t m, int32_t k, const double* __restrict__ axp,
                                                        const double* __restrict__ rl, const double* __restrict__ ru,
                                                        const double* __restrict__ yp, const double* __restrict__ y,
                                                        const double* __restrict__ y0,
@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(kBlock) k_check_rows(int32_t m, int32_t k, con
 // (src/pdhg/pdhg.cpp:181-196) + diff2(X, XP) + diff2(XP, X0).
 // `atyp` (k = 1 only) is A^T y+ computed by the binned SpMV; when NULL the
 // row sums are computed here.
-__global__ void __launch_bounds__(kBlock) k_check_cols(int32_t n, int32_t k, CsrView AT, const double* __restrict__ yp,
+static __global__ void __launch_bounds__(kBlock) k_check_cols(int32_t n, int32_t k, CsrView AT, const double* __restrict__ yp,
                                                        const double* __restrict__ atyp_in,
                                                        const double* __restrict__ xp, const double* __restrict__ x,
                                                        const double* __restrict__ x0, const double* __restrict__ c,
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(kBlock) k_check_cols(int32_t n, int32_t k, Csr
 
 // Sums the block partials of case b (grid = k) into out[b*10 + CheckSum] and
 // advances the interval clock by L iterations.
-__global__ void __launch_bounds__(kBlock) k_check_finalize(int32_t k, int32_t g_rows, int32_t g_cols,
+static __global__ void __launch_bounds__(kBlock) k_check_finalize(int32_t k, int32_t g_rows, int32_t g_cols,
                                                            const double* __restrict__ prow,
                                                            const double* __restrict__ pcol, double* __restrict__ out,
                                                            int64_t* __restrict__ it_base, int32_t L) {
@@ -332,7 +332,7 @@ __global__ void __launch_bounds__(kBlock) k_check_finalize(int32_t k, int32_t g_
 }
 
 // Plain k-interleaved CSR SpMV y = M x (CpuBackend::mult order).
-__global__ void __launch_bounds__(kBlock) k_spmv(int32_t rows, int32_t k, CsrView M, const double* __restrict__ x,
+static __global__ void __launch_bounds__(kBlock) k_spmv(int32_t rows, int32_t k, CsrView M, const double* __restrict__ x,
                                                  double* __restrict__ y) {
   const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= static_cast<int64_t>(rows) * k) return;

@@ -310,8 +310,27 @@ def csr_spmv(ptr, idx, val, x, rows: int, cols: int, k: int = 1) -> np.ndarray:
     return y
 
 
+def kktResidual(lp: Model, x, rowDual, cases: list[LpCase] | None = None) -> np.ndarray:
+    """Relative KKT error (relP, relD, gap, max) of points (x, rowDual) in the
+    original space, evaluated on the GPU; one row per case."""
+    lib = _lib.load()
+    s, keep = _lp_struct(lp)
+    k = len(cases) if cases else 1
+    arr, keep2 = (_cases_struct(cases, lp.num_cols, lp.num_rows) if cases else (None, []))
+    x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+    y = np.ascontiguousarray(rowDual, dtype=np.float64).reshape(-1)
+    if len(x) != k * lp.num_cols or len(y) != k * lp.num_rows:
+        raise ValueError("x / rowDual have the wrong length")
+    out = np.zeros(4 * k)
+    _lib.check(lib.b2p_kkt_residual(C.byref(s), arr, len(cases) if cases else 0, x.ctypes.data_as(_lib.dptr),
+                                    y.ctypes.data_as(_lib.dptr), out.ctypes.data_as(_lib.dptr)))
+    del keep, keep2
+    return out.reshape(k, 4)
+
+
 # snake_case aliases
 solve_pdhg = solvePdhg
 solve_pdhg_batch = solvePdhgBatch
 gpu_available = gpuAvailable
 gpu_info_json = gpuInfoJson
+kkt_residual = kktResidual

@@ -272,3 +272,31 @@ def test_c2_full_size_properties(oracle_mod, mode):
     lb = oracle_mod.safe_dual_bound(lp, g.rowDual)
     assert lb <= g.objective + 1e-9 * abs(g.objective)
     assert abs(g.objective - lb) <= 1e-4 * (1 + abs(g.objective))
+
+
+@pytest.mark.parametrize("which", ["c1", "edge", "batch"])
+def test_kkt_residual_matches_host(which):
+    """b2p_kkt_residual against the same KKT formula evaluated on the host."""
+    if which == "batch":
+        lp = G.random_lp(150, 300, 4.0, 90, 13)
+        cases = lp_cases.mixed_cases(lp, 5)
+        rs = pdhg.solvePdhgBatch(lp, cases, opts(tolerance=1e-5))
+        x = np.concatenate([r.x for r in rs])
+        y = np.concatenate([r.rowDual for r in rs])
+        got = pdhg.kktResidual(lp, x, y, cases)
+        for b, cs in enumerate(cases):
+            one = Model(**{**lp.__dict__, **{f: getattr(cs, f) for f in ("row_lower", "row_upper", "col_lower",
+                                                                          "col_upper") if getattr(cs, f) is not None},
+                           "col_cost": cs.cost if cs.cost is not None else lp.col_cost})
+            want = _host_kkt(one, rs[b].x, rs[b].rowDual)
+            assert np.allclose(got[b, :3], want, rtol=1e-9, atol=1e-15)
+            assert abs(got[b, 3] - rs[b].relativeKkt) <= 1e-9 * max(1e-12, rs[b].relativeKkt) + 1e-15
+        return
+    lp = G.config1(1) if which == "c1" else lp_cases.edge_lp(6)
+    r = pdhg.solvePdhg(lp, opts(tolerance=1e-6))
+    got = pdhg.kktResidual(lp, r.x, r.rowDual)[0]
+    want = _host_kkt(lp, r.x, r.rowDual)
+    assert np.allclose(got[:3], want, rtol=1e-9, atol=1e-15)
+    assert got[3] == max(got[:3])
+    # the engine's own KKT at termination is the same quantity
+    assert abs(got[3] - r.relativeKkt) <= 1e-9 * r.relativeKkt + 1e-15
