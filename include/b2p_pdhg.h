@@ -214,6 +214,34 @@ int b2p_engine_kernel_bytes(b2p_engine* e, int32_t kernel_class, double* bytes);
 int b2p_kkt_residual(const b2p_lp* lp, const b2p_case* cases, int32_t num_cases, const double* x,
                      const double* row_dual, double* out);
 
+/* Allocation-free form of b2p_kkt_residual.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory (a host
+ * framework that owns all device memory through its own pool, code inside a
+ * stream-capture region, or a path where allocation is forbidden): every
+ * array is a caller-owned DEVICE pointer, and the call itself allocates
+ * nothing.  Inputs: A as CSR (a_ptr[num_rows+1], a_idx, a_val) and as CSC read
+ * as the CSR of A^T (at_ptr[num_cols+1], at_idx, at_val), and per point b
+ * (case-major) cost, col_lower, col_upper (num_points x num_cols), row_lower,
+ * row_upper (num_points x num_rows), x and row_dual.  Output: out[4b..4b+3]
+ * as in b2p_kkt_residual, written on `stream` (a cudaStream_t; NULL = the
+ * legacy default stream) -- the call only enqueues; synchronize the stream
+ * before reading out.
+ * Scratch: the reductions' block partials live in one file-scope device array
+ * of 458,752 bytes, which every GPU that loads this library holds until the
+ * process exits.  num_points above 32 is rejected with B2P_ERR_TOO_LARGE.
+ * Every call shares that array and it keeps the last call's contents (the
+ * kernels write every partial before reading it, so nothing has to start at
+ * zero); calls that overlap on the GPU -- on different streams or from
+ * different threads without ordering -- race on it.  The first call on a
+ * device looks the array's device address up (cudaGetSymbolAddress, once per
+ * device, with that device current); make that first call before any stream
+ * capture. */
+int b2p_kkt_residual_noalloc(int32_t num_rows, int32_t num_cols, int32_t num_points, const int32_t* a_ptr,
+                             const int32_t* a_idx, const double* a_val, const int32_t* at_ptr, const int32_t* at_idx,
+                             const double* at_val, const double* cost, const double* col_lower,
+                             const double* col_upper, const double* row_lower, const double* row_upper,
+                             const double* x, const double* row_dual, double* out, void* stream);
+
 /* ---- Kernel-level entry -------------------------------------------------
  * y(i,b) = sum_p val[p] * x(idx[p], b) for a CSR matrix (rows x cols) and k
  * interleaved right-hand sides (element (i,b) at i*k+b), summed left to right

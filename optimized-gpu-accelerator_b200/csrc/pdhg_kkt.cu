@@ -18,6 +18,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "pdhg_host_common.h"
@@ -253,5 +255,93 @@ extern "C" int b2p_kkt_residual(const b2p_lp* lp, const b2p_case* cases, int32_t
     enqueue_kkt(s, m, n, k, A, AT, dx, dy, dc, dlo, dup, drl, dru, prow, pcol, dout);
     B2P_CUDA(cudaMemcpyAsync(out, dout, sizeof(double) * 4 * k, cudaMemcpyDeviceToHost, s));
     B2P_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the KKT evaluation.
+//
+// Some callers cannot allocate device memory: code running inside another
+// framework's memory manager (a solver host that owns every device byte
+// through its own pool), inside a stream-capture region where cudaMalloc is
+// not allowed, or under a hard no-allocation rule on a latency-critical
+// path.  For them b2p_kkt_residual_noalloc takes every input and output as a
+// caller-owned device pointer and keeps its only scratch -- the per-block
+// partial sums of the reductions -- in the file-scope array below, which
+// every GPU that loads this library holds until the process exits.
+// ---------------------------------------------------------------------------
+namespace b2p {
+
+constexpr int kNoAllocMaxPoints = 32;  // points per call
+constexpr size_t kNoAllocScratchDoubles =
+    static_cast<size_t>(kNoAllocMaxPoints) * kKktMaxBlocks * (kKktRowSums + kKktColSums);  // 458,752 bytes
+
+static __device__ __align__(256) double g_kkt_noalloc_scratch[kNoAllocScratchDoubles];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_scratch[64] = {};  // device address of the array, per device ordinal
+
+// Device address of the scratch array on the current device.  The name of a
+// __device__ array in host code is only a host-side stand-in, so the address
+// is looked up once per device, with that device current.
+double* noalloc_scratch_on_current_device() {
+  int dev = 0;
+  B2P_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw Error(B2P_ERR_INVALID, "device ordinal beyond 63");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_scratch[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_kkt_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      throw Error(B2P_ERR_CUDA, std::string("cudaGetSymbolAddress of the scratch array failed: ") +
+                                    cudaGetErrorString(e));
+    g_noalloc_scratch[dev] = static_cast<double*>(p);
+  }
+  return g_noalloc_scratch[dev];
+}
+
+void require_device_pointer(const void* p, const char* what) {
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(B2P_ERR_INVALID, std::string(what) + " is not a device pointer");
+  }
+  if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)
+    throw Error(B2P_ERR_INVALID, std::string(what) + " is not a device pointer");
+}
+
+}  // namespace
+}  // namespace b2p
+
+extern "C" int b2p_kkt_residual_noalloc(int32_t num_rows, int32_t num_cols, int32_t num_points,
+                                        const int32_t* a_ptr, const int32_t* a_idx, const double* a_val,
+                                        const int32_t* at_ptr, const int32_t* at_idx, const double* at_val,
+                                        const double* cost, const double* col_lower, const double* col_upper,
+                                        const double* row_lower, const double* row_upper, const double* x,
+                                        const double* row_dual, double* out, void* stream) {
+  using namespace b2p;
+  return guarded([&] {
+    if (num_rows < 0 || num_cols < 0) throw Error(B2P_ERR_INVALID, "negative dimension");
+    if (num_points < 1) throw Error(B2P_ERR_INVALID, "num_points must be at least 1");
+    if (num_points > kNoAllocMaxPoints)
+      throw Error(B2P_ERR_TOO_LARGE, "num_points " + std::to_string(num_points) + " exceeds the maximum of " +
+                                         std::to_string(kNoAllocMaxPoints) + " points per call");
+    if (!a_ptr || !at_ptr || !out || (num_cols > 0 && (!cost || !col_lower || !col_upper || !x)) ||
+        (num_rows > 0 && (!row_lower || !row_upper || !row_dual)))
+      throw Error(B2P_ERR_INVALID, "NULL argument");
+    require_device_pointer(out, "out");
+    require_device_pointer(a_ptr, "a_ptr");
+    require_device_pointer(at_ptr, "at_ptr");
+    if (num_cols > 0) require_device_pointer(x, "x");
+    if (num_rows > 0) require_device_pointer(row_dual, "row_dual");
+    double* scratch = noalloc_scratch_on_current_device();
+    double* prow = scratch;
+    double* pcol = scratch + static_cast<size_t>(kNoAllocMaxPoints) * kKktMaxBlocks * kKktRowSums;
+    const CsrView A{a_ptr, a_idx, a_val, num_rows};
+    const CsrView AT{at_ptr, at_idx, at_val, num_cols};
+    enqueue_kkt(static_cast<cudaStream_t>(stream), num_rows, num_cols, num_points, A, AT, x, row_dual, cost,
+                col_lower, col_upper, row_lower, row_upper, prow, pcol, out);
   });
 }

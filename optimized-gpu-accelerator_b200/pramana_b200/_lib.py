@@ -83,6 +83,10 @@ SIGNATURES = {
     "b2p_engine_kernel_bytes": (C.c_int, [C.c_void_p, C.c_int32, dptr]),
     "b2p_csr_spmv": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, iptr, iptr, dptr, dptr, dptr]),
     "b2p_kkt_residual": (C.c_int, [C.POINTER(B2pLp), C.POINTER(B2pCase), C.c_int32, dptr, dptr, dptr]),
+    "b2p_kkt_residual_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p]),
 }
 
 _lock = threading.Lock()
