@@ -118,12 +118,13 @@ def measured_peak():
 
 
 def ncu_traffic(kernel: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    """DRAM bytes (read + write) per unit of work of `kernel` -- the unit the
+    roofline uses -- from the committed ncu summary, if any."""
     p = os.path.join(ROOT, "profiles", f"{kernel}_c2_traffic.txt")
     try:
         with open(p) as f:
             for ln in f:
-                if ln.startswith("dram_bytes_per_launch:"):
+                if ln.startswith("dram_bytes_per_unit:"):
                     return float(ln.split(":", 1)[1])
     except OSError:
         pass
