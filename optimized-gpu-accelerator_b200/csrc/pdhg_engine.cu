@@ -284,6 +284,7 @@ struct Engine {
     po.ruiz_iterations = opt.ruiz_iterations;
     po.pock_chambolle = opt.pock_chambolle != 0;
     po.rescale = opt.rescale_objective_and_bounds != 0;
+    po.norm_on_host = false;  // estimated on the device below, bit-identically
     P = prepare(m, n, lp->start, lp->index, lp->value, lp->col_cost, lp->row_lower, lp->row_upper, lp->obj_offset,
                 po);
     stats.prepare_seconds = seconds_since(t0);
@@ -328,7 +329,6 @@ struct Engine {
       }
       if (cn > 1e-20 && bn > 1e-20) omega0[b] = std::sqrt(cn) / std::sqrt(bn);
     }
-    eta = 0.998 / P.normA;
 
     // ---- device state (GpuBackend::init, src/pdhg/pdhg.cpp:238-277) ----
     const auto tx = Clock::now();
@@ -338,6 +338,10 @@ struct Engine {
     dT_ptr = upload(P.AT.ptr);
     dT_idx = upload(P.AT.idx);
     dT_val = upload(P.AT.val);
+    const auto tn = Clock::now();
+    P.normA = device_power_iteration(40) * 1.01;
+    stats.prepare_seconds += seconds_since(tn);
+    eta = 0.998 / P.normA;
     d_rfac = upload(P.rfac);
     d_cfac = upload(P.cfac);
     if (k == 1) {
@@ -391,6 +395,43 @@ struct Engine {
     stats.upload_seconds = transfer_seconds;
     stats.setup_seconds = seconds_since(t0);
     stats.spectral_norm = P.normA;
+  }
+
+  // ||A||_2 estimate of powerIteration (src/pdhg/pdhg.cpp:404-422) with the
+  // products on the device: A x and A^T y by CSR row sums in increasing column
+  // order, which is exactly the addition order of SparseMatrix::multiply /
+  // multiplyTranspose (src/core/sparse.cpp:67-82); the norm of z is summed on
+  // the host in index order.  The result is bit-identical to the reference's.
+  double device_power_iteration(int iters) {
+    if (P.A.val.empty() || n == 0 || m == 0) return 1.0;
+    double* dx = dalloc<double>(n);
+    double* dy = dalloc<double>(m);
+    double* dz = dalloc<double>(n);
+    std::vector<double> hx(n, 1.0 / std::sqrt(static_cast<double>(n > 1 ? n : 1)));
+    B2P_CUDA(cudaMemcpyAsync(dx, hx.data(), sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+    double* hz = nullptr;
+    B2P_CUDA(cudaMallocHost(&hz, sizeof(double) * n));
+    struct PinnedGuard {
+      double* p;
+      ~PinnedGuard() { cudaFreeHost(p); }
+    } guard{hz};
+    double s = 1;
+    for (int it = 0; it < iters; ++it) {
+      k_spmv<<<blocks(m), kBlock, 0, stream>>>(m, 1, viewA(), dx, dy);
+      k_spmv<<<blocks(n), kBlock, 0, stream>>>(n, 1, viewAT(), dy, dz);
+      B2P_CUDA(cudaGetLastError());
+      B2P_CUDA(cudaMemcpyAsync(hz, dz, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+      B2P_CUDA(cudaStreamSynchronize(stream));
+      double nz = 0;
+      for (int j = 0; j < n; ++j) nz += hz[j] * hz[j];
+      nz = std::sqrt(nz);
+      if (nz == 0) return 1.0;
+      s = std::sqrt(nz);
+      k_div_scalar<<<blocks(n), kBlock, 0, stream>>>(n, dz, nz, dx);
+      B2P_CUDA(cudaGetLastError());
+    }
+    B2P_CUDA(cudaStreamSynchronize(stream));
+    return s;
   }
 
   // Resident form if the LP's slices fit in shared memory, one block per SM.

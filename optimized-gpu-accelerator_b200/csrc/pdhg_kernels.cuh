@@ -331,6 +331,13 @@ static __global__ void __launch_bounds__(kBlock) k_check_finalize(int32_t k, int
   }
 }
 
+// x = z / nz (one power-iteration normalisation step, src/pdhg/pdhg.cpp:419).
+static __global__ void __launch_bounds__(kBlock) k_div_scalar(int32_t len, const double* __restrict__ z, double nz,
+                                                             double* __restrict__ x) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t < len) x[t] = __ddiv_rn(z[t], nz);
+}
+
 // Plain k-interleaved CSR SpMV y = M x (CpuBackend::mult order).
 static __global__ void __launch_bounds__(kBlock) k_spmv(int32_t rows, int32_t k, CsrView M, const double* __restrict__ x,
                                                  double* __restrict__ y) {

@@ -158,7 +158,7 @@ Prepared prepare(int32_t m, int32_t n, const int32_t* start, const int32_t* inde
   P.cfac.resize(n);
   for (int32_t i = 0; i < m; ++i) P.rfac[i] = P.beta / P.R[i];
   for (int32_t j = 0; j < n; ++j) P.cfac[j] = P.gamma / P.Cs[j];
-  P.normA = power_iteration(m, n, start, index, sval.data(), 40) * 1.01;
+  if (opt.norm_on_host) P.normA = power_iteration(m, n, start, index, sval.data(), 40) * 1.01;
   return P;
 }
 

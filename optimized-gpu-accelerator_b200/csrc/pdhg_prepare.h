@@ -36,6 +36,7 @@ struct PrepareOptions {
   int ruiz_iterations = 10;
   bool pock_chambolle = true;
   bool rescale = true;
+  bool norm_on_host = true;  // false: normA is left 0 for the caller to estimate (on the device)
 };
 
 // A given in CSC (start/index/value) with m rows and n columns.

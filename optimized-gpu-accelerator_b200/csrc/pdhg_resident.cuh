@@ -102,8 +102,13 @@ __device__ __forceinline__ double res_tree(double s) {
 // Sum of entries p = p0, p0+S, ... < end of a shared-memory CSR slice, left
 // to right; the gathers of each round of kResUnroll entries are issued
 // together and the values are read from shared memory as they are consumed.
+// The gathered vector is written by other blocks between phases, so it is
+// read with ld.global.ca (L1-cacheable, not the read-only path): every phase
+// starts after the grid barrier's acquire, which the PTX memory model orders
+// before these loads through bar.sync, so a cached line can never be stale
+// across phases, and entries repeated within a phase hit in L1.
 __device__ __forceinline__ double res_lane_sum(const int32_t* s_idx, const double* s_val, int p0, int end, int S,
-                                               const double* __restrict__ xg) {
+                                               const double* xg) {
   double s = 0.0;
   bool first = true;
   for (int p = p0; p < end; p += kResUnroll * S) {
@@ -111,7 +116,7 @@ __device__ __forceinline__ double res_lane_sum(const int32_t* s_idx, const doubl
 #pragma unroll
     for (int u = 0; u < kResUnroll; ++u) {
       const int q = p + u * S;
-      xv[u] = q < end ? __ldcg(xg + s_idx[q]) : 0.0;
+      xv[u] = q < end ? __ldca(xg + s_idx[q]) : 0.0;
     }
 #pragma unroll
     for (int u = 0; u < kResUnroll; ++u) {
@@ -152,8 +157,7 @@ __device__ __forceinline__ int res_long_list(const int32_t* s_ptr, int nrows, in
 // the block must call.
 template <int G, class Epi>
 __device__ __forceinline__ void res_rows(const int32_t* s_ptr, const int32_t* s_idx, const double* s_val, int nrows,
-                                         int lt, const int32_t* s_long, int nlong, const double* __restrict__ xg,
-                                         Epi&& epi) {
+                                         int lt, const int32_t* s_long, int nlong, const double* xg, Epi&& epi) {
   const int gid = threadIdx.x / G, gl = threadIdx.x & (G - 1);
   constexpr int kGroups = kResidentThreads / G;
   for (int base = 0; base < nrows; base += kGroups) {

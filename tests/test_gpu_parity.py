@@ -300,3 +300,12 @@ def test_kkt_residual_matches_host(which):
     assert got[3] == max(got[:3])
     # the engine's own KKT at termination is the same quantity
     assert abs(got[3] - r.relativeKkt) <= 1e-9 * r.relativeKkt + 1e-15
+
+
+@pytest.mark.parametrize("which", ["c1", "c2", "edge"])
+def test_spectral_norm_bitexact(oracle_mod, which):
+    """The ||A|| estimate (products on the device, norm on the host) is bit-identical to the reference's."""
+    lp = {"c1": lambda: G.config1(1), "c2": lambda: G.config2(2), "edge": lambda: lp_cases.edge_lp(5)}[which]()
+    g = pdhg.solvePdhg(lp, opts(tolerance=1e-30, maxIterations=1))
+    oracle_mod.solve(lp, "oracle", tolerance=1e-30, max_iterations=1)
+    assert g.stats.spectralNorm == oracle_mod.solve.last_stats["spectral_norm"]
