@@ -61,7 +61,15 @@ enum {
 
 /* Arithmetic of the iterates. */
 enum {
-  B2P_PRECISION_FP64 = 0 /* plain form: FP64 everywhere, iterate parity with the reference */
+  B2P_PRECISION_FP64 = 0, /* plain form: FP64 everywhere, iterate parity with the reference */
+  /* mixed form (single LP in the resident form): operator values, iterates
+   * and their updates in FP32 with FP64-accumulated row sums; check sums,
+   * termination, restarts and primal weight in FP64.  A point that meets the
+   * tolerance in FP32 is re-measured in FP64 before it is returned; when that
+   * fails, or the FP32 run stalls, the solve continues in FP64 from the FP32
+   * point (the FP64 polish).  Batches and LPs too large for the resident form
+   * run in FP64. */
+  B2P_PRECISION_MIXED = 1
 };
 
 /* A minimisation LP  min c'x + offset, L <= Ax <= U, l <= x <= u, with A in
@@ -140,6 +148,9 @@ typedef struct b2p_stats {
   int32_t kernel_mode;                        /* B2P_KERNELS_FUSED or B2P_KERNELS_RESIDENT (batches: FUSED) */
   int32_t resident_blocks;                    /* cooperative grid size in resident form */
   int64_t resident_smem_bytes;                /* largest block's shared memory in resident form */
+  int32_t precision_used;                     /* B2P_PRECISION_* actually run */
+  int32_t pad1;
+  int64_t fp32_iterations;                    /* mixed form: iterations run in FP32 */
 } b2p_stats;
 
 /* Replaces pramana::PdhgResult (src/pdhg/pdhg.h:58-65) minus the vectors,

@@ -117,24 +117,26 @@ void launch(void (*kern)(KArgs...), unsigned grid, cudaStream_t stream, bool pdl
     default: F(32); break;                           \
   }
 
-using ResidentFn = void (*)(ResidentArgs);
+template <class T>
+using ResidentFn = void (*)(ResidentArgs<T>);
 
-template <int GC>
-ResidentFn resident_fn_rows(int gr) {
+template <class T, int GC>
+ResidentFn<T> resident_fn_rows(int gr) {
   switch (gr) {
-    case 1: return k_resident<GC, 1>;
-    case 2: return k_resident<GC, 2>;
-    case 4: return k_resident<GC, 4>;
-    default: return k_resident<GC, 8>;
+    case 1: return k_resident<GC, 1, T>;
+    case 2: return k_resident<GC, 2, T>;
+    case 4: return k_resident<GC, 4, T>;
+    default: return k_resident<GC, 8, T>;
   }
 }
 
-ResidentFn resident_fn(int gc, int gr) {
+template <class T>
+ResidentFn<T> resident_fn(int gc, int gr) {
   switch (gc) {
-    case 1: return resident_fn_rows<1>(gr);
-    case 2: return resident_fn_rows<2>(gr);
-    case 4: return resident_fn_rows<4>(gr);
-    default: return resident_fn_rows<8>(gr);
+    case 1: return resident_fn_rows<T, 1>(gr);
+    case 2: return resident_fn_rows<T, 2>(gr);
+    case 4: return resident_fn_rows<T, 4>(gr);
+    default: return resident_fn_rows<T, 8>(gr);
   }
 }
 
@@ -204,7 +206,15 @@ struct Engine {
   unsigned* d_sync = nullptr;  // arrive, generation, error flag
   double* d_rpartial = nullptr;
   int32_t* h_error = nullptr;
-  ResidentFn res_fn = nullptr;
+  ResidentFn<double> res_fn = nullptr;
+  // mixed form: FP32 operator values and iterates for the resident kernel
+  bool mixed = false;    // precision MIXED requested and the FP32 resident form fits
+  bool phase32 = false;  // the current interval runs in FP32
+  size_t res_smem32 = 0;
+  ResidentFn<float> res_fn32 = nullptr;
+  float *a_val32 = nullptr, *t_val32 = nullptr;
+  enum Slot32 : int { X32, XP32, X032, Y32, YP32, Y032, AX32, AX032, AXP32, C32, LO32, UP32, RL32, RU32, NSLOT32 };
+  float* v32[NSLOT32] = {};
 
   // ---- pinned host ----
   double* h_sums = nullptr;   // k * kNumSums
@@ -268,7 +278,8 @@ struct Engine {
     check_lp(lp);
     if (o) opt = *o; else b2p_default_options(&opt);
     if (opt.check_every <= 0) throw Error(B2P_ERR_INVALID, "check_every must be positive");
-    if (opt.precision != B2P_PRECISION_FP64) throw Error(B2P_ERR_INVALID, "unsupported precision");
+    if (opt.precision != B2P_PRECISION_FP64 && opt.precision != B2P_PRECISION_MIXED)
+      throw Error(B2P_ERR_INVALID, "unsupported precision");
     device = pick_device(opt.device);
     B2P_CUDA(cudaSetDevice(device));
     B2P_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
@@ -359,7 +370,8 @@ struct Engine {
       setup_resident(sms);
       stats.graph_seconds += seconds_since(tk);
     }
-    stats.kernel_mode = resident ? B2P_KERNELS_RESIDENT : B2P_KERNELS_FUSED;
+    stats.kernel_mode = (resident || mixed) ? B2P_KERNELS_RESIDENT : B2P_KERNELS_FUSED;
+    stats.precision_used = mixed ? B2P_PRECISION_MIXED : B2P_PRECISION_FP64;
     for (int s = 0; s < NSLOT; ++s) v[s] = dalloc<double>(row_slot(s) ? mk : nk);
     auto put = [&](int s, const std::vector<double>& h) {
       if (!h.empty())
@@ -385,6 +397,7 @@ struct Engine {
     B2P_CUDA(cudaMallocHost(&h_sums, sizeof(double) * k * kNumSums));
     B2P_CUDA(cudaMallocHost(&h_steps, sizeof(double) * 2 * k));
     B2P_CUDA(cudaMallocHost(&h_mask, sizeof(int32_t) * k));
+    if (mixed) setup_mixed();
     // AX = A x0 on the device (pdhg.cpp:540-545), kept as the restart point of every solve.
     if (m > 0) {
       k_spmv<<<blocks(static_cast<int64_t>(m) * k), kBlock, 0, stream>>>(m, k, viewA(), v[XINIT], v[AXINIT]);
@@ -434,69 +447,102 @@ struct Engine {
     return s;
   }
 
-  // Resident form if the LP's slices fit in shared memory, one block per SM.
+  // Resident form if the LP's slices fit in shared memory, one block per SM
+  // (FP64 for the plain form; FP32 too when the mixed form is requested).
   void setup_resident(int sms) {
     if (opt.kernel_mode == B2P_KERNELS_FUSED || n == 0 || m == 0) return;
     int optin = 0;
     B2P_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
     const int nb = sms;
     std::vector<int32_t> cb = balanced_split(P.AT, nb), rb = balanced_split(P.A, nb);
-    size_t need = 0;
+    size_t need64 = 0, need32 = 0;
     for (int b = 0; b < nb; ++b) {
       const int nc = cb[b + 1] - cb[b], nr = rb[b + 1] - rb[b];
       const int tn = P.AT.ptr[cb[b + 1]] - P.AT.ptr[cb[b]], an = P.A.ptr[rb[b + 1]] - P.A.ptr[rb[b]];
-      need = std::max(need, resident_smem_bytes(nc, nr, tn, an));
+      need64 = std::max(need64, resident_smem_bytes<double>(nc, nr, tn, an));
+      need32 = std::max(need32, resident_smem_bytes<float>(nc, nr, tn, an));
     }
     const size_t reserve = 1024;  // static shared memory of the kernel
-    if (need + reserve > static_cast<size_t>(optin)) {
-      if (opt.kernel_mode == B2P_KERNELS_RESIDENT)
-        throw Error(B2P_ERR_TOO_LARGE, "LP does not fit the resident form (shared memory)");
-      return;
-    }
     res_gc = resident_lanes(P.AT, cb);
     res_gr = resident_lanes(P.A, rb);
-    res_fn = resident_fn(res_gc, res_gr);
-    B2P_CUDA(cudaFuncSetAttribute(res_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(need)));
-    int per_sm = 0;
-    B2P_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, res_fn, kResidentThreads, need));
-    if (per_sm < 1) {
-      if (opt.kernel_mode == B2P_KERNELS_RESIDENT)
-        throw Error(B2P_ERR_TOO_LARGE, "resident kernel cannot be resident on an SM");
-      return;
+    bool ok64 = need64 + reserve <= static_cast<size_t>(optin);
+    bool ok32 = opt.precision == B2P_PRECISION_MIXED && need32 + reserve <= static_cast<size_t>(optin);
+    if (ok64) {
+      res_fn = resident_fn<double>(res_gc, res_gr);
+      B2P_CUDA(cudaFuncSetAttribute(res_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(need64)));
+      int per_sm = 0;
+      B2P_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, res_fn, kResidentThreads, need64));
+      ok64 = per_sm >= 1;
     }
+    if (ok32) {
+      res_fn32 = resident_fn<float>(res_gc, res_gr);
+      B2P_CUDA(cudaFuncSetAttribute(res_fn32, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(need32)));
+      int per_sm = 0;
+      B2P_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, res_fn32, kResidentThreads, need32));
+      ok32 = per_sm >= 1;
+    }
+    if (!ok64 && opt.kernel_mode == B2P_KERNELS_RESIDENT && !ok32)
+      throw Error(B2P_ERR_TOO_LARGE, "LP does not fit the resident form (shared memory)");
+    if (!ok64 && !ok32) return;
     d_cb = upload(cb);
     d_rb = upload(rb);
     d_sync = dalloc<unsigned>(4);
     d_rpartial = dalloc<double>(static_cast<size_t>(nb) * kNumSums);
     B2P_CUDA(cudaMallocHost(&h_error, sizeof(int32_t)));
     res_blocks = nb;
-    res_smem = need;
-    resident = true;
+    res_smem = ok64 ? need64 : 0;
+    res_smem32 = ok32 ? need32 : 0;
+    resident = ok64;
+    mixed = ok32;
     stats.resident_blocks = nb;
-    stats.resident_smem_bytes = static_cast<int64_t>(need);
+    stats.resident_smem_bytes = static_cast<int64_t>(ok64 ? need64 : need32);
   }
 
-  void launch_resident(int L) {
+  // FP32 copies of the operators and case vectors for the mixed form.
+  void setup_mixed() {
+    std::vector<float> av(P.A.val.begin(), P.A.val.end()), tv(P.AT.val.begin(), P.AT.val.end());
+    a_val32 = upload(av);
+    t_val32 = upload(tv);
+    for (int q = 0; q < NSLOT32; ++q) v32[q] = dalloc<float>(q >= Y32 && q != C32 && q != LO32 && q != UP32 ? m : n);
+    const int src[5] = {C, LO, UP, RL, RU}, dst[5] = {C32, LO32, UP32, RL32, RU32};
+    for (int q = 0; q < 5; ++q) {
+      const int64_t len = row_slot(src[q]) ? m : n;
+      if (len) k_convert<double, float><<<blocks(len), kBlock, 0, stream>>>(len, v[src[q]], v32[dst[q]]);
+    }
+    B2P_CUDA(cudaGetLastError());
+  }
+
+  template <class T>
+  void launch_resident(int L, ResidentFn<T> fn, size_t smem, const T* a_val, const T* t_val, T* const* vs) {
     B2P_CUDA(cudaMemsetAsync(d_sync, 0, 4 * sizeof(unsigned), stream));
-    ResidentArgs ra{};
+    ResidentArgs<T> ra{};
     ra.cb = d_cb;
     ra.rb = d_rb;
-    ra.A = viewA();
-    ra.AT = viewAT();
-    ra.x = v[X];
-    ra.x0 = v[X0];
-    ra.xp = v[XP];
-    ra.y = v[Y];
-    ra.y0 = v[Y0];
-    ra.yp = v[YP];
-    ra.ax = v[AX];
-    ra.ax0 = v[AX0];
-    ra.axp = v[AXP];
-    ra.c = v[C];
-    ra.lo = v[LO];
-    ra.up = v[UP];
-    ra.rl = v[RL];
-    ra.ru = v[RU];
+    ra.a_ptr = dA_ptr;
+    ra.a_idx = dA_idx;
+    ra.a_val = a_val;
+    ra.t_ptr = dT_ptr;
+    ra.t_idx = dT_idx;
+    ra.t_val = t_val;
+    ra.x = vs[0];
+    ra.xp = vs[1];
+    ra.x0 = vs[2];
+    ra.y = vs[3];
+    ra.yp = vs[4];
+    ra.y0 = vs[5];
+    ra.ax = vs[6];
+    ra.ax0 = vs[7];
+    ra.axp = vs[8];
+    ra.c = vs[9];
+    ra.lo = vs[10];
+    ra.up = vs[11];
+    ra.rl = vs[12];
+    ra.ru = vs[13];
+    ra.c64 = v[C];
+    ra.lo64 = v[LO];
+    ra.up64 = v[UP];
+    ra.rl64 = v[RL];
+    ra.ru64 = v[RU];
     ra.rfac = d_rfac;
     ra.cfac = d_cfac;
     ra.tau = d_tau;
@@ -516,11 +562,77 @@ struct Engine {
     ra.it_base = d_it_base;
     void* args[] = {&ra};
     if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[0], stream));
-    B2P_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(res_fn), dim3(res_blocks), dim3(kResidentThreads),
-                                         args, res_smem, stream));
+    B2P_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(fn), dim3(res_blocks), dim3(kResidentThreads), args,
+                                         smem, stream));
     if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[1], stream));
     B2P_CUDA(cudaMemcpyAsync(h_sums, d_sums, sizeof(double) * kNumSums, cudaMemcpyDeviceToHost, stream));
     B2P_CUDA(cudaMemcpyAsync(h_error, ra.error, sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+  }
+
+  void launch_resident64(int L) {
+    double* const vs[14] = {v[X], v[XP], v[X0], v[Y], v[YP], v[Y0], v[AX], v[AX0], v[AXP],
+                            v[C], v[LO], v[UP], v[RL], v[RU]};
+    launch_resident<double>(L, res_fn, res_smem, dA_val, dT_val, vs);
+  }
+
+  void launch_resident32(int L) {
+    float* const vs[14] = {v32[X32], v32[XP32], v32[X032], v32[Y32], v32[YP32], v32[Y032], v32[AX32],
+                           v32[AX032], v32[AXP32], v32[C32], v32[LO32], v32[UP32], v32[RL32], v32[RU32]};
+    launch_resident<float>(L, res_fn32, res_smem32, a_val32, t_val32, vs);
+  }
+
+  // FP32 state from the FP64 state (start of the mixed form's FP32 phase).
+  void state_to_fp32() {
+    const int pairs[6][2] = {{X, X32}, {X0, X032}, {Y, Y32}, {Y0, Y032}, {AX, AX32}, {AX0, AX032}};
+    for (auto& pr : pairs) {
+      const int64_t len = row_slot(pr[0]) ? m : n;
+      if (len) k_convert<double, float><<<blocks(len), kBlock, 0, stream>>>(len, v[pr[0]], v32[pr[1]]);
+    }
+    B2P_CUDA(cudaGetLastError());
+  }
+
+  // x+, y+ of the FP32 phase in FP64, and A x+ recomputed in FP64.
+  void fp32_point_to_fp64() {
+    if (n) k_convert<float, double><<<blocks(n), kBlock, 0, stream>>>(n, v32[XP32], v[XP]);
+    if (m) k_convert<float, double><<<blocks(m), kBlock, 0, stream>>>(m, v32[YP32], v[YP]);
+    if (m) k_spmv<<<blocks(m), kBlock, 0, stream>>>(m, 1, viewA(), v[XP], v[AXP]);
+    B2P_CUDA(cudaGetLastError());
+    launches += 3;
+  }
+
+  // FP64 check sums of the FP64 point (XP, YP, AXP) into h_sums (the movement
+  // norms of this call are not meaningful).
+  void verify_fp64() {
+    if (n) k_spmv<<<blocks(n), kBlock, 0, stream>>>(n, 1, viewAT(), v[YP], v[ATYP]);
+    k_check_rows<<<dim3(g_rows, 1), kBlock, 0, stream>>>(m, 1, v[AXP], v[RL], v[RU], v[YP], v[Y], v[Y0], d_rfac,
+                                                         d_prow);
+    k_check_cols<<<dim3(g_cols, 1), kBlock, 0, stream>>>(n, 1, viewAT(), v[YP], v[ATYP], v[XP], v[X], v[X0], v[C],
+                                                         v[LO], v[UP], d_cfac, d_pcol);
+    k_check_finalize<<<1, kBlock, 0, stream>>>(1, g_rows, g_cols, d_prow, d_pcol, d_sums, d_it_base, 0);
+    B2P_CUDA(cudaGetLastError());
+    B2P_CUDA(cudaMemcpyAsync(h_sums, d_sums, sizeof(double) * kNumSums, cudaMemcpyDeviceToHost, stream));
+    B2P_CUDA(cudaStreamSynchronize(stream));
+    launches += 5;
+  }
+
+  // Continue in FP64 from the FP32 phase's x+, y+ as from a restart.
+  void switch_to_fp64() {
+    fp32_point_to_fp64();
+    const int64_t nn = n, mm = m;
+    if (nn) {
+      B2P_CUDA(cudaMemcpyAsync(v[X], v[XP], sizeof(double) * nn, cudaMemcpyDeviceToDevice, stream));
+      B2P_CUDA(cudaMemcpyAsync(v[X0], v[XP], sizeof(double) * nn, cudaMemcpyDeviceToDevice, stream));
+    }
+    if (mm) {
+      B2P_CUDA(cudaMemcpyAsync(v[Y], v[YP], sizeof(double) * mm, cudaMemcpyDeviceToDevice, stream));
+      B2P_CUDA(cudaMemcpyAsync(v[Y0], v[YP], sizeof(double) * mm, cudaMemcpyDeviceToDevice, stream));
+      B2P_CUDA(cudaMemcpyAsync(v[AX], v[AXP], sizeof(double) * mm, cudaMemcpyDeviceToDevice, stream));
+      B2P_CUDA(cudaMemcpyAsync(v[AX0], v[AXP], sizeof(double) * mm, cudaMemcpyDeviceToDevice, stream));
+    }
+    k_restart_clock<<<1, 32, 0, stream>>>(1, d_it_base, d_restart_at);
+    B2P_CUDA(cudaGetLastError());
+    ++launches;
+    phase32 = false;
   }
 
   RowBins device_bins(const HostCsr& M, int64_t wave, int g_override, int rounds) {
@@ -683,8 +795,11 @@ struct Engine {
 
   void run_interval(int L) {
     if (profiling) ensure_prof_events(L);
-    if (resident) {
-      launch_resident(L);
+    if (phase32 || resident) {
+      if (phase32)
+        launch_resident32(L);
+      else
+        launch_resident64(L);
       launches += 1;
       bytes_down += static_cast<int64_t>(sizeof(double) * kNumSums + sizeof(int32_t));
       return;
@@ -719,7 +834,7 @@ struct Engine {
 
   void collect_profile(int L) {
     if (!profiling) return;
-    if (resident) {
+    if (phase32 || resident) {
       float ms = 0;
       B2P_CUDA(cudaEventElapsedTime(&ms, prof_ev[0], prof_ev[1]));
       prof_ms[2] += ms;
@@ -763,6 +878,12 @@ struct Engine {
     prof_launches[0] = prof_launches[1] = prof_launches[2] = 0;
     prof_ms[0] = prof_ms[1] = prof_ms[2] = 0;
     reset_state(omega);
+    phase32 = mixed;
+    if (phase32) state_to_fp32();
+    stats.fp32_iterations = 0;
+    double best32 = INFINITY;  // mixed form: best FP32-phase KKT and checks since it improved
+    int stale32 = 0;
+    constexpr int kStallChecks = 20;
     results.assign(k, b2p_result{});
     x_out.assign(static_cast<size_t>(n) * k, 0.0);
     y_out.assign(static_cast<size_t>(m) * k, 0.0);
@@ -799,13 +920,63 @@ struct Engine {
       const int L = static_cast<int>(std::min<int64_t>(cE, opt.max_iterations - it));
       run_interval(L);
       B2P_CUDA(cudaStreamSynchronize(stream));
-      if (resident && *h_error)
+      if ((resident || phase32) && *h_error)
         throw Error(B2P_ERR_CUDA, "resident kernel: grid barrier timed out (kernel left the interval)");
       collect_profile(L);
+      if (phase32) stats.fp32_iterations += L;
       it += L - 1;  // index of the check iteration
       ++checks;
       bool anyRestart = false, fetched = false;
       for (int b = 0; b < k; ++b) h_mask[b] = 0;
+      if (phase32) {
+        // Mixed form (k == 1): an FP32 point that meets the tolerance is
+        // re-measured in FP64; failing that, or after kStallChecks checks
+        // without a 10% gain, the solve continues in FP64 from this point.
+        const double* s = h_sums;
+        const double pobj = s[CS_POBJ] * scaleObj, dobj = (s[CS_ROW_DOBJ] + s[CS_COL_DOBJ]) * scaleObj;
+        const double relP = std::sqrt(s[CS_ROW_RES2]) / (1.0 + rhsNorm[0]);
+        const double relD = std::sqrt(s[CS_COL_RES2]) / (1.0 + cNorm[0]);
+        const double gap = std::fabs(pobj - dobj) / (1.0 + std::fabs(pobj) + std::fabs(dobj));
+        const double kkt32 = smax(relP, smax(relD, gap));
+        bool to_fp64 = false;
+        if (relP <= opt.tolerance && relD <= opt.tolerance && gap <= opt.tolerance) {
+          fp32_point_to_fp64();
+          verify_fp64();
+          const double vpobj = h_sums[CS_POBJ] * scaleObj;
+          const double vdobj = (h_sums[CS_ROW_DOBJ] + h_sums[CS_COL_DOBJ]) * scaleObj;
+          const double vrelP = std::sqrt(h_sums[CS_ROW_RES2]) / (1.0 + rhsNorm[0]);
+          const double vrelD = std::sqrt(h_sums[CS_COL_RES2]) / (1.0 + cNorm[0]);
+          const double vgap = std::fabs(vpobj - vdobj) / (1.0 + std::fabs(vpobj) + std::fabs(vdobj));
+          stats.primal_residual = vrelP;
+          stats.dual_residual = vrelD;
+          stats.gap = vgap;
+          if (vrelP <= opt.tolerance && vrelD <= opt.tolerance && vgap <= opt.tolerance) {
+            download_iterates(xs, ys);
+            extract(0, B2P_STATUS_OPTIMAL, smax(vrelP, smax(vrelD, vgap)), vpobj, vdobj, it);
+            done[0] = 1;
+            remaining = 0;
+            break;
+          }
+          to_fp64 = true;
+        } else if (kkt32 < 0.9 * best32) {
+          best32 = kkt32;
+          stale32 = 0;
+        } else if (++stale32 >= kStallChecks) {
+          to_fp64 = true;
+        }
+        if (to_fp64) {
+          switch_to_fp64();
+          fpRestart[0] = fpPrev[0] = INFINITY;
+          sinceRestart[0] = 0;
+          stats.restarts++;
+          if (expired()) {
+            expiredStop = true;
+            break;
+          }
+          ++it;
+          continue;
+        }
+      }
       for (int b = 0; b < k; ++b) {
         if (done[b]) continue;
         const double* s = h_sums + static_cast<size_t>(b) * kNumSums;
@@ -825,7 +996,7 @@ struct Engine {
                        "  pdhg %8lld  pobj % .8e  dobj % .8e  relP %.2e  relD %.2e  gap %.2e  w %.2e  restarts %d  %.2fs\n",
                        static_cast<long long>(it + 1), pobj + P.offset, dobj + P.offset, relP, relD, gap, omega[b],
                        stats.restarts, seconds_since(t_solve));
-        if (relP <= opt.tolerance && relD <= opt.tolerance && gap <= opt.tolerance) {
+        if (!phase32 && relP <= opt.tolerance && relD <= opt.tolerance && gap <= opt.tolerance) {
           if (!fetched) {
             download_iterates(xs, ys);
             fetched = true;
@@ -869,8 +1040,14 @@ struct Engine {
         const int64_t nk = static_cast<int64_t>(n) * k, mk = static_cast<int64_t>(m) * k;
         B2P_CUDA(cudaMemcpyAsync(d_mask, h_mask, sizeof(int32_t) * k, cudaMemcpyHostToDevice, stream));
         bytes_up += static_cast<int64_t>(sizeof(int32_t) * k);
-        k_restart<<<blocks(std::max<int64_t>(nk + mk, k)), kBlock, 0, stream>>>(
-            n, m, k, d_mask, v[X], v[X0], v[XP], v[Y], v[Y0], v[YP], v[AX], v[AX0], v[AXP], d_it_base, d_restart_at);
+        if (phase32)
+          k_restart<float><<<blocks(std::max<int64_t>(nk + mk, k)), kBlock, 0, stream>>>(
+              n, m, k, d_mask, v32[X32], v32[X032], v32[XP32], v32[Y32], v32[Y032], v32[YP32], v32[AX32],
+              v32[AX032], v32[AXP32], d_it_base, d_restart_at);
+        else
+          k_restart<double><<<blocks(std::max<int64_t>(nk + mk, k)), kBlock, 0, stream>>>(
+              n, m, k, d_mask, v[X], v[X0], v[XP], v[Y], v[Y0], v[YP], v[AX], v[AX0], v[AXP], d_it_base,
+              d_restart_at);
         B2P_CUDA(cudaGetLastError());
         ++launches;
       }
@@ -886,7 +1063,12 @@ struct Engine {
     stats.primal_weight = omega.empty() ? 1 : omega[0];
     if (remaining > 0) {
       // Unconverged cases: the last check's sums are the KKT of (x+, y+)
-      // (the reference recomputes the same quantities, pdhg.cpp:668-680).
+      // (the reference recomputes the same quantities, pdhg.cpp:668-680);
+      // an FP32 point is re-measured in FP64 first.
+      if (phase32) {
+        fp32_point_to_fp64();
+        verify_fp64();
+      }
       download_iterates(xs, ys);
       for (int b = 0; b < k; ++b) {
         if (done[b]) continue;

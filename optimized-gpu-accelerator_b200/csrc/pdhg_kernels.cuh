@@ -173,13 +173,13 @@ static __global__ void __launch_bounds__(kBlock) k_halpern_all(int32_t n, int32_
 
 // Masked restart z = z0 = z+ for x, y, Ax and iteration counter reset
 // (src/pdhg/pdhg.cpp:153-165).  Runs after the interval's clock advanced, so
-// the next iteration (index *it_base) has counter 0.
-static __global__ void __launch_bounds__(kBlock) k_restart(int32_t n, int32_t m, int32_t k, const int32_t* __restrict__ mask,
-                                                    double* __restrict__ x, double* __restrict__ x0,
-                                                    const double* __restrict__ xp, double* __restrict__ y,
-                                                    double* __restrict__ y0, const double* __restrict__ yp,
-                                                    double* __restrict__ ax, double* __restrict__ ax0,
-                                                    const double* __restrict__ axp, const int64_t* __restrict__ it_base,
+// the next iteration (index *it_base) has counter 0.  T: iterate type.
+template <class T>
+__global__ void __launch_bounds__(kBlock) k_restart(int32_t n, int32_t m, int32_t k, const int32_t* __restrict__ mask,
+                                                    T* __restrict__ x, T* __restrict__ x0, const T* __restrict__ xp,
+                                                    T* __restrict__ y, T* __restrict__ y0, const T* __restrict__ yp,
+                                                    T* __restrict__ ax, T* __restrict__ ax0,
+                                                    const T* __restrict__ axp, const int64_t* __restrict__ it_base,
                                                     int64_t* __restrict__ restart_at) {
   const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t nx = static_cast<int64_t>(n) * k, ny = static_cast<int64_t>(m) * k;
@@ -193,6 +193,19 @@ static __global__ void __launch_bounds__(kBlock) k_restart(int32_t n, int32_t m,
       ax[u] = ax0[u] = axp[u];
     }
   }
+}
+
+// dst = src with a change of floating-point type (round to nearest).
+template <class S, class D>
+__global__ void __launch_bounds__(kBlock) k_convert(int64_t len, const S* __restrict__ src, D* __restrict__ dst) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t < len) dst[t] = static_cast<D>(src[t]);
+}
+
+// restart_at[b] = *it_base for all cases (a fresh restart at the next iteration).
+static __global__ void k_restart_clock(int32_t k, const int64_t* __restrict__ it_base, int64_t* __restrict__ restart_at) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < k) restart_at[t] = *it_base;
 }
 
 // ---- check reductions --------------------------------------------------------

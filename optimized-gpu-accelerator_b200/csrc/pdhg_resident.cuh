@@ -22,6 +22,12 @@
 // for the host's restart / extraction, and block 0 sums the per-block
 // partials in a fixed order (deterministic).
 //
+// The kernel is templated on the iterate type T.  T = double is the plain
+// form.  T = float is the mixed form: operator values, iterates and their
+// updates in FP32 (each row sum still accumulates exact FP32 x FP32 products in
+// FP64), while every check sum accumulates in FP64 against the FP64 costs and
+// bounds, and the host's decisions stay FP64.
+//
 // The grid barrier is a monotonic arrival counter with a generation word;
 // waits are bounded: after kSpinLimit polls a block records an error and all
 // blocks leave the interval at the next barrier, so a fault can never hang
@@ -38,14 +44,45 @@ constexpr int kResidentThreads = 1024;
 constexpr int kResUnroll = 8;
 constexpr unsigned kSpinLimit = 1u << 22;  // ~2 s of polling at ~0.5 us per poll
 
+// Round-to-nearest arithmetic without contraction, per iterate type.
+template <class T>
+struct Rn;
+template <>
+struct Rn<double> {
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+};
+template <>
+struct Rn<float> {
+  static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+  static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+  static __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+  static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+};
+
+// z = lam((1+rho) z+ - rho z) + (1-lam) z0 in type T.
+template <class T>
+__device__ __forceinline__ T halpern_t(T z, T zp, T z0, T lam, T rho) {
+  using R = Rn<T>;
+  const T a = R::sub(R::mul(R::add(T(1), rho), zp), R::mul(rho, z));
+  return R::add(R::mul(lam, a), R::mul(R::sub(T(1), lam), z0));
+}
+
+template <class T>
 struct ResidentArgs {
   // partition: block b owns columns [cb[b], cb[b+1]) and rows [rb[b], rb[b+1])
   const int32_t* __restrict__ cb;
   const int32_t* __restrict__ rb;
-  CsrView A, AT;
-  // global state
-  double *x, *x0, *xp, *y, *y0, *yp, *ax, *ax0, *axp;
-  const double *c, *lo, *up, *rl, *ru, *rfac, *cfac;
+  // A (CSR, m rows) and A^T (CSR, n rows): shared pointers, values of type T
+  const int32_t *a_ptr, *a_idx, *t_ptr, *t_idx;
+  const T *a_val, *t_val;
+  // global state (type T)
+  T *x, *x0, *xp, *y, *y0, *yp, *ax, *ax0, *axp;
+  const T *c, *lo, *up, *rl, *ru;
+  // FP64 data of the check
+  const double *c64, *lo64, *up64, *rl64, *ru64, *rfac, *cfac;
   const double *tau, *sigma;
   IterClock ck;  // ck.local unused (the kernel walks l = 0..L-1)
   double rho;
@@ -66,7 +103,8 @@ struct ResidentArgs {
 // acquire loads until all gridDim.x blocks of this epoch have arrived (the
 // __syncthreads on both sides extend the ordering to the whole block).
 // Returns false (on every thread) once any block has recorded a timeout.
-__device__ __forceinline__ bool grid_barrier(const ResidentArgs& a, unsigned& epoch) {
+template <class T>
+__device__ __forceinline__ bool grid_barrier(const ResidentArgs<T>& a, unsigned& epoch) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -107,22 +145,24 @@ __device__ __forceinline__ double res_tree(double s) {
 // starts after the grid barrier's acquire, which the PTX memory model orders
 // before these loads through bar.sync, so a cached line can never be stale
 // across phases, and entries repeated within a phase hit in L1.
-__device__ __forceinline__ double res_lane_sum(const int32_t* s_idx, const double* s_val, int p0, int end, int S,
-                                               const double* xg) {
+template <class T>
+__device__ __forceinline__ double res_lane_sum(const int32_t* s_idx, const T* s_val, int p0, int end, int S,
+                                               const T* xg) {
   double s = 0.0;
   bool first = true;
   for (int p = p0; p < end; p += kResUnroll * S) {
-    double xv[kResUnroll];
+    T xv[kResUnroll];
 #pragma unroll
     for (int u = 0; u < kResUnroll; ++u) {
       const int q = p + u * S;
-      xv[u] = q < end ? __ldca(xg + s_idx[q]) : 0.0;
+      xv[u] = q < end ? __ldca(xg + s_idx[q]) : T(0);
     }
 #pragma unroll
     for (int u = 0; u < kResUnroll; ++u) {
       const int q = p + u * S;
       if (q < end) {
-        const double prod = __dmul_rn(s_val[q], xv[u]);
+        // exact for FP32 inputs; the reference's rounded product for FP64
+        const double prod = __dmul_rn(static_cast<double>(s_val[q]), static_cast<double>(xv[u]));
         s = first ? prod : __dadd_rn(s, prod);
         first = false;
       }
@@ -155,9 +195,9 @@ __device__ __forceinline__ int res_long_list(const int32_t* s_ptr, int nrows, in
 // groups of G lanes, then the long rows of `s_long` (> lt) by whole warps.
 // epi(local_row, value) runs on one fixed thread per row.  Every thread of
 // the block must call.
-template <int G, class Epi>
-__device__ __forceinline__ void res_rows(const int32_t* s_ptr, const int32_t* s_idx, const double* s_val, int nrows,
-                                         int lt, const int32_t* s_long, int nlong, const double* xg, Epi&& epi) {
+template <int G, class T, class Epi>
+__device__ __forceinline__ void res_rows(const int32_t* s_ptr, const int32_t* s_idx, const T* s_val, int nrows, int lt,
+                                         const int32_t* s_long, int nlong, const T* xg, Epi&& epi) {
   const int gid = threadIdx.x / G, gl = threadIdx.x & (G - 1);
   constexpr int kGroups = kResidentThreads / G;
   for (int base = 0; base < nrows; base += kGroups) {
@@ -205,39 +245,42 @@ __device__ __forceinline__ void res_block_sum(double (&v)[NQ], double* s_red /* 
 }
 
 // Shared-memory bytes of a block with nc columns, nr rows, tn / an nonzeros
-// in its A^T / A slices.
+// in its A^T / A slices, iterates of type T.
+template <class T>
 __host__ __device__ inline size_t resident_smem_bytes(int nc, int nr, int tn, int an) {
-  size_t d = static_cast<size_t>(tn) + an + 6ull * nc + 8ull * nr + kNumSums * 32;
-  size_t i = static_cast<size_t>(tn) + an + nc + 1 + nr + 1 + nc + nr + 2;
-  return 8 * d + 4 * i + 16;
+  const size_t d = kNumSums * 32;
+  const size_t t = static_cast<size_t>(tn) + an + 6ull * nc + 8ull * nr;
+  const size_t i = static_cast<size_t>(tn) + an + nc + 1 + nr + 1 + nc + nr + 2;
+  return 8 * d + sizeof(T) * t + 4 * i + 16;
 }
 
-template <int GC, int GR>
-__global__ void __launch_bounds__(kResidentThreads, 1) k_resident(ResidentArgs a) {
+template <int GC, int GR, class T>
+__global__ void __launch_bounds__(kResidentThreads, 1) k_resident(ResidentArgs<T> a) {
+  using R = Rn<T>;
   extern __shared__ __align__(16) unsigned char smem[];
   const int c0 = a.cb[blockIdx.x], c1 = a.cb[blockIdx.x + 1];
   const int r0 = a.rb[blockIdx.x], r1 = a.rb[blockIdx.x + 1];
   const int nc = c1 - c0, nr = r1 - r0;
-  const int tb = a.AT.ptr[c0], tn = a.AT.ptr[c1] - tb;
-  const int ab = a.A.ptr[r0], an = a.A.ptr[r1] - ab;
-  double* s_tval = reinterpret_cast<double*>(smem);
-  double* s_aval = s_tval + tn;
-  double* s_x = s_aval + an;
-  double* s_x0 = s_x + nc;
-  double* s_c = s_x0 + nc;
-  double* s_lo = s_c + nc;
-  double* s_up = s_lo + nc;
-  double* s_xp = s_up + nc;
-  double* s_y = s_xp + nc;
-  double* s_y0 = s_y + nr;
-  double* s_ax = s_y0 + nr;
-  double* s_ax0 = s_ax + nr;
-  double* s_rl = s_ax0 + nr;
-  double* s_ru = s_rl + nr;
-  double* s_axp = s_ru + nr;
-  double* s_yp = s_axp + nr;
-  double* s_red = s_yp + nr;
-  int32_t* s_tidx = reinterpret_cast<int32_t*>(s_red + kNumSums * 32);
+  const int tb = a.t_ptr[c0], tn = a.t_ptr[c1] - tb;
+  const int ab = a.a_ptr[r0], an = a.a_ptr[r1] - ab;
+  double* s_red = reinterpret_cast<double*>(smem);
+  T* s_tval = reinterpret_cast<T*>(s_red + kNumSums * 32);
+  T* s_aval = s_tval + tn;
+  T* s_x = s_aval + an;
+  T* s_x0 = s_x + nc;
+  T* s_c = s_x0 + nc;
+  T* s_lo = s_c + nc;
+  T* s_up = s_lo + nc;
+  T* s_xp = s_up + nc;
+  T* s_y = s_xp + nc;
+  T* s_y0 = s_y + nr;
+  T* s_ax = s_y0 + nr;
+  T* s_ax0 = s_ax + nr;
+  T* s_rl = s_ax0 + nr;
+  T* s_ru = s_rl + nr;
+  T* s_axp = s_ru + nr;
+  T* s_yp = s_axp + nr;
+  int32_t* s_tidx = reinterpret_cast<int32_t*>(s_yp + nr);
   int32_t* s_aidx = s_tidx + tn;
   int32_t* s_tptr = s_aidx + an;
   int32_t* s_aptr = s_tptr + nc + 1;
@@ -247,15 +290,15 @@ __global__ void __launch_bounds__(kResidentThreads, 1) k_resident(ResidentArgs a
 
   // ---- load the block's slices and owned state ----
   for (int q = threadIdx.x; q < tn; q += blockDim.x) {
-    s_tval[q] = __ldg(a.AT.val + tb + q);
-    s_tidx[q] = __ldg(a.AT.idx + tb + q);
+    s_tval[q] = __ldg(a.t_val + tb + q);
+    s_tidx[q] = __ldg(a.t_idx + tb + q);
   }
   for (int q = threadIdx.x; q < an; q += blockDim.x) {
-    s_aval[q] = __ldg(a.A.val + ab + q);
-    s_aidx[q] = __ldg(a.A.idx + ab + q);
+    s_aval[q] = __ldg(a.a_val + ab + q);
+    s_aidx[q] = __ldg(a.a_idx + ab + q);
   }
-  for (int q = threadIdx.x; q <= nc; q += blockDim.x) s_tptr[q] = a.AT.ptr[c0 + q] - tb;
-  for (int q = threadIdx.x; q <= nr; q += blockDim.x) s_aptr[q] = a.A.ptr[r0 + q] - ab;
+  for (int q = threadIdx.x; q <= nc; q += blockDim.x) s_tptr[q] = a.t_ptr[c0 + q] - tb;
+  for (int q = threadIdx.x; q <= nr; q += blockDim.x) s_aptr[q] = a.a_ptr[r0 + q] - ab;
   for (int q = threadIdx.x; q < nc; q += blockDim.x) {
     const int j = c0 + q;
     s_x[q] = __ldcg(a.x + j);
@@ -273,7 +316,8 @@ __global__ void __launch_bounds__(kResidentThreads, 1) k_resident(ResidentArgs a
     s_rl[q] = __ldg(a.rl + i);
     s_ru[q] = __ldg(a.ru + i);
   }
-  const double tau = __ldcg(a.tau), sigma = __ldcg(a.sigma), rho = a.rho;
+  const T tau = static_cast<T>(__ldcg(a.tau)), sigma = static_cast<T>(__ldcg(a.sigma));
+  const T rho = static_cast<T>(a.rho);
   const int64_t it0 = *a.it_base - a.ck.restart_at[0];
   __syncthreads();
   const int ntlong = res_long_list(s_tptr, nc, a.lt_cols, s_tlong, s_counts);
@@ -281,38 +325,40 @@ __global__ void __launch_bounds__(kResidentThreads, 1) k_resident(ResidentArgs a
 
   unsigned epoch = 0;
   bool ok = true;
-  double lam = 0.0;
+  T lam = T(0);
   for (int l = 0; l < a.L && ok; ++l) {
     const bool last = l == a.L - 1;
-    const double j = static_cast<double>(it0 + l);
-    lam = __ddiv_rn(__dadd_rn(j, 1.0), __dadd_rn(j, 2.0));
+    const double jj = static_cast<double>(it0 + l);
+    lam = static_cast<T>(__ddiv_rn(__dadd_rn(jj, 1.0), __dadd_rn(jj, 2.0)));
     // primal phase: x+ = proj(x - tau (c - A^T y)); publish x+; Halpern x
-    res_rows<GC>(s_tptr, s_tidx, s_tval, nc, a.lt_cols, s_tlong, ntlong, a.y, [&](int q, double aty) {
-      const double xv = s_x[q];
-      double v = __dsub_rn(xv, __dmul_rn(tau, __dsub_rn(s_c[q], aty)));
+    res_rows<GC>(s_tptr, s_tidx, s_tval, nc, a.lt_cols, s_tlong, ntlong, a.y, [&](int q, double atyd) {
+      const T aty = static_cast<T>(atyd);
+      const T xv = s_x[q];
+      T v = R::sub(xv, R::mul(tau, R::sub(s_c[q], aty)));
       v = (v < s_lo[q]) ? s_lo[q] : v;
       v = (s_up[q] < v) ? s_up[q] : v;
       s_xp[q] = v;
       a.xp[c0 + q] = v;
-      if (!last) s_x[q] = halpern_step(xv, v, s_x0[q], lam, rho);
+      if (!last) s_x[q] = halpern_t(xv, v, s_x0[q], lam, rho);
     });
     ok = grid_barrier(a, epoch);
     if (!ok) break;
     // dual phase: y+ = v + sigma proj(-v/sigma); Halpern y, Ax; publish y (y+ at the check)
-    res_rows<GR>(s_aptr, s_aidx, s_aval, nr, a.lt_rows, s_along, nalong, a.xp, [&](int q, double axpv) {
-      const double axv = s_ax[q], yv = s_y[q];
-      const double v = __dsub_rn(yv, __dmul_rn(sigma, __dsub_rn(__dmul_rn(2.0, axpv), axv)));
-      double w = __ddiv_rn(-v, sigma);
+    res_rows<GR>(s_aptr, s_aidx, s_aval, nr, a.lt_rows, s_along, nalong, a.xp, [&](int q, double axpd) {
+      const T axpv = static_cast<T>(axpd);
+      const T axv = s_ax[q], yv = s_y[q];
+      const T v = R::sub(yv, R::mul(sigma, R::sub(R::mul(T(2), axpv), axv)));
+      T w = R::div(-v, sigma);
       w = (w < s_rl[q]) ? s_rl[q] : w;
       w = (s_ru[q] < w) ? s_ru[q] : w;
-      const double ypv = __dadd_rn(v, __dmul_rn(sigma, w));
+      const T ypv = R::add(v, R::mul(sigma, w));
       s_axp[q] = axpv;
       s_yp[q] = ypv;
       if (!last) {
-        const double yn = halpern_step(yv, ypv, s_y0[q], lam, rho);
+        const T yn = halpern_t(yv, ypv, s_y0[q], lam, rho);
         s_y[q] = yn;
         a.y[r0 + q] = yn;
-        s_ax[q] = halpern_step(axv, axpv, s_ax0[q], lam, rho);
+        s_ax[q] = halpern_t(axv, axpv, s_ax0[q], lam, rho);
       } else {
         a.yp[r0 + q] = ypv;
       }
@@ -320,13 +366,14 @@ __global__ void __launch_bounds__(kResidentThreads, 1) k_resident(ResidentArgs a
     ok = grid_barrier(a, epoch);
   }
 
-  // ---- check: the block's part of kkt_rows/kkt_cols and the movement norms ----
+  // ---- check: the block's part of kkt_rows/kkt_cols and the movement norms, in FP64 ----
   double v[kNumSums];
 #pragma unroll
   for (int q = 0; q < kNumSums; ++q) v[q] = 0.0;
   if (ok) {
     res_rows<GC>(s_tptr, s_tidx, s_tval, nc, a.lt_cols, s_tlong, ntlong, a.yp, [&](int q, double atyp) {
-      const double cv = s_c[q], l = s_lo[q], u = s_up[q], xpv = s_xp[q];
+      const int j = c0 + q;
+      const double cv = a.c64[j], l = a.lo64[j], u = a.up64[j], xpv = static_cast<double>(s_xp[q]);
       const double d = cv - atyp;
       const bool hl = l > -1e300, hu = u < 1e300;
       double res = 0.0;
@@ -336,31 +383,32 @@ __global__ void __launch_bounds__(kResidentThreads, 1) k_resident(ResidentArgs a
         res = (d < 0.0) ? 0.0 : d;
       else if (!hu)
         res = (-d < 0.0) ? 0.0 : -d;
-      res *= a.cfac[c0 + q];
+      res *= a.cfac[j];
       v[CS_COL_RES2] += res * res;
       v[CS_POBJ] += cv * xpv;
       if (d > 0.0 && hl)
         v[CS_COL_DOBJ] += d * l;
       else if (d < 0.0 && hu)
         v[CS_COL_DOBJ] += d * u;
-      const double d1 = s_x[q] - xpv, d2 = xpv - s_x0[q];
+      const double d1 = static_cast<double>(s_x[q]) - xpv, d2 = xpv - static_cast<double>(s_x0[q]);
       v[CS_DX2] += d1 * d1;
       v[CS_AX2] += d2 * d2;
     });
     for (int q = threadIdx.x; q < nr; q += blockDim.x) {
-      const double av = s_axp[q], l = s_rl[q], u = s_ru[q];
+      const int i = r0 + q;
+      const double av = static_cast<double>(s_axp[q]), l = a.rl64[i], u = a.ru64[i];
       double e1 = l - av, e2 = av - u;
       e1 = (e1 < 0.0) ? 0.0 : e1;
       e2 = (e2 < 0.0) ? 0.0 : e2;
-      const double res = (e1 + e2) * a.rfac[r0 + q];
+      const double res = (e1 + e2) * a.rfac[i];
       v[CS_ROW_RES2] += res * res;
-      const double yv = s_yp[q];
+      const double yv = static_cast<double>(s_yp[q]);
       if (yv > 0.0 && l > -1e300)
         v[CS_ROW_DOBJ] += yv * l;
       else if (yv < 0.0 && u < 1e300)
         v[CS_ROW_DOBJ] += yv * u;
       v[CS_Y2] += yv * yv;
-      const double d1 = s_y[q] - yv, d2 = yv - s_y0[q];
+      const double d1 = static_cast<double>(s_y[q]) - yv, d2 = yv - static_cast<double>(s_y0[q]);
       v[CS_DY2] += d1 * d1;
       v[CS_AY2] += d2 * d2;
     }
@@ -372,14 +420,11 @@ __global__ void __launch_bounds__(kResidentThreads, 1) k_resident(ResidentArgs a
 
   // ---- deferred Halpern step and write-back of the block's state ----
   if (ok) {
-    for (int q = threadIdx.x; q < nc; q += blockDim.x) {
-      const int jj = c0 + q;
-      a.x[jj] = halpern_step(s_x[q], s_xp[q], s_x0[q], lam, rho);
-    }
+    for (int q = threadIdx.x; q < nc; q += blockDim.x) a.x[c0 + q] = halpern_t(s_x[q], s_xp[q], s_x0[q], lam, rho);
     for (int q = threadIdx.x; q < nr; q += blockDim.x) {
       const int i = r0 + q;
-      a.y[i] = halpern_step(s_y[q], s_yp[q], s_y0[q], lam, rho);
-      a.ax[i] = halpern_step(s_ax[q], s_axp[q], s_ax0[q], lam, rho);
+      a.y[i] = halpern_t(s_y[q], s_yp[q], s_y0[q], lam, rho);
+      a.ax[i] = halpern_t(s_ax[q], s_axp[q], s_ax0[q], lam, rho);
       a.axp[i] = s_axp[q];
     }
   }

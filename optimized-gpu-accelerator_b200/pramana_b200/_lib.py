@@ -17,6 +17,7 @@ ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "no usable sm_100 device", 
           5: "size beyond maximum"}
 STATUS_NAMES = {0: "NotSolved", 1: "Optimal", 5: "TimeLimit", 6: "IterationLimit"}
 PRECISION_FP64 = 0
+PRECISION_MIXED = 1
 KERNELS_AUTO, KERNELS_FUSED, KERNELS_RESIDENT = 0, 1, 2
 
 dptr = C.POINTER(C.c_double)
@@ -52,7 +53,8 @@ class B2pStats(C.Structure):
                 ("bytes_downloaded", C.c_int64), ("kernel_launches", C.c_int64), ("spectral_norm", C.c_double),
                 ("prepare_seconds", C.c_double), ("upload_seconds", C.c_double), ("graph_seconds", C.c_double),
                 ("lanes_per_row_a", C.c_int32), ("lanes_per_row_at", C.c_int32), ("kernel_mode", C.c_int32),
-                ("resident_blocks", C.c_int32), ("resident_smem_bytes", C.c_int64)]
+                ("resident_blocks", C.c_int32), ("resident_smem_bytes", C.c_int64), ("precision_used", C.c_int32),
+                ("pad1", C.c_int32), ("fp32_iterations", C.c_int64)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_ if not f.startswith("pad")}

@@ -309,3 +309,31 @@ def test_spectral_norm_bitexact(oracle_mod, which):
     g = pdhg.solvePdhg(lp, opts(tolerance=1e-30, maxIterations=1))
     oracle_mod.solve(lp, "oracle", tolerance=1e-30, max_iterations=1)
     assert g.stats.spectralNorm == oracle_mod.solve.last_stats["spectral_norm"]
+
+
+MIXED = 1  # B2P_PRECISION_MIXED
+
+
+@pytest.mark.parametrize("which,tol", [("c1", 1e-4), ("c1", 1e-6), ("edge", 1e-6), ("c2", 1e-6), ("c2", 1e-8)])
+def test_mixed_precision_meets_tolerance_in_fp64(which, tol):
+    """Mixed form: FP32 iterates, FP64 checks; the returned point's KKT,
+    recomputed on the host in FP64, meets the tolerance, and its objective
+    stays within a few tolerances of the plain FP64 solve's."""
+    lp = {"c1": lambda: G.config1(1), "c2": lambda: G.config2(2), "edge": lambda: lp_cases.edge_lp(6)}[which]()
+    with pdhg.Engine(lp, opts(tolerance=tol, precision=MIXED)) as e:
+        r = e.solve()[0]
+        st = e.last_stats
+    assert r.status == "Optimal"
+    assert st.precision_used == MIXED and st.fp32_iterations > 0
+    relP, relD, gap = _host_kkt(lp, r.x, r.rowDual)
+    assert max(relP, relD, gap) <= tol * (1 + 1e-6)
+    ref = pdhg.solvePdhg(lp, opts(tolerance=tol))
+    assert abs(r.objective - ref.objective) <= 10 * tol * (1 + abs(ref.objective))
+
+
+def test_mixed_falls_back_to_fp64_for_batches():
+    lp = G.random_lp(150, 300, 4.0, 90, 13)
+    cases = lp_cases.cost_sweep_cases(lp, 3)
+    st = pdhg.PdhgStats()
+    rs = pdhg.solvePdhgBatch(lp, cases, opts(tolerance=1e-6, precision=MIXED), batchStats=st)
+    assert all(r.status == "Optimal" for r in rs)
