@@ -5,11 +5,13 @@ Workload: the seeded random LP with m=40,000 rows, n=80,000 columns and
 solved by restarted-Halpern PDHG to relative KKT 1e-6.  One step = one full
 solve from the cold start.
 
-Metric: time to relative KKT 1e-6, in seconds (lower is better).
+Metric: time to relative KKT 1e-6, in seconds (lower is better), of the chosen
+form -- mixed precision: FP32 iterates, FP64 checks, FP64 verification and
+polish -- with the plain FP64 form's time on the same LP reported beside it.
   value : device time of the PDHG loop (CUDA events on the engine's stream),
           with the prepared problem already resident in HBM; L2 is flushed
           (a 512 MiB write) before every step.
-  e2e   : the same solve through the public C ABI (b2p_solve_pdhg) from host
+  e2e   : the chosen form through the public C ABI (b2p_solve_pdhg) from host
           arrays: host preprocessing, host->device upload, the loop and the
           device->host read of x and y, wall clock per step.
 N > 1 (torchrun): N independent replicas of the same solve, one per GPU
@@ -44,7 +46,7 @@ REF_ITERS_TO_TOL = 20288  # loop iterations of the reference CPU PDHG on this LP
 def workload_config(lp, extra=None):
     cfg = {"workload": f"config-2 random LP m={lp.num_rows} n={lp.num_cols} nnz={lp.nnz} "
                        f"(1% rows hold 10% nnz), seed {SEED}, to rel KKT {TOL:g}",
-           "form": "plain FP64 (iterate parity with the reference)", "check_every": 64,
+           "form": "mixed precision (plain FP64 form timed beside it)", "check_every": 64,
            "l2": "flushed before every step (512 MiB device write); the LP itself (~20 MB/iteration) is L2-resident "
                  "within a solve"}
     if extra:
@@ -208,9 +210,10 @@ def main():
     from pramana_b200 import pdhg
 
     lp = G.config2(SEED)
-    po = pdhg.PdhgOptions(tolerance=TOL, device=dev)
+    po_plain = pdhg.PdhgOptions(tolerance=TOL, device=dev, precision=0)
+    po = pdhg.PdhgOptions(tolerance=TOL, device=dev, precision=1)  # the chosen form: mixed precision
     if args.profile_iters > 0:
-        po.maxIterations = args.profile_iters
+        po.maxIterations = po_plain.maxIterations = args.profile_iters
     flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{dev}")
 
     def barrier():
@@ -218,28 +221,41 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    # ---- value: device-timed loop, problem resident in HBM ----
-    eng = pdhg.Engine(lp, po)
-    for _ in range(args.warmup):
-        flush.zero_()
-        torch.cuda.synchronize()
-        eng.solve()
-    times, launches, iters = [], 0, None
-    barrier()
-    with ClockSampler(dev) as clk:
-        for _ in range(args.steps):
+    def timed_solves(eng, steps, sampler=None):
+        """K solves from the cold start; device time of each loop (CUDA events on the engine's stream)."""
+        out = []
+        for _ in range(steps):
             flush.zero_()
             torch.cuda.synchronize()
             r = eng.solve()[0]
             st = eng.last_stats
-            times.append(st.kernel_seconds)
-            launches += st.kernel_launches
-            iters = r.iterations
             assert r.status == "Optimal" or args.profile_iters > 0, r.status
-        barrier()
-    t_dev = statistics.mean(times)
+            out.append((st.kernel_seconds, st.kernel_launches, r, st.fp32_iterations))
+        return out
 
-    # ---- roofline of the dominant kernel: a profiled solve (events around every SpMV kernel) ----
+    # ---- value: device-timed loop of the chosen (mixed) form, problem resident in HBM ----
+    eng = pdhg.Engine(lp, po)
+    timed_solves(eng, args.warmup)
+    barrier()
+    with ClockSampler(dev) as clk:
+        res = timed_solves(eng, args.steps)
+        barrier()
+    t_dev = statistics.mean(x[0] for x in res)
+    launches = sum(x[1] for x in res)
+    r_mixed, fp32_iters = res[-1][2], res[-1][3]
+    iters = r_mixed.iterations
+    eng.close()
+
+    # ---- the plain FP64 form on the same LP, for the comparison the metric asks for ----
+    eng = pdhg.Engine(lp, po_plain)
+    timed_solves(eng, args.warmup)
+    barrier()
+    res_plain = timed_solves(eng, args.steps)
+    barrier()
+    t_plain = statistics.mean(x[0] for x in res_plain)
+    r_plain = res_plain[-1][2]
+
+    # ---- roofline of the dominant kernel: a profiled plain solve (events around every launch) ----
     eng.set_profiling(True)
     flush.zero_()
     torch.cuda.synchronize()
@@ -266,7 +282,7 @@ def main():
                           "dominant_kernel": kname, "avg_launch_us": avg_s * 1e6}))
         return 0
 
-    # ---- e2e: public C ABI from host arrays ----
+    # ---- e2e: public C ABI from host arrays, chosen form ----
     e2e_times, h2d, d2h = [], 0, 0
     for s in range(args.warmup + args.steps):
         flush.zero_()
@@ -280,9 +296,9 @@ def main():
     t_e2e = statistics.mean(e2e_times)
 
     if dist is not None:
-        tt = torch.tensor([t_dev, t_e2e], dtype=torch.float64, device=f"cuda:{dev}")
+        tt = torch.tensor([t_dev, t_e2e, t_plain], dtype=torch.float64, device=f"cuda:{dev}")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_dev, t_e2e = tt.tolist()
+        t_dev, t_e2e, t_plain = tt.tolist()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -297,9 +313,18 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": t_dev, "unit": "s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_dev * 1e3, "higher_is_better": False, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+                "vs_baseline": None, "dtype": "f32 iterates, f64 checks and polish",
+                "data": "synthetic (seeded generator)",
                 "config": workload_config(lp, {"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                                               "iterations": iters, "kernel_form": form}),
+                                               "iterations": iters, "fp32_iterations": fp32_iters,
+                                               "kernel_form": form, "chosen_form": "mixed precision"}),
+                "forms": {
+                    "mixed": {"value": t_dev, "iterations": iters, "fp32_iterations": fp32_iters,
+                              "relative_kkt_fp64": r_mixed.relativeKkt,
+                              "objective_rel_diff_vs_fp64": abs(r_mixed.objective - r_plain.objective)
+                              / (1 + abs(r_plain.objective))},
+                    "plain_fp64": {"value": t_plain, "iterations": r_plain.iterations,
+                                   "relative_kkt": r_plain.relativeKkt}},
                 "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches,
                 "spmv_gbs": spmv_total_bytes / spmv_total_s / 1e9,

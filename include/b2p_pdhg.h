@@ -225,6 +225,27 @@ int b2p_engine_kernel_bytes(b2p_engine* e, int32_t kernel_class, double* bytes);
 int b2p_kkt_residual(const b2p_lp* lp, const b2p_case* cases, int32_t num_cases, const double* x,
                      const double* row_dual, double* out);
 
+/* ---- Certification ----------------------------------------------------------
+ * Rigorous outward-rounded Neumaier-Shcherbina lower bound on
+ * min { c'x : L <= Ax <= U, l <= x <= u } (objective offset excluded) that is
+ * valid for ANY row dual y, for num_cases cases of a shared A at once
+ * (num_cases <= 0: one case, the base model).  Replaces safeDualBound /
+ * SafeBoundResult (src/cert/certifier.h:79-96, certifier.cpp:58-118) and gives
+ * bit-identical results: same projection of y, same outward-rounded interval
+ * reduced costs in column order, same in-order downward sum.  row_dual is
+ * num_cases x num_rows (case-major); out has num_cases entries. */
+typedef struct b2p_safe_bound {
+  double bound;                  /* -inf when a wrong-signed reduced cost sits on an infinite bound */
+  int32_t infinite_terms;        /* columns that forced -inf */
+  int32_t pad0;
+  double max_dual_infeasibility; /* largest clipped wrong-signed reduced cost */
+  double row_projection;         /* largest change of y by the sign-cone projection */
+  double cost_perturbation;      /* relative cost change the clipped bound is rigorous for */
+} b2p_safe_bound;
+
+int b2p_safe_dual_bound(const b2p_lp* lp, const b2p_case* cases, int32_t num_cases, const double* row_dual,
+                        b2p_safe_bound* out);
+
 /* Allocation-free form of b2p_kkt_residual.  No counterpart in the
  * reference.  For callers that cannot allocate device memory (a host
  * framework that owns all device memory through its own pool, code inside a

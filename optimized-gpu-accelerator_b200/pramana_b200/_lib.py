@@ -60,6 +60,12 @@ class B2pStats(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_ if not f.startswith("pad")}
 
 
+class B2pSafeBound(C.Structure):
+    _fields_ = [("bound", C.c_double), ("infinite_terms", C.c_int32), ("pad0", C.c_int32),
+                ("max_dual_infeasibility", C.c_double), ("row_projection", C.c_double),
+                ("cost_perturbation", C.c_double)]
+
+
 class B2pResult(C.Structure):
     _fields_ = [("status", C.c_int32), ("pad0", C.c_int32), ("iterations", C.c_int64),
                 ("objective", C.c_double), ("dual_objective", C.c_double), ("relative_kkt", C.c_double)]
@@ -84,6 +90,8 @@ SIGNATURES = {
     "b2p_engine_kernel_times": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64), dptr]),
     "b2p_engine_kernel_bytes": (C.c_int, [C.c_void_p, C.c_int32, dptr]),
     "b2p_csr_spmv": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, iptr, iptr, dptr, dptr, dptr]),
+    "b2p_safe_dual_bound": (C.c_int, [C.POINTER(B2pLp), C.POINTER(B2pCase), C.c_int32, dptr,
+                                      C.POINTER(B2pSafeBound)]),
     "b2p_kkt_residual": (C.c_int, [C.POINTER(B2pLp), C.POINTER(B2pCase), C.c_int32, dptr, dptr, dptr]),
     "b2p_kkt_residual_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

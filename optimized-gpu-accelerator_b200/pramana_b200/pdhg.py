@@ -328,9 +328,27 @@ def kktResidual(lp: Model, x, rowDual, cases: list[LpCase] | None = None) -> np.
     return out.reshape(k, 4)
 
 
+def safeDualBound(lp: Model, rowDual, cases: list[LpCase] | None = None) -> list[dict]:
+    """Outward-rounded Neumaier-Shcherbina lower bound (objective offset
+    excluded), valid for any row dual, per case; bit-identical to the
+    reference's safeDualBound."""
+    lib = _lib.load()
+    s, keep = _lp_struct(lp)
+    k = len(cases) if cases else 1
+    arr, keep2 = (_cases_struct(cases, lp.num_cols, lp.num_rows) if cases else (None, []))
+    y = np.ascontiguousarray(rowDual, dtype=np.float64).reshape(-1)
+    if len(y) != k * lp.num_rows:
+        raise ValueError("rowDual has the wrong length")
+    out = (_lib.B2pSafeBound * k)()
+    _lib.check(lib.b2p_safe_dual_bound(C.byref(s), arr, len(cases) if cases else 0, y.ctypes.data_as(_lib.dptr), out))
+    del keep, keep2
+    return [{f: getattr(out[b], f) for f, _ in _lib.B2pSafeBound._fields_ if f != "pad0"} for b in range(k)]
+
+
 # snake_case aliases
 solve_pdhg = solvePdhg
 solve_pdhg_batch = solvePdhgBatch
 gpu_available = gpuAvailable
 gpu_info_json = gpuInfoJson
 kkt_residual = kktResidual
+safe_dual_bound = safeDualBound

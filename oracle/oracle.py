@@ -157,19 +157,25 @@ def solve(lp, lib: str = "oracle", cases=None, **opts) -> list[OracleResult] | O
     return out if cases is not None else out[0]
 
 
-def safe_dual_bound(lp, y, col_lower=None, col_upper=None) -> float:
-    """The reference's outward-rounded Neumaier-Shcherbina bound (needs the ref build)."""
+def safe_dual_bound(lp, y, col_lower=None, col_upper=None, full: bool = False):
+    """The reference's outward-rounded Neumaier-Shcherbina bound (needs the ref
+    build), plus the objective offset; with full=True the whole SafeBoundResult
+    (bound without offset)."""
     h = _load("ref")
     lo = np.ascontiguousarray(lp.col_lower if col_lower is None else col_lower, dtype=np.float64)
     up = np.ascontiguousarray(lp.col_upper if col_upper is None else col_upper, dtype=np.float64)
     y = np.ascontiguousarray(y, dtype=np.float64)
     bound = C.c_double()
     inf_terms = C.c_int()
+    extra = np.zeros(3)
     rc = h.ref_safe_dual_bound(C.c_int(lp.num_rows), C.c_int(lp.num_cols), _ip(lp.start), _ip(lp.index),
                                _dp(lp.value), _dp(lp.col_cost), _dp(lo), _dp(up), _dp(lp.row_lower),
-                               _dp(lp.row_upper), _dp(y), C.byref(bound), C.byref(inf_terms))
+                               _dp(lp.row_upper), _dp(y), C.byref(bound), C.byref(inf_terms), _dp(extra))
     if rc != 0:
         raise RuntimeError("safe bound failed")
+    if full:
+        return {"bound": bound.value, "infinite_terms": inf_terms.value, "max_dual_infeasibility": extra[0],
+                "row_projection": extra[1], "cost_perturbation": extra[2]}
     return bound.value + lp.obj_offset
 
 

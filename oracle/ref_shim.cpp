@@ -165,9 +165,10 @@ int ref_pdhg_solve(int m, int n, const int* start, const int* index, const doubl
 }
 
 // Outward-rounded lower bound on min c^T x over the given boxes, valid for any y.
+// extra (optional): maxDualInfeasibility, rowProjection, costPerturbation
 int ref_safe_dual_bound(int m, int n, const int* start, const int* index, const double* value, const double* cost,
                         const double* colLower, const double* colUpper, const double* rowLower,
-                        const double* rowUpper, const double* y, double* bound, int* infiniteTerms) {
+                        const double* rowUpper, const double* y, double* bound, int* infiniteTerms, double* extra) {
   try {
     SparseMatrix A(m, n);
     A.start.assign(start, start + n + 1);
@@ -180,6 +181,11 @@ int ref_safe_dual_bound(int m, int n, const int* start, const int* index, const 
                                        std::vector<double>(rowUpper, rowUpper + m), std::vector<double>(y, y + m));
     *bound = sb.bound;
     if (infiniteTerms) *infiniteTerms = sb.infiniteTerms;
+    if (extra) {
+      extra[0] = sb.maxDualInfeasibility;
+      extra[1] = sb.rowProjection;
+      extra[2] = sb.costPerturbation;
+    }
     return 0;
   } catch (std::exception& e) {
     gErr = e.what();
