@@ -177,6 +177,18 @@ int b2p_solve_pdhg(const b2p_lp* lp, const b2p_options* opts, double* x, double*
 int b2p_solve_pdhg_batch(const b2p_lp* base, const b2p_case* cases, int32_t num_cases, const b2p_options* opts,
                          double* x, double* row_dual, b2p_result* results, b2p_stats* batch_stats);
 
+/* Many independent LPs of different sizes (each with its own A) in one
+ * solve.  No counterpart in the reference, which batches only cases sharing
+ * one A (solvePdhgBatch); each LP here gets exactly the reference's algorithm
+ * (its own scaling, steps, primal weight, restarts and termination), and all
+ * of them advance together as one block-diagonal operator on the GPU.
+ * x[b] (num_cols of LP b) and row_dual[b] (num_rows) receive LP b's
+ * solution (either array, or any entry, may be NULL); results has num_lps
+ * entries.  stats: kernel_seconds is the device time of the loop;
+ * iterations the global iteration count. */
+int b2p_solve_pdhg_multi(const b2p_lp* lps, int32_t num_lps, const b2p_options* opts, double* const* x,
+                         double* const* row_dual, b2p_result* results, b2p_stats* stats);
+
 /* gpuAvailable (src/pdhg/pdhg.cpp:730): 1 if an sm_100 device is usable. */
 int b2p_gpu_available(void);
 

@@ -31,6 +31,7 @@
 #include "pdhg_kernels.cuh"
 #include "pdhg_prepare.h"
 #include "pdhg_resident.cuh"
+#include "pdhg_sched.h"
 #include "pdhg_spmv.cuh"
 
 namespace b2p {
@@ -41,81 +42,6 @@ namespace {
 // ATY/ATYP which the fused kernels never store, plus the initial point).
 enum Slot : int { X, XP, X0, C, LO, UP, XINIT, ATYP, NCOLVEC, Y = NCOLVEC, YP, Y0, AX, AXP, AX0, RL, RU, AXINIT, NSLOT };
 inline bool row_slot(int s) { return s >= Y; }
-
-void check_lp(const b2p_lp* lp) {
-  if (!lp) throw Error(B2P_ERR_INVALID, "lp is NULL");
-  if (lp->num_rows < 0 || lp->num_cols < 0) throw Error(B2P_ERR_INVALID, "negative dimension");
-  if (!lp->start) throw Error(B2P_ERR_INVALID, "start is NULL");
-  if (lp->start[0] != 0) throw Error(B2P_ERR_INVALID, "start[0] must be 0");
-  for (int32_t j = 0; j < lp->num_cols; ++j)
-    if (lp->start[j + 1] < lp->start[j]) throw Error(B2P_ERR_INVALID, "start must be non-decreasing");
-  const int32_t nnz = lp->start[lp->num_cols];
-  if (nnz > 0 && (!lp->index || !lp->value)) throw Error(B2P_ERR_INVALID, "index/value are NULL");
-  for (int32_t q = 0; q < nnz; ++q)
-    if (lp->index[q] < 0 || lp->index[q] >= lp->num_rows) throw Error(B2P_ERR_INVALID, "row index out of range");
-  if (lp->num_cols > 0 && (!lp->col_cost || !lp->col_lower || !lp->col_upper))
-    throw Error(B2P_ERR_INVALID, "column vectors are NULL");
-  if (lp->num_rows > 0 && (!lp->row_lower || !lp->row_upper)) throw Error(B2P_ERR_INVALID, "row vectors are NULL");
-}
-
-// Row-length bins of one CSR operator (see pdhg_spmv.cuh).
-struct HostBins {
-  std::vector<int32_t> long_rows, vlong_rows;
-  int g = 1;
-  int long_thr = kUnroll;
-};
-
-// Lanes per short row: enough that 90% of the rows finish in one round of
-// kUnroll entries per lane, but no more than fit the grid in one wave of
-// `wave_threads`; `rounds` rounds of kUnroll entries stay on the short path.
-HostBins make_bins(const HostCsr& M, int64_t wave_threads, int g_override, int rounds) {
-  HostBins hb;
-  std::vector<int32_t> len(M.rows);
-  for (int32_t i = 0; i < M.rows; ++i) len[i] = M.ptr[i + 1] - M.ptr[i];
-  if (g_override > 0) {
-    while (hb.g < 32 && hb.g * 2 <= g_override) hb.g *= 2;
-  } else if (M.rows > 0) {
-    std::vector<int32_t> sorted(len);
-    const size_t q = static_cast<size_t>(0.9 * (sorted.size() - 1));
-    std::nth_element(sorted.begin(), sorted.begin() + q, sorted.end());
-    const int p90 = sorted[q];
-    while (hb.g < 32 && hb.g * kUnroll < p90) hb.g *= 2;
-    while (hb.g > 1 && static_cast<int64_t>(M.rows) * hb.g > wave_threads) hb.g /= 2;
-  }
-  hb.long_thr = std::max(1, rounds) * kUnroll * hb.g;
-  for (int32_t i = 0; i < M.rows; ++i) {
-    if (len[i] > kVeryLongRow)
-      hb.vlong_rows.push_back(i);
-    else if (len[i] > hb.long_thr)
-      hb.long_rows.push_back(i);
-  }
-  return hb;
-}
-
-template <typename... KArgs, typename... Args>
-void launch(void (*kern)(KArgs...), unsigned grid, cudaStream_t stream, bool pdl, Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(kBlock);
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = pdl ? attr : nullptr;
-  cfg.numAttrs = pdl ? 1 : 0;
-  B2P_CUDA(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
-}
-
-#define B2P_G_SWITCH(g, F)                           \
-  switch (g) {                                       \
-    case 1: F(1); break;                             \
-    case 2: F(2); break;                             \
-    case 4: F(4); break;                             \
-    case 8: F(8); break;                             \
-    case 16: F(16); break;                           \
-    default: F(32); break;                           \
-  }
 
 template <class T>
 using ResidentFn = void (*)(ResidentArgs<T>);
@@ -707,10 +633,10 @@ struct Engine {
 #define B2P_PRIMAL(G)                                                                                     \
   if (last)                                                                                               \
     launch(k_primal_binned<G, false>, gp, stream, true, AT, binsT, v[Y], v[C], v[LO], v[UP], v[X], v[XP], v[X0], \
-           d_tau, ck, rho);                                                                               \
+           d_tau, ck, rho, InstanceMap{nullptr, nullptr});                                                \
   else                                                                                                    \
     launch(k_primal_binned<G, true>, gp, stream, true, AT, binsT, v[Y], v[C], v[LO], v[UP], v[X], v[XP], v[X0],  \
-           d_tau, ck, rho);
+           d_tau, ck, rho, InstanceMap{nullptr, nullptr});
         B2P_G_SWITCH(binsT.g, B2P_PRIMAL)
 #undef B2P_PRIMAL
       }
@@ -720,10 +646,10 @@ struct Engine {
 #define B2P_DUAL(G)                                                                                        \
   if (last)                                                                                                \
     launch(k_dual_binned<G, false>, gd, stream, true, A, binsA, v[XP], v[RL], v[RU], v[Y], v[YP], v[Y0], v[AX], \
-           v[AXP], v[AX0], d_sigma, ck, rho);                                                              \
+           v[AXP], v[AX0], d_sigma, ck, rho, InstanceMap{nullptr, nullptr});                               \
   else                                                                                                     \
     launch(k_dual_binned<G, true>, gd, stream, true, A, binsA, v[XP], v[RL], v[RU], v[Y], v[YP], v[Y0], v[AX],  \
-           v[AXP], v[AX0], d_sigma, ck, rho);
+           v[AXP], v[AX0], d_sigma, ck, rho, InstanceMap{nullptr, nullptr});
         B2P_G_SWITCH(binsA.g, B2P_DUAL)
 #undef B2P_DUAL
       }
@@ -731,7 +657,7 @@ struct Engine {
     }
     // A^T y+ for the dual residual, then the check reductions.
     if (n) {
-#define B2P_ATY(G) launch(k_spmv_binned<G>, gp, stream, false, AT, binsT, v[YP], v[ATYP]);
+#define B2P_ATY(G) launch(k_spmv_binned<G>, gp, stream, false, AT, binsT, v[YP], v[ATYP], InstanceMap{nullptr, nullptr});
       B2P_G_SWITCH(binsT.g, B2P_ATY)
 #undef B2P_ATY
     }

@@ -1,0 +1,733 @@
+// Many LPs of different sizes, each with its own A, solved together.
+//
+// The reference batches only cases that share one A (solvePdhgBatch,
+// src/pdhg/pdhg.cpp:719-728, k-interleaved vectors).  Uneven families -- many
+// independent LPs -- are solved here as ONE block-diagonal LP: the instances'
+// A (and A^T) are concatenated with row and column offsets, so every
+// iteration is a single pair of fused, row-binned SpMV kernels over all
+// instances (the same kernels as the single-LP fused form, with a per-row
+// instance id that selects the instance's tau, sigma and Halpern counter).
+// Each instance keeps its own scaling, step sizes, primal weight, restart
+// state and termination: the host takes the reference's decisions per
+// instance at every check, and a terminated instance's rows are skipped by
+// every kernel from then on.  Check reductions are segmented by instance with
+// a fixed block table, so results are deterministic; one check interval is
+// one CUDA graph.  Instance b's iterates are those of its own single solve up
+// to the rounding order of the sums.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <thread>
+#include <vector>
+
+#include "pdhg_host_common.h"
+#include "pdhg_kernels.cuh"
+#include "pdhg_prepare.h"
+#include "pdhg_sched.h"
+#include "pdhg_spmv.cuh"
+
+namespace b2p {
+
+constexpr int kSegRows = 2048;  // rows (or columns) per check-reduction block
+
+// Per check block: its instance and its [beg, end) range of global rows.
+struct SegTable {
+  const int32_t* __restrict__ inst;
+  const int32_t* __restrict__ beg;
+  const int32_t* __restrict__ end;
+};
+
+// Row part of the check for every live instance (see k_check_rows).
+__global__ void __launch_bounds__(kBlock) k_check_rows_multi(SegTable t, const int32_t* __restrict__ done,
+                                                             const double* __restrict__ axp,
+                                                             const double* __restrict__ rl,
+                                                             const double* __restrict__ ru,
+                                                             const double* __restrict__ yp,
+                                                             const double* __restrict__ y,
+                                                             const double* __restrict__ y0,
+                                                             const double* __restrict__ rfac,
+                                                             double* __restrict__ partial) {
+  __shared__ double sh[kRowSums * (kBlock / 32)];
+  double s[kRowSums] = {0, 0, 0, 0, 0};
+  const int blk = blockIdx.x;
+  if (!done[t.inst[blk]]) {
+    for (int i = t.beg[blk] + threadIdx.x; i < t.end[blk]; i += blockDim.x) {
+      const double a = axp[i], l = rl[i], u = ru[i];
+      double e1 = l - a, e2 = a - u;
+      e1 = (e1 < 0.0) ? 0.0 : e1;
+      e2 = (e2 < 0.0) ? 0.0 : e2;
+      const double res = (e1 + e2) * rfac[i];
+      s[0] += res * res;
+      const double yv = yp[i];
+      if (yv > 0.0 && l > -1e300)
+        s[1] += yv * l;
+      else if (yv < 0.0 && u < 1e300)
+        s[1] += yv * u;
+      s[2] += yv * yv;
+      const double d1 = y[i] - yv, d2 = yv - y0[i];
+      s[3] += d1 * d1;
+      s[4] += d2 * d2;
+    }
+  }
+  block_reduce<kRowSums>(s, sh);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < kRowSums; ++q) partial[blk * kRowSums + q] = s[q];
+}
+
+// Column part (A^T y+ precomputed by the binned SpMV).
+__global__ void __launch_bounds__(kBlock) k_check_cols_multi(SegTable t, const int32_t* __restrict__ done,
+                                                             const double* __restrict__ atyp,
+                                                             const double* __restrict__ xp,
+                                                             const double* __restrict__ x,
+                                                             const double* __restrict__ x0,
+                                                             const double* __restrict__ c,
+                                                             const double* __restrict__ lo,
+                                                             const double* __restrict__ up,
+                                                             const double* __restrict__ cfac,
+                                                             double* __restrict__ partial) {
+  __shared__ double sh[kRowSums * (kBlock / 32)];
+  double s[kRowSums] = {0, 0, 0, 0, 0};
+  const int blk = blockIdx.x;
+  if (!done[t.inst[blk]]) {
+    for (int j = t.beg[blk] + threadIdx.x; j < t.end[blk]; j += blockDim.x) {
+      const double cv = c[j], l = lo[j], u = up[j], xpv = xp[j];
+      const double d = cv - atyp[j];
+      const bool hl = l > -1e300, hu = u < 1e300;
+      double res = 0.0;
+      if (!hl && !hu)
+        res = fabs(d);
+      else if (!hl)
+        res = (d < 0.0) ? 0.0 : d;
+      else if (!hu)
+        res = (-d < 0.0) ? 0.0 : -d;
+      res *= cfac[j];
+      s[0] += res * res;
+      s[1] += cv * xpv;
+      if (d > 0.0 && hl)
+        s[2] += d * l;
+      else if (d < 0.0 && hu)
+        s[2] += d * u;
+      const double d1 = x[j] - xpv, d2 = xpv - x0[j];
+      s[3] += d1 * d1;
+      s[4] += d2 * d2;
+    }
+  }
+  block_reduce<kRowSums>(s, sh);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < kRowSums; ++q) partial[blk * kRowSums + q] = s[q];
+}
+
+// grid = instances: sums of the instance's blocks, in block order.
+__global__ void __launch_bounds__(kBlock) k_check_finalize_multi(const int32_t* __restrict__ rblk_off,
+                                                                 const int32_t* __restrict__ cblk_off,
+                                                                 const int32_t* __restrict__ done,
+                                                                 const double* __restrict__ prow,
+                                                                 const double* __restrict__ pcol,
+                                                                 double* __restrict__ out,
+                                                                 int64_t* __restrict__ it_base, int32_t L) {
+  __shared__ double sh[kNumSums * (kBlock / 32)];
+  const int b = blockIdx.x;
+  double s[kNumSums] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (!done[b]) {
+    for (int g = rblk_off[b] + threadIdx.x; g < rblk_off[b + 1]; g += blockDim.x)
+#pragma unroll
+      for (int q = 0; q < kRowSums; ++q) s[q] += prow[g * kRowSums + q];
+    for (int g = cblk_off[b] + threadIdx.x; g < cblk_off[b + 1]; g += blockDim.x)
+#pragma unroll
+      for (int q = 0; q < kRowSums; ++q) s[kRowSums + q] += pcol[g * kRowSums + q];
+  }
+  block_reduce<kNumSums>(s, sh);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < kNumSums; ++q) out[static_cast<int64_t>(b) * kNumSums + q] = s[q];
+    if (b == 0) *it_base += L;
+  }
+}
+
+// Deferred Halpern steps at a check iteration, per element's instance.
+__global__ void __launch_bounds__(kBlock) k_halpern_all_multi(int32_t n, int32_t m, const int32_t* __restrict__ cinst,
+                                                              const int32_t* __restrict__ rinst,
+                                                              const int32_t* __restrict__ done,
+                                                              double* __restrict__ x, const double* __restrict__ xp,
+                                                              const double* __restrict__ x0, double* __restrict__ y,
+                                                              const double* __restrict__ yp,
+                                                              const double* __restrict__ y0, double* __restrict__ ax,
+                                                              const double* __restrict__ axp,
+                                                              const double* __restrict__ ax0, IterClock ck,
+                                                              double rho) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t < n) {
+    const int b = cinst[t];
+    if (!done[b]) x[t] = halpern_step(x[t], xp[t], x0[t], halpern_lambda(ck, b), rho);
+  } else if (t < static_cast<int64_t>(n) + m) {
+    const int64_t u = t - n;
+    const int b = rinst[u];
+    if (!done[b]) {
+      const double lam = halpern_lambda(ck, b);
+      y[u] = halpern_step(y[u], yp[u], y0[u], lam, rho);
+      ax[u] = halpern_step(ax[u], axp[u], ax0[u], lam, rho);
+    }
+  }
+}
+
+// Masked restart per instance (src/pdhg/pdhg.cpp:153-165).
+__global__ void __launch_bounds__(kBlock) k_restart_multi(int32_t n, int32_t m, int32_t k,
+                                                          const int32_t* __restrict__ cinst,
+                                                          const int32_t* __restrict__ rinst,
+                                                          const int32_t* __restrict__ mask, double* __restrict__ x,
+                                                          double* __restrict__ x0, const double* __restrict__ xp,
+                                                          double* __restrict__ y, double* __restrict__ y0,
+                                                          const double* __restrict__ yp, double* __restrict__ ax,
+                                                          double* __restrict__ ax0, const double* __restrict__ axp,
+                                                          const int64_t* __restrict__ it_base,
+                                                          int64_t* __restrict__ restart_at) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t < k && mask[t]) restart_at[t] = *it_base;
+  if (t < n) {
+    if (mask[cinst[t]]) x[t] = x0[t] = xp[t];
+  } else if (t < static_cast<int64_t>(n) + m) {
+    const int64_t u = t - n;
+    if (mask[rinst[u]]) {
+      y[u] = y0[u] = yp[u];
+      ax[u] = ax0[u] = axp[u];
+    }
+  }
+}
+
+namespace {
+
+enum MSlot : int { MX, MXP, MX0, MC, MLO, MUP, MXINIT, MATYP, MNCOL, MY = MNCOL, MYP, MY0, MAX, MAXP, MAX0, MRL, MRU,
+                   MAXINIT, MNSLOT };
+
+struct MultiEngine {
+  int device = 0;
+  int K = 0;
+  b2p_options opt{};
+  std::vector<Prepared> P;
+  std::vector<int64_t> roff, coff;  // row / column offsets of instance b
+  int32_t M = 0, N = 0;
+  std::vector<double> cNorm, rhsNorm, omega0, eta;
+  cudaStream_t stream = nullptr;
+  std::vector<void*> allocs;
+  int32_t *dA_ptr = nullptr, *dA_idx = nullptr, *dT_ptr = nullptr, *dT_idx = nullptr;
+  double *dA_val = nullptr, *dT_val = nullptr, *d_rfac = nullptr, *d_cfac = nullptr;
+  double* v[MNSLOT] = {};
+  int32_t *d_rinst = nullptr, *d_cinst = nullptr, *d_done = nullptr, *d_mask = nullptr;
+  double *d_tau = nullptr, *d_sigma = nullptr, *d_prow = nullptr, *d_pcol = nullptr, *d_sums = nullptr;
+  int64_t *d_it_base = nullptr, *d_restart_at = nullptr;
+  SegTable rtab{}, ctab{};
+  int32_t *d_rblk_off = nullptr, *d_cblk_off = nullptr;
+  int g_rows = 0, g_cols = 0;
+  RowBins binsA{}, binsT{};
+  double* h_sums = nullptr;
+  double* h_steps = nullptr;
+  int32_t *h_mask = nullptr, *h_done = nullptr;
+  std::map<int, cudaGraphExec_t> graphs;
+  std::map<int, cudaGraph_t> graph_defs;
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+  b2p_stats stats{};
+  std::vector<b2p_result> results;
+  std::vector<std::vector<double>> xs, ys;  // per instance, original space
+  int64_t launches = 0, bytes_up = 0, bytes_down = 0;
+
+  template <class T>
+  T* dalloc(size_t count) {
+    void* p = nullptr;
+    B2P_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    allocs.push_back(p);
+    return static_cast<T*>(p);
+  }
+  template <class T>
+  T* upload(const std::vector<T>& h) {
+    T* d = dalloc<T>(h.size());
+    if (!h.empty()) B2P_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+    bytes_up += static_cast<int64_t>(h.size() * sizeof(T));
+    return d;
+  }
+  static unsigned blocks(int64_t len) { return static_cast<unsigned>(std::max<int64_t>(1, (len + kBlock - 1) / kBlock)); }
+  CsrView viewA() const { return CsrView{dA_ptr, dA_idx, dA_val, M}; }
+  CsrView viewAT() const { return CsrView{dT_ptr, dT_idx, dT_val, N}; }
+
+  ~MultiEngine() {
+    for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+    for (auto& g : graph_defs) cudaGraphDestroy(g.second);
+    if (ev_start) cudaEventDestroy(ev_start);
+    if (ev_stop) cudaEventDestroy(ev_stop);
+    for (void* p : allocs) cudaFree(p);
+    if (h_sums) cudaFreeHost(h_sums);
+    if (h_steps) cudaFreeHost(h_steps);
+    if (h_mask) cudaFreeHost(h_mask);
+    if (h_done) cudaFreeHost(h_done);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  void create(const b2p_lp* lps, int num, const b2p_options* o) {
+    if (!lps || num <= 0) throw Error(B2P_ERR_INVALID, "no LPs");
+    for (int b = 0; b < num; ++b) check_lp(&lps[b]);
+    if (o) opt = *o; else b2p_default_options(&opt);
+    if (opt.check_every <= 0) throw Error(B2P_ERR_INVALID, "check_every must be positive");
+    device = pick_device(opt.device);
+    B2P_CUDA(cudaSetDevice(device));
+    B2P_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    B2P_CUDA(cudaEventCreate(&ev_start));
+    B2P_CUDA(cudaEventCreate(&ev_stop));
+    K = num;
+    const auto t0 = Clock::now();
+    // ---- host preparation of every instance, on all host threads ----
+    P.resize(K);
+    PrepareOptions po;
+    po.ruiz_iterations = opt.ruiz_iterations;
+    po.pock_chambolle = opt.pock_chambolle != 0;
+    po.rescale = opt.rescale_objective_and_bounds != 0;
+    po.norm_on_host = true;
+    std::atomic<int> next{0};
+    const int nth = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), static_cast<unsigned>(K)));
+    std::vector<std::thread> pool;
+    std::vector<std::string> errs(nth);
+    for (int t = 0; t < nth; ++t)
+      pool.emplace_back([&, t] {
+        try {
+          for (int b; (b = next.fetch_add(1)) < K;) {
+            const b2p_lp& l = lps[b];
+            P[b] = prepare(l.num_rows, l.num_cols, l.start, l.index, l.value, l.col_cost, l.row_lower, l.row_upper,
+                           l.obj_offset, po);
+          }
+        } catch (std::exception& e) {
+          errs[t] = e.what();
+        }
+      });
+    for (auto& th : pool) th.join();
+    for (auto& e : errs)
+      if (!e.empty()) throw Error(B2P_ERR_INVALID, e);
+    stats.prepare_seconds = seconds_since(t0);
+    // ---- block-diagonal concatenation ----
+    roff.assign(K + 1, 0);
+    coff.assign(K + 1, 0);
+    int64_t annz = 0;
+    for (int b = 0; b < K; ++b) {
+      roff[b + 1] = roff[b] + P[b].m;
+      coff[b + 1] = coff[b] + P[b].n;
+      annz += static_cast<int64_t>(P[b].A.val.size());
+    }
+    if (roff[K] >= INT32_MAX || coff[K] >= INT32_MAX || annz >= INT32_MAX)
+      throw Error(B2P_ERR_TOO_LARGE, "family exceeds 2^31 rows, columns or nonzeros");
+    M = static_cast<int32_t>(roff[K]);
+    N = static_cast<int32_t>(coff[K]);
+    HostCsr A, AT;
+    A.rows = M;
+    A.cols = N;
+    AT.rows = N;
+    AT.cols = M;
+    A.ptr.reserve(static_cast<size_t>(M) + 1);
+    AT.ptr.reserve(static_cast<size_t>(N) + 1);
+    A.ptr.push_back(0);
+    AT.ptr.push_back(0);
+    A.idx.reserve(annz);
+    A.val.reserve(annz);
+    AT.idx.reserve(annz);
+    AT.val.reserve(annz);
+    std::vector<int32_t> rinst(M), cinst(N);
+    std::vector<double> rfac(M), cfac(N), c(N), lo(N), up(N), rl(M), ru(M), x0(N);
+    cNorm.assign(K, 0);
+    rhsNorm.assign(K, 0);
+    omega0.assign(K, 1.0);
+    eta.assign(K, 0);
+    for (int b = 0; b < K; ++b) {
+      const Prepared& p = P[b];
+      const b2p_lp& l = lps[b];
+      const int32_t base_a = A.ptr.back(), base_t = AT.ptr.back();
+      for (int32_t i = 0; i < p.m; ++i) A.ptr.push_back(base_a + p.A.ptr[i + 1]);
+      for (size_t q = 0; q < p.A.idx.size(); ++q) {
+        A.idx.push_back(static_cast<int32_t>(coff[b]) + p.A.idx[q]);
+        A.val.push_back(p.A.val[q]);
+      }
+      for (int32_t j = 0; j < p.n; ++j) AT.ptr.push_back(base_t + p.AT.ptr[j + 1]);
+      for (size_t q = 0; q < p.AT.idx.size(); ++q) {
+        AT.idx.push_back(static_cast<int32_t>(roff[b]) + p.AT.idx[q]);
+        AT.val.push_back(p.AT.val[q]);
+      }
+      // scaled case vectors (src/pdhg/pdhg.cpp:466-481, 506-530), k = 1 per instance
+      double s = 0;
+      for (int32_t j = 0; j < p.n; ++j) s += l.col_cost[j] * l.col_cost[j];
+      cNorm[b] = std::sqrt(s);
+      s = 0;
+      for (int32_t i = 0; i < p.m; ++i) {
+        if (finite_bound(l.row_lower[i])) s += l.row_lower[i] * l.row_lower[i];
+        if (finite_bound(l.row_upper[i]) && l.row_upper[i] != l.row_lower[i]) s += l.row_upper[i] * l.row_upper[i];
+      }
+      rhsNorm[b] = std::sqrt(s);
+      double cn = 0, bn = 0;
+      for (int32_t j = 0; j < p.n; ++j) {
+        const size_t t = static_cast<size_t>(coff[b] + j);
+        cinst[t] = b;
+        cfac[t] = p.cfac[j];
+        c[t] = l.col_cost[j] * p.Cs[j] / p.gamma;
+        lo[t] = finite_bound(l.col_lower[j]) ? l.col_lower[j] / p.Cs[j] / p.beta : -HUGE_VAL;
+        up[t] = finite_bound(l.col_upper[j]) ? l.col_upper[j] / p.Cs[j] / p.beta : HUGE_VAL;
+        x0[t] = smin(smax(0.0, lo[t]), up[t]);
+        cn += c[t] * c[t];
+      }
+      for (int32_t i = 0; i < p.m; ++i) {
+        const size_t t = static_cast<size_t>(roff[b] + i);
+        rinst[t] = b;
+        rfac[t] = p.rfac[i];
+        rl[t] = finite_bound(l.row_lower[i]) ? l.row_lower[i] * p.R[i] / p.beta : -HUGE_VAL;
+        ru[t] = finite_bound(l.row_upper[i]) ? l.row_upper[i] * p.R[i] / p.beta : HUGE_VAL;
+        if (finite_bound(rl[t])) bn += rl[t] * rl[t];
+        if (finite_bound(ru[t]) && ru[t] != rl[t]) bn += ru[t] * ru[t];
+      }
+      if (cn > 1e-20 && bn > 1e-20) omega0[b] = std::sqrt(cn) / std::sqrt(bn);
+      eta[b] = 0.998 / p.normA;
+    }
+    // ---- device ----
+    const auto tx = Clock::now();
+    dA_ptr = upload(A.ptr);
+    dA_idx = upload(A.idx);
+    dA_val = upload(A.val);
+    dT_ptr = upload(AT.ptr);
+    dT_idx = upload(AT.idx);
+    dT_val = upload(AT.val);
+    d_rfac = upload(rfac);
+    d_cfac = upload(cfac);
+    d_rinst = upload(rinst);
+    d_cinst = upload(cinst);
+    for (int q = 0; q < MNSLOT; ++q) v[q] = dalloc<double>(q >= MY ? M : N);
+    auto put = [&](int q, const std::vector<double>& h) {
+      if (!h.empty()) B2P_CUDA(cudaMemcpyAsync(v[q], h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+      bytes_up += static_cast<int64_t>(h.size() * sizeof(double));
+    };
+    put(MC, c);
+    put(MLO, lo);
+    put(MUP, up);
+    put(MRL, rl);
+    put(MRU, ru);
+    put(MXINIT, x0);
+    d_tau = dalloc<double>(K);
+    d_sigma = dalloc<double>(K);
+    d_it_base = dalloc<int64_t>(1);
+    d_restart_at = dalloc<int64_t>(K);
+    d_done = dalloc<int32_t>(K);
+    d_mask = dalloc<int32_t>(K);
+    // segmented check tables
+    auto seg = [&](const std::vector<int64_t>& off, SegTable& tab, int32_t*& dofs, int& g) {
+      std::vector<int32_t> inst, beg, end, bo(K + 1, 0);
+      for (int b = 0; b < K; ++b) {
+        bo[b] = static_cast<int32_t>(inst.size());
+        for (int64_t s0 = off[b]; s0 < off[b + 1]; s0 += kSegRows) {
+          inst.push_back(b);
+          beg.push_back(static_cast<int32_t>(s0));
+          end.push_back(static_cast<int32_t>(std::min<int64_t>(off[b + 1], s0 + kSegRows)));
+        }
+      }
+      bo[K] = static_cast<int32_t>(inst.size());
+      g = static_cast<int>(inst.size());
+      tab = SegTable{upload(inst), upload(beg), upload(end)};
+      dofs = upload(bo);
+    };
+    seg(roff, rtab, d_rblk_off, g_rows);
+    seg(coff, ctab, d_cblk_off, g_cols);
+    d_prow = dalloc<double>(static_cast<size_t>(std::max(1, g_rows)) * kRowSums);
+    d_pcol = dalloc<double>(static_cast<size_t>(std::max(1, g_cols)) * kRowSums);
+    d_sums = dalloc<double>(static_cast<size_t>(K) * kNumSums);
+    B2P_CUDA(cudaMallocHost(&h_sums, sizeof(double) * K * kNumSums));
+    B2P_CUDA(cudaMallocHost(&h_steps, sizeof(double) * 2 * K));
+    B2P_CUDA(cudaMallocHost(&h_mask, sizeof(int32_t) * K));
+    B2P_CUDA(cudaMallocHost(&h_done, sizeof(int32_t) * K));
+    // fused-kernel schedules of the concatenated operators
+    int per_sm = 0, sms = 0;
+    B2P_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dual_binned<4, true, true>, kBlock, 0));
+    B2P_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int64_t wave = static_cast<int64_t>(std::max(1, per_sm)) * sms * kBlock;
+    const int rounds = opt.short_row_rounds > 0 ? opt.short_row_rounds : 2;
+    binsA = device_bins(make_bins(A, wave, opt.lanes_per_row_a, rounds), M);
+    binsT = device_bins(make_bins(AT, wave, opt.lanes_per_row_at, rounds), N);
+    stats.lanes_per_row_a = binsA.g;
+    stats.lanes_per_row_at = binsT.g;
+    if (M > 0) {
+      k_spmv<<<blocks(M), kBlock, 0, stream>>>(M, 1, viewA(), v[MXINIT], v[MAXINIT]);
+      B2P_CUDA(cudaGetLastError());
+    }
+    B2P_CUDA(cudaStreamSynchronize(stream));
+    stats.upload_seconds = seconds_since(tx);
+    stats.setup_seconds = seconds_since(t0);
+    stats.kernel_mode = B2P_KERNELS_FUSED;
+    stats.precision_used = B2P_PRECISION_FP64;
+  }
+
+  RowBins device_bins(const HostBins& hb, int32_t rows) {
+    RowBins b{};
+    b.long_rows = upload(hb.long_rows);
+    b.vlong_rows = upload(hb.vlong_rows);
+    b.n_long = static_cast<int32_t>(hb.long_rows.size());
+    b.n_vlong = static_cast<int32_t>(hb.vlong_rows.size());
+    b.long_thr = hb.long_thr;
+    b.vlong_blocks = b.n_vlong;
+    b.long_blocks = (b.n_long + kBlock / 32 - 1) / (kBlock / 32);
+    b.short_blocks = static_cast<int32_t>((static_cast<int64_t>(rows) * hb.g + kBlock - 1) / kBlock);
+    b.g = hb.g;
+    return b;
+  }
+  static unsigned bin_grid(const RowBins& b) {
+    return static_cast<unsigned>(std::max(1, b.vlong_blocks + b.long_blocks + b.short_blocks));
+  }
+
+  void upload_steps(const std::vector<double>& omega) {
+    for (int b = 0; b < K; ++b) {
+      h_steps[b] = eta[b] / omega[b];
+      h_steps[K + b] = eta[b] * omega[b];
+    }
+    B2P_CUDA(cudaMemcpyAsync(d_tau, h_steps, sizeof(double) * K, cudaMemcpyHostToDevice, stream));
+    B2P_CUDA(cudaMemcpyAsync(d_sigma, h_steps + K, sizeof(double) * K, cudaMemcpyHostToDevice, stream));
+    bytes_up += static_cast<int64_t>(2 * K * sizeof(double));
+  }
+
+  void enqueue_interval(int L) {
+    const double rho = opt.reflection;
+    const CsrView A = viewA(), AT = viewAT();
+    const InstanceMap imc{d_cinst, d_done}, imr{d_rinst, d_done};
+    const unsigned gp = bin_grid(binsT), gd = bin_grid(binsA);
+    for (int l = 0; l < L; ++l) {
+      const bool last = l == L - 1;
+      const IterClock ck{d_it_base, d_restart_at, l};
+      if (N) {
+#define B2P_MPRIMAL(G)                                                                                       \
+  if (last)                                                                                                  \
+    launch(k_primal_binned<G, false, true>, gp, stream, true, AT, binsT, v[MY], v[MC], v[MLO], v[MUP], v[MX], \
+           v[MXP], v[MX0], d_tau, ck, rho, imc);                                                             \
+  else                                                                                                       \
+    launch(k_primal_binned<G, true, true>, gp, stream, true, AT, binsT, v[MY], v[MC], v[MLO], v[MUP], v[MX],  \
+           v[MXP], v[MX0], d_tau, ck, rho, imc);
+        B2P_G_SWITCH(binsT.g, B2P_MPRIMAL)
+#undef B2P_MPRIMAL
+      }
+      if (M) {
+#define B2P_MDUAL(G)                                                                                         \
+  if (last)                                                                                                  \
+    launch(k_dual_binned<G, false, true>, gd, stream, true, A, binsA, v[MXP], v[MRL], v[MRU], v[MY], v[MYP],  \
+           v[MY0], v[MAX], v[MAXP], v[MAX0], d_sigma, ck, rho, imr);                                         \
+  else                                                                                                       \
+    launch(k_dual_binned<G, true, true>, gd, stream, true, A, binsA, v[MXP], v[MRL], v[MRU], v[MY], v[MYP],   \
+           v[MY0], v[MAX], v[MAXP], v[MAX0], d_sigma, ck, rho, imr);
+        B2P_G_SWITCH(binsA.g, B2P_MDUAL)
+#undef B2P_MDUAL
+      }
+    }
+    if (N) {
+#define B2P_MATY(G) launch(k_spmv_binned<G, true>, gp, stream, false, AT, binsT, v[MYP], v[MATYP], imc);
+      B2P_G_SWITCH(binsT.g, B2P_MATY)
+#undef B2P_MATY
+    }
+    const IterClock ck{d_it_base, d_restart_at, L - 1};
+    if (g_rows)
+      k_check_rows_multi<<<g_rows, kBlock, 0, stream>>>(rtab, d_done, v[MAXP], v[MRL], v[MRU], v[MYP], v[MY], v[MY0],
+                                                        d_rfac, d_prow);
+    if (g_cols)
+      k_check_cols_multi<<<g_cols, kBlock, 0, stream>>>(ctab, d_done, v[MATYP], v[MXP], v[MX], v[MX0], v[MC], v[MLO],
+                                                        v[MUP], d_cfac, d_pcol);
+    k_halpern_all_multi<<<blocks(static_cast<int64_t>(N) + M), kBlock, 0, stream>>>(
+        N, M, d_cinst, d_rinst, d_done, v[MX], v[MXP], v[MX0], v[MY], v[MYP], v[MY0], v[MAX], v[MAXP], v[MAX0], ck, rho);
+    k_check_finalize_multi<<<K, kBlock, 0, stream>>>(d_rblk_off, d_cblk_off, d_done, d_prow, d_pcol, d_sums, d_it_base,
+                                                     L);
+    B2P_CUDA(cudaGetLastError());
+    B2P_CUDA(cudaMemcpyAsync(h_sums, d_sums, sizeof(double) * K * kNumSums, cudaMemcpyDeviceToHost, stream));
+  }
+
+  void run_interval(int L) {
+    if (opt.use_graphs) {
+      auto it = graphs.find(L);
+      if (it == graphs.end()) {
+        const auto tg = Clock::now();
+        cudaGraph_t g;
+        B2P_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        try {
+          enqueue_interval(L);
+        } catch (...) {
+          cudaStreamEndCapture(stream, &g);
+          if (g) cudaGraphDestroy(g);
+          throw;
+        }
+        B2P_CUDA(cudaStreamEndCapture(stream, &g));
+        cudaGraphExec_t ge;
+        B2P_CUDA(cudaGraphInstantiate(&ge, g, 0));
+        graph_defs[L] = g;
+        it = graphs.emplace(L, ge).first;
+        stats.graph_seconds += seconds_since(tg);
+      }
+      B2P_CUDA(cudaGraphLaunch(it->second, stream));
+    } else {
+      enqueue_interval(L);
+    }
+    launches += static_cast<int64_t>(L) * 2 + 5;
+    bytes_down += static_cast<int64_t>(sizeof(double) * K * kNumSums);
+  }
+
+  void extract(int b, int status, double relKkt, double pobj, double dobj, int64_t it) {
+    const Prepared& p = P[b];
+    std::vector<double> xp(p.n), yp(p.m);
+    if (p.n)
+      B2P_CUDA(cudaMemcpyAsync(xp.data(), v[MXP] + coff[b], sizeof(double) * p.n, cudaMemcpyDeviceToHost, stream));
+    if (p.m)
+      B2P_CUDA(cudaMemcpyAsync(yp.data(), v[MYP] + roff[b], sizeof(double) * p.m, cudaMemcpyDeviceToHost, stream));
+    B2P_CUDA(cudaStreamSynchronize(stream));
+    bytes_down += static_cast<int64_t>(sizeof(double) * (p.n + p.m));
+    xs[b].resize(p.n);
+    ys[b].resize(p.m);
+    for (int32_t j = 0; j < p.n; ++j) xs[b][j] = xp[j] * p.Cs[j] * p.beta;
+    for (int32_t i = 0; i < p.m; ++i) ys[b][i] = yp[i] * p.R[i] * p.gamma;
+    b2p_result& r = results[b];
+    r.status = status;
+    r.iterations = it;
+    r.relative_kkt = relKkt;
+    r.objective = pobj + p.offset;
+    r.dual_objective = dobj + p.offset;
+  }
+
+  // runPdhg's loop for every instance at once (src/pdhg/pdhg.cpp:560-687).
+  void solve(Clock::time_point deadline_start) {
+    B2P_CUDA(cudaSetDevice(device));
+    const auto t_solve = Clock::now();
+    launches = 0;
+    // initial state
+    auto cp = [&](int dst, int src, int64_t len) {
+      if (len) B2P_CUDA(cudaMemcpyAsync(v[dst], v[src], len * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    };
+    cp(MX, MXINIT, N);
+    cp(MX0, MXINIT, N);
+    cp(MAX, MAXINIT, M);
+    cp(MAX0, MAXINIT, M);
+    if (M) {
+      B2P_CUDA(cudaMemsetAsync(v[MY], 0, sizeof(double) * M, stream));
+      B2P_CUDA(cudaMemsetAsync(v[MY0], 0, sizeof(double) * M, stream));
+    }
+    B2P_CUDA(cudaMemsetAsync(d_it_base, 0, sizeof(int64_t), stream));
+    B2P_CUDA(cudaMemsetAsync(d_restart_at, 0, sizeof(int64_t) * K, stream));
+    B2P_CUDA(cudaMemsetAsync(d_done, 0, sizeof(int32_t) * K, stream));
+    std::vector<double> omega = omega0;
+    upload_steps(omega);
+    results.assign(K, b2p_result{});
+    xs.assign(K, {});
+    ys.assign(K, {});
+    stats.restarts = 0;
+    std::vector<char> done(K, 0);
+    std::vector<double> fpRestart(K, INFINITY), fpPrev(K, INFINITY);
+    std::vector<int64_t> sinceRestart(K, 0);
+    int remaining = K;
+    const int cE = opt.check_every;
+    auto expired = [&]() {
+      if (opt.cancel_flag && *opt.cancel_flag) return true;
+      return opt.time_limit > 0 && seconds_since(deadline_start) >= opt.time_limit;
+    };
+    B2P_CUDA(cudaEventRecord(ev_start, stream));
+    int64_t it = 0;
+    bool expiredStop = false;
+    while (it < opt.max_iterations) {
+      const int L = static_cast<int>(std::min<int64_t>(cE, opt.max_iterations - it));
+      run_interval(L);
+      B2P_CUDA(cudaStreamSynchronize(stream));
+      it += L - 1;
+      bool anyRestart = false, anyDone = false;
+      for (int b = 0; b < K; ++b) h_mask[b] = 0;
+      for (int b = 0; b < K; ++b) {
+        if (done[b]) continue;
+        const double* s = h_sums + static_cast<size_t>(b) * kNumSums;
+        const double scaleObj = P[b].beta * P[b].gamma;
+        const double pobj = s[CS_POBJ] * scaleObj;
+        const double dobj = (s[CS_ROW_DOBJ] + s[CS_COL_DOBJ]) * scaleObj;
+        const double relP = std::sqrt(s[CS_ROW_RES2]) / (1.0 + rhsNorm[b]);
+        const double relD = std::sqrt(s[CS_COL_RES2]) / (1.0 + cNorm[b]);
+        const double gap = std::fabs(pobj - dobj) / (1.0 + std::fabs(pobj) + std::fabs(dobj));
+        if (relP <= opt.tolerance && relD <= opt.tolerance && gap <= opt.tolerance) {
+          extract(b, B2P_STATUS_OPTIMAL, smax(relP, smax(relD, gap)), pobj, dobj, it);
+          done[b] = 1;
+          anyDone = true;
+          --remaining;
+          continue;
+        }
+        sinceRestart[b] += cE;
+        const double fp = std::sqrt(omega[b] * s[CS_DX2] + s[CS_DY2] / omega[b]);
+        if (fpRestart[b] == INFINITY) fpRestart[b] = fp;
+        const bool restart = fp <= 0.2 * fpRestart[b] || (fp <= 0.8 * fpRestart[b] && fp > fpPrev[b]) ||
+                             sinceRestart[b] >= static_cast<int64_t>(0.36 * static_cast<double>(it + 1));
+        fpPrev[b] = fp;
+        if (restart) {
+          h_mask[b] = 1;
+          anyRestart = true;
+          const double dxn = std::sqrt(s[CS_AX2]), dyn = std::sqrt(s[CS_AY2]);
+          if (dxn > 1e-10 && dyn > 1e-10) omega[b] = std::exp(0.5 * std::log(dyn / dxn) + 0.5 * std::log(omega[b]));
+          fpRestart[b] = std::sqrt(omega[b] * s[CS_DX2] + s[CS_DY2] / omega[b]);
+          fpPrev[b] = INFINITY;
+          sinceRestart[b] = 0;
+          stats.restarts++;
+        }
+      }
+      if (anyRestart) upload_steps(omega);
+      if (remaining == 0) break;
+      if (expired()) {
+        expiredStop = true;
+        break;
+      }
+      if (anyDone) {
+        for (int b = 0; b < K; ++b) h_done[b] = done[b];
+        B2P_CUDA(cudaMemcpyAsync(d_done, h_done, sizeof(int32_t) * K, cudaMemcpyHostToDevice, stream));
+      }
+      if (anyRestart) {
+        B2P_CUDA(cudaMemcpyAsync(d_mask, h_mask, sizeof(int32_t) * K, cudaMemcpyHostToDevice, stream));
+        k_restart_multi<<<blocks(std::max<int64_t>(static_cast<int64_t>(N) + M, K)), kBlock, 0, stream>>>(
+            N, M, K, d_cinst, d_rinst, d_mask, v[MX], v[MX0], v[MXP], v[MY], v[MY0], v[MYP], v[MAX], v[MAX0],
+            v[MAXP], d_it_base, d_restart_at);
+        B2P_CUDA(cudaGetLastError());
+        ++launches;
+      }
+      ++it;
+    }
+    B2P_CUDA(cudaEventRecord(ev_stop, stream));
+    B2P_CUDA(cudaEventSynchronize(ev_stop));
+    float ms = 0;
+    B2P_CUDA(cudaEventElapsedTime(&ms, ev_start, ev_stop));
+    stats.kernel_seconds = ms / 1000.0;
+    stats.solve_seconds = seconds_since(t_solve);
+    stats.iterations = it + (remaining == 0 ? 1 : 0);
+    stats.primal_weight = omega.empty() ? 1 : omega[0];
+    for (int b = 0; b < K; ++b) {
+      if (done[b]) continue;
+      const double* s = h_sums + static_cast<size_t>(b) * kNumSums;
+      const double scaleObj = P[b].beta * P[b].gamma;
+      const double pobj = s[CS_POBJ] * scaleObj, dobj = (s[CS_ROW_DOBJ] + s[CS_COL_DOBJ]) * scaleObj;
+      const double relP = std::sqrt(s[CS_ROW_RES2]) / (1 + rhsNorm[b]);
+      const double relD = std::sqrt(s[CS_COL_RES2]) / (1 + cNorm[b]);
+      const double gap = std::fabs(pobj - dobj) / (1 + std::fabs(pobj) + std::fabs(dobj));
+      extract(b, (expiredStop || expired()) ? B2P_STATUS_TIME_LIMIT : B2P_STATUS_ITERATION_LIMIT,
+              smax(relP, smax(relD, gap)), pobj, dobj, it);
+    }
+    stats.kernel_launches = launches;
+    stats.bytes_uploaded = bytes_up;
+    stats.bytes_downloaded = bytes_down;
+  }
+};
+
+}  // namespace
+}  // namespace b2p
+
+extern "C" int b2p_solve_pdhg_multi(const b2p_lp* lps, int32_t num_lps, const b2p_options* opts, double* const* x,
+                                    double* const* row_dual, b2p_result* results, b2p_stats* stats) {
+  using namespace b2p;
+  return guarded([&] {
+    const auto t0 = Clock::now();
+    MultiEngine e;
+    e.create(lps, num_lps, opts);
+    e.solve(t0);
+    for (int b = 0; b < e.K; ++b) {
+      if (x && x[b] && !e.xs[b].empty()) std::memcpy(x[b], e.xs[b].data(), sizeof(double) * e.xs[b].size());
+      if (row_dual && row_dual[b] && !e.ys[b].empty())
+        std::memcpy(row_dual[b], e.ys[b].data(), sizeof(double) * e.ys[b].size());
+      if (results) results[b] = e.results[b];
+    }
+    if (stats) *stats = e.stats;
+  });
+}

@@ -43,6 +43,14 @@ struct RowBins {
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" :::); }
 
+// Several LPs solved together as one block-diagonal operator: inst[row] is
+// the row's instance, done[instance] != 0 once that instance has terminated
+// (its rows are then skipped).  Unused (null) for a single LP.
+struct InstanceMap {
+  const int32_t* __restrict__ inst;
+  const int32_t* __restrict__ done;
+};
+
 // What one thread does for its row: entries beg+lane0, +stride, ... < end.
 struct RowPlan {
   int32_t row;     // -1: no row
@@ -56,8 +64,8 @@ struct RowPlan {
 };
 
 // Pre-wait part: row assignment and the first kUnroll (index, value) pairs.
-template <int G>
-__device__ __forceinline__ RowPlan plan_row(const CsrView& M, const RowBins& bins) {
+template <int G, bool MULTI = false>
+__device__ __forceinline__ RowPlan plan_row(const CsrView& M, const RowBins& bins, InstanceMap im = {nullptr, nullptr}) {
   RowPlan pl;
   pl.row = -1;
   pl.p = 0;
@@ -96,6 +104,10 @@ __device__ __forceinline__ RowPlan plan_row(const CsrView& M, const RowBins& bin
         pl.leader = (threadIdx.x & (G - 1)) == 0;
       }
     }
+  }
+  if (MULTI && pl.row >= 0 && im.done[im.inst[pl.row]]) {
+    pl.end = pl.p;  // terminated instance: no work
+    pl.leader = false;
   }
 #pragma unroll
   for (int u = 0; u < kUnroll; ++u) {
@@ -154,16 +166,19 @@ __device__ __forceinline__ double finish_row(const RowPlan& pl, const CsrView& M
 }
 
 // x+ = proj(x - tau (c - A^T y)), Halpern step of x (skipped at a check
-// iteration).  One LP; A^T rows binned.
-template <int G, bool HALPERN>
+// iteration).  A^T rows binned.  MULTI: several LPs, per-row instance b
+// selects tau[b] and the Halpern counter of b.
+template <int G, bool HALPERN, bool MULTI = false>
 __global__ void __launch_bounds__(kBlock) k_primal_binned(CsrView AT, RowBins bins, const double* __restrict__ y,
                                                           const double* __restrict__ c, const double* __restrict__ lo,
                                                           const double* __restrict__ up, double* __restrict__ x,
                                                           double* __restrict__ xp, const double* __restrict__ x0,
-                                                          const double* __restrict__ tau, IterClock ck, double rho) {
+                                                          const double* __restrict__ tau, IterClock ck, double rho,
+                                                          InstanceMap im = {nullptr, nullptr}) {
   __shared__ double sh[kBlock / 32];
-  const RowPlan pl = plan_row<G>(AT, bins);
+  const RowPlan pl = plan_row<G, MULTI>(AT, bins, im);
   const int j = pl.row;
+  const int b = (MULTI && pl.leader) ? im.inst[j] : 0;
   double cj = 0, l = 0, u = 0;
   if (pl.leader) {
     cj = __ldg(c + j);
@@ -174,10 +189,10 @@ __global__ void __launch_bounds__(kBlock) k_primal_binned(CsrView AT, RowBins bi
   double xv = 0, x0v = 0, t = 0, lam = 0;
   if (pl.leader) {
     xv = __ldcg(x + j);
-    t = __ldcg(tau);
+    t = __ldcg(tau + b);
     if (HALPERN) {
       x0v = __ldcg(x0 + j);
-      lam = halpern_lambda(ck, 0);
+      lam = halpern_lambda(ck, b);
     }
   }
   const double aty = finish_row<G>(pl, AT, y, sh);
@@ -191,16 +206,18 @@ __global__ void __launch_bounds__(kBlock) k_primal_binned(CsrView AT, RowBins bi
 }
 
 // y+ = v + sigma proj(-v/sigma), v = y - sigma (2 A x+ - A x); Halpern steps of y and Ax.
-template <int G, bool HALPERN>
+template <int G, bool HALPERN, bool MULTI = false>
 __global__ void __launch_bounds__(kBlock) k_dual_binned(CsrView A, RowBins bins, const double* __restrict__ xp,
                                                         const double* __restrict__ rl, const double* __restrict__ ru,
                                                         double* __restrict__ y, double* __restrict__ yp,
                                                         const double* __restrict__ y0, double* __restrict__ ax,
                                                         double* __restrict__ axp, const double* __restrict__ ax0,
-                                                        const double* __restrict__ sigma, IterClock ck, double rho) {
+                                                        const double* __restrict__ sigma, IterClock ck, double rho,
+                                                        InstanceMap im = {nullptr, nullptr}) {
   __shared__ double sh[kBlock / 32];
-  const RowPlan pl = plan_row<G>(A, bins);
+  const RowPlan pl = plan_row<G, MULTI>(A, bins, im);
   const int i = pl.row;
+  const int b = (MULTI && pl.leader) ? im.inst[i] : 0;
   double l = 0, u = 0;
   if (pl.leader) {
     l = __ldg(rl + i);
@@ -211,11 +228,11 @@ __global__ void __launch_bounds__(kBlock) k_dual_binned(CsrView A, RowBins bins,
   if (pl.leader) {
     axv = __ldcg(ax + i);
     yv = __ldcg(y + i);
-    s = __ldcg(sigma);
+    s = __ldcg(sigma + b);
     if (HALPERN) {
       y0v = __ldcg(y0 + i);
       ax0v = __ldcg(ax0 + i);
-      lam = halpern_lambda(ck, 0);
+      lam = halpern_lambda(ck, b);
     }
   }
   const double axpv = finish_row<G>(pl, A, xp, sh);
@@ -235,11 +252,11 @@ __global__ void __launch_bounds__(kBlock) k_dual_binned(CsrView A, RowBins bins,
 }
 
 // out = M x with the binned schedule (used for A^T y+ at a check).
-template <int G>
+template <int G, bool MULTI = false>
 __global__ void __launch_bounds__(kBlock) k_spmv_binned(CsrView M, RowBins bins, const double* __restrict__ x,
-                                                        double* __restrict__ out) {
+                                                        double* __restrict__ out, InstanceMap im = {nullptr, nullptr}) {
   __shared__ double sh[kBlock / 32];
-  const RowPlan pl = plan_row<G>(M, bins);
+  const RowPlan pl = plan_row<G, MULTI>(M, bins, im);
   pdl_wait();
   const double s = finish_row<G>(pl, M, x, sh);
   pdl_launch_dependents();

@@ -218,6 +218,39 @@ def solvePdhgBatch(base: Model, cases: list[LpCase], opts: PdhgOptions | None = 
     return _results(base, res, x, y, k, stats)
 
 
+def solvePdhgMulti(lps: list[Model], opts: PdhgOptions | None = None,
+                   batchStats: PdhgStats | None = None) -> list[PdhgResult]:
+    """Independent LPs of different sizes solved together on the GPU, each with
+    the reference's algorithm (no counterpart in the reference)."""
+    if not lps:
+        return []
+    opts = opts or PdhgOptions()
+    lib = _lib.load()
+    k = len(lps)
+    structs, keep = [], []
+    arr = (_lib.B2pLp * k)()
+    for b, lp in enumerate(lps):
+        s, kp = _lp_struct(lp)
+        arr[b] = s
+        keep.append(kp)
+    xs = [np.zeros(lp.num_cols) for lp in lps]
+    ys = [np.zeros(lp.num_rows) for lp in lps]
+    xp = (_lib.dptr * k)(*[a.ctypes.data_as(_lib.dptr) for a in xs])
+    yp = (_lib.dptr * k)(*[a.ctypes.data_as(_lib.dptr) for a in ys])
+    res = (_lib.B2pResult * k)()
+    st = _lib.B2pStats()
+    o = opts.to_c()
+    _lib.check(lib.b2p_solve_pdhg_multi(arr, k, C.byref(o), xp, yp, res, C.byref(st)))
+    del keep, structs
+    stats = PdhgStats.from_c(st, _device_name())
+    if batchStats is not None:
+        batchStats.__dict__.update(stats.__dict__)
+    solvePdhgMulti.last_stats = st
+    return [PdhgResult(status=Status.get(res[b].status, str(res[b].status)), objective=res[b].objective,
+                       dualObjective=res[b].dual_objective, x=xs[b], rowDual=ys[b], iterations=res[b].iterations,
+                       relativeKkt=res[b].relative_kkt, stats=stats) for b in range(k)]
+
+
 def gpuAvailable() -> bool:
     """pramana::gpuAvailable (src/pdhg/pdhg.cpp:730)."""
     return bool(_lib.load().b2p_gpu_available())
@@ -352,3 +385,4 @@ gpu_available = gpuAvailable
 gpu_info_json = gpuInfoJson
 kkt_residual = kktResidual
 safe_dual_bound = safeDualBound
+solve_pdhg_multi = solvePdhgMulti

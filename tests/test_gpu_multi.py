@@ -1,0 +1,51 @@
+"""Independent LPs of different sizes solved together (b2p_solve_pdhg_multi):
+every instance must follow the reference algorithm as if solved alone --
+checked against the oracle at fixed iteration counts and to convergence."""
+import numpy as np
+import pytest
+
+import lp_cases
+from pramana_b200 import generators as G
+from pramana_b200 import pdhg
+from pramana_b200.model import Model
+from test_gpu_parity import _host_kkt, assert_close, opts
+
+pytestmark = pytest.mark.gpu
+
+
+def family():
+    lps = [G.random_lp(m, 2 * m, 4.0, int(0.6 * m), 100 + i) for i, m in enumerate([50, 300, 120, 1000, 10])]
+    lps.append(G.random_lp(2000, 4000, 6.4, 1200, 7, heavy_row_frac=0.01, heavy_nnz_frac=0.1))
+    lps.append(lp_cases.edge_lp(5))
+    n = 5
+    lps.append(Model(num_rows=0, num_cols=n, start=np.zeros(n + 1), index=[], value=[], col_cost=[1, -1, 2, 0, 3],
+                     col_lower=np.zeros(n), col_upper=np.full(n, 4.0), row_lower=[], row_upper=[]))
+    return lps
+
+
+@pytest.mark.parametrize("iters", [1, 64, 1000])
+def test_multi_fixed_iterations_vs_oracle(oracle_mod, iters):
+    lps = family()
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-30, maxIterations=iters))
+    for lp, r in zip(lps, rs):
+        assert_close(r, oracle_mod.solve(lp, "oracle", tolerance=1e-30, max_iterations=iters))
+
+
+def test_multi_converged_vs_oracle(oracle_mod):
+    lps = family()
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, maxIterations=200000))
+    for lp, r in zip(lps, rs):
+        o = oracle_mod.solve(lp, "oracle", tolerance=1e-6, max_iterations=200000)
+        assert r.status == "Optimal" and o.status == 1
+        assert abs(r.iterations - o.iterations) <= 4 * 64
+        assert abs(r.objective - o.objective) <= 1e-5 * (1 + abs(o.objective))
+        if lp.num_rows:
+            assert max(_host_kkt(lp, r.x, r.rowDual)) <= 1e-6 * (1 + 1e-6)
+
+
+def test_multi_iteration_limit_reports_every_instance(oracle_mod):
+    lps = family()
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-30, maxIterations=100))
+    for lp, r in zip(lps, rs):
+        o = oracle_mod.solve(lp, "oracle", tolerance=1e-30, max_iterations=100)
+        assert r.status == {1: "Optimal", 6: "IterationLimit"}[o.status] and r.iterations == o.iterations
