@@ -566,6 +566,8 @@ struct Engine {
     RowBins b{};
     b.long_rows = upload(hb.long_rows);
     b.vlong_rows = upload(hb.vlong_rows);
+    b.short_rows = nullptr;
+    b.n_short = 0;
     b.n_long = static_cast<int32_t>(hb.long_rows.size());
     b.n_vlong = static_cast<int32_t>(hb.vlong_rows.size());
     b.long_thr = hb.long_thr;

@@ -225,6 +225,12 @@ struct MultiEngine {
   int32_t *d_rblk_off = nullptr, *d_cblk_off = nullptr;
   int g_rows = 0, g_cols = 0;
   RowBins binsA{}, binsT{};
+  // host copies for compaction: row pointers of the concatenated operators,
+  // nonzeros of each instance, and the nonzeros the current schedule covers
+  std::vector<int32_t> hA_ptr, hT_ptr;
+  std::vector<int64_t> inst_nnz;
+  int64_t sched_nnz = 0;
+  int ltA = 0, ltT = 0;
   double* h_sums = nullptr;
   double* h_steps = nullptr;
   int32_t *h_mask = nullptr, *h_done = nullptr;
@@ -235,6 +241,7 @@ struct MultiEngine {
   std::vector<b2p_result> results;
   std::vector<std::vector<double>> xs, ys;  // per instance, original space
   int64_t launches = 0, bytes_up = 0, bytes_down = 0;
+  int compactions = 0;
 
   template <class T>
   T* dalloc(size_t count) {
@@ -445,8 +452,17 @@ struct MultiEngine {
     B2P_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     const int64_t wave = static_cast<int64_t>(std::max(1, per_sm)) * sms * kBlock;
     const int rounds = opt.short_row_rounds > 0 ? opt.short_row_rounds : 2;
-    binsA = device_bins(make_bins(A, wave, opt.lanes_per_row_a, rounds), M);
-    binsT = device_bins(make_bins(AT, wave, opt.lanes_per_row_at, rounds), N);
+    const HostBins hbA = make_bins(A, wave, opt.lanes_per_row_a, rounds);
+    const HostBins hbT = make_bins(AT, wave, opt.lanes_per_row_at, rounds);
+    binsA = device_bins(hbA, M);
+    binsT = device_bins(hbT, N);
+    ltA = hbA.long_thr;
+    ltT = hbT.long_thr;
+    hA_ptr = A.ptr;
+    hT_ptr = AT.ptr;
+    inst_nnz.assign(K, 0);
+    for (int b = 0; b < K; ++b) inst_nnz[b] = static_cast<int64_t>(P[b].A.val.size());
+    sched_nnz = annz;
     stats.lanes_per_row_a = binsA.g;
     stats.lanes_per_row_at = binsT.g;
     if (M > 0) {
@@ -464,6 +480,8 @@ struct MultiEngine {
     RowBins b{};
     b.long_rows = upload(hb.long_rows);
     b.vlong_rows = upload(hb.vlong_rows);
+    b.short_rows = nullptr;
+    b.n_short = 0;
     b.n_long = static_cast<int32_t>(hb.long_rows.size());
     b.n_vlong = static_cast<int32_t>(hb.vlong_rows.size());
     b.long_thr = hb.long_thr;
@@ -473,6 +491,55 @@ struct MultiEngine {
     b.g = hb.g;
     return b;
   }
+  // Schedule over the rows of live instances only (instance compaction).
+  RowBins live_bins(const std::vector<int32_t>& ptr, const std::vector<int64_t>& off, const std::vector<char>& done,
+                    int g, int lt) {
+    std::vector<int32_t> sh, lg, vl;
+    for (int b = 0; b < K; ++b) {
+      if (done[b]) continue;
+      for (int64_t i = off[b]; i < off[b + 1]; ++i) {
+        const int32_t len = ptr[i + 1] - ptr[i];
+        if (len > kVeryLongRow)
+          vl.push_back(static_cast<int32_t>(i));
+        else if (len > lt)
+          lg.push_back(static_cast<int32_t>(i));
+        else
+          sh.push_back(static_cast<int32_t>(i));
+      }
+    }
+    RowBins r{};
+    r.long_rows = upload(lg);
+    r.vlong_rows = upload(vl);
+    r.short_rows = upload(sh);
+    r.n_short = static_cast<int32_t>(sh.size());
+    r.n_long = static_cast<int32_t>(lg.size());
+    r.n_vlong = static_cast<int32_t>(vl.size());
+    r.long_thr = lt;
+    r.vlong_blocks = r.n_vlong;
+    r.long_blocks = (r.n_long + kBlock / 32 - 1) / (kBlock / 32);
+    r.short_blocks = static_cast<int32_t>((static_cast<int64_t>(r.n_short) * g + kBlock - 1) / kBlock);
+    r.g = g;
+    return r;
+  }
+
+  // Rebuild the schedules when the live instances hold less than half of the
+  // nonzeros the current ones cover; the graphs are captured again.
+  void maybe_compact(const std::vector<char>& done) {
+    int64_t live = 0;
+    for (int b = 0; b < K; ++b)
+      if (!done[b]) live += inst_nnz[b];
+    if (live == 0 || 2 * live >= sched_nnz) return;
+    B2P_CUDA(cudaStreamSynchronize(stream));
+    binsA = live_bins(hA_ptr, roff, done, binsA.g, ltA);
+    binsT = live_bins(hT_ptr, coff, done, binsT.g, ltT);
+    for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+    for (auto& g : graph_defs) cudaGraphDestroy(g.second);
+    graphs.clear();
+    graph_defs.clear();
+    sched_nnz = live;
+    ++compactions;
+  }
+
   static unsigned bin_grid(const RowBins& b) {
     return static_cast<unsigned>(std::max(1, b.vlong_blocks + b.long_blocks + b.short_blocks));
   }
@@ -675,6 +742,7 @@ struct MultiEngine {
       if (anyDone) {
         for (int b = 0; b < K; ++b) h_done[b] = done[b];
         B2P_CUDA(cudaMemcpyAsync(d_done, h_done, sizeof(int32_t) * K, cudaMemcpyHostToDevice, stream));
+        maybe_compact(done);
       }
       if (anyRestart) {
         B2P_CUDA(cudaMemcpyAsync(d_mask, h_mask, sizeof(int32_t) * K, cudaMemcpyHostToDevice, stream));

@@ -32,6 +32,8 @@ constexpr int kVeryLongRow = 2048;  // rows longer than this get a 256-thread bl
 struct RowBins {
   const int32_t* __restrict__ long_rows;   // rows for the warp path
   const int32_t* __restrict__ vlong_rows;  // rows for the block path
+  const int32_t* __restrict__ short_rows;  // rows for the short path (NULL: every row 0..rows-1)
+  int32_t n_short;                         // entries of short_rows
   int32_t n_long, n_vlong;
   int32_t long_thr;      // rows longer than this are not in the short path
   int32_t vlong_blocks;  // == n_vlong
@@ -94,7 +96,8 @@ __device__ __forceinline__ RowPlan plan_row(const CsrView& M, const RowBins& bin
     blk -= bins.long_blocks;
     pl.path = 0;
     pl.stride = G;
-    const int row = (blk * kBlock + threadIdx.x) / G;
+    const int q = (blk * kBlock + threadIdx.x) / G;
+    const int row = bins.short_rows ? (q < bins.n_short ? __ldg(bins.short_rows + q) : M.rows) : q;
     if (row < M.rows) {
       const int beg = __ldg(M.ptr + row), end = __ldg(M.ptr + row + 1);
       if (end - beg <= bins.long_thr) {
