@@ -182,12 +182,15 @@ int b2p_solve_pdhg_batch(const b2p_lp* base, const b2p_case* cases, int32_t num_
  * one A (solvePdhgBatch); each LP here gets exactly the reference's algorithm
  * (its own scaling, steps, primal weight, restarts and termination), and all
  * of them advance together as one block-diagonal operator on the GPU.
+ * x_start[b] / row_dual_start[b], when given (either array or entry may be
+ * NULL), warm-start LP b (original space; x is projected onto the bounds).
  * x[b] (num_cols of LP b) and row_dual[b] (num_rows) receive LP b's
  * solution (either array, or any entry, may be NULL); results has num_lps
  * entries.  stats: kernel_seconds is the device time of the loop;
  * iterations the global iteration count. */
-int b2p_solve_pdhg_multi(const b2p_lp* lps, int32_t num_lps, const b2p_options* opts, double* const* x,
-                         double* const* row_dual, b2p_result* results, b2p_stats* stats);
+int b2p_solve_pdhg_multi(const b2p_lp* lps, int32_t num_lps, const b2p_options* opts, const double* const* x_start,
+                         const double* const* row_dual_start, double* const* x, double* const* row_dual,
+                         b2p_result* results, b2p_stats* stats);
 
 /* gpuAvailable (src/pdhg/pdhg.cpp:730): 1 if an sm_100 device is usable. */
 int b2p_gpu_available(void);
@@ -213,6 +216,14 @@ int b2p_engine_create(const b2p_lp* lp, const b2p_case* cases, int32_t num_cases
 int b2p_engine_solve(b2p_engine* e, b2p_result* results, b2p_stats* stats);
 int b2p_engine_fetch(b2p_engine* e, double* x, double* row_dual);
 int b2p_engine_destroy(b2p_engine* e);
+/* Warm start: the starting point of the following b2p_engine_solve calls, in
+ * the original space -- x is num_cases x num_cols, row_dual num_cases x
+ * num_rows (case-major; num_cases = 1 for a single solve); x is projected
+ * onto the bounds; primal_weight > 0 replaces the initial primal weight of
+ * every case.  NULL x and NULL row_dual restore the cold start.  No
+ * counterpart in the reference, whose PDHG always starts from x = projection
+ * of 0, y = 0 (src/pdhg/pdhg.cpp:509, 519, 536-539). */
+int b2p_engine_set_start(b2p_engine* e, const double* x, const double* row_dual, double primal_weight);
 /* When on, every fused SpMV kernel launch (and, in resident form, every
  * interval launch) of the next solve is bracketed by CUDA events;
  * b2p_engine_kernel_times then returns, per kernel class (0 = A^T y + primal

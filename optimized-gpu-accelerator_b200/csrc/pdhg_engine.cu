@@ -40,7 +40,8 @@ namespace {
 
 // Device vector slots (the reference's enum V, src/pdhg/pdhg.cpp:45, minus
 // ATY/ATYP which the fused kernels never store, plus the initial point).
-enum Slot : int { X, XP, X0, C, LO, UP, XINIT, ATYP, NCOLVEC, Y = NCOLVEC, YP, Y0, AX, AXP, AX0, RL, RU, AXINIT, NSLOT };
+enum Slot : int { X, XP, X0, C, LO, UP, XINIT, ATYP, NCOLVEC, Y = NCOLVEC, YP, Y0, AX, AXP, AX0, RL, RU, AXINIT,
+                  YINIT, NSLOT };
 inline bool row_slot(int s) { return s >= Y; }
 
 template <class T>
@@ -111,6 +112,8 @@ struct Engine {
   b2p_options opt{};
   Prepared P;
   std::vector<double> cNorm, rhsNorm, omega0;
+  std::vector<double> omega_cold, x_cold;  // the reference's starting weights and x (scaled, interleaved)
+  bool warm = false;                       // a caller-given start replaces x0 = proj(0), y0 = 0
   double eta = 0;
 
   // ---- device ----
@@ -310,6 +313,9 @@ struct Engine {
     put(RL, rl);
     put(RU, ru);
     put(XINIT, x);
+    x_cold = x;
+    omega_cold = omega0;
+    if (mk) B2P_CUDA(cudaMemsetAsync(v[YINIT], 0, mk * sizeof(double), stream));
     d_tau = dalloc<double>(k);
     d_sigma = dalloc<double>(k);
     d_it_base = dalloc<int64_t>(1);
@@ -590,9 +596,9 @@ struct Engine {
     cp(X0, XINIT, nk);
     cp(AX, AXINIT, mk);
     cp(AX0, AXINIT, mk);
+    cp(Y, YINIT, mk);
+    cp(Y0, YINIT, mk);
     if (mk) {
-      B2P_CUDA(cudaMemsetAsync(v[Y], 0, mk * sizeof(double), stream));
-      B2P_CUDA(cudaMemsetAsync(v[Y0], 0, mk * sizeof(double), stream));
       B2P_CUDA(cudaMemsetAsync(v[YP], 0, mk * sizeof(double), stream));
       B2P_CUDA(cudaMemsetAsync(v[AXP], 0, mk * sizeof(double), stream));
     }
@@ -601,6 +607,42 @@ struct Engine {
     B2P_CUDA(cudaMemsetAsync(d_restart_at, 0, sizeof(int64_t) * k, stream));
     omega = omega0;
     upload_steps(omega);
+  }
+
+  // Starting point of the next solves, in the original space (case-major
+  // k x n, k x m): x is scaled and projected onto the bounds, y scaled, A x
+  // recomputed; NULL x and y restore the reference's cold start.
+  void set_start(const double* x, const double* y, double primal_weight) {
+    B2P_CUDA(cudaSetDevice(device));
+    const size_t nk = static_cast<size_t>(n) * k, mk = static_cast<size_t>(m) * k;
+    std::vector<double> lo(nk), up(nk);
+    if (nk) {
+      B2P_CUDA(cudaMemcpyAsync(lo.data(), v[LO], nk * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      B2P_CUDA(cudaMemcpyAsync(up.data(), v[UP], nk * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      B2P_CUDA(cudaStreamSynchronize(stream));
+    }
+    std::vector<double> xs(x_cold), ys(mk, 0.0);
+    warm = x || y;
+    if (x)
+      for (int b = 0; b < k; ++b)
+        for (int j = 0; j < n; ++j) {
+          const size_t t = static_cast<size_t>(j) * k + b;
+          xs[t] = smin(smax(x[static_cast<size_t>(b) * n + j] / P.Cs[j] / P.beta, lo[t]), up[t]);
+        }
+    if (y)
+      for (int b = 0; b < k; ++b)
+        for (int i = 0; i < m; ++i)
+          ys[static_cast<size_t>(i) * k + b] = y[static_cast<size_t>(b) * m + i] / P.R[i] / P.gamma;
+    if (nk) B2P_CUDA(cudaMemcpyAsync(v[XINIT], xs.data(), nk * sizeof(double), cudaMemcpyHostToDevice, stream));
+    if (mk) {
+      B2P_CUDA(cudaMemcpyAsync(v[YINIT], ys.data(), mk * sizeof(double), cudaMemcpyHostToDevice, stream));
+      k_spmv<<<blocks(static_cast<int64_t>(m) * k), kBlock, 0, stream>>>(m, k, viewA(), v[XINIT], v[AXINIT]);
+      B2P_CUDA(cudaGetLastError());
+    }
+    B2P_CUDA(cudaStreamSynchronize(stream));
+    bytes_up += static_cast<int64_t>((nk + mk) * sizeof(double));
+    omega0 = omega_cold;
+    if (primal_weight > 0) omega0.assign(k, primal_weight);
   }
 
   void upload_steps(const std::vector<double>& omega) {
@@ -1097,6 +1139,13 @@ int b2p_engine_fetch(b2p_engine* h, double* x, double* y) {
 
 int b2p_engine_destroy(b2p_engine* h) {
   return guarded([&] { delete reinterpret_cast<Engine*>(h); });
+}
+
+int b2p_engine_set_start(b2p_engine* h, const double* x, const double* row_dual, double primal_weight) {
+  return guarded([&] {
+    if (!h) throw Error(B2P_ERR_INVALID, "engine is NULL");
+    reinterpret_cast<Engine*>(h)->set_start(x, row_dual, primal_weight);
+  });
 }
 
 int b2p_engine_set_profiling(b2p_engine* h, int32_t on) {

@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(kBlock) k_restart_multi(int32_t n, int32_t m, 
 namespace {
 
 enum MSlot : int { MX, MXP, MX0, MC, MLO, MUP, MXINIT, MATYP, MNCOL, MY = MNCOL, MYP, MY0, MAX, MAXP, MAX0, MRL, MRU,
-                   MAXINIT, MNSLOT };
+                   MAXINIT, MYINIT, MNSLOT };
 
 struct MultiEngine {
   int device = 0;
@@ -476,6 +476,36 @@ struct MultiEngine {
     stats.precision_used = B2P_PRECISION_FP64;
   }
 
+  // Warm starts of some instances (original space); others keep the cold start.
+  void set_start(const double* const* xst, const double* const* yst) {
+    if (M) B2P_CUDA(cudaMemsetAsync(v[MYINIT], 0, sizeof(double) * M, stream));
+    if (!xst && !yst) return;
+    std::vector<double> lo(N), up(N), x0(N), y0(M, 0.0);
+    if (N) {
+      B2P_CUDA(cudaMemcpyAsync(lo.data(), v[MLO], sizeof(double) * N, cudaMemcpyDeviceToHost, stream));
+      B2P_CUDA(cudaMemcpyAsync(up.data(), v[MUP], sizeof(double) * N, cudaMemcpyDeviceToHost, stream));
+      B2P_CUDA(cudaMemcpyAsync(x0.data(), v[MXINIT], sizeof(double) * N, cudaMemcpyDeviceToHost, stream));
+    }
+    B2P_CUDA(cudaStreamSynchronize(stream));
+    for (int b = 0; b < K; ++b) {
+      const Prepared& p = P[b];
+      if (xst && xst[b])
+        for (int32_t j = 0; j < p.n; ++j) {
+          const size_t t = static_cast<size_t>(coff[b] + j);
+          x0[t] = smin(smax(xst[b][j] / p.Cs[j] / p.beta, lo[t]), up[t]);
+        }
+      if (yst && yst[b])
+        for (int32_t i = 0; i < p.m; ++i) y0[static_cast<size_t>(roff[b] + i)] = yst[b][i] / p.R[i] / p.gamma;
+    }
+    if (N) B2P_CUDA(cudaMemcpyAsync(v[MXINIT], x0.data(), sizeof(double) * N, cudaMemcpyHostToDevice, stream));
+    if (M) {
+      B2P_CUDA(cudaMemcpyAsync(v[MYINIT], y0.data(), sizeof(double) * M, cudaMemcpyHostToDevice, stream));
+      k_spmv<<<blocks(M), kBlock, 0, stream>>>(M, 1, viewA(), v[MXINIT], v[MAXINIT]);
+      B2P_CUDA(cudaGetLastError());
+    }
+    B2P_CUDA(cudaStreamSynchronize(stream));
+  }
+
   RowBins device_bins(const HostBins& hb, int32_t rows) {
     RowBins b{};
     b.long_rows = upload(hb.long_rows);
@@ -668,10 +698,8 @@ struct MultiEngine {
     cp(MX0, MXINIT, N);
     cp(MAX, MAXINIT, M);
     cp(MAX0, MAXINIT, M);
-    if (M) {
-      B2P_CUDA(cudaMemsetAsync(v[MY], 0, sizeof(double) * M, stream));
-      B2P_CUDA(cudaMemsetAsync(v[MY0], 0, sizeof(double) * M, stream));
-    }
+    cp(MY, MYINIT, M);
+    cp(MY0, MYINIT, M);
     B2P_CUDA(cudaMemsetAsync(d_it_base, 0, sizeof(int64_t), stream));
     B2P_CUDA(cudaMemsetAsync(d_restart_at, 0, sizeof(int64_t) * K, stream));
     B2P_CUDA(cudaMemsetAsync(d_done, 0, sizeof(int32_t) * K, stream));
@@ -782,13 +810,15 @@ struct MultiEngine {
 }  // namespace
 }  // namespace b2p
 
-extern "C" int b2p_solve_pdhg_multi(const b2p_lp* lps, int32_t num_lps, const b2p_options* opts, double* const* x,
-                                    double* const* row_dual, b2p_result* results, b2p_stats* stats) {
+extern "C" int b2p_solve_pdhg_multi(const b2p_lp* lps, int32_t num_lps, const b2p_options* opts,
+                                    const double* const* x_start, const double* const* row_dual_start,
+                                    double* const* x, double* const* row_dual, b2p_result* results, b2p_stats* stats) {
   using namespace b2p;
   return guarded([&] {
     const auto t0 = Clock::now();
     MultiEngine e;
     e.create(lps, num_lps, opts);
+    e.set_start(x_start, row_dual_start);
     e.solve(t0);
     for (int b = 0; b < e.K; ++b) {
       if (x && x[b] && !e.xs[b].empty()) std::memcpy(x[b], e.xs[b].data(), sizeof(double) * e.xs[b].size());

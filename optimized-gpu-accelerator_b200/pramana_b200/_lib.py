@@ -79,7 +79,9 @@ SIGNATURES = {
     "b2p_solve_pdhg_batch": (C.c_int, [C.POINTER(B2pLp), C.POINTER(B2pCase), C.c_int32, C.POINTER(B2pOptions),
                                        dptr, dptr, C.POINTER(B2pResult), C.POINTER(B2pStats)]),
     "b2p_solve_pdhg_multi": (C.c_int, [C.POINTER(B2pLp), C.c_int32, C.POINTER(B2pOptions), C.POINTER(dptr),
-                                       C.POINTER(dptr), C.POINTER(B2pResult), C.POINTER(B2pStats)]),
+                                       C.POINTER(dptr), C.POINTER(dptr), C.POINTER(dptr), C.POINTER(B2pResult),
+                                       C.POINTER(B2pStats)]),
+    "b2p_engine_set_start": (C.c_int, [C.c_void_p, dptr, dptr, C.c_double]),
     "b2p_gpu_available": (C.c_int, []),
     "b2p_gpu_info_json": (C.c_int, [C.c_char_p, C.c_size_t]),
     "b2p_last_error": (C.c_char_p, []),

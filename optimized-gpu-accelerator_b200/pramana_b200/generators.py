@@ -95,3 +95,143 @@ def scaled_random_lp(m: int, seed: int, skew: bool = False) -> Model:
     if skew:
         return random_lp(m, 2 * m, 6.4, int(0.6 * m), seed, heavy_row_frac=0.01, heavy_nnz_frac=0.10)
     return random_lp(m, 2 * m, 5.0, int(0.6 * m), seed)
+
+
+def refinery_lp(periods: int = 12, crudes: int = 6, units: int = 10, pools: int = 15, regions: int = 10,
+                streams: int = 12, properties: int = 8, pools_per_stream: int = 4, seed: int = 3,
+                crude_prices=None, demand_scales=None, scale_exponent: float = 3.0, name: str | None = None) -> Model:
+    """Synthetic multi-period refinery-planning LP (the "C3" workload).
+
+    Per region and period: crude feeds f[c,u] into process units, each unit
+    turning its feed into `streams` intermediate streams with yields
+    U(0.01, 0.6) (material-balance equalities), streams blended into product
+    pools (pool balances, blending-quality <= rows with property coefficients
+    U(0.5, 2.0) against specs), unit capacity rows with rhs U(1e3, 1e5),
+    product sales bounded by demand U(5e2, 5e4), and stream / pool / crude
+    inventories linking consecutive periods; crude purchases are shared by the
+    regions.  Objective: crude cost + small operating and holding costs minus
+    product revenue.  Every row and column is then rescaled by 10^U(-e, e)
+    (an equivalent, badly scaled LP).  x = 0 is feasible and the LP is bounded.
+
+    Family parameters: `crude_prices` (one per crude, default U(40, 120)) and
+    `demand_scales` (multiplying the demand of the first len() pools).
+    Defaults give 48,072 rows, 99,144 columns and about 0.75M nonzeros.
+    """
+    rng = np.random.default_rng(seed)
+    T, C, U, P, R, S, Q = periods, crudes, units, pools, regions, streams, properties
+    yld = rng.uniform(0.01, 0.6, size=(R, C, U, S))
+    cap = rng.uniform(1e3, 1e5, size=(R, U))
+    supply = rng.uniform(1e3, 1e5, size=C) * R
+    demand = rng.uniform(5e2, 5e4, size=(R, P))
+    prop = rng.uniform(0.5, 2.0, size=(R, U, S, Q))
+    spec = rng.uniform(0.8, 1.6, size=(R, P, Q))
+    price = rng.uniform(150.0, 300.0, size=P)
+    op_cost = rng.uniform(1.0, 5.0, size=U)
+    elig = np.array([[rng.choice(P, size=pools_per_stream, replace=False) for _ in range(S)] for _ in range(U)])
+    cprice = rng.uniform(40.0, 120.0, size=C) if crude_prices is None else np.asarray(crude_prices, dtype=float)
+    if demand_scales is not None:
+        ds = np.asarray(demand_scales, dtype=float)
+        demand = demand.copy()
+        demand[:, :len(ds)] *= ds
+
+    cols = {"cost": [], "lo": [], "up": []}
+
+    def new_cols(k, cost, up=np.inf):
+        base = len(cols["cost"])
+        cols["cost"].extend(np.broadcast_to(cost, (k,)).tolist())
+        cols["lo"].extend([0.0] * k)
+        cols["up"].extend(np.broadcast_to(up, (k,)).tolist())
+        return np.arange(base, base + k)
+
+    # column blocks
+    buy = np.zeros((T, C), dtype=np.int64)
+    cinv = np.zeros((T, C), dtype=np.int64)
+    for t in range(T):
+        buy[t] = new_cols(C, cprice, supply)
+        cinv[t] = new_cols(C, 0.5)
+    f = np.zeros((R, T, C, U), dtype=np.int64)
+    prod = np.zeros((R, T, U, S), dtype=np.int64)
+    blend = np.zeros((R, T, U, S, pools_per_stream), dtype=np.int64)
+    sinv = np.zeros((R, T, U, S), dtype=np.int64)
+    vol = np.zeros((R, T, P), dtype=np.int64)
+    pinv = np.zeros((R, T, P), dtype=np.int64)
+    sale = np.zeros((R, T, P), dtype=np.int64)
+    for r in range(R):
+        for t in range(T):
+            f[r, t] = new_cols(C * U, np.tile(op_cost, C)).reshape(C, U)
+            prod[r, t] = new_cols(U * S, 0.0).reshape(U, S)
+            blend[r, t] = new_cols(U * S * pools_per_stream, 0.0).reshape(U, S, pools_per_stream)
+            sinv[r, t] = new_cols(U * S, 0.2).reshape(U, S)
+            vol[r, t] = new_cols(P, 0.0)
+            pinv[r, t] = new_cols(P, 0.3)
+            sale[r, t] = new_cols(P, -price, demand[r])
+    rows_r, rows_c, rows_v, rlo, rup = [], [], [], [], []
+
+    def add_row(cidx, vals, lo, up):
+        i = len(rlo)
+        rows_r.extend([i] * len(cidx))
+        rows_c.extend(list(cidx))
+        rows_v.extend(list(vals))
+        rlo.append(lo)
+        rup.append(up)
+
+    for t in range(T):
+        for c in range(C):  # crude balance: buy + inv(t-1) = feeds + inv(t)
+            idx = [buy[t, c], cinv[t, c]] + list(f[:, t, c, :].ravel())
+            val = [1.0, -1.0] + [-1.0] * (R * U)
+            if t > 0:
+                idx.append(cinv[t - 1, c])
+                val.append(1.0)
+            add_row(idx, val, 0.0, 0.0)
+    for r in range(R):
+        for t in range(T):
+            for u in range(U):
+                add_row(f[r, t, :, u], np.ones(C), -np.inf, cap[r, u])  # unit capacity
+                for s in range(S):  # yields: prod = sum_c yld f
+                    add_row([prod[r, t, u, s]] + list(f[r, t, :, u]), [1.0] + list(-yld[r, :, u, s]), 0.0, 0.0)
+                    idx = [prod[r, t, u, s], sinv[r, t, u, s]] + list(blend[r, t, u, s])
+                    val = [1.0, -1.0] + [-1.0] * pools_per_stream
+                    if t > 0:
+                        idx.append(sinv[r, t - 1, u, s])
+                        val.append(1.0)
+                    add_row(idx, val, 0.0, 0.0)  # stream balance with inventory
+            for p in range(P):
+                src = [(u, s, k) for u in range(U) for s in range(S) for k in range(pools_per_stream)
+                       if elig[u, s, k] == p]
+                bidx = [blend[r, t, u, s, k] for (u, s, k) in src]
+                add_row(bidx + [vol[r, t, p]], [1.0] * len(bidx) + [-1.0], 0.0, 0.0)  # pool balance
+                for q in range(Q):  # blending quality: sum prop b <= spec vol
+                    add_row(bidx + [vol[r, t, p]], [prop[r, u, s, q] for (u, s, k) in src] + [-spec[r, p, q]],
+                            -np.inf, 0.0)
+                idx = [vol[r, t, p], pinv[r, t, p], sale[r, t, p]]
+                val = [1.0, -1.0, -1.0]
+                if t > 0:
+                    idx.append(pinv[r, t - 1, p])
+                    val.append(1.0)
+                add_row(idx, val, 0.0, 0.0)  # pool inventory
+    n, m = len(cols["cost"]), len(rlo)
+    ri, ci, vv = np.array(rows_r), np.array(rows_c), np.array(rows_v)
+    cost, lo, up = np.array(cols["cost"]), np.array(cols["lo"]), np.array(cols["up"])
+    rl, ru = np.array(rlo), np.array(rup)
+    # badly scaled equivalent LP: A' = Dr A Dc, x = Dc x'
+    dr = 10.0 ** rng.uniform(-scale_exponent, scale_exponent, size=m)
+    dc = 10.0 ** rng.uniform(-scale_exponent, scale_exponent, size=n)
+    vv = vv * dr[ri] * dc[ci]
+    cost = cost * dc
+    lo = lo / dc
+    up = np.where(np.isfinite(up), up / dc, np.inf)
+    rl = np.where(np.isfinite(rl), rl * dr, rl)
+    ru = np.where(np.isfinite(ru), ru * dr, ru)
+    order = np.lexsort((ri, ci))
+    ri, ci, vv = ri[order], ci[order], vv[order]
+    start = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(np.bincount(ci, minlength=n), out=start[1:])
+    return Model(num_rows=m, num_cols=n, start=start, index=ri, value=vv, col_cost=cost, col_lower=lo, col_upper=up,
+                 row_lower=rl, row_upper=ru, name=name or f"refinery_T{T}_R{R}_s{seed}",
+                 meta={"seed": seed, "periods": T, "regions": R, "crude_prices": cprice.tolist()})
+
+
+def config3(seed: int = 3) -> Model:
+    """The multi-period refinery-planning LP at its default size (12 periods,
+    6 crudes, 10 units, 15 pools, 10 regions)."""
+    return refinery_lp(seed=seed, name=f"c3_s{seed}")

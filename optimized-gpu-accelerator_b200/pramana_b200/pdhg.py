@@ -218,10 +218,11 @@ def solvePdhgBatch(base: Model, cases: list[LpCase], opts: PdhgOptions | None = 
     return _results(base, res, x, y, k, stats)
 
 
-def solvePdhgMulti(lps: list[Model], opts: PdhgOptions | None = None,
-                   batchStats: PdhgStats | None = None) -> list[PdhgResult]:
+def solvePdhgMulti(lps: list[Model], opts: PdhgOptions | None = None, batchStats: PdhgStats | None = None,
+                   starts: list | None = None) -> list[PdhgResult]:
     """Independent LPs of different sizes solved together on the GPU, each with
-    the reference's algorithm (no counterpart in the reference)."""
+    the reference's algorithm (no counterpart in the reference).  starts[b] =
+    (x, y) warm-starts LP b (None entries: cold start)."""
     if not lps:
         return []
     opts = opts or PdhgOptions()
@@ -240,7 +241,14 @@ def solvePdhgMulti(lps: list[Model], opts: PdhgOptions | None = None,
     res = (_lib.B2pResult * k)()
     st = _lib.B2pStats()
     o = opts.to_c()
-    _lib.check(lib.b2p_solve_pdhg_multi(arr, k, C.byref(o), xp, yp, res, C.byref(st)))
+    xst = yst = None
+    if starts is not None:
+        sx = [None if s is None or s[0] is None else np.ascontiguousarray(s[0], dtype=np.float64) for s in starts]
+        sy = [None if s is None or s[1] is None else np.ascontiguousarray(s[1], dtype=np.float64) for s in starts]
+        keep.append((sx, sy))
+        xst = (_lib.dptr * k)(*[a.ctypes.data_as(_lib.dptr) if a is not None else None for a in sx])
+        yst = (_lib.dptr * k)(*[a.ctypes.data_as(_lib.dptr) if a is not None else None for a in sy])
+    _lib.check(lib.b2p_solve_pdhg_multi(arr, k, C.byref(o), xst, yst, xp, yp, res, C.byref(st)))
     del keep, structs
     stats = PdhgStats.from_c(st, _device_name())
     if batchStats is not None:
@@ -293,6 +301,14 @@ class Engine:
         self.last_stats = st
         x, y = self.fetch()
         return _results(self.lp, res, x, y, self.k, PdhgStats.from_c(st))
+
+    def set_start(self, x=None, y=None, primal_weight: float = 0.0) -> None:
+        """Warm start of the following solves (original space); None, None = cold start."""
+        xa = None if x is None else np.ascontiguousarray(x, dtype=np.float64)
+        ya = None if y is None else np.ascontiguousarray(y, dtype=np.float64)
+        _lib.check(self._lib.b2p_engine_set_start(self._h, None if xa is None else xa.ctypes.data_as(_lib.dptr),
+                                                  None if ya is None else ya.ctypes.data_as(_lib.dptr),
+                                                  float(primal_weight)))
 
     def fetch(self):
         x = np.zeros(self.k * self.lp.num_cols)

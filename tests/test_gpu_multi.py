@@ -49,3 +49,16 @@ def test_multi_iteration_limit_reports_every_instance(oracle_mod):
     for lp, r in zip(lps, rs):
         o = oracle_mod.solve(lp, "oracle", tolerance=1e-30, max_iterations=100)
         assert r.status == {1: "Optimal", 6: "IterationLimit"}[o.status] and r.iterations == o.iterations
+
+
+def test_multi_warm_start():
+    lps = family()[:6]
+    cold = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6))
+    starts = [(r.x, r.rowDual) if b % 2 == 0 else None for b, r in enumerate(cold)]
+    warm = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6), starts=starts)
+    for b, (c, w) in enumerate(zip(cold, warm)):
+        assert w.status == "Optimal"
+        if b % 2 == 0:
+            assert w.iterations <= 64
+        else:
+            assert w.iterations == c.iterations

@@ -337,3 +337,18 @@ def test_mixed_falls_back_to_fp64_for_batches():
     st = pdhg.PdhgStats()
     rs = pdhg.solvePdhgBatch(lp, cases, opts(tolerance=1e-6, precision=MIXED), batchStats=st)
     assert all(r.status == "Optimal" for r in rs)
+
+
+@pytest.mark.parametrize("mode", FORMS)
+def test_warm_start_from_solution_and_back_to_cold(mode):
+    lp = G.config1(1)
+    with pdhg.Engine(lp, opts(tolerance=1e-6, kernelMode=mode)) as e:
+        cold = e.solve()[0]
+        e.set_start(cold.x, cold.rowDual, cold.stats.primalWeight)
+        warm = e.solve()[0]
+        e.set_start(None, None)
+        cold2 = e.solve()[0]
+    assert cold.status == warm.status == "Optimal"
+    assert warm.iterations <= 64  # the first check already meets the tolerance
+    assert abs(warm.objective - cold.objective) <= 1e-5 * (1 + abs(cold.objective))
+    assert cold2.iterations == cold.iterations and np.array_equal(cold2.x, cold.x)
