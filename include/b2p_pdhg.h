@@ -269,6 +269,51 @@ typedef struct b2p_safe_bound {
 int b2p_safe_dual_bound(const b2p_lp* lp, const b2p_case* cases, int32_t num_cases, const double* row_dual,
                         b2p_safe_bound* out);
 
+/* Constraint-implied column bounds by activity-based bound propagation
+ * (30 rounds, continuous columns), each tightened bound relaxed by
+ * 1e-6 (1 + |bound|), untightened bounds left as given: the certifier's
+ * fallback for first-order duals (src/cert/certifier.cpp:340-356, calling
+ * Propagator::propagate of src/mip/propagate.cpp:23-138; the same steps as
+ * impliedBounds, src/parametric/parametric.cpp:62-73), bit-identical.
+ * Host computation, no GPU needed.  Outputs are num_cases x num_cols
+ * (case-major; num_cases <= 0: one case, the base model). */
+int b2p_implied_bounds(const b2p_lp* lp, const b2p_case* cases, int32_t num_cases, double* col_lower_out,
+                       double* col_upper_out);
+
+/* The certifier's verdict on an OPTIMAL claim (x, row_dual) of an LP
+ * (certify, src/cert/certifier.cpp:208-380, LP branch): relative column and
+ * row violations (compensated row activities) against primal_feasibility,
+ * the safe dual bound -- retried with constraint-implied column bounds when it
+ * is -inf -- and the relative gap (pobj - LB) / max(1, |pobj|) against
+ * relative_gap; without a finite bound the wrong-signed reduced cost is held
+ * against dual_feasibility.  Primal checks run on host threads, the bounds on
+ * the GPU (b2p_safe_dual_bound); every field is bit-identical to the
+ * reference's Certificate.  x is num_cases x num_cols, row_dual num_cases x
+ * num_rows (case-major). */
+typedef struct b2p_cert_tolerances {
+  double primal_feasibility; /* CertTolerances::primalFeas, 1e-6 */
+  double dual_feasibility;   /* CertTolerances::dualFeas, 1e-6 */
+  double relative_gap;       /* CertTolerances::relGap, 1e-6 */
+} b2p_cert_tolerances;
+
+typedef struct b2p_certificate {
+  int32_t accepted;              /* Certificate::accepted */
+  int32_t used_implied_bounds;   /* the bound came from constraint-implied column bounds */
+  double primal_objective;       /* c'x + offset */
+  double safe_dual_bound;        /* rigorous lower bound incl. offset, -inf if none */
+  double certified_gap;          /* relative gap, +inf without a bound */
+  double max_primal_violation;   /* max of the two below */
+  double max_col_violation;      /* relative column-bound violation */
+  double max_row_violation;      /* relative row violation */
+  double max_dual_violation;     /* SafeBoundResult::maxDualInfeasibility */
+  double cost_perturbation;      /* SafeBoundResult::costPerturbation */
+  int32_t infinite_terms;
+  int32_t worst_row;             /* row of max_row_violation, -1 if none */
+} b2p_certificate;
+
+int b2p_certify_lp(const b2p_lp* lp, const b2p_case* cases, int32_t num_cases, const double* x,
+                   const double* row_dual, const b2p_cert_tolerances* tol, b2p_certificate* out);
+
 /* Allocation-free form of b2p_kkt_residual.  No counterpart in the
  * reference.  For callers that cannot allocate device memory (a host
  * framework that owns all device memory through its own pool, code inside a

@@ -1,0 +1,227 @@
+// BF16 tensor-core GEMM for the warm-start network, on the 5th-generation
+// tensor cores (tcgen05): C[M x N] = alpha * A[M x K] B[K x N] with FP32
+// accumulation in tensor memory, plus a fused epilogue (bias, ReLU, a 0/1
+// mask from a BF16 array, FP32 and/or BF16 output).
+//
+// One CTA (128 threads) computes a 128 x kBN tile.  Per K chunk of 64 the
+// threads copy A (128 x 64) and B (kBN x 64) into shared memory in the
+// K-major, non-swizzled canonical layout of the UMMA descriptors -- core
+// matrices of 8 rows x 16 bytes, the two 8-element K halves of a 16-wide slab
+// LBO = 128 B apart, consecutive 8-row groups SBO = 256 B apart -- then one
+// elected thread issues four tcgen05.mma (K = 16 each) into the TMEM
+// accumulator and commits them to an mbarrier that every thread waits on
+// before the shared memory is refilled.  The epilogue reads the accumulator
+// with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = tile rows).
+// A and B are read from global memory through element strides, so either
+// operand may be used transposed.  Waits are bounded: on a timeout the kernel
+// records an error, frees its TMEM and returns.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include <cstdint>
+
+namespace b2p {
+
+constexpr int kGemmBM = 128;
+constexpr int kGemmBN = 128;
+constexpr int kGemmBK = 64;
+constexpr int kGemmThreads = 128;
+constexpr unsigned kMbarSpinLimit = 1u << 24;
+// shared memory: A chunk 16 KB + B chunk 16 KB; padded to 96 KB so that at
+// most two CTAs share an SM (2 x 128 TMEM columns <= 512)
+constexpr int kGemmSmemBytes = 96 * 1024;
+
+struct GemmArgs {
+  int32_t M, N, K;
+  const __nv_bfloat16* A;
+  int64_t sam, sak;  // A(m, k) = A[m * sam + k * sak]
+  const __nv_bfloat16* B;
+  int64_t sbk, sbn;  // B(k, n) = B[k * sbk + n * sbn]
+  float alpha;
+  const float* bias;  // bias[n] added after alpha, or NULL
+  int32_t relu;
+  const __nv_bfloat16* mask;  // C(m, n) *= (mask[m * ldm + n] > 0), or NULL
+  int64_t ldm;
+  float* cf;  // FP32 output C[m * ldcf + n], or NULL
+  int64_t ldcf;
+  __nv_bfloat16* cb;  // BF16 output, or NULL
+  int64_t ldcb;
+  int32_t* error;  // set to 1 on an mbarrier timeout
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// UMMA shared-memory descriptor, K-major, no swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((addr >> 4) & 0x3FFF);
+  d |= static_cast<uint64_t>((lbo_bytes >> 4) & 0x3FFF) << 16;
+  d |= static_cast<uint64_t>((sbo_bytes >> 4) & 0x3FFF) << 32;
+  d |= static_cast<uint64_t>(1) << 46;  // descriptor version (Blackwell)
+  // base offset 0, legacy LBO mode, layout type 0 = SWIZZLE_NONE
+  return d;
+}
+
+// Instruction descriptor: kind::f16, BF16 x BF16 -> F32, both K-major, M = 128.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int n) {
+  return (1u << 4)                                   // D format F32
+         | (1u << 7)                                 // A format BF16
+         | (1u << 10)                                // B format BF16
+         | (static_cast<uint32_t>(n >> 3) << 17)     // N / 8
+         | (static_cast<uint32_t>(kGemmBM >> 4) << 24);  // M / 16
+}
+
+// byte offset of element (r, k) of a row-major-in-K chunk of 64 columns
+__device__ __forceinline__ uint32_t chunk_offset(int r, int k, int rows) {
+  const int s = k >> 4, kk = k & 15;
+  return static_cast<uint32_t>(s * (rows / 8) * 256 + (r >> 3) * 256 + (kk >> 3) * 128 + (r & 7) * 16 + (kk & 7) * 2);
+}
+
+// Copy the rows [r0, r0 + rows) x K columns [k0, k0 + 64) of an operand
+// X(r, k) = X[r * sr + k * sk] into the canonical layout, zero-filling past
+// R and K.  vec: sk == 1 and 16-byte aligned rows, so one thread moves one
+// 8-element core-matrix row (16 bytes) per step; otherwise single elements,
+// row index fastest when sr == 1 (a transposed operand) for coalescing.
+__device__ __forceinline__ void stage_operand(unsigned char* dst, const __nv_bfloat16* X, int64_t sr, int64_t sk,
+                                              int r0, int R, int k0, int K, int rows, bool vec, int tid) {
+  if (vec) {
+    for (int e = tid; e < rows * (kGemmBK / 8); e += kGemmThreads) {
+      const int r = e / (kGemmBK / 8), k = (e % (kGemmBK / 8)) * 8;
+      const int gr = r0 + r, gk = k0 + k;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (gr < R && gk < K) v = *reinterpret_cast<const uint4*>(X + gr * sr + gk);
+      *reinterpret_cast<uint4*>(dst + chunk_offset(r, k, rows)) = v;
+    }
+    return;
+  }
+  const bool row_fast = sr == 1;
+  for (int e = tid; e < rows * kGemmBK; e += kGemmThreads) {
+    const int r = row_fast ? e % rows : e / kGemmBK, k = row_fast ? e / rows : e % kGemmBK;
+    const int gr = r0 + r, gk = k0 + k;
+    __nv_bfloat16 v = __float2bfloat16(0.0f);
+    if (gr < R && gk < K) v = X[gr * sr + gk * sk];
+    *reinterpret_cast<__nv_bfloat16*>(dst + chunk_offset(r, k, rows)) = v;
+  }
+}
+
+// vectorised staging applies: unit K stride, K and the row stride multiples
+// of 8 elements, 16-byte aligned base
+__host__ __device__ inline bool stage_vec_ok(const void* X, int64_t sr, int64_t sk, int K) {
+  return sk == 1 && K % 8 == 0 && sr % 8 == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+  for (unsigned spin = 0; spin < kMbarSpinLimit; ++spin) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+static __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tc(GemmArgs g) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ int failed_sh;
+  unsigned char* sA = smem;
+  unsigned char* sB = smem + kGemmBM * kGemmBK * 2;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * kGemmBM, n0 = blockIdx.y * kGemmBN;
+
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    failed_sh = 0;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                 "r"(kGemmBN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base_sh;
+  const uint32_t idesc = umma_idesc_bf16(kGemmBN);
+  const int nchunks = (g.K + kGemmBK - 1) / kGemmBK;
+  const bool vec_a = stage_vec_ok(g.A, g.sam, g.sak, g.K), vec_b = stage_vec_ok(g.B, g.sbn, g.sbk, g.K);
+  uint32_t phase = 0;
+  for (int ch = 0; ch < nchunks; ++ch) {
+    const int k0 = ch * kGemmBK;
+    stage_operand(sA, g.A, g.sam, g.sak, m0, g.M, k0, g.K, kGemmBM, vec_a, tid);
+    stage_operand(sB, g.B, g.sbn, g.sbk, n0, g.N, k0, g.K, kGemmBN, vec_b, tid);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+      for (int s = 0; s < kGemmBK / 16; ++s) {
+        const uint64_t da = umma_desc(smem_u32(sA) + s * (kGemmBM / 8) * 256, 128, 256);
+        const uint64_t db = umma_desc(smem_u32(sB) + s * (kGemmBN / 8) * 256, 128, 256);
+        const uint32_t acc = (ch > 0 || s > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+            :
+            : "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&mbar))
+                   : "memory");
+    }
+    // every thread waits for the MMAs before the shared memory is reused
+    if (!mbar_wait(smem_u32(&mbar), phase)) failed_sh = 1;
+    phase ^= 1u;
+    __syncthreads();
+    if (failed_sh) break;
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (!failed_sh) {
+    // epilogue: thread = tile row (TMEM lane), 8 columns per tcgen05.ld
+    const int row = warp * 32 + lane;
+    const int gm = m0 + row;
+    for (int c = 0; c < kGemmBN; c += 8) {
+      uint32_t r[8];
+      const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (gm < g.M) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int gn = n0 + c + q;
+          if (gn >= g.N) continue;
+          float v = __uint_as_float(r[q]) * g.alpha;
+          if (g.bias) v += g.bias[gn];
+          if (g.relu) v = v > 0.0f ? v : 0.0f;
+          if (g.mask && !(__bfloat162float(g.mask[gm * g.ldm + gn]) > 0.0f)) v = 0.0f;
+          if (g.cf) g.cf[gm * g.ldcf + gn] = v;
+          if (g.cb) g.cb[gm * g.ldcb + gn] = __float2bfloat16(v);
+        }
+      }
+    }
+  } else if (tid == 0) {
+    atomicExch(g.error, 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kGemmBN) : "memory");
+}
+
+}  // namespace b2p

@@ -1,4 +1,5 @@
-"""ctypes declarations of include/b2p_pdhg.h and the loader of libb2p_pdhg.so.
+"""ctypes declarations of include/b2p_pdhg.h and include/b2p_mlp.h, and the
+loader of libb2p_pdhg.so.
 
 The library is built in-tree (``make -C optimized-gpu-accelerator_b200``).
 There is no fallback: if the shared library is missing, ``load()`` raises.
@@ -71,7 +72,28 @@ class B2pResult(C.Structure):
                 ("objective", C.c_double), ("dual_objective", C.c_double), ("relative_kkt", C.c_double)]
 
 
-# Every symbol the header declares, with its ctypes signature.
+class B2pCertTolerances(C.Structure):
+    _fields_ = [("primal_feasibility", C.c_double), ("dual_feasibility", C.c_double), ("relative_gap", C.c_double)]
+
+
+class B2pCertificate(C.Structure):
+    _fields_ = [("accepted", C.c_int32), ("used_implied_bounds", C.c_int32), ("primal_objective", C.c_double),
+                ("safe_dual_bound", C.c_double), ("certified_gap", C.c_double),
+                ("max_primal_violation", C.c_double), ("max_col_violation", C.c_double),
+                ("max_row_violation", C.c_double), ("max_dual_violation", C.c_double),
+                ("cost_perturbation", C.c_double), ("infinite_terms", C.c_int32), ("worst_row", C.c_int32)]
+
+
+class B2pMlpTrainOptions(C.Structure):
+    _fields_ = [("epochs", C.c_int32), ("batch", C.c_int32), ("lr", C.c_float), ("lr_final", C.c_float),
+                ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float), ("weight_decay", C.c_float),
+                ("seed", C.c_uint64)]
+
+
+fptr = C.POINTER(C.c_float)
+u16ptr = C.c_void_p
+
+# Every symbol the headers declare, with its ctypes signature.
 SIGNATURES = {
     "b2p_default_options": (None, [C.POINTER(B2pOptions)]),
     "b2p_solve_pdhg": (C.c_int, [C.POINTER(B2pLp), C.POINTER(B2pOptions), dptr, dptr, C.POINTER(B2pResult),
@@ -96,11 +118,28 @@ SIGNATURES = {
     "b2p_csr_spmv": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, iptr, iptr, dptr, dptr, dptr]),
     "b2p_safe_dual_bound": (C.c_int, [C.POINTER(B2pLp), C.POINTER(B2pCase), C.c_int32, dptr,
                                       C.POINTER(B2pSafeBound)]),
+    "b2p_implied_bounds": (C.c_int, [C.POINTER(B2pLp), C.POINTER(B2pCase), C.c_int32, dptr, dptr]),
+    "b2p_certify_lp": (C.c_int, [C.POINTER(B2pLp), C.POINTER(B2pCase), C.c_int32, dptr, dptr,
+                                 C.POINTER(B2pCertTolerances), C.POINTER(B2pCertificate)]),
     "b2p_kkt_residual": (C.c_int, [C.POINTER(B2pLp), C.POINTER(B2pCase), C.c_int32, dptr, dptr, dptr]),
     "b2p_kkt_residual_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p]),
+    # include/b2p_mlp.h
+    "b2p_mlp_default_train_options": (B2pMlpTrainOptions, []),
+    "b2p_mlp_create": (C.c_int, [iptr, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
+    "b2p_mlp_destroy": (C.c_int, [C.c_void_p]),
+    "b2p_mlp_num_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "b2p_mlp_set_params": (C.c_int, [C.c_void_p, fptr]),
+    "b2p_mlp_get_params": (C.c_int, [C.c_void_p, fptr]),
+    "b2p_mlp_forward": (C.c_int, [C.c_void_p, fptr, C.c_int64, fptr]),
+    "b2p_mlp_forward_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]),
+    "b2p_mlp_loss_grad": (C.c_int, [C.c_void_p, fptr, fptr, C.c_int32, dptr, fptr]),
+    "b2p_mlp_train": (C.c_int, [C.c_void_p, fptr, fptr, C.c_int64, C.POINTER(B2pMlpTrainOptions), fptr]),
+    "b2p_mlp_gemm_bf16": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, u16ptr, C.c_int64, C.c_int64, u16ptr,
+                                    C.c_int64, C.c_int64, C.c_float, C.c_void_p, C.c_int32, u16ptr, C.c_int64,
+                                    C.c_void_p, C.c_int64, u16ptr, C.c_int64, C.c_void_p]),
 }
 
 _lock = threading.Lock()

@@ -114,7 +114,10 @@ def refinery_lp(periods: int = 12, crudes: int = 6, units: int = 10, pools: int 
     (an equivalent, badly scaled LP).  x = 0 is feasible and the LP is bounded.
 
     Family parameters: `crude_prices` (one per crude, default U(40, 120)) and
-    `demand_scales` (multiplying the demand of the first len() pools).
+    `demand_scales` (multiplying the demand of the first len() pools).  meta
+    holds the column indices of the crude purchases (`buy_cols`, T x C) and
+    product sales (`sale_cols`, R x T x P), the demand (R x P) and the column
+    scales, so that family members can be formed without rebuilding.
     Defaults give 48,072 rows, 99,144 columns and about 0.75M nonzeros.
     """
     rng = np.random.default_rng(seed)
@@ -128,7 +131,9 @@ def refinery_lp(periods: int = 12, crudes: int = 6, units: int = 10, pools: int 
     price = rng.uniform(150.0, 300.0, size=P)
     op_cost = rng.uniform(1.0, 5.0, size=U)
     elig = np.array([[rng.choice(P, size=pools_per_stream, replace=False) for _ in range(S)] for _ in range(U)])
-    cprice = rng.uniform(40.0, 120.0, size=C) if crude_prices is None else np.asarray(crude_prices, dtype=float)
+    cprice = rng.uniform(40.0, 120.0, size=C)  # drawn always, so the scalings below do not depend on it
+    if crude_prices is not None:
+        cprice = np.asarray(crude_prices, dtype=float)
     if demand_scales is not None:
         ds = np.asarray(demand_scales, dtype=float)
         demand = demand.copy()
@@ -228,7 +233,8 @@ def refinery_lp(periods: int = 12, crudes: int = 6, units: int = 10, pools: int 
     np.cumsum(np.bincount(ci, minlength=n), out=start[1:])
     return Model(num_rows=m, num_cols=n, start=start, index=ri, value=vv, col_cost=cost, col_lower=lo, col_upper=up,
                  row_lower=rl, row_upper=ru, name=name or f"refinery_T{T}_R{R}_s{seed}",
-                 meta={"seed": seed, "periods": T, "regions": R, "crude_prices": cprice.tolist()})
+                 meta={"seed": seed, "periods": T, "regions": R, "crude_prices": cprice.tolist(),
+                       "buy_cols": buy, "sale_cols": sale, "demand": demand, "col_scale": dc})
 
 
 def config3(seed: int = 3) -> Model:

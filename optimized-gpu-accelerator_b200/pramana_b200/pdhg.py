@@ -394,6 +394,42 @@ def safeDualBound(lp: Model, rowDual, cases: list[LpCase] | None = None) -> list
     return [{f: getattr(out[b], f) for f, _ in _lib.B2pSafeBound._fields_ if f != "pad0"} for b in range(k)]
 
 
+def impliedBounds(lp: Model, cases: list[LpCase] | None = None):
+    """Constraint-implied column bounds per case (the certifier's fallback,
+    src/cert/certifier.cpp:340-356), computed on host threads; returns
+    (lower, upper), each num_cases x num_cols."""
+    lib = _lib.load()
+    s, keep = _lp_struct(lp)
+    k = len(cases) if cases else 1
+    arr, keep2 = (_cases_struct(cases, lp.num_cols, lp.num_rows) if cases else (None, []))
+    lo = np.zeros((k, lp.num_cols))
+    up = np.zeros((k, lp.num_cols))
+    _lib.check(lib.b2p_implied_bounds(C.byref(s), arr, len(cases) if cases else 0, lo.ctypes.data_as(_lib.dptr),
+                                      up.ctypes.data_as(_lib.dptr)))
+    del keep, keep2
+    return lo, up
+
+
+def certifyLp(lp: Model, x, rowDual, cases: list[LpCase] | None = None, primalFeas: float = 1e-6,
+              dualFeas: float = 1e-6, relGap: float = 1e-6) -> list[dict]:
+    """pramana::certify of OPTIMAL claims (x, rowDual) per case, bit-identical
+    to the reference's Certificate; the safe bounds run on the GPU."""
+    lib = _lib.load()
+    s, keep = _lp_struct(lp)
+    k = len(cases) if cases else 1
+    arr, keep2 = (_cases_struct(cases, lp.num_cols, lp.num_rows) if cases else (None, []))
+    xa = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+    ya = np.ascontiguousarray(rowDual, dtype=np.float64).reshape(-1)
+    if len(xa) != k * lp.num_cols or len(ya) != k * lp.num_rows:
+        raise ValueError("x / rowDual have the wrong length")
+    tol = _lib.B2pCertTolerances(primalFeas, dualFeas, relGap)
+    out = (_lib.B2pCertificate * k)()
+    _lib.check(lib.b2p_certify_lp(C.byref(s), arr, len(cases) if cases else 0, xa.ctypes.data_as(_lib.dptr),
+                                  ya.ctypes.data_as(_lib.dptr), C.byref(tol), out))
+    del keep, keep2
+    return [{f: getattr(out[b], f) for f, _ in _lib.B2pCertificate._fields_} for b in range(k)]
+
+
 # snake_case aliases
 solve_pdhg = solvePdhg
 solve_pdhg_batch = solvePdhgBatch
@@ -401,4 +437,6 @@ gpu_available = gpuAvailable
 gpu_info_json = gpuInfoJson
 kkt_residual = kktResidual
 safe_dual_bound = safeDualBound
+implied_bounds = impliedBounds
+certify_lp = certifyLp
 solve_pdhg_multi = solvePdhgMulti

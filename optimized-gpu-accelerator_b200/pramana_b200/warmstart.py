@@ -1,0 +1,308 @@
+"""Learned warm start for a parametric LP family.
+
+A family member differs from its base LP only in some costs and bounds, so a
+whole batch shares A and is solved as one batched PDHG run (the reference's
+solvePdhgBatch with per-case overrides, src/pdhg/pdhg.h:67-70 -- the same
+shape as its "batched PDHG" family strategy, src/parametric/parametric.cpp:
+486-520).  The pieces:
+
+* ``RefineryFamily`` -- the multi-period refinery-planning LP with 16
+  parameters: the crude prices and the demand scales of 10 product pools;
+* ``PcaBasis`` -- standardised PCA of stacked primal-dual solutions [x; y];
+* ``LearnedWarmStart`` -- a ReLU MLP (``MlpNetwork``, trained and evaluated
+  on the tensor cores) from normalised parameters to PCA coefficients, whose
+  decoded [x; y] starts PDHG;
+* ``NearestWarmStart`` -- the baseline: the stored solution of the nearest
+  training parameter vector;
+* ``solve_family`` / ``certify_family`` -- batched solves from any start
+  (one shared-A batch per chunk, or the multi-LP engine that drops members
+  as they finish) and their certification: the KKT error recomputed on the
+  GPU, the reference's family rule for the safe dual bound, and the
+  reference certifier's full verdict.
+
+A start only moves PDHG's initial point: the solve, its termination test and
+the certification are the same as from a cold start, which stays the
+fallback (``solve_family`` with ``starts=None``).
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import generators as G
+from .mlp import MlpNetwork, TrainOptions
+from .model import LpCase, Model
+from .pdhg import (Engine, PdhgOptions, certifyLp, impliedBounds, kktResidual, safeDualBound,
+                   solvePdhgMulti)
+
+N_DEMAND = 10
+
+
+class RefineryFamily:
+    """Refinery-planning LPs (generators.refinery_lp) over one fixed
+    structure; parameters p = (crude prices (crudes), demand scales (10))."""
+
+    def __init__(self, seed: int = 5, crudes: int = 6, price_range=(40.0, 120.0), scale_range=(0.8, 1.2), **size):
+        size.setdefault("pools", N_DEMAND)
+        if size["pools"] < N_DEMAND:
+            raise ValueError("the family scales the demand of 10 pools")
+        self.crudes = crudes
+        self.lo = np.array([price_range[0]] * crudes + [scale_range[0]] * N_DEMAND)
+        self.hi = np.array([price_range[1]] * crudes + [scale_range[1]] * N_DEMAND)
+        mid = 0.5 * (self.lo + self.hi)
+        self.base: Model = G.refinery_lp(seed=seed, crudes=crudes, crude_prices=mid[:crudes],
+                                         demand_scales=mid[crudes:], **size)
+        meta = self.base.meta
+        self.buy = np.asarray(meta["buy_cols"])        # T x C
+        self.sale = np.asarray(meta["sale_cols"])      # R x T x P
+        self.col_scale = np.asarray(meta["col_scale"])
+        demand = np.asarray(meta["demand"]).copy()     # R x P, at the mid scales
+        demand[:, :N_DEMAND] /= mid[crudes:]
+        self.demand = demand                           # unscaled base demand
+        self.num_params = crudes + N_DEMAND
+
+    def sample(self, count: int, seed: int) -> np.ndarray:
+        rng = np.random.default_rng(seed)
+        return self.lo + (self.hi - self.lo) * rng.random((count, self.num_params))
+
+    def normalize(self, params) -> np.ndarray:
+        p = np.asarray(params, dtype=np.float64).reshape(-1, self.num_params)
+        return ((p - 0.5 * (self.lo + self.hi)) / (0.5 * (self.hi - self.lo))).astype(np.float32)
+
+    def case(self, p) -> LpCase:
+        p = np.asarray(p, dtype=np.float64)
+        cost = self.base.col_cost.copy()
+        up = self.base.col_upper.copy()
+        prices, scales = p[:self.crudes], p[self.crudes:]
+        cost[self.buy] = prices[None, :] * self.col_scale[self.buy]
+        dem = self.demand.copy()
+        dem[:, :N_DEMAND] *= scales[None, :]
+        R, T, P = self.sale.shape
+        up[self.sale] = dem[:, None, :] / self.col_scale[self.sale]
+        return LpCase(cost=cost, col_upper=up)
+
+    def instance(self, p) -> Model:
+        c = self.case(p)
+        b = self.base
+        return Model(num_rows=b.num_rows, num_cols=b.num_cols, start=b.start, index=b.index, value=b.value,
+                     col_cost=c.cost, col_lower=b.col_lower, col_upper=c.col_upper, row_lower=b.row_lower,
+                     row_upper=b.row_upper, obj_offset=b.obj_offset, name=f"{b.name}_member")
+
+
+class PcaBasis:
+    """Standardised PCA: z -> ((z - mean) / scale) V, V the leading right
+    singular vectors of the standardised training matrix."""
+
+    def fit(self, Z: np.ndarray, rank: int) -> "PcaBasis":
+        Z = np.asarray(Z, dtype=np.float64)
+        self.mean = Z.mean(axis=0)
+        sd = Z.std(axis=0)
+        self.scale = np.where(sd > 1e-12 * max(1.0, float(np.abs(Z).max())), sd, 1.0)
+        S = (Z - self.mean) / self.scale
+        _, sv, vt = np.linalg.svd(S, full_matrices=False)
+        r = min(rank, vt.shape[0])
+        self.V = vt[:r].T.copy()
+        if r < rank:  # pad with zero directions so the coefficient count stays `rank`
+            self.V = np.hstack([self.V, np.zeros((self.V.shape[0], rank - r))])
+        energy = sv ** 2
+        self.explained = float(energy[:r].sum() / max(energy.sum(), 1e-300))
+        return self
+
+    def encode(self, Z) -> np.ndarray:
+        return ((np.asarray(Z, dtype=np.float64) - self.mean) / self.scale) @ self.V
+
+    def decode(self, Cf) -> np.ndarray:
+        return self.mean + (np.asarray(Cf, dtype=np.float64) @ self.V.T) * self.scale
+
+
+class LearnedWarmStart:
+    """MLP (normalised parameters -> PCA coefficients of [x; y])."""
+
+    def __init__(self, family: RefineryFamily, hidden=(512, 512, 512), rank: int = 128, max_batch: int = 1024,
+                 seed: int = 0, device: int = -1):
+        self.family = family
+        self.rank = rank
+        self.widths = [family.num_params, *hidden, rank]
+        # the input width is padded to a multiple of 8 with zero features
+        self.in_width = -(-family.num_params // 8) * 8
+        self.widths[0] = self.in_width
+        self.net = MlpNetwork(self.widths, max_batch=max_batch, device=device, seed=seed)
+        self.basis: PcaBasis | None = None
+        self.coef_scale = 1.0
+        self.train_seconds = 0.0
+
+    def _features(self, params) -> np.ndarray:
+        f = self.family.normalize(params)
+        if self.in_width > f.shape[1]:
+            f = np.hstack([f, np.zeros((f.shape[0], self.in_width - f.shape[1]), dtype=np.float32)])
+        return f
+
+    def fit(self, params, X, Y, opts: TrainOptions | None = None) -> np.ndarray:
+        Z = np.hstack([np.asarray(X), np.asarray(Y)])
+        self.n = np.asarray(X).shape[1]
+        self.basis = PcaBasis().fit(Z, self.rank)
+        Cf = self.basis.encode(Z)
+        self.coef_scale = float(np.sqrt(np.mean(Cf ** 2))) or 1.0
+        t0 = time.perf_counter()
+        losses = self.net.train(self._features(params), (Cf / self.coef_scale).astype(np.float32), opts)
+        self.train_seconds = time.perf_counter() - t0
+        return losses
+
+    def predict(self, params):
+        """Starts (X, Y) in the original space; a member whose prediction is
+        not finite gets x = 0, y = 0, which the engine turns into exactly
+        the cold start (x projected onto the bounds)."""
+        Cf = self.net.forward(self._features(params)).astype(np.float64) * self.coef_scale
+        Z = self.basis.decode(Cf)
+        bad = ~np.all(np.isfinite(Z), axis=1)
+        Z[bad] = 0.0
+        return Z[:, :self.n], Z[:, self.n:]
+
+
+class NearestWarmStart:
+    """Start from the stored solution of the nearest training parameters."""
+
+    def __init__(self, family: RefineryFamily):
+        self.family = family
+
+    def fit(self, params, X, Y):
+        self.P = self.family.normalize(params).astype(np.float64)
+        self.X, self.Y = np.asarray(X), np.asarray(Y)
+        return self
+
+    def predict(self, params):
+        Q = self.family.normalize(params).astype(np.float64)
+        d = (Q ** 2).sum(1)[:, None] - 2.0 * Q @ self.P.T + (self.P ** 2).sum(1)[None, :]
+        j = np.argmin(d, axis=1)
+        return self.X[j], self.Y[j]
+
+
+@dataclass
+class FamilySolve:
+    status: np.ndarray          # per instance (1 = Optimal)
+    iterations: np.ndarray
+    relative_kkt: np.ndarray
+    objective: np.ndarray
+    X: np.ndarray
+    Y: np.ndarray
+    seconds: float = 0.0        # wall time: engine setup + start + solve + fetch
+    solve_seconds: float = 0.0  # the PDHG loop alone
+    batches: list = field(default_factory=list)
+
+
+def solve_family(family: RefineryFamily, params, opts: PdhgOptions | None = None, starts=None,
+                 batch: int = 1024, engine: str = "batch") -> FamilySolve:
+    """Batched PDHG over the family members `params`, in batches of `batch`
+    members; `starts` = (X, Y) in the original space, or None (cold start).
+    engine "batch": one shared-A k-case solve per chunk (every case advances
+    until the last one stops); "multi": the multi-LP engine, whose schedule
+    shrinks to the members still running."""
+    opts = opts or PdhgOptions()
+    params = np.asarray(params, dtype=np.float64).reshape(-1, family.num_params)
+    n, m = family.base.num_cols, family.base.num_rows
+    out = FamilySolve(*(np.zeros(0) for _ in range(4)), X=np.zeros((0, n)), Y=np.zeros((0, m)))
+    parts = []
+    for b0 in range(0, len(params), batch):
+        sl = slice(b0, min(b0 + batch, len(params)))
+        t0 = time.perf_counter()
+        if engine == "multi":
+            lps = [family.instance(p) for p in params[sl]]
+            st = None if starts is None else list(zip(np.asarray(starts[0])[sl], np.asarray(starts[1])[sl]))
+            t1 = time.perf_counter()
+            res = solvePdhgMulti(lps, opts, starts=st)
+            t2 = time.perf_counter()
+            t1 = t2 - res[0].stats.solveSeconds if res else t1
+        else:
+            cases = [family.case(p) for p in params[sl]]
+            eng = Engine(family.base, opts, cases)
+            try:
+                if starts is not None:
+                    eng.set_start(np.asarray(starts[0])[sl], np.asarray(starts[1])[sl])
+                t1 = time.perf_counter()
+                res = eng.solve()
+                t2 = time.perf_counter()
+            finally:
+                eng.close()
+        wall = time.perf_counter() - t0
+        parts.append(res)
+        out.seconds += wall
+        out.solve_seconds += t2 - t1
+        out.batches.append({"cases": len(res), "seconds": wall, "solve_seconds": t2 - t1,
+                            "iterations": int(max(r.iterations for r in res))})
+    res = [r for p in parts for r in p]
+    out.status = np.array([1 if r.status == "Optimal" else 0 for r in res])
+    out.iterations = np.array([r.iterations for r in res])
+    out.relative_kkt = np.array([r.relativeKkt for r in res])
+    out.objective = np.array([r.objective for r in res])
+    out.X = np.array([r.x for r in res]).reshape(-1, n)
+    out.Y = np.array([r.rowDual for r in res]).reshape(-1, m)
+    return out
+
+
+def certify_family(family: RefineryFamily, params, X, Y, kkt_tol: float = 1e-6, family_gap: float = 1e-4):
+    """Judges solutions of family members three ways, per member:
+
+    * ``kkt``: the relative KKT error (relP, relD, gap, max) recomputed on the
+      GPU from (x, y) in the original space (b2p_kkt_residual);
+    * ``family_certified``: the reference's family rule
+      (src/parametric/parametric.cpp:510-526): the safe dual bound over the
+      constraint-implied column bounds is finite and within `family_gap`
+      (1 + |obj|) of the objective;
+    * ``certificate``: the reference certifier's full verdict on an OPTIMAL
+      claim (b2p_certify_lp; 1e-6 primal, dual and gap tolerances).
+
+    ``certified`` = max KKT <= kkt_tol and family_certified."""
+    params = np.asarray(params, dtype=np.float64).reshape(-1, family.num_params)
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    Y = np.ascontiguousarray(Y, dtype=np.float64)
+    base = family.base
+    out = {k: [] for k in ("kkt", "objective", "bound", "family_certified", "accepted", "certified_gap",
+                           "primal_violation")}
+    for b0 in range(0, len(params), 1024):
+        sl = slice(b0, b0 + 1024)
+        cases = [family.case(p) for p in params[sl]]
+        out["kkt"].append(kktResidual(base, X[sl].reshape(-1), Y[sl].reshape(-1), cases))
+        lo, up = impliedBounds(base, cases)
+        icases = [LpCase(cost=c.cost, col_lower=lo[q], col_upper=up[q]) for q, c in enumerate(cases)]
+        sb = safeDualBound(base, Y[sl].reshape(-1), icases)
+        obj = np.array([float(np.dot(c.cost, x)) for c, x in zip(cases, X[sl])]) + base.obj_offset
+        bound = np.array([d["bound"] for d in sb]) + base.obj_offset
+        out["objective"].append(obj)
+        out["bound"].append(bound)
+        out["family_certified"].append(np.isfinite(bound) & (np.abs(obj - bound) <= family_gap * (1 + np.abs(obj))))
+        certs = certifyLp(base, X[sl].reshape(-1), Y[sl].reshape(-1), cases)
+        out["accepted"].append(np.array([c["accepted"] for c in certs], dtype=bool))
+        out["certified_gap"].append(np.array([c["certified_gap"] for c in certs]))
+        out["primal_violation"].append(np.array([c["max_primal_violation"] for c in certs]))
+    res = {k: (np.concatenate(v) if v else np.zeros(0)) for k, v in out.items()}
+    res["certified"] = (res["kkt"][:, 3] <= kkt_tol) & res["family_certified"]
+    return res
+
+
+def solve_warm(family: RefineryFamily, params, predictor=None, opts: PdhgOptions | None = None, batch: int = 1024,
+               engine: str = "batch", kkt_tol: float | None = None):
+    """Solve from the predictor's starts, judge every answer with
+    certify_family, and re-solve the members that fail from a cold start
+    (the fallback).  Returns (FamilySolve, certification, fallback mask)."""
+    opts = opts or PdhgOptions()
+    kkt_tol = opts.tolerance if kkt_tol is None else kkt_tol
+    starts = predictor.predict(params) if predictor is not None else None
+    res = solve_family(family, params, opts, starts=starts, batch=batch, engine=engine)
+    cert = certify_family(family, params, res.X, res.Y, kkt_tol=kkt_tol)
+    redo = ~cert["certified"]
+    if predictor is not None and redo.any():
+        idx = np.flatnonzero(redo)
+        again = solve_family(family, np.asarray(params)[idx], opts, batch=batch, engine=engine)
+        c2 = certify_family(family, np.asarray(params)[idx], again.X, again.Y, kkt_tol=kkt_tol)
+        warm_its = res.iterations[idx].copy()
+        for f in ("status", "iterations", "relative_kkt", "objective"):
+            getattr(res, f)[idx] = getattr(again, f)
+        res.iterations[idx] += warm_its  # the work of both attempts
+        res.X[idx], res.Y[idx] = again.X, again.Y
+        res.seconds += again.seconds
+        res.solve_seconds += again.solve_seconds
+        for k in cert:
+            cert[k][idx] = c2[k]
+    return res, cert, redo

@@ -179,6 +179,43 @@ def safe_dual_bound(lp, y, col_lower=None, col_upper=None, full: bool = False):
     return bound.value + lp.obj_offset
 
 
+def implied_bounds(lp, col_lower=None, col_upper=None):
+    """The reference certifier's constraint-implied column bounds (ref build)."""
+    h = _load("ref")
+    lo = np.ascontiguousarray(lp.col_lower if col_lower is None else col_lower, dtype=np.float64)
+    up = np.ascontiguousarray(lp.col_upper if col_upper is None else col_upper, dtype=np.float64)
+    lo_out, up_out = np.zeros(lp.num_cols), np.zeros(lp.num_cols)
+    rc = h.ref_implied_bounds(C.c_int(lp.num_rows), C.c_int(lp.num_cols), _ip(lp.start), _ip(lp.index),
+                              _dp(lp.value), _dp(lo), _dp(up), _dp(lp.row_lower), _dp(lp.row_upper), _dp(lo_out),
+                              _dp(up_out))
+    if rc != 0:
+        raise RuntimeError("implied bounds failed")
+    return lo_out, up_out
+
+
+CERT_FIELDS = ("accepted", "primal_objective", "safe_dual_bound", "certified_gap", "max_primal_violation",
+               "max_col_violation", "max_row_violation", "max_dual_violation", "cost_perturbation",
+               "used_implied_bounds")
+
+
+def certify(lp, x, y, tol=(1e-6, 1e-6, 1e-6)) -> dict:
+    """pramana::certify of an OPTIMAL claim (x, y) of a min-form LP (ref build)."""
+    h = _load("ref")
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    t = np.ascontiguousarray(tol, dtype=np.float64)
+    out = np.zeros(10)
+    rc = h.ref_certify_lp(C.c_int(lp.num_rows), C.c_int(lp.num_cols), _ip(lp.start), _ip(lp.index), _dp(lp.value),
+                          _dp(lp.col_cost), _dp(lp.col_lower), _dp(lp.col_upper), _dp(lp.row_lower),
+                          _dp(lp.row_upper), C.c_double(lp.obj_offset), _dp(x), _dp(y), _dp(t), _dp(out))
+    if rc != 0:
+        raise RuntimeError("certify failed")
+    d = dict(zip(CERT_FIELDS, out.tolist()))
+    d["accepted"] = int(d["accepted"])
+    d["used_implied_bounds"] = int(d["used_implied_bounds"])
+    return d
+
+
 def ruiz(lp, lib: str = "oracle", iterations: int = 10, pock_chambolle: bool = True):
     h = _load(lib)
     fn = h.oracle_ruiz_scaling if lib == "oracle" else h.ref_ruiz_scaling

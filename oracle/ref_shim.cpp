@@ -9,6 +9,8 @@
 //   - pramana::safeDualBound, the outward-rounded Neumaier-Shcherbina bound
 //                                          (src/cert/certifier.h:93)
 //   - pramana::ruizScaling                 (src/lp/scaling.cpp:97-139)
+//   - pramana::certify of an OPTIMAL LP claim (src/cert/certifier.cpp:208-380)
+//     and its constraint-implied column bounds (Propagator, src/mip/propagate.cpp)
 // The GPU path of the reference is switched off (PRAMANA_DISABLE_GPU) so that
 // loading this library never brings up a CUDA context or NVRTC.
 #include <cstdint>
@@ -21,6 +23,7 @@
 #include "cert/certifier.h"
 #include "core/model.h"
 #include "lp/scaling.h"
+#include "mip/propagate.h"
 #include "pdhg/pdhg.h"
 #include "util/log.h"
 #include "util/parallel.h"
@@ -186,6 +189,78 @@ int ref_safe_dual_bound(int m, int n, const int* start, const int* index, const 
       extra[1] = sb.rowProjection;
       extra[2] = sb.costPerturbation;
     }
+    return 0;
+  } catch (std::exception& e) {
+    gErr = e.what();
+    return 1;
+  }
+}
+
+// The certifier's constraint-implied column bounds (certifier.cpp:346-356):
+// Propagator on the continuous relaxation, 30 rounds, tightened bounds relaxed.
+int ref_implied_bounds(int m, int n, const int* start, const int* index, const double* value,
+                       const double* colLower, const double* colUpper, const double* rowLower, const double* rowUpper,
+                       double* loOut, double* upOut) {
+  try {
+    std::vector<double> zero(n, 0.0);
+    Model relaxed = buildModel(m, n, start, index, value, zero.data(), colLower, colUpper, rowLower, rowUpper, 0.0);
+    Propagator prop;
+    prop.setup(relaxed);
+    std::vector<double> lo = relaxed.colLower, up = relaxed.colUpper;
+    prop.propagate(lo, up, 30);
+    for (int j = 0; j < n; ++j) {
+      if (std::fabs(lo[j]) < kInfBoundThreshold &&
+          (!(std::fabs(relaxed.colLower[j]) < kInfBoundThreshold) || lo[j] > relaxed.colLower[j]))
+        lo[j] -= 1e-6 * (1 + std::fabs(lo[j]));
+      else lo[j] = relaxed.colLower[j];
+      if (std::fabs(up[j]) < kInfBoundThreshold &&
+          (!(std::fabs(relaxed.colUpper[j]) < kInfBoundThreshold) || up[j] < relaxed.colUpper[j]))
+        up[j] += 1e-6 * (1 + std::fabs(up[j]));
+      else up[j] = relaxed.colUpper[j];
+    }
+    std::memcpy(loOut, lo.data(), sizeof(double) * n);
+    std::memcpy(upOut, up.data(), sizeof(double) * n);
+    return 0;
+  } catch (std::exception& e) {
+    gErr = e.what();
+    return 1;
+  }
+}
+
+// pramana::certify of an OPTIMAL claim (x, y) on a min-form LP.
+// out: accepted, primalObjective, safeDualBound, certifiedGap, maxPrimalViolation,
+//      column violation, row violation, maxDualViolation, costPerturbation,
+//      used implied bounds (0/1)
+int ref_certify_lp(int m, int n, const int* start, const int* index, const double* value, const double* cost,
+                   const double* colLower, const double* colUpper, const double* rowLower, const double* rowUpper,
+                   double offset, const double* x, const double* y, const double* tol3, double* out) {
+  try {
+    Model lp = buildModel(m, n, start, index, value, cost, colLower, colUpper, rowLower, rowUpper, offset);
+    SolutionClaim claim;
+    claim.status = Status::Optimal;
+    claim.x.assign(x, x + n);
+    claim.rowDual.assign(y, y + m);
+    CertTolerances tol;
+    if (tol3) {
+      tol.primalFeas = tol3[0];
+      tol.dualFeas = tol3[1];
+      tol.relGap = tol3[2];
+    }
+    Certificate c = certify(lp, claim, tol);
+    out[0] = c.accepted ? 1.0 : 0.0;
+    out[1] = c.primalObjective;
+    out[2] = c.safeDualBound;
+    out[3] = c.certifiedGap;
+    out[4] = c.maxPrimalViolation;
+    out[5] = out[6] = 0.0;
+    out[9] = 0.0;
+    for (const CertCheck& k : c.checks) {
+      if (k.name == "primal_bound_violation") out[5] = k.value;
+      if (k.name == "primal_row_violation") out[6] = k.value;
+      if (k.name == "safe_dual_bound_gap" && k.detail.find("constraint-implied") != std::string::npos) out[9] = 1.0;
+    }
+    out[7] = c.maxDualViolation;
+    out[8] = c.costPerturbation;
     return 0;
   } catch (std::exception& e) {
     gErr = e.what();

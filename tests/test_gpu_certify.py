@@ -72,3 +72,66 @@ def test_safe_bound_batch_bitexact(oracle_mod):
         assert_same(got[b], oracle_mod.safe_dual_bound(one, rs[b].rowDual, full=True))
         # certified in the family sense: a finite safe bound within 1e-4 of the objective
         assert abs(rs[b].objective - (got[b]["bound"] + lp.obj_offset)) <= 1e-4 * (1 + abs(rs[b].objective))
+
+
+CERT_FIELDS = ("accepted", "primal_objective", "safe_dual_bound", "certified_gap", "max_primal_violation",
+               "max_col_violation", "max_row_violation", "max_dual_violation", "cost_perturbation",
+               "used_implied_bounds")
+
+
+def assert_same_cert(got: dict, want: dict):
+    for f in CERT_FIELDS:
+        g, w = got[f], want[f]
+        assert g == w or (np.isnan(g) and np.isnan(w)), (f, g, w)
+
+
+def _refinery():
+    from pramana_b200 import warmstart as W
+    return W.RefineryFamily(seed=5, periods=2, regions=1, units=4, streams=4, properties=2, scale_exponent=0.0)
+
+
+@pytest.mark.parametrize("which", ["c1", "edge", "refinery", "refinery_perturbed", "random_dual"])
+def test_certify_bitexact_vs_reference(oracle_mod, which):
+    """b2p_certify_lp against the reference's certify() on OPTIMAL claims:
+    accepted claims, a bound that needs the implied-bounds retry, a perturbed
+    (rejected) point, and a random dual (no rigorous bound)."""
+    if which == "c1":
+        lp = G.config1(1)
+        r = pdhg.solvePdhg(lp, pdhg.PdhgOptions(tolerance=1e-8))
+        x, y = r.x, r.rowDual
+    elif which == "edge":
+        lp = lp_cases.edge_lp(5)
+        r = pdhg.solvePdhg(lp, pdhg.PdhgOptions(tolerance=1e-8, maxIterations=200000))
+        x, y = r.x, r.rowDual
+    elif which.startswith("refinery"):
+        fam = _refinery()
+        lp = fam.instance(fam.sample(1, 8)[0])
+        r = pdhg.solvePdhg(lp, pdhg.PdhgOptions(tolerance=1e-6, maxIterations=200000))
+        x, y = r.x.copy(), r.rowDual
+        if which == "refinery_perturbed":
+            x *= 1.01
+    else:
+        lp = G.config1(2)
+        x = pdhg.solvePdhg(lp, pdhg.PdhgOptions(tolerance=1e-4)).x
+        y = np.random.default_rng(5).normal(size=lp.num_rows)
+    got = pdhg.certifyLp(lp, x, y)[0]
+    want = oracle_mod.certify(lp, x, y)
+    assert_same_cert(got, want)
+    if which == "c1":
+        assert got["accepted"] == 1
+    if which == "refinery_perturbed":
+        assert got["accepted"] == 0
+    if which == "refinery":
+        assert got["used_implied_bounds"] == 1 and np.isfinite(got["safe_dual_bound"])
+
+
+def test_certify_family_batch_bitexact(oracle_mod):
+    fam = _refinery()
+    params = fam.sample(6, 9)
+    cases = [fam.case(p) for p in params]
+    rs = pdhg.solvePdhgBatch(fam.base, cases, pdhg.PdhgOptions(tolerance=1e-6, maxIterations=200000))
+    X = np.concatenate([r.x for r in rs])
+    Y = np.concatenate([r.rowDual for r in rs])
+    got = pdhg.certifyLp(fam.base, X, Y, cases)
+    for b, p in enumerate(params):
+        assert_same_cert(got[b], oracle_mod.certify(fam.instance(p), rs[b].x, rs[b].rowDual))

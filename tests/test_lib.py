@@ -1,5 +1,5 @@
 """CPU checks of the C-ABI library: it loads, exports every symbol that
-include/b2p_pdhg.h declares, validates its inputs, and fails loudly (no CPU
+the headers under include/ declare, validates its inputs, and fails loudly (no CPU
 fallback) when no sm_100 device is present.  No kernel runs here."""
 import ctypes as C
 import json
@@ -12,11 +12,12 @@ import pytest
 from pramana_b200 import _lib, generators as G
 from pramana_b200.pdhg import PdhgOptions, _lp_struct
 
-HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "b2p_pdhg.h")
+INCLUDE = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+HEADERS = [os.path.join(INCLUDE, h) for h in sorted(os.listdir(INCLUDE)) if h.endswith(".h")]
 
 
 def declared_symbols():
-    text = open(HEADER).read()
+    text = "\n".join(open(h).read() for h in HEADERS)
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(b2p_[a-z0-9_]+)\s*\(", text)))
 
