@@ -241,3 +241,18 @@ def config3(seed: int = 3) -> Model:
     """The multi-period refinery-planning LP at its default size (12 periods,
     6 crudes, 10 units, 15 pools, 10 regions)."""
     return refinery_lp(seed=seed, name=f"c3_s{seed}")
+
+
+def uneven_family(count: int, nnz_lo: float = 1e4, nnz_hi: float = 2e6, seed: int = 4) -> list[Model]:
+    """Batched uneven workload: `count` LPs of the config-2 generator, instance i
+    with seed `seed` + i and a nonzero count drawn log-uniform from
+    [nnz_lo, nnz_hi] (m = nnz / 12.8 rows, n = 2m columns, 6.4 nonzeros per
+    column, 1% of the rows holding 10% of the nonzeros)."""
+    rng = np.random.default_rng(seed)
+    nnz = np.exp(rng.uniform(np.log(nnz_lo), np.log(nnz_hi), size=count))
+    out = []
+    for i, z in enumerate(nnz):
+        m = max(10, int(round(z / 12.8)))
+        out.append(random_lp(m, 2 * m, 6.4, int(0.6 * m), seed + i, heavy_row_frac=0.01, heavy_nnz_frac=0.10,
+                             name=f"c4_s{seed + i}"))
+    return out
