@@ -126,7 +126,16 @@ typedef struct b2p_options {
   /* Single-LP kernel form: B2P_KERNELS_AUTO picks the resident form when the
    * LP's operators fit in the SMs' shared memory. */
   int32_t kernel_mode;
+  /* SpMV schedule of the multi-LP engine's fused kernels, per operator:
+   * B2P_SCHEDULE_BINNED (rows binned by length, lanes per short row),
+   * B2P_SCHEDULE_TILED (TMA-staged tiles of short rows, for operators far
+   * larger than L2), B2P_SCHEDULE_TUNED (the autotuner times every binned
+   * lane count and the tiles on the device and keeps the fastest), or
+   * B2P_SCHEDULE_AUTO (TUNED from 2^20 nonzeros on, BINNED below). */
+  int32_t spmv_schedule;
 } b2p_options;
+
+enum { B2P_SCHEDULE_AUTO = 0, B2P_SCHEDULE_BINNED = 1, B2P_SCHEDULE_TILED = 2, B2P_SCHEDULE_TUNED = 3 };
 
 /* Replaces pramana::PdhgStats (src/pdhg/pdhg.h:44-56). */
 typedef struct b2p_stats {
@@ -151,6 +160,9 @@ typedef struct b2p_stats {
   int32_t precision_used;                     /* B2P_PRECISION_* actually run */
   int32_t pad1;
   int64_t fp32_iterations;                    /* mixed form: iterations run in FP32 */
+  int32_t schedule_a, schedule_at;            /* multi-LP: B2P_SCHEDULE_BINNED or _TILED per operator */
+  double autotune_seconds;                    /* multi-LP: time the autotuner took (part of setup) */
+  int32_t streaming_a, streaming_at;          /* multi-LP binned schedules: evict-first streaming loads */
 } b2p_stats;
 
 /* Replaces pramana::PdhgResult (src/pdhg/pdhg.h:58-65) minus the vectors,

@@ -1105,6 +1105,7 @@ void b2p_default_options(b2p_options* o) {
   o->precision = B2P_PRECISION_FP64;
   o->use_graphs = 1;
   o->kernel_mode = B2P_KERNELS_AUTO;
+  o->spmv_schedule = B2P_SCHEDULE_AUTO;
 }
 
 const char* b2p_last_error(void) { return b2p::last_error().c_str(); }

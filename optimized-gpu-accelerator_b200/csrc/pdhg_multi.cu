@@ -29,6 +29,7 @@
 #include "pdhg_prepare.h"
 #include "pdhg_sched.h"
 #include "pdhg_spmv.cuh"
+#include "pdhg_tiled.cuh"
 
 namespace b2p {
 
@@ -231,6 +232,19 @@ struct MultiEngine {
   std::vector<int64_t> inst_nnz;
   int64_t sched_nnz = 0;
   int ltA = 0, ltT = 0;
+  int64_t wave = 0;
+  int rounds = 2;
+  // Per operator, when chosen: the TMA-staged tile schedule of the short rows
+  // plus a binned schedule of the long rows only (pdhg_tiled.cuh).
+  struct TileSched {
+    bool on = false;
+    TileSet ts{};
+    RowBins longb{};
+  };
+  TileSched tilesA, tilesT;
+  bool streamA = false, streamT = false;  // binned schedules: evict-first streaming loads
+  int32_t* d_tile_err = nullptr;
+  int tile_ctas = 0;  // persistent CTAs of a tile launch
   double* h_sums = nullptr;
   double* h_steps = nullptr;
   int32_t *h_mask = nullptr, *h_done = nullptr;
@@ -253,6 +267,16 @@ struct MultiEngine {
   template <class T>
   T* upload(const std::vector<T>& h) {
     T* d = dalloc<T>(h.size());
+    if (!h.empty()) B2P_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+    bytes_up += static_cast<int64_t>(h.size() * sizeof(T));
+    return d;
+  }
+  // operator index / value arrays carry kTilePad zero entries for the
+  // 16-byte-rounded bulk copies of the tiled kernels
+  template <class T>
+  T* upload_padded(const std::vector<T>& h) {
+    T* d = dalloc<T>(h.size() + kTilePad);
+    B2P_CUDA(cudaMemsetAsync(d + h.size(), 0, kTilePad * sizeof(T), stream));
     if (!h.empty()) B2P_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
     bytes_up += static_cast<int64_t>(h.size() * sizeof(T));
     return d;
@@ -395,11 +419,11 @@ struct MultiEngine {
     // ---- device ----
     const auto tx = Clock::now();
     dA_ptr = upload(A.ptr);
-    dA_idx = upload(A.idx);
-    dA_val = upload(A.val);
+    dA_idx = upload_padded(A.idx);
+    dA_val = upload_padded(A.val);
     dT_ptr = upload(AT.ptr);
-    dT_idx = upload(AT.idx);
-    dT_val = upload(AT.val);
+    dT_idx = upload_padded(AT.idx);
+    dT_val = upload_padded(AT.val);
     d_rfac = upload(rfac);
     d_cfac = upload(cfac);
     d_rinst = upload(rinst);
@@ -415,6 +439,7 @@ struct MultiEngine {
     put(MRL, rl);
     put(MRU, ru);
     put(MXINIT, x0);
+    if (M) B2P_CUDA(cudaMemsetAsync(v[MYINIT], 0, sizeof(double) * M, stream));
     d_tau = dalloc<double>(K);
     d_sigma = dalloc<double>(K);
     d_it_base = dalloc<int64_t>(1);
@@ -450,8 +475,8 @@ struct MultiEngine {
     int per_sm = 0, sms = 0;
     B2P_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dual_binned<4, true, true>, kBlock, 0));
     B2P_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-    const int64_t wave = static_cast<int64_t>(std::max(1, per_sm)) * sms * kBlock;
-    const int rounds = opt.short_row_rounds > 0 ? opt.short_row_rounds : 2;
+    wave = static_cast<int64_t>(std::max(1, per_sm)) * sms * kBlock;
+    rounds = opt.short_row_rounds > 0 ? opt.short_row_rounds : 2;
     const HostBins hbA = make_bins(A, wave, opt.lanes_per_row_a, rounds);
     const HostBins hbT = make_bins(AT, wave, opt.lanes_per_row_at, rounds);
     binsA = device_bins(hbA, M);
@@ -463,12 +488,34 @@ struct MultiEngine {
     inst_nnz.assign(K, 0);
     for (int b = 0; b < K; ++b) inst_nnz[b] = static_cast<int64_t>(P[b].A.val.size());
     sched_nnz = annz;
-    stats.lanes_per_row_a = binsA.g;
-    stats.lanes_per_row_at = binsT.g;
     if (M > 0) {
       k_spmv<<<blocks(M), kBlock, 0, stream>>>(M, 1, viewA(), v[MXINIT], v[MAXINIT]);
       B2P_CUDA(cudaGetLastError());
     }
+    // tiled kernels: shared-memory opt-in and one persistent CTA per free slot
+    d_tile_err = dalloc<int32_t>(1);
+    B2P_CUDA(cudaMemsetAsync(d_tile_err, 0, sizeof(int32_t), stream));
+    for (const void* f : {(const void*)k_primal_tiled<true, true>, (const void*)k_primal_tiled<false, true>,
+                          (const void*)k_dual_tiled<true, true>, (const void*)k_dual_tiled<false, true>,
+                          (const void*)k_spmv_tiled<true>})
+      B2P_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmemBytes));
+    int tper = 0;
+    B2P_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tper, k_dual_tiled<true, true>, kBlock, kTileSmemBytes));
+    tile_ctas = std::max(1, tper) * sms;
+    const bool tune = opt.spmv_schedule == B2P_SCHEDULE_TUNED ||
+                      (opt.spmv_schedule == B2P_SCHEDULE_AUTO && annz >= (int64_t(1) << 20));
+    if (opt.spmv_schedule == B2P_SCHEDULE_TILED) {
+      tilesA = device_tiles(hA_ptr, roff, nullptr);
+      tilesT = device_tiles(hT_ptr, coff, nullptr);
+    } else if (tune) {
+      autotune(A, AT);
+    }
+    stats.lanes_per_row_a = binsA.g;
+    stats.lanes_per_row_at = binsT.g;
+    stats.schedule_a = tilesA.on ? B2P_SCHEDULE_TILED : B2P_SCHEDULE_BINNED;
+    stats.schedule_at = tilesT.on ? B2P_SCHEDULE_TILED : B2P_SCHEDULE_BINNED;
+    stats.streaming_a = !tilesA.on && streamA;
+    stats.streaming_at = !tilesT.on && streamT;
     B2P_CUDA(cudaStreamSynchronize(stream));
     stats.upload_seconds = seconds_since(tx);
     stats.setup_seconds = seconds_since(t0);
@@ -504,6 +551,222 @@ struct MultiEngine {
       B2P_CUDA(cudaGetLastError());
     }
     B2P_CUDA(cudaStreamSynchronize(stream));
+  }
+
+  // Tile schedule of an operator over the live LPs (all when done == NULL).
+  TileSched device_tiles(const std::vector<int32_t>& ptr, const std::vector<int64_t>& off,
+                         const std::vector<char>* done) {
+    const HostTiles h = make_tiles(ptr, off, done);
+    TileSched t;
+    t.on = true;
+    t.ts.tiles = upload(h.tiles);
+    t.ts.inst = upload(h.inst);
+    t.ts.n_tiles = static_cast<int32_t>(h.tiles.size());
+    t.ts.grid = std::max(1, std::min(t.ts.n_tiles, tile_ctas));
+    t.ts.err = d_tile_err;
+    RowBins& lb = t.longb;
+    lb.long_rows = upload(h.long_rows);
+    lb.vlong_rows = upload(h.vlong_rows);
+    lb.short_rows = nullptr;
+    lb.n_short = 0;
+    lb.n_long = static_cast<int32_t>(h.long_rows.size());
+    lb.n_vlong = static_cast<int32_t>(h.vlong_rows.size());
+    lb.long_thr = kTileRowMax;
+    lb.vlong_blocks = lb.n_vlong;
+    lb.long_blocks = (lb.n_long + kBlock / 32 - 1) / (kBlock / 32);
+    lb.short_blocks = 0;
+    lb.g = 1;
+    return t;
+  }
+
+  // The state every solve starts from (also the autotuner's playground).
+  void reset_state() {
+    auto cp = [&](int dst, int src, int64_t len) {
+      if (len) B2P_CUDA(cudaMemcpyAsync(v[dst], v[src], len * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    };
+    cp(MX, MXINIT, N);
+    cp(MX0, MXINIT, N);
+    cp(MAX, MAXINIT, M);
+    cp(MAX0, MAXINIT, M);
+    cp(MY, MYINIT, M);
+    cp(MY0, MYINIT, M);
+    B2P_CUDA(cudaMemsetAsync(d_it_base, 0, sizeof(int64_t), stream));
+    B2P_CUDA(cudaMemsetAsync(d_restart_at, 0, sizeof(int64_t) * K, stream));
+    B2P_CUDA(cudaMemsetAsync(d_done, 0, sizeof(int32_t) * K, stream));
+    upload_steps(omega0);
+  }
+
+  // One primal / dual / A^T y launch set with the operator's current schedule.
+  void enqueue_primal(bool halpern, const IterClock& ck) {
+    if (!N) return;
+    const double rho = opt.reflection;
+    const CsrView AT = viewAT();
+    const InstanceMap im{d_cinst, d_done};
+    if (tilesT.on) {
+      const RowBins& lb = tilesT.longb;
+      if (lb.vlong_blocks + lb.long_blocks > 0) {
+        if (halpern)
+          launch(k_primal_binned<1, true, true, true>, bin_grid(lb), stream, true, AT, lb, v[MY], v[MC], v[MLO],
+                 v[MUP], v[MX], v[MXP], v[MX0], d_tau, ck, rho, im);
+        else
+          launch(k_primal_binned<1, false, true, true>, bin_grid(lb), stream, true, AT, lb, v[MY], v[MC], v[MLO],
+                 v[MUP], v[MX], v[MXP], v[MX0], d_tau, ck, rho, im);
+      }
+      if (tilesT.ts.n_tiles > 0) {
+        if (halpern)
+          launch_smem(k_primal_tiled<true, true>, tilesT.ts.grid, kTileSmemBytes, stream, true, AT, tilesT.ts, v[MY],
+                      v[MC], v[MLO], v[MUP], v[MX], v[MXP], v[MX0], d_tau, ck, rho, im);
+        else
+          launch_smem(k_primal_tiled<false, true>, tilesT.ts.grid, kTileSmemBytes, stream, true, AT, tilesT.ts,
+                      v[MY], v[MC], v[MLO], v[MUP], v[MX], v[MXP], v[MX0], d_tau, ck, rho, im);
+      }
+      return;
+    }
+    const unsigned gp = bin_grid(binsT);
+#define B2P_MPRIMAL_S(G, H, S)                                                                              \
+  launch(k_primal_binned<G, H, true, S>, gp, stream, true, AT, binsT, v[MY], v[MC], v[MLO], v[MUP], v[MX], v[MXP], \
+         v[MX0], d_tau, ck, rho, im);
+#define B2P_MPRIMAL(G)                    \
+  if (streamT) {                          \
+    if (halpern) B2P_MPRIMAL_S(G, true, true) \
+    else B2P_MPRIMAL_S(G, false, true)    \
+  } else {                                \
+    if (halpern) B2P_MPRIMAL_S(G, true, false) \
+    else B2P_MPRIMAL_S(G, false, false)   \
+  }
+    B2P_G_SWITCH(binsT.g, B2P_MPRIMAL)
+#undef B2P_MPRIMAL
+#undef B2P_MPRIMAL_S
+  }
+
+  void enqueue_dual(bool halpern, const IterClock& ck) {
+    if (!M) return;
+    const double rho = opt.reflection;
+    const CsrView A = viewA();
+    const InstanceMap im{d_rinst, d_done};
+    if (tilesA.on) {
+      const RowBins& lb = tilesA.longb;
+      if (lb.vlong_blocks + lb.long_blocks > 0) {
+        if (halpern)
+          launch(k_dual_binned<1, true, true, true>, bin_grid(lb), stream, true, A, lb, v[MXP], v[MRL], v[MRU], v[MY],
+                 v[MYP], v[MY0], v[MAX], v[MAXP], v[MAX0], d_sigma, ck, rho, im);
+        else
+          launch(k_dual_binned<1, false, true, true>, bin_grid(lb), stream, true, A, lb, v[MXP], v[MRL], v[MRU],
+                 v[MY], v[MYP], v[MY0], v[MAX], v[MAXP], v[MAX0], d_sigma, ck, rho, im);
+      }
+      if (tilesA.ts.n_tiles > 0) {
+        if (halpern)
+          launch_smem(k_dual_tiled<true, true>, tilesA.ts.grid, kTileSmemBytes, stream, true, A, tilesA.ts, v[MXP],
+                      v[MRL], v[MRU], v[MY], v[MYP], v[MY0], v[MAX], v[MAXP], v[MAX0], d_sigma, ck, rho, im);
+        else
+          launch_smem(k_dual_tiled<false, true>, tilesA.ts.grid, kTileSmemBytes, stream, true, A, tilesA.ts, v[MXP],
+                      v[MRL], v[MRU], v[MY], v[MYP], v[MY0], v[MAX], v[MAXP], v[MAX0], d_sigma, ck, rho, im);
+      }
+      return;
+    }
+    const unsigned gd = bin_grid(binsA);
+#define B2P_MDUAL_S(G, H, S)                                                                                 \
+  launch(k_dual_binned<G, H, true, S>, gd, stream, true, A, binsA, v[MXP], v[MRL], v[MRU], v[MY], v[MYP], v[MY0], \
+         v[MAX], v[MAXP], v[MAX0], d_sigma, ck, rho, im);
+#define B2P_MDUAL(G)                      \
+  if (streamA) {                          \
+    if (halpern) B2P_MDUAL_S(G, true, true) \
+    else B2P_MDUAL_S(G, false, true)      \
+  } else {                                \
+    if (halpern) B2P_MDUAL_S(G, true, false) \
+    else B2P_MDUAL_S(G, false, false)     \
+  }
+    B2P_G_SWITCH(binsA.g, B2P_MDUAL)
+#undef B2P_MDUAL
+#undef B2P_MDUAL_S
+  }
+
+  void enqueue_aty() {
+    if (!N) return;
+    const CsrView AT = viewAT();
+    const InstanceMap im{d_cinst, d_done};
+    if (tilesT.on) {
+      const RowBins& lb = tilesT.longb;
+      if (lb.vlong_blocks + lb.long_blocks > 0)
+        launch(k_spmv_binned<1, true>, bin_grid(lb), stream, false, AT, lb, v[MYP], v[MATYP], im);
+      if (tilesT.ts.n_tiles > 0)
+        launch_smem(k_spmv_tiled<true>, tilesT.ts.grid, kTileSmemBytes, stream, false, AT, tilesT.ts, v[MYP],
+                    v[MATYP], im);
+      return;
+    }
+    const unsigned gp = bin_grid(binsT);
+#define B2P_MATY(G) launch(k_spmv_binned<G, true>, gp, stream, false, AT, binsT, v[MYP], v[MATYP], im);
+    B2P_G_SWITCH(binsT.g, B2P_MATY)
+#undef B2P_MATY
+  }
+
+  // Kernel launches of one iteration / of the A^T y+ product.
+  static int sched_launches(const TileSched& t) {
+    if (!t.on) return 1;
+    return (t.longb.vlong_blocks + t.longb.long_blocks > 0 ? 1 : 0) + (t.ts.n_tiles > 0 ? 1 : 0);
+  }
+
+  void check_tile_error() {
+    int32_t h = 0;
+    B2P_CUDA(cudaMemcpy(&h, d_tile_err, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (h) throw Error(B2P_ERR_CUDA, "tiled SpMV: a bulk copy did not complete (mbarrier wait timed out)");
+  }
+
+  // Autotuner: for A^T (primal kernel) and A (dual kernel) separately, time
+  // every binned schedule (1..32 lanes per short row, with cached or
+  // evict-first streaming loads) and the tile schedule on the device, from the
+  // solve's starting state, and keep the fastest.
+  void autotune(const HostCsr& A, const HostCsr& AT) {
+    const auto t0 = Clock::now();
+    reset_state();
+    cudaEvent_t e0, e1;
+    B2P_CUDA(cudaEventCreate(&e0));
+    B2P_CUDA(cudaEventCreate(&e1));
+    const IterClock ck{d_it_base, d_restart_at, 0};
+    auto timed = [&](auto&& enq) {
+      enq();
+      B2P_CUDA(cudaEventRecord(e0, stream));
+      for (int r = 0; r < 3; ++r) enq();
+      B2P_CUDA(cudaEventRecord(e1, stream));
+      B2P_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      B2P_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      return ms / 3.0;
+    };
+    auto tune = [&](const HostCsr& Op, int32_t rows, RowBins& bins, TileSched& tiles, bool& streaming,
+                    const std::vector<int32_t>& ptr, const std::vector<int64_t>& off, auto&& enq) {
+      double best = INFINITY;
+      int best_g = bins.g;
+      bool best_s = false;
+      tiles.on = false;
+      for (int g = 1; g <= 32; g *= 2) {
+        bins = device_bins(make_bins(Op, wave, g, rounds), rows);
+        for (int st = 0; st < 2; ++st) {
+          streaming = st != 0;
+          const double t = timed(enq);
+          if (t < best) {
+            best = t;
+            best_g = g;
+            best_s = streaming;
+          }
+        }
+      }
+      TileSched cand = device_tiles(ptr, off, nullptr);
+      tiles = cand;
+      const double tt = timed(enq);
+      if (tt < best) return;  // keep the tiles
+      tiles.on = false;
+      streaming = best_s;
+      bins = device_bins(make_bins(Op, wave, best_g, rounds), rows);
+    };
+    tune(AT, N, binsT, tilesT, streamT, hT_ptr, coff, [&] { enqueue_primal(true, ck); });
+    tune(A, M, binsA, tilesA, streamA, hA_ptr, roff, [&] { enqueue_dual(true, ck); });
+    ltA = binsA.long_thr;
+    ltT = binsT.long_thr;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    check_tile_error();
+    stats.autotune_seconds = seconds_since(t0);
   }
 
   RowBins device_bins(const HostBins& hb, int32_t rows) {
@@ -560,8 +823,10 @@ struct MultiEngine {
       if (!done[b]) live += inst_nnz[b];
     if (live == 0 || 2 * live >= sched_nnz) return;
     B2P_CUDA(cudaStreamSynchronize(stream));
-    binsA = live_bins(hA_ptr, roff, done, binsA.g, ltA);
-    binsT = live_bins(hT_ptr, coff, done, binsT.g, ltT);
+    if (tilesA.on) tilesA = device_tiles(hA_ptr, roff, &done);
+    else binsA = live_bins(hA_ptr, roff, done, binsA.g, ltA);
+    if (tilesT.on) tilesT = device_tiles(hT_ptr, coff, &done);
+    else binsT = live_bins(hT_ptr, coff, done, binsT.g, ltT);
     for (auto& g : graphs) cudaGraphExecDestroy(g.second);
     for (auto& g : graph_defs) cudaGraphDestroy(g.second);
     graphs.clear();
@@ -586,40 +851,12 @@ struct MultiEngine {
 
   void enqueue_interval(int L) {
     const double rho = opt.reflection;
-    const CsrView A = viewA(), AT = viewAT();
-    const InstanceMap imc{d_cinst, d_done}, imr{d_rinst, d_done};
-    const unsigned gp = bin_grid(binsT), gd = bin_grid(binsA);
     for (int l = 0; l < L; ++l) {
-      const bool last = l == L - 1;
       const IterClock ck{d_it_base, d_restart_at, l};
-      if (N) {
-#define B2P_MPRIMAL(G)                                                                                       \
-  if (last)                                                                                                  \
-    launch(k_primal_binned<G, false, true>, gp, stream, true, AT, binsT, v[MY], v[MC], v[MLO], v[MUP], v[MX], \
-           v[MXP], v[MX0], d_tau, ck, rho, imc);                                                             \
-  else                                                                                                       \
-    launch(k_primal_binned<G, true, true>, gp, stream, true, AT, binsT, v[MY], v[MC], v[MLO], v[MUP], v[MX],  \
-           v[MXP], v[MX0], d_tau, ck, rho, imc);
-        B2P_G_SWITCH(binsT.g, B2P_MPRIMAL)
-#undef B2P_MPRIMAL
-      }
-      if (M) {
-#define B2P_MDUAL(G)                                                                                         \
-  if (last)                                                                                                  \
-    launch(k_dual_binned<G, false, true>, gd, stream, true, A, binsA, v[MXP], v[MRL], v[MRU], v[MY], v[MYP],  \
-           v[MY0], v[MAX], v[MAXP], v[MAX0], d_sigma, ck, rho, imr);                                         \
-  else                                                                                                       \
-    launch(k_dual_binned<G, true, true>, gd, stream, true, A, binsA, v[MXP], v[MRL], v[MRU], v[MY], v[MYP],   \
-           v[MY0], v[MAX], v[MAXP], v[MAX0], d_sigma, ck, rho, imr);
-        B2P_G_SWITCH(binsA.g, B2P_MDUAL)
-#undef B2P_MDUAL
-      }
+      enqueue_primal(l != L - 1, ck);
+      enqueue_dual(l != L - 1, ck);
     }
-    if (N) {
-#define B2P_MATY(G) launch(k_spmv_binned<G, true>, gp, stream, false, AT, binsT, v[MYP], v[MATYP], imc);
-      B2P_G_SWITCH(binsT.g, B2P_MATY)
-#undef B2P_MATY
-    }
+    enqueue_aty();
     const IterClock ck{d_it_base, d_restart_at, L - 1};
     if (g_rows)
       k_check_rows_multi<<<g_rows, kBlock, 0, stream>>>(rtab, d_done, v[MAXP], v[MRL], v[MRU], v[MYP], v[MY], v[MY0],
@@ -660,7 +897,8 @@ struct MultiEngine {
     } else {
       enqueue_interval(L);
     }
-    launches += static_cast<int64_t>(L) * 2 + 5;
+    launches += static_cast<int64_t>(L) * (sched_launches(tilesT) + sched_launches(tilesA)) +
+                sched_launches(tilesT) + 4;
     bytes_down += static_cast<int64_t>(sizeof(double) * K * kNumSums);
   }
 
@@ -690,21 +928,8 @@ struct MultiEngine {
     B2P_CUDA(cudaSetDevice(device));
     const auto t_solve = Clock::now();
     launches = 0;
-    // initial state
-    auto cp = [&](int dst, int src, int64_t len) {
-      if (len) B2P_CUDA(cudaMemcpyAsync(v[dst], v[src], len * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-    };
-    cp(MX, MXINIT, N);
-    cp(MX0, MXINIT, N);
-    cp(MAX, MAXINIT, M);
-    cp(MAX0, MAXINIT, M);
-    cp(MY, MYINIT, M);
-    cp(MY0, MYINIT, M);
-    B2P_CUDA(cudaMemsetAsync(d_it_base, 0, sizeof(int64_t), stream));
-    B2P_CUDA(cudaMemsetAsync(d_restart_at, 0, sizeof(int64_t) * K, stream));
-    B2P_CUDA(cudaMemsetAsync(d_done, 0, sizeof(int32_t) * K, stream));
+    reset_state();
     std::vector<double> omega = omega0;
-    upload_steps(omega);
     results.assign(K, b2p_result{});
     xs.assign(K, {});
     ys.assign(K, {});
@@ -801,6 +1026,7 @@ struct MultiEngine {
       extract(b, (expiredStop || expired()) ? B2P_STATUS_TIME_LIMIT : B2P_STATUS_ITERATION_LIMIT,
               smax(relP, smax(relD, gap)), pobj, dobj, it);
     }
+    check_tile_error();
     stats.kernel_launches = launches;
     stats.bytes_uploaded = bytes_up;
     stats.bytes_downloaded = bytes_down;

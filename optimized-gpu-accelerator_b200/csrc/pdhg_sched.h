@@ -11,6 +11,7 @@
 #include "pdhg_host_common.h"
 #include "pdhg_prepare.h"
 #include "pdhg_spmv.cuh"
+#include "pdhg_tiled.cuh"
 
 namespace b2p {
 
@@ -66,6 +67,61 @@ inline HostBins make_bins(const HostCsr& M, int64_t wave_threads, int g_override
       hb.long_rows.push_back(i);
   }
   return hb;
+}
+
+// Tiles of consecutive short rows for the TMA-staged kernels (pdhg_tiled.cuh)
+// over the row ranges [off[b], off[b+1]) of the LPs not marked done: at most
+// kBlock rows and kTileEntries entries per tile, never crossing an LP; rows
+// longer than kTileRowMax go to the binned long / very-long lists.
+struct HostTiles {
+  std::vector<int4> tiles;
+  std::vector<int32_t> inst;
+  std::vector<int32_t> long_rows, vlong_rows;
+};
+
+inline HostTiles make_tiles(const std::vector<int32_t>& ptr, const std::vector<int64_t>& off,
+                            const std::vector<char>* done) {
+  HostTiles h;
+  const int K = static_cast<int>(off.size()) - 1;
+  for (int b = 0; b < K; ++b) {
+    if (done && (*done)[b]) continue;
+    int64_t r0 = -1;
+    auto close = [&](int64_t r1) {
+      if (r0 >= 0 && r1 > r0) {
+        h.tiles.push_back(make_int4(static_cast<int>(r0), static_cast<int>(r1), ptr[r0], ptr[r1]));
+        h.inst.push_back(b);
+      }
+      r0 = -1;
+    };
+    for (int64_t r = off[b]; r < off[b + 1]; ++r) {
+      const int32_t len = ptr[r + 1] - ptr[r];
+      if (len > kTileRowMax) {
+        close(r);
+        (len > kVeryLongRow ? h.vlong_rows : h.long_rows).push_back(static_cast<int32_t>(r));
+        continue;
+      }
+      if (r0 >= 0 && (r - r0 + 1 > kBlock || ptr[r + 1] - ptr[r0] > kTileEntries)) close(r);
+      if (r0 < 0) r0 = r;
+    }
+    close(off[b + 1]);
+  }
+  return h;
+}
+
+template <typename... KArgs, typename... Args>
+inline void launch_smem(void (*kern)(KArgs...), unsigned grid, size_t smem, cudaStream_t stream, bool pdl,
+                        Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kBlock);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = pdl ? attr : nullptr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  B2P_CUDA(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
 }
 
 template <typename... KArgs, typename... Args>

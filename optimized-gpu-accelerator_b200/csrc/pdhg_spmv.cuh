@@ -12,6 +12,11 @@
 // the sum is deterministic (it differs from the reference's strictly
 // sequential row sum only in rounding order).
 //
+// STREAM (operators much larger than L2): every load that is used once per
+// launch -- the operator's indices and values and the epilogue's vectors --
+// is an evict-first streaming load (ld.global.cs), so that L2 keeps the one
+// vector the rows gather from (written by the previous kernel).
+//
 // Latency hiding: a lane loads the column indices and values of its first
 // kUnroll chunks before anything else (these are constant during a solve, so
 // this happens before griddepcontrol.wait, while the previous kernel is still
@@ -65,8 +70,13 @@ struct RowPlan {
   double cv[kUnroll];
 };
 
+template <bool STREAM, class T>
+__device__ __forceinline__ T ld_once(const T* p) {
+  return STREAM ? __ldcs(p) : __ldg(p);
+}
+
 // Pre-wait part: row assignment and the first kUnroll (index, value) pairs.
-template <int G, bool MULTI = false>
+template <int G, bool MULTI = false, bool STREAM = false>
 __device__ __forceinline__ RowPlan plan_row(const CsrView& M, const RowBins& bins, InstanceMap im = {nullptr, nullptr}) {
   RowPlan pl;
   pl.row = -1;
@@ -108,16 +118,20 @@ __device__ __forceinline__ RowPlan plan_row(const CsrView& M, const RowBins& bin
       }
     }
   }
-  if (MULTI && pl.row >= 0 && im.done[im.inst[pl.row]]) {
-    pl.end = pl.p;  // terminated instance: no work
-    pl.leader = false;
-  }
+  // multi-LP: the row's instance is fetched beside the pairs, and a
+  // terminated instance's row drops its gathers and epilogue afterwards (so
+  // the pair loads do not wait for the instance's done flag)
+  const int32_t inst = (MULTI && pl.row >= 0) ? __ldg(im.inst + pl.row) : 0;
 #pragma unroll
   for (int u = 0; u < kUnroll; ++u) {
     const int q = pl.p + u * pl.stride;
     const bool ok = q < pl.end;
-    pl.ci[u] = ok ? __ldg(M.idx + q) : 0;
-    pl.cv[u] = ok ? __ldg(M.val + q) : 0.0;
+    pl.ci[u] = ok ? ld_once<STREAM>(M.idx + q) : 0;
+    pl.cv[u] = ok ? ld_once<STREAM>(M.val + q) : 0.0;
+  }
+  if (MULTI && pl.row >= 0 && __ldcg(im.done + inst)) {
+    pl.end = pl.p;  // terminated instance: no work
+    pl.leader = false;
   }
   return pl;
 }
@@ -132,7 +146,7 @@ __device__ __forceinline__ double lane_tree(double s) {
 // Post-wait part: the gathers, the lane sums and the tree.  Called by every
 // thread of the block (warp shuffles; __syncthreads on the block path, which
 // is block-uniform).  The result is valid on the leader thread.
-template <int G>
+template <int G, bool STREAM = false>
 __device__ __forceinline__ double finish_row(const RowPlan& pl, const CsrView& M, const double* __restrict__ x,
                                              double* sh /* kBlock/32 doubles */) {
   double xv[kUnroll];
@@ -149,8 +163,8 @@ __device__ __forceinline__ double finish_row(const RowPlan& pl, const CsrView& M
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) {
       const int q = p + u * pl.stride;
-      ci[u] = q < pl.end ? __ldg(M.idx + q) : 0;
-      cv[u] = q < pl.end ? __ldg(M.val + q) : 0.0;
+      ci[u] = q < pl.end ? ld_once<STREAM>(M.idx + q) : 0;
+      cv[u] = q < pl.end ? ld_once<STREAM>(M.val + q) : 0.0;
     }
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) xv[u] = (p + u * pl.stride < pl.end) ? __ldcg(x + ci[u]) : 0.0;
@@ -171,7 +185,7 @@ __device__ __forceinline__ double finish_row(const RowPlan& pl, const CsrView& M
 // x+ = proj(x - tau (c - A^T y)), Halpern step of x (skipped at a check
 // iteration).  A^T rows binned.  MULTI: several LPs, per-row instance b
 // selects tau[b] and the Halpern counter of b.
-template <int G, bool HALPERN, bool MULTI = false>
+template <int G, bool HALPERN, bool MULTI = false, bool STREAM = false>
 __global__ void __launch_bounds__(kBlock) k_primal_binned(CsrView AT, RowBins bins, const double* __restrict__ y,
                                                           const double* __restrict__ c, const double* __restrict__ lo,
                                                           const double* __restrict__ up, double* __restrict__ x,
@@ -179,26 +193,26 @@ __global__ void __launch_bounds__(kBlock) k_primal_binned(CsrView AT, RowBins bi
                                                           const double* __restrict__ tau, IterClock ck, double rho,
                                                           InstanceMap im = {nullptr, nullptr}) {
   __shared__ double sh[kBlock / 32];
-  const RowPlan pl = plan_row<G, MULTI>(AT, bins, im);
+  const RowPlan pl = plan_row<G, MULTI, STREAM>(AT, bins, im);
   const int j = pl.row;
   const int b = (MULTI && pl.leader) ? im.inst[j] : 0;
   double cj = 0, l = 0, u = 0;
   if (pl.leader) {
-    cj = __ldg(c + j);
-    l = __ldg(lo + j);
-    u = __ldg(up + j);
+    cj = ld_once<STREAM>(c + j);
+    l = ld_once<STREAM>(lo + j);
+    u = ld_once<STREAM>(up + j);
   }
   pdl_wait();
   double xv = 0, x0v = 0, t = 0, lam = 0;
   if (pl.leader) {
-    xv = __ldcg(x + j);
+    xv = STREAM ? __ldcs(x + j) : __ldcg(x + j);
     t = __ldcg(tau + b);
     if (HALPERN) {
-      x0v = __ldcg(x0 + j);
+      x0v = STREAM ? __ldcs(x0 + j) : __ldcg(x0 + j);
       lam = halpern_lambda(ck, b);
     }
   }
-  const double aty = finish_row<G>(pl, AT, y, sh);
+  const double aty = finish_row<G, STREAM>(pl, AT, y, sh);
   pdl_launch_dependents();
   if (!pl.leader) return;
   double v = __dsub_rn(xv, __dmul_rn(t, __dsub_rn(cj, aty)));
@@ -209,7 +223,7 @@ __global__ void __launch_bounds__(kBlock) k_primal_binned(CsrView AT, RowBins bi
 }
 
 // y+ = v + sigma proj(-v/sigma), v = y - sigma (2 A x+ - A x); Halpern steps of y and Ax.
-template <int G, bool HALPERN, bool MULTI = false>
+template <int G, bool HALPERN, bool MULTI = false, bool STREAM = false>
 __global__ void __launch_bounds__(kBlock) k_dual_binned(CsrView A, RowBins bins, const double* __restrict__ xp,
                                                         const double* __restrict__ rl, const double* __restrict__ ru,
                                                         double* __restrict__ y, double* __restrict__ yp,
@@ -218,27 +232,27 @@ __global__ void __launch_bounds__(kBlock) k_dual_binned(CsrView A, RowBins bins,
                                                         const double* __restrict__ sigma, IterClock ck, double rho,
                                                         InstanceMap im = {nullptr, nullptr}) {
   __shared__ double sh[kBlock / 32];
-  const RowPlan pl = plan_row<G, MULTI>(A, bins, im);
+  const RowPlan pl = plan_row<G, MULTI, STREAM>(A, bins, im);
   const int i = pl.row;
   const int b = (MULTI && pl.leader) ? im.inst[i] : 0;
   double l = 0, u = 0;
   if (pl.leader) {
-    l = __ldg(rl + i);
-    u = __ldg(ru + i);
+    l = ld_once<STREAM>(rl + i);
+    u = ld_once<STREAM>(ru + i);
   }
   pdl_wait();
   double axv = 0, yv = 0, s = 0, y0v = 0, ax0v = 0, lam = 0;
   if (pl.leader) {
-    axv = __ldcg(ax + i);
-    yv = __ldcg(y + i);
+    axv = STREAM ? __ldcs(ax + i) : __ldcg(ax + i);
+    yv = STREAM ? __ldcs(y + i) : __ldcg(y + i);
     s = __ldcg(sigma + b);
     if (HALPERN) {
-      y0v = __ldcg(y0 + i);
-      ax0v = __ldcg(ax0 + i);
+      y0v = STREAM ? __ldcs(y0 + i) : __ldcg(y0 + i);
+      ax0v = STREAM ? __ldcs(ax0 + i) : __ldcg(ax0 + i);
       lam = halpern_lambda(ck, b);
     }
   }
-  const double axpv = finish_row<G>(pl, A, xp, sh);
+  const double axpv = finish_row<G, STREAM>(pl, A, xp, sh);
   pdl_launch_dependents();
   if (!pl.leader) return;
   const double v = __dsub_rn(yv, __dmul_rn(s, __dsub_rn(__dmul_rn(2.0, axpv), axv)));

@@ -20,6 +20,7 @@ STATUS_NAMES = {0: "NotSolved", 1: "Optimal", 5: "TimeLimit", 6: "IterationLimit
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 KERNELS_AUTO, KERNELS_FUSED, KERNELS_RESIDENT = 0, 1, 2
+SCHEDULE_AUTO, SCHEDULE_BINNED, SCHEDULE_TILED, SCHEDULE_TUNED = 0, 1, 2, 3
 
 dptr = C.POINTER(C.c_double)
 iptr = C.POINTER(C.c_int32)
@@ -43,7 +44,7 @@ class B2pOptions(C.Structure):
                 ("log_interval", C.c_int32), ("device", C.c_int32), ("time_limit", C.c_double),
                 ("cancel_flag", C.POINTER(C.c_int32)), ("precision", C.c_int32), ("use_graphs", C.c_int32),
                 ("lanes_per_row_a", C.c_int32), ("lanes_per_row_at", C.c_int32), ("short_row_rounds", C.c_int32),
-                ("kernel_mode", C.c_int32)]
+                ("kernel_mode", C.c_int32), ("spmv_schedule", C.c_int32)]
 
 
 class B2pStats(C.Structure):
@@ -55,7 +56,9 @@ class B2pStats(C.Structure):
                 ("prepare_seconds", C.c_double), ("upload_seconds", C.c_double), ("graph_seconds", C.c_double),
                 ("lanes_per_row_a", C.c_int32), ("lanes_per_row_at", C.c_int32), ("kernel_mode", C.c_int32),
                 ("resident_blocks", C.c_int32), ("resident_smem_bytes", C.c_int64), ("precision_used", C.c_int32),
-                ("pad1", C.c_int32), ("fp32_iterations", C.c_int64)]
+                ("pad1", C.c_int32), ("fp32_iterations", C.c_int64), ("schedule_a", C.c_int32),
+                ("schedule_at", C.c_int32), ("autotune_seconds", C.c_double), ("streaming_a", C.c_int32),
+                ("streaming_at", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_ if not f.startswith("pad")}

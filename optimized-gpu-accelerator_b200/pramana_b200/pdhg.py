@@ -47,6 +47,7 @@ class PdhgOptions:
     lanesPerRowAT: int = 0
     shortRowRounds: int = 0
     kernelMode: int = _lib.KERNELS_AUTO   # KERNELS_FUSED / KERNELS_RESIDENT to force a form
+    spmvSchedule: int = _lib.SCHEDULE_AUTO  # multi-LP SpMV schedule (SCHEDULE_BINNED / _TILED / _TUNED)
 
     def to_c(self, cancel_flag=None) -> _lib.B2pOptions:
         if not self.useGpu:
@@ -69,6 +70,7 @@ class PdhgOptions:
         o.lanes_per_row_at = int(self.lanesPerRowAT)
         o.short_row_rounds = int(self.shortRowRounds)
         o.kernel_mode = int(self.kernelMode)
+        o.spmv_schedule = int(self.spmvSchedule)
         if cancel_flag is not None:
             o.cancel_flag = C.cast(cancel_flag, C.POINTER(C.c_int32))
         return o

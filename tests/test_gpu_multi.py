@@ -62,3 +62,57 @@ def test_multi_warm_start():
             assert w.iterations <= 64
         else:
             assert w.iterations == c.iterations
+
+
+# ---- SpMV schedules of the multi-LP engine: TMA-staged tiles and the autotuner ----
+
+from pramana_b200 import _lib  # noqa: E402
+
+
+@pytest.mark.parametrize("sched", [_lib.SCHEDULE_TILED, _lib.SCHEDULE_TUNED])
+@pytest.mark.parametrize("iters", [1, 64, 1000])
+def test_multi_schedules_fixed_iterations_vs_oracle(oracle_mod, sched, iters):
+    lps = family()
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-30, maxIterations=iters, spmvSchedule=sched))
+    st = pdhg.solvePdhgMulti.last_stats
+    if sched == _lib.SCHEDULE_TILED:
+        assert st.schedule_a == _lib.SCHEDULE_TILED and st.schedule_at == _lib.SCHEDULE_TILED
+    else:
+        assert st.autotune_seconds > 0
+    for lp, r in zip(lps, rs):
+        assert_close(r, oracle_mod.solve(lp, "oracle", tolerance=1e-30, max_iterations=iters))
+
+
+@pytest.mark.parametrize("iters", [1, 2, 63])
+def test_tiled_rows_sum_in_reference_order(oracle_mod, iters):
+    """Every row and column of config-1 has at most 32 entries, so the tiled
+    kernels sum every row left to right exactly as the reference does: before
+    the first check the iterates are bit-identical to the oracle's."""
+    lp = G.config1(1)
+    assert np.diff(lp.start).max() <= 32 and np.bincount(lp.index).max() <= 32
+    r = pdhg.solvePdhgMulti([lp], opts(tolerance=1e-30, maxIterations=iters,
+                                       spmvSchedule=_lib.SCHEDULE_TILED))[0]
+    o = oracle_mod.solve(lp, "oracle", tolerance=1e-30, max_iterations=iters)
+    assert np.array_equal(r.x, o.x) and np.array_equal(r.rowDual, o.y)
+
+
+def test_tiled_many_tiles_per_cta_matches_binned():
+    """~3M nonzeros: several tiles per persistent CTA (double-buffered bulk
+    copies), long rows on the binned path beside them."""
+    lps = G.uneven_family(8, 2e5, 6e5, seed=11)
+    kw = dict(tolerance=1e-30, maxIterations=200)
+    rb = pdhg.solvePdhgMulti(lps, opts(spmvSchedule=_lib.SCHEDULE_BINNED, **kw))
+    rt = pdhg.solvePdhgMulti(lps, opts(spmvSchedule=_lib.SCHEDULE_TILED, **kw))
+    for a, b in zip(rb, rt):
+        assert np.linalg.norm(a.x - b.x) <= 1e-9 * np.linalg.norm(a.x)
+        assert np.linalg.norm(a.rowDual - b.rowDual) <= 1e-9 * np.linalg.norm(a.rowDual)
+
+
+def test_tiled_converged_and_compacted(oracle_mod):
+    lps = family() + [G.random_lp(3000, 6000, 6.4, 1800, 21, heavy_row_frac=0.01, heavy_nnz_frac=0.1)]
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, maxIterations=200000, spmvSchedule=_lib.SCHEDULE_TILED))
+    for lp, r in zip(lps, rs):
+        o = oracle_mod.solve(lp, "oracle", tolerance=1e-6, max_iterations=200000)
+        assert r.status == "Optimal" and o.status == 1
+        assert abs(r.iterations - o.iterations) <= 4 * 64
+        assert max(_host_kkt(lp, r.x, r.rowDual)) <= 1.5e-6
