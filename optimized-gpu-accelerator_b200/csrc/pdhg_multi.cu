@@ -234,8 +234,8 @@ struct MultiEngine {
   int ltA = 0, ltT = 0;
   int64_t wave = 0;
   int rounds = 2;
-  // Per operator, when chosen: the TMA-staged tile schedule of the short rows
-  // plus a binned schedule of the long rows only (pdhg_tiled.cuh).
+  // Per operator, when chosen: the warp-tile schedule of the short rows plus a
+  // binned schedule of the long rows only (pdhg_tiled.cuh).
   struct TileSched {
     bool on = false;
     TileSet ts{};
@@ -243,8 +243,6 @@ struct MultiEngine {
   };
   TileSched tilesA, tilesT;
   bool streamA = false, streamT = false;  // binned schedules: evict-first streaming loads
-  int32_t* d_tile_err = nullptr;
-  int tile_ctas = 0;  // persistent CTAs of a tile launch
   double* h_sums = nullptr;
   double* h_steps = nullptr;
   int32_t *h_mask = nullptr, *h_done = nullptr;
@@ -271,8 +269,7 @@ struct MultiEngine {
     bytes_up += static_cast<int64_t>(h.size() * sizeof(T));
     return d;
   }
-  // operator index / value arrays carry kTilePad zero entries for the
-  // 16-byte-rounded bulk copies of the tiled kernels
+  // operator index / value arrays carry kTilePad zero entries past the end
   template <class T>
   T* upload_padded(const std::vector<T>& h) {
     T* d = dalloc<T>(h.size() + kTilePad);
@@ -492,16 +489,6 @@ struct MultiEngine {
       k_spmv<<<blocks(M), kBlock, 0, stream>>>(M, 1, viewA(), v[MXINIT], v[MAXINIT]);
       B2P_CUDA(cudaGetLastError());
     }
-    // tiled kernels: shared-memory opt-in and one persistent CTA per free slot
-    d_tile_err = dalloc<int32_t>(1);
-    B2P_CUDA(cudaMemsetAsync(d_tile_err, 0, sizeof(int32_t), stream));
-    for (const void* f : {(const void*)k_primal_tiled<true, true>, (const void*)k_primal_tiled<false, true>,
-                          (const void*)k_dual_tiled<true, true>, (const void*)k_dual_tiled<false, true>,
-                          (const void*)k_spmv_tiled<true>})
-      B2P_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmemBytes));
-    int tper = 0;
-    B2P_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tper, k_dual_tiled<true, true>, kBlock, kTileSmemBytes));
-    tile_ctas = std::max(1, tper) * sms;
     const bool tune = opt.spmv_schedule == B2P_SCHEDULE_TUNED ||
                       (opt.spmv_schedule == B2P_SCHEDULE_AUTO && annz >= (int64_t(1) << 20));
     if (opt.spmv_schedule == B2P_SCHEDULE_TILED) {
@@ -562,8 +549,7 @@ struct MultiEngine {
     t.ts.tiles = upload(h.tiles);
     t.ts.inst = upload(h.inst);
     t.ts.n_tiles = static_cast<int32_t>(h.tiles.size());
-    t.ts.grid = std::max(1, std::min(t.ts.n_tiles, tile_ctas));
-    t.ts.err = d_tile_err;
+    t.ts.grid = std::max(1, (t.ts.n_tiles + kBlock / 32 - 1) / (kBlock / 32));
     RowBins& lb = t.longb;
     lb.long_rows = upload(h.long_rows);
     lb.vlong_rows = upload(h.vlong_rows);
@@ -614,10 +600,10 @@ struct MultiEngine {
       }
       if (tilesT.ts.n_tiles > 0) {
         if (halpern)
-          launch_smem(k_primal_tiled<true, true>, tilesT.ts.grid, kTileSmemBytes, stream, true, AT, tilesT.ts, v[MY],
+          launch(k_primal_tiled<true, true>, tilesT.ts.grid, stream, true, AT, tilesT.ts, v[MY],
                       v[MC], v[MLO], v[MUP], v[MX], v[MXP], v[MX0], d_tau, ck, rho, im);
         else
-          launch_smem(k_primal_tiled<false, true>, tilesT.ts.grid, kTileSmemBytes, stream, true, AT, tilesT.ts,
+          launch(k_primal_tiled<false, true>, tilesT.ts.grid, stream, true, AT, tilesT.ts,
                       v[MY], v[MC], v[MLO], v[MUP], v[MX], v[MXP], v[MX0], d_tau, ck, rho, im);
       }
       return;
@@ -656,10 +642,10 @@ struct MultiEngine {
       }
       if (tilesA.ts.n_tiles > 0) {
         if (halpern)
-          launch_smem(k_dual_tiled<true, true>, tilesA.ts.grid, kTileSmemBytes, stream, true, A, tilesA.ts, v[MXP],
+          launch(k_dual_tiled<true, true>, tilesA.ts.grid, stream, true, A, tilesA.ts, v[MXP],
                       v[MRL], v[MRU], v[MY], v[MYP], v[MY0], v[MAX], v[MAXP], v[MAX0], d_sigma, ck, rho, im);
         else
-          launch_smem(k_dual_tiled<false, true>, tilesA.ts.grid, kTileSmemBytes, stream, true, A, tilesA.ts, v[MXP],
+          launch(k_dual_tiled<false, true>, tilesA.ts.grid, stream, true, A, tilesA.ts, v[MXP],
                       v[MRL], v[MRU], v[MY], v[MYP], v[MY0], v[MAX], v[MAXP], v[MAX0], d_sigma, ck, rho, im);
       }
       return;
@@ -690,7 +676,7 @@ struct MultiEngine {
       if (lb.vlong_blocks + lb.long_blocks > 0)
         launch(k_spmv_binned<1, true>, bin_grid(lb), stream, false, AT, lb, v[MYP], v[MATYP], im);
       if (tilesT.ts.n_tiles > 0)
-        launch_smem(k_spmv_tiled<true>, tilesT.ts.grid, kTileSmemBytes, stream, false, AT, tilesT.ts, v[MYP],
+        launch(k_spmv_tiled<true>, tilesT.ts.grid, stream, false, AT, tilesT.ts, v[MYP],
                     v[MATYP], im);
       return;
     }
@@ -704,12 +690,6 @@ struct MultiEngine {
   static int sched_launches(const TileSched& t) {
     if (!t.on) return 1;
     return (t.longb.vlong_blocks + t.longb.long_blocks > 0 ? 1 : 0) + (t.ts.n_tiles > 0 ? 1 : 0);
-  }
-
-  void check_tile_error() {
-    int32_t h = 0;
-    B2P_CUDA(cudaMemcpy(&h, d_tile_err, sizeof(int32_t), cudaMemcpyDeviceToHost));
-    if (h) throw Error(B2P_ERR_CUDA, "tiled SpMV: a bulk copy did not complete (mbarrier wait timed out)");
   }
 
   // Autotuner: for A^T (primal kernel) and A (dual kernel) separately, time
@@ -765,7 +745,6 @@ struct MultiEngine {
     ltT = binsT.long_thr;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    check_tile_error();
     stats.autotune_seconds = seconds_since(t0);
   }
 
@@ -1026,7 +1005,6 @@ struct MultiEngine {
       extract(b, (expiredStop || expired()) ? B2P_STATUS_TIME_LIMIT : B2P_STATUS_ITERATION_LIMIT,
               smax(relP, smax(relD, gap)), pobj, dobj, it);
     }
-    check_tile_error();
     stats.kernel_launches = launches;
     stats.bytes_uploaded = bytes_up;
     stats.bytes_downloaded = bytes_down;

@@ -69,10 +69,10 @@ inline HostBins make_bins(const HostCsr& M, int64_t wave_threads, int g_override
   return hb;
 }
 
-// Tiles of consecutive short rows for the TMA-staged kernels (pdhg_tiled.cuh)
-// over the row ranges [off[b], off[b+1]) of the LPs not marked done: at most
-// kBlock rows and kTileEntries entries per tile, never crossing an LP; rows
-// longer than kTileRowMax go to the binned long / very-long lists.
+// Warp tiles of consecutive short rows (pdhg_tiled.cuh) over the row ranges
+// [off[b], off[b+1]) of the LPs not marked done: at most kTileRows rows and
+// kTileEntries entries per tile, never crossing an LP; rows longer than
+// kTileRowMax go to the binned long / very-long lists.
 struct HostTiles {
   std::vector<int4> tiles;
   std::vector<int32_t> inst;
@@ -100,28 +100,12 @@ inline HostTiles make_tiles(const std::vector<int32_t>& ptr, const std::vector<i
         (len > kVeryLongRow ? h.vlong_rows : h.long_rows).push_back(static_cast<int32_t>(r));
         continue;
       }
-      if (r0 >= 0 && (r - r0 + 1 > kBlock || ptr[r + 1] - ptr[r0] > kTileEntries)) close(r);
+      if (r0 >= 0 && (r - r0 + 1 > kTileRows || ptr[r + 1] - ptr[r0] > kTileEntries)) close(r);
       if (r0 < 0) r0 = r;
     }
     close(off[b + 1]);
   }
   return h;
-}
-
-template <typename... KArgs, typename... Args>
-inline void launch_smem(void (*kern)(KArgs...), unsigned grid, size_t smem, cudaStream_t stream, bool pdl,
-                        Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(kBlock);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = pdl ? attr : nullptr;
-  cfg.numAttrs = pdl ? 1 : 0;
-  B2P_CUDA(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
 }
 
 template <typename... KArgs, typename... Args>
