@@ -238,6 +238,7 @@ struct MultiEngine {
   // binned schedule of the long rows only (pdhg_tiled.cuh).
   struct TileSched {
     bool on = false;
+    bool capped = false;  // kernels compiled for 4 resident blocks per SM (64 registers)
     TileSet ts{};
     RowBins longb{};
   };
@@ -549,7 +550,7 @@ struct MultiEngine {
     t.ts.tiles = upload(h.tiles);
     t.ts.inst = upload(h.inst);
     t.ts.n_tiles = static_cast<int32_t>(h.tiles.size());
-    t.ts.grid = std::max(1, (t.ts.n_tiles + kBlock / 32 - 1) / (kBlock / 32));
+    t.ts.grid = 0;  // set below, after the long-row blocks are known
     RowBins& lb = t.longb;
     lb.long_rows = upload(h.long_rows);
     lb.vlong_rows = upload(h.vlong_rows);
@@ -562,6 +563,7 @@ struct MultiEngine {
     lb.long_blocks = (lb.n_long + kBlock / 32 - 1) / (kBlock / 32);
     lb.short_blocks = 0;
     lb.g = 1;
+    t.ts.grid = std::max(1, lb.vlong_blocks + lb.long_blocks + (t.ts.n_tiles + kBlock / 32 - 1) / (kBlock / 32));
     return t;
   }
 
@@ -590,22 +592,18 @@ struct MultiEngine {
     const InstanceMap im{d_cinst, d_done};
     if (tilesT.on) {
       const RowBins& lb = tilesT.longb;
-      if (lb.vlong_blocks + lb.long_blocks > 0) {
-        if (halpern)
-          launch(k_primal_binned<1, true, true, true>, bin_grid(lb), stream, true, AT, lb, v[MY], v[MC], v[MLO],
-                 v[MUP], v[MX], v[MXP], v[MX0], d_tau, ck, rho, im);
-        else
-          launch(k_primal_binned<1, false, true, true>, bin_grid(lb), stream, true, AT, lb, v[MY], v[MC], v[MLO],
-                 v[MUP], v[MX], v[MXP], v[MX0], d_tau, ck, rho, im);
+      const unsigned g = static_cast<unsigned>(tilesT.ts.grid);
+#define B2P_PT(H, MB)                                                                                            \
+  launch(k_primal_tiled<H, true, MB>, g, stream, true, AT, tilesT.ts, lb, v[MY], v[MC], v[MLO], v[MUP], v[MX], \
+         v[MXP], v[MX0], d_tau, ck, rho, im)
+      if (tilesT.capped) {
+        if (halpern) B2P_PT(true, 4);
+        else B2P_PT(false, 4);
+      } else {
+        if (halpern) B2P_PT(true, 1);
+        else B2P_PT(false, 1);
       }
-      if (tilesT.ts.n_tiles > 0) {
-        if (halpern)
-          launch(k_primal_tiled<true, true>, tilesT.ts.grid, stream, true, AT, tilesT.ts, v[MY],
-                      v[MC], v[MLO], v[MUP], v[MX], v[MXP], v[MX0], d_tau, ck, rho, im);
-        else
-          launch(k_primal_tiled<false, true>, tilesT.ts.grid, stream, true, AT, tilesT.ts,
-                      v[MY], v[MC], v[MLO], v[MUP], v[MX], v[MXP], v[MX0], d_tau, ck, rho, im);
-      }
+#undef B2P_PT
       return;
     }
     const unsigned gp = bin_grid(binsT);
@@ -632,22 +630,18 @@ struct MultiEngine {
     const InstanceMap im{d_rinst, d_done};
     if (tilesA.on) {
       const RowBins& lb = tilesA.longb;
-      if (lb.vlong_blocks + lb.long_blocks > 0) {
-        if (halpern)
-          launch(k_dual_binned<1, true, true, true>, bin_grid(lb), stream, true, A, lb, v[MXP], v[MRL], v[MRU], v[MY],
-                 v[MYP], v[MY0], v[MAX], v[MAXP], v[MAX0], d_sigma, ck, rho, im);
-        else
-          launch(k_dual_binned<1, false, true, true>, bin_grid(lb), stream, true, A, lb, v[MXP], v[MRL], v[MRU],
-                 v[MY], v[MYP], v[MY0], v[MAX], v[MAXP], v[MAX0], d_sigma, ck, rho, im);
+      const unsigned g = static_cast<unsigned>(tilesA.ts.grid);
+#define B2P_DT(H, MB)                                                                                             \
+  launch(k_dual_tiled<H, true, MB>, g, stream, true, A, tilesA.ts, lb, v[MXP], v[MRL], v[MRU], v[MY], v[MYP],   \
+         v[MY0], v[MAX], v[MAXP], v[MAX0], d_sigma, ck, rho, im)
+      if (tilesA.capped) {
+        if (halpern) B2P_DT(true, 4);
+        else B2P_DT(false, 4);
+      } else {
+        if (halpern) B2P_DT(true, 1);
+        else B2P_DT(false, 1);
       }
-      if (tilesA.ts.n_tiles > 0) {
-        if (halpern)
-          launch(k_dual_tiled<true, true>, tilesA.ts.grid, stream, true, A, tilesA.ts, v[MXP],
-                      v[MRL], v[MRU], v[MY], v[MYP], v[MY0], v[MAX], v[MAXP], v[MAX0], d_sigma, ck, rho, im);
-        else
-          launch(k_dual_tiled<false, true>, tilesA.ts.grid, stream, true, A, tilesA.ts, v[MXP],
-                      v[MRL], v[MRU], v[MY], v[MYP], v[MY0], v[MAX], v[MAXP], v[MAX0], d_sigma, ck, rho, im);
-      }
+#undef B2P_DT
       return;
     }
     const unsigned gd = bin_grid(binsA);
@@ -672,12 +666,8 @@ struct MultiEngine {
     const CsrView AT = viewAT();
     const InstanceMap im{d_cinst, d_done};
     if (tilesT.on) {
-      const RowBins& lb = tilesT.longb;
-      if (lb.vlong_blocks + lb.long_blocks > 0)
-        launch(k_spmv_binned<1, true>, bin_grid(lb), stream, false, AT, lb, v[MYP], v[MATYP], im);
-      if (tilesT.ts.n_tiles > 0)
-        launch(k_spmv_tiled<true>, tilesT.ts.grid, stream, false, AT, tilesT.ts, v[MYP],
-                    v[MATYP], im);
+      launch(k_spmv_tiled<true>, static_cast<unsigned>(tilesT.ts.grid), stream, false, AT, tilesT.ts, tilesT.longb,
+             v[MYP], v[MATYP], im);
       return;
     }
     const unsigned gp = bin_grid(binsT);
@@ -687,10 +677,7 @@ struct MultiEngine {
   }
 
   // Kernel launches of one iteration / of the A^T y+ product.
-  static int sched_launches(const TileSched& t) {
-    if (!t.on) return 1;
-    return (t.longb.vlong_blocks + t.longb.long_blocks > 0 ? 1 : 0) + (t.ts.n_tiles > 0 ? 1 : 0);
-  }
+  static int sched_launches(const TileSched&) { return 1; }
 
   // Autotuner: for A^T (primal kernel) and A (dual kernel) separately, time
   // every binned schedule (1..32 lanes per short row, with cached or
@@ -731,10 +718,21 @@ struct MultiEngine {
           }
         }
       }
-      TileSched cand = device_tiles(ptr, off, nullptr);
-      tiles = cand;
-      const double tt = timed(enq);
-      if (tt < best) return;  // keep the tiles
+      tiles = device_tiles(ptr, off, nullptr);
+      double tbest = INFINITY;
+      bool tcap = false;
+      for (int cap = 0; cap < 2; ++cap) {
+        tiles.capped = cap != 0;
+        const double tt = timed(enq);
+        if (tt < tbest) {
+          tbest = tt;
+          tcap = tiles.capped;
+        }
+      }
+      if (tbest < best) {  // keep the tiles
+        tiles.capped = tcap;
+        return;
+      }
       tiles.on = false;
       streaming = best_s;
       bins = device_bins(make_bins(Op, wave, best_g, rounds), rows);
@@ -802,9 +800,17 @@ struct MultiEngine {
       if (!done[b]) live += inst_nnz[b];
     if (live == 0 || 2 * live >= sched_nnz) return;
     B2P_CUDA(cudaStreamSynchronize(stream));
-    if (tilesA.on) tilesA = device_tiles(hA_ptr, roff, &done);
+    if (tilesA.on) {
+      const bool cap = tilesA.capped;
+      tilesA = device_tiles(hA_ptr, roff, &done);
+      tilesA.capped = cap;
+    }
     else binsA = live_bins(hA_ptr, roff, done, binsA.g, ltA);
-    if (tilesT.on) tilesT = device_tiles(hT_ptr, coff, &done);
+    if (tilesT.on) {
+      const bool cap = tilesT.capped;
+      tilesT = device_tiles(hT_ptr, coff, &done);
+      tilesT.capped = cap;
+    }
     else binsT = live_bins(hT_ptr, coff, done, binsT.g, ltT);
     for (auto& g : graphs) cudaGraphExecDestroy(g.second);
     for (auto& g : graph_defs) cudaGraphDestroy(g.second);

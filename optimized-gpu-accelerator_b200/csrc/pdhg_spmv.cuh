@@ -185,14 +185,15 @@ __device__ __forceinline__ double finish_row(const RowPlan& pl, const CsrView& M
 // x+ = proj(x - tau (c - A^T y)), Halpern step of x (skipped at a check
 // iteration).  A^T rows binned.  MULTI: several LPs, per-row instance b
 // selects tau[b] and the Halpern counter of b.
-template <int G, bool HALPERN, bool MULTI = false, bool STREAM = false>
-__global__ void __launch_bounds__(kBlock) k_primal_binned(CsrView AT, RowBins bins, const double* __restrict__ y,
-                                                          const double* __restrict__ c, const double* __restrict__ lo,
-                                                          const double* __restrict__ up, double* __restrict__ x,
-                                                          double* __restrict__ xp, const double* __restrict__ x0,
-                                                          const double* __restrict__ tau, IterClock ck, double rho,
-                                                          InstanceMap im = {nullptr, nullptr}) {
-  __shared__ double sh[kBlock / 32];
+// (the kernel bodies are device functions so that the tiled kernels can run
+// the long rows in the same launch; sh: kBlock / 32 doubles of shared memory)
+template <int G, bool HALPERN, bool MULTI, bool STREAM>
+__device__ __forceinline__ void primal_binned_body(const CsrView& AT, const RowBins& bins, const double* __restrict__ y,
+                                                   const double* __restrict__ c, const double* __restrict__ lo,
+                                                   const double* __restrict__ up, double* __restrict__ x,
+                                                   double* __restrict__ xp, const double* __restrict__ x0,
+                                                   const double* __restrict__ tau, const IterClock& ck, double rho,
+                                                   const InstanceMap& im, double* sh) {
   const RowPlan pl = plan_row<G, MULTI, STREAM>(AT, bins, im);
   const int j = pl.row;
   const int b = (MULTI && pl.leader) ? im.inst[j] : 0;
@@ -222,16 +223,26 @@ __global__ void __launch_bounds__(kBlock) k_primal_binned(CsrView AT, RowBins bi
   if (HALPERN) x[j] = halpern_step(xv, v, x0v, lam, rho);
 }
 
-// y+ = v + sigma proj(-v/sigma), v = y - sigma (2 A x+ - A x); Halpern steps of y and Ax.
 template <int G, bool HALPERN, bool MULTI = false, bool STREAM = false>
-__global__ void __launch_bounds__(kBlock) k_dual_binned(CsrView A, RowBins bins, const double* __restrict__ xp,
-                                                        const double* __restrict__ rl, const double* __restrict__ ru,
-                                                        double* __restrict__ y, double* __restrict__ yp,
-                                                        const double* __restrict__ y0, double* __restrict__ ax,
-                                                        double* __restrict__ axp, const double* __restrict__ ax0,
-                                                        const double* __restrict__ sigma, IterClock ck, double rho,
-                                                        InstanceMap im = {nullptr, nullptr}) {
+__global__ void __launch_bounds__(kBlock) k_primal_binned(CsrView AT, RowBins bins, const double* __restrict__ y,
+                                                          const double* __restrict__ c, const double* __restrict__ lo,
+                                                          const double* __restrict__ up, double* __restrict__ x,
+                                                          double* __restrict__ xp, const double* __restrict__ x0,
+                                                          const double* __restrict__ tau, IterClock ck, double rho,
+                                                          InstanceMap im = {nullptr, nullptr}) {
   __shared__ double sh[kBlock / 32];
+  primal_binned_body<G, HALPERN, MULTI, STREAM>(AT, bins, y, c, lo, up, x, xp, x0, tau, ck, rho, im, sh);
+}
+
+// y+ = v + sigma proj(-v/sigma), v = y - sigma (2 A x+ - A x); Halpern steps of y and Ax.
+template <int G, bool HALPERN, bool MULTI, bool STREAM>
+__device__ __forceinline__ void dual_binned_body(const CsrView& A, const RowBins& bins, const double* __restrict__ xp,
+                                                 const double* __restrict__ rl, const double* __restrict__ ru,
+                                                 double* __restrict__ y, double* __restrict__ yp,
+                                                 const double* __restrict__ y0, double* __restrict__ ax,
+                                                 double* __restrict__ axp, const double* __restrict__ ax0,
+                                                 const double* __restrict__ sigma, const IterClock& ck, double rho,
+                                                 const InstanceMap& im, double* sh) {
   const RowPlan pl = plan_row<G, MULTI, STREAM>(A, bins, im);
   const int i = pl.row;
   const int b = (MULTI && pl.leader) ? im.inst[i] : 0;
@@ -268,16 +279,34 @@ __global__ void __launch_bounds__(kBlock) k_dual_binned(CsrView A, RowBins bins,
   }
 }
 
+template <int G, bool HALPERN, bool MULTI = false, bool STREAM = false>
+__global__ void __launch_bounds__(kBlock) k_dual_binned(CsrView A, RowBins bins, const double* __restrict__ xp,
+                                                        const double* __restrict__ rl, const double* __restrict__ ru,
+                                                        double* __restrict__ y, double* __restrict__ yp,
+                                                        const double* __restrict__ y0, double* __restrict__ ax,
+                                                        double* __restrict__ axp, const double* __restrict__ ax0,
+                                                        const double* __restrict__ sigma, IterClock ck, double rho,
+                                                        InstanceMap im = {nullptr, nullptr}) {
+  __shared__ double sh[kBlock / 32];
+  dual_binned_body<G, HALPERN, MULTI, STREAM>(A, bins, xp, rl, ru, y, yp, y0, ax, axp, ax0, sigma, ck, rho, im, sh);
+}
+
 // out = M x with the binned schedule (used for A^T y+ at a check).
+template <int G, bool MULTI, bool STREAM>
+__device__ __forceinline__ void spmv_binned_body(const CsrView& M, const RowBins& bins, const double* __restrict__ x,
+                                                 double* __restrict__ out, const InstanceMap& im, double* sh) {
+  const RowPlan pl = plan_row<G, MULTI, STREAM>(M, bins, im);
+  pdl_wait();
+  const double s = finish_row<G, STREAM>(pl, M, x, sh);
+  pdl_launch_dependents();
+  if (pl.leader) out[pl.row] = s;
+}
+
 template <int G, bool MULTI = false>
 __global__ void __launch_bounds__(kBlock) k_spmv_binned(CsrView M, RowBins bins, const double* __restrict__ x,
                                                         double* __restrict__ out, InstanceMap im = {nullptr, nullptr}) {
   __shared__ double sh[kBlock / 32];
-  const RowPlan pl = plan_row<G, MULTI>(M, bins, im);
-  pdl_wait();
-  const double s = finish_row<G>(pl, M, x, sh);
-  pdl_launch_dependents();
-  if (pl.leader) out[pl.row] = s;
+  spmv_binned_body<G, MULTI, false>(M, bins, x, out, im, sh);
 }
 
 }  // namespace b2p

@@ -4,7 +4,8 @@
 // The host cuts the short rows (<= kTileRowMax = 32 entries) of a CSR operator
 // into tiles of consecutive rows -- at most 32 rows and kTileEntries = 256
 // entries, never crossing an LP of a multi-LP batch -- and leaves the longer
-// rows to the binned warp / block paths (a separate launch).  One warp per
+// rows to the binned warp / block paths, which the first blocks of the same
+// launch run (RowBins of the long rows only).  One warp per
 // tile: the tile's (index, value) pairs are one contiguous range, so lane l
 // loads entries e0 + l + 32k (k < 8; fully coalesced, all independent, issued
 // before griddepcontrol.wait since the operator is constant), gathers the 8
@@ -40,7 +41,7 @@ struct TileSet {
   const int4* __restrict__ tiles;    // (row begin, row end, entry begin, entry end)
   const int32_t* __restrict__ inst;  // LP of each tile (multi-LP), or NULL
   int32_t n_tiles;
-  int32_t grid;                      // blocks of kBlock / 32 warps
+  int32_t grid;                      // blocks: the long-row blocks, then one warp per tile
 };
 
 namespace tiled {
@@ -93,16 +94,21 @@ __device__ __forceinline__ double row_sum(const double* prod, int4 d, int rb, in
 
 // x+ = proj(x - tau (c - A^T y)) and the Halpern step of x, over the tiled
 // short rows of A^T (see k_primal_binned for the arithmetic).
-template <bool HALPERN, bool MULTI>
-__global__ void __launch_bounds__(kBlock) k_primal_tiled(CsrView AT, TileSet ts, const double* __restrict__ y,
+template <bool HALPERN, bool MULTI, int MINB = 1>
+__global__ void __launch_bounds__(kBlock, MINB) k_primal_tiled(CsrView AT, TileSet ts, RowBins lb, const double* __restrict__ y,
                                                          const double* __restrict__ c, const double* __restrict__ lo,
                                                          const double* __restrict__ up, double* __restrict__ x,
                                                          double* __restrict__ xp, const double* __restrict__ x0,
                                                          const double* __restrict__ tau, IterClock ck, double rho,
                                                          InstanceMap im) {
   __shared__ double prod_all[kBlock / 32][kTileEntries];
+  const int nlb = lb.vlong_blocks + lb.long_blocks;  // leading blocks: the long rows
+  if (static_cast<int>(blockIdx.x) < nlb) {
+    primal_binned_body<1, HALPERN, MULTI, true>(AT, lb, y, c, lo, up, x, xp, x0, tau, ck, rho, im, &prod_all[0][0]);
+    return;
+  }
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int t = blockIdx.x * (kBlock / 32) + w;
+  const int t = (static_cast<int>(blockIdx.x) - nlb) * (kBlock / 32) + w;
   if (t >= ts.n_tiles) return;
   const int4 d = __ldg(ts.tiles + t);
   const int b = MULTI ? __ldg(ts.inst + t) : 0;
@@ -143,8 +149,8 @@ __global__ void __launch_bounds__(kBlock) k_primal_tiled(CsrView AT, TileSet ts,
 
 // y+ = v + sigma proj(-v/sigma), v = y - sigma (2 A x+ - A x); Halpern steps
 // of y and Ax, over the tiled short rows of A (see k_dual_binned).
-template <bool HALPERN, bool MULTI>
-__global__ void __launch_bounds__(kBlock) k_dual_tiled(CsrView A, TileSet ts, const double* __restrict__ xp,
+template <bool HALPERN, bool MULTI, int MINB = 1>
+__global__ void __launch_bounds__(kBlock, MINB) k_dual_tiled(CsrView A, TileSet ts, RowBins lb, const double* __restrict__ xp,
                                                        const double* __restrict__ rl, const double* __restrict__ ru,
                                                        double* __restrict__ y, double* __restrict__ yp,
                                                        const double* __restrict__ y0, double* __restrict__ ax,
@@ -152,8 +158,13 @@ __global__ void __launch_bounds__(kBlock) k_dual_tiled(CsrView A, TileSet ts, co
                                                        const double* __restrict__ sigma, IterClock ck, double rho,
                                                        InstanceMap im) {
   __shared__ double prod_all[kBlock / 32][kTileEntries];
+  const int nlb = lb.vlong_blocks + lb.long_blocks;  // leading blocks: the long rows
+  if (static_cast<int>(blockIdx.x) < nlb) {
+    dual_binned_body<1, HALPERN, MULTI, true>(A, lb, xp, rl, ru, y, yp, y0, ax, axp, ax0, sigma, ck, rho, im, &prod_all[0][0]);
+    return;
+  }
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int t = blockIdx.x * (kBlock / 32) + w;
+  const int t = (static_cast<int>(blockIdx.x) - nlb) * (kBlock / 32) + w;
   if (t >= ts.n_tiles) return;
   const int4 d = __ldg(ts.tiles + t);
   const int b = MULTI ? __ldg(ts.inst + t) : 0;
@@ -201,11 +212,16 @@ __global__ void __launch_bounds__(kBlock) k_dual_tiled(CsrView A, TileSet ts, co
 
 // out = M x over the tiled short rows (A^T y+ at a check).
 template <bool MULTI>
-__global__ void __launch_bounds__(kBlock) k_spmv_tiled(CsrView M, TileSet ts, const double* __restrict__ x,
+__global__ void __launch_bounds__(kBlock) k_spmv_tiled(CsrView M, TileSet ts, RowBins lb, const double* __restrict__ x,
                                                        double* __restrict__ out, InstanceMap im) {
   __shared__ double prod_all[kBlock / 32][kTileEntries];
+  const int nlb = lb.vlong_blocks + lb.long_blocks;  // leading blocks: the long rows
+  if (static_cast<int>(blockIdx.x) < nlb) {
+    spmv_binned_body<1, MULTI, true>(M, lb, x, out, im, &prod_all[0][0]);
+    return;
+  }
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int t = blockIdx.x * (kBlock / 32) + w;
+  const int t = (static_cast<int>(blockIdx.x) - nlb) * (kBlock / 32) + w;
   if (t >= ts.n_tiles) return;
   const int4 d = __ldg(ts.tiles + t);
   const tiled::Pairs pr = tiled::load_pairs(M, d, lane);
