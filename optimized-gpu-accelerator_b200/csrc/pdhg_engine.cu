@@ -170,7 +170,7 @@ struct Engine {
   template <class T>
   T* dalloc(size_t count) {
     void* p = nullptr;
-    B2P_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    B2P_CUDA(cudaMallocFromPoolAsync(&p, std::max<size_t>(count, 1) * sizeof(T), device_pool(device), stream));
     allocs.push_back(p);
     return static_cast<T*>(p);
   }
@@ -188,7 +188,11 @@ struct Engine {
     for (auto e : prof_ev) cudaEventDestroy(e);
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
-    for (void* p : allocs) cudaFree(p);
+    cudaSetDevice(device);
+    if (stream) {
+      for (void* p : allocs) cudaFreeAsync(p, stream);
+      cudaStreamSynchronize(stream);
+    }
     if (h_sums) cudaFreeHost(h_sums);
     if (h_steps) cudaFreeHost(h_steps);
     if (h_mask) cudaFreeHost(h_mask);

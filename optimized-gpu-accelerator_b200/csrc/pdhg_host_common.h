@@ -6,6 +6,9 @@
 #include <cuda_runtime.h>
 
 #include <chrono>
+#include <cstdint>
+#include <map>
+#include <mutex>
 #include <cstdlib>
 #include <new>
 #include <stdexcept>
@@ -55,6 +58,32 @@ int guarded(F&& f) {
     last_error() = e.what();
     return B2P_ERR_CUDA;
   }
+}
+
+// The engines' device memory comes from one stream-ordered pool per device
+// (cudaMallocFromPoolAsync / cudaFreeAsync on the engine's stream): freed
+// blocks stay cached for the next engine, so a solve's set-up does not pay a
+// cudaMalloc / cudaFree per buffer.  Up to kPoolKeepBytes of freed memory is
+// kept per device (held until the process exits); beyond that it goes back to
+// the driver at the next synchronisation.
+constexpr uint64_t kPoolKeepBytes = uint64_t(8) << 30;
+
+inline cudaMemPool_t device_pool(int dev) {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = pools.find(dev);
+  if (it != pools.end()) return it->second;
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t pool = nullptr;
+  B2P_CUDA(cudaMemPoolCreate(&pool, &props));
+  uint64_t keep = kPoolKeepBytes;
+  B2P_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  pools.emplace(dev, pool);
+  return pool;
 }
 
 // Ordinal of the sm_100 device to use: `requested`, else PRAMANA_GPU_DEVICE,

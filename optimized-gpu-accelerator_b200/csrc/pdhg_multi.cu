@@ -259,7 +259,7 @@ struct MultiEngine {
   template <class T>
   T* dalloc(size_t count) {
     void* p = nullptr;
-    B2P_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    B2P_CUDA(cudaMallocFromPoolAsync(&p, std::max<size_t>(count, 1) * sizeof(T), device_pool(device), stream));
     allocs.push_back(p);
     return static_cast<T*>(p);
   }
@@ -288,7 +288,11 @@ struct MultiEngine {
     for (auto& g : graph_defs) cudaGraphDestroy(g.second);
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
-    for (void* p : allocs) cudaFree(p);
+    cudaSetDevice(device);
+    if (stream) {
+      for (void* p : allocs) cudaFreeAsync(p, stream);
+      cudaStreamSynchronize(stream);
+    }
     if (h_sums) cudaFreeHost(h_sums);
     if (h_steps) cudaFreeHost(h_steps);
     if (h_mask) cudaFreeHost(h_mask);
@@ -315,6 +319,7 @@ struct MultiEngine {
     po.pock_chambolle = opt.pock_chambolle != 0;
     po.rescale = opt.rescale_objective_and_bounds != 0;
     po.norm_on_host = true;
+    po.parallel = false;  // the LPs themselves are prepared on all host threads
     std::atomic<int> next{0};
     const int nth = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), static_cast<unsigned>(K)));
     std::vector<std::thread> pool;

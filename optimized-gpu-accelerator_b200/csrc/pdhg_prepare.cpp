@@ -15,69 +15,104 @@ double pow2_round(double v) {
   return std::ldexp(1.0, e);
 }
 
-// Row-major copy of a CSC matrix: rows list their entries by increasing
-// column, which is the order SparseMatrix::transpose produces
-// (src/core/sparse.cpp:49-65) and hence the order of every row sum.
-HostCsr csr_from_csc(int32_t m, int32_t n, const int32_t* start, const int32_t* index, const double* value) {
-  HostCsr c;
-  c.rows = m;
-  c.cols = n;
+// Row-major view of a CSC matrix: for every row, its entries by increasing
+// column -- the order SparseMatrix::transpose produces
+// (src/core/sparse.cpp:49-65) and hence the order of every row sum -- as
+// (column, CSC position) pairs.
+struct RowMap {
+  std::vector<int32_t> ptr, col, pos;
+};
+
+RowMap row_map(int32_t m, int32_t n, const int32_t* start, const int32_t* index) {
+  RowMap r;
   const int32_t nnz = start[n];
-  c.ptr.assign(static_cast<size_t>(m) + 1, 0);
-  c.idx.resize(nnz);
-  c.val.resize(nnz);
-  for (int32_t q = 0; q < nnz; ++q) c.ptr[index[q] + 1]++;
-  for (int32_t i = 0; i < m; ++i) c.ptr[i + 1] += c.ptr[i];
-  std::vector<int32_t> pos(c.ptr.begin(), c.ptr.end() - 1);
+  r.ptr.assign(static_cast<size_t>(m) + 1, 0);
+  r.col.resize(nnz);
+  r.pos.resize(nnz);
+  for (int32_t q = 0; q < nnz; ++q) r.ptr[index[q] + 1]++;
+  for (int32_t i = 0; i < m; ++i) r.ptr[i + 1] += r.ptr[i];
+  std::vector<int32_t> next(r.ptr.begin(), r.ptr.end() - 1);
   for (int32_t j = 0; j < n; ++j)
     for (int32_t q = start[j]; q < start[j + 1]; ++q) {
-      int32_t p = pos[index[q]]++;
-      c.idx[p] = j;
-      c.val[p] = value[q];
+      const int32_t e = next[index[q]]++;
+      r.col[e] = j;
+      r.pos[e] = q;
     }
-  return c;
+  return r;
 }
+
+// OpenMP only above this many nonzeros (the team's start-up costs more below)
+constexpr int32_t kParallelNnz = 1 << 15;
 
 }  // namespace
 
-void ruiz_scaling(int32_t m, int32_t n, const int32_t* start, const int32_t* index, const double* value,
-                  int iterations, bool pock_chambolle, std::vector<double>& rs, std::vector<double>& cs) {
+// Each pass computes every row and column quantity with the same expression
+// and, for the Pock-Chambolle sums, in the same order as the reference's
+// column sweep (a row's terms by increasing column), so the result does not
+// depend on `parallel`.
+namespace {
+
+void ruiz_impl(int32_t m, int32_t n, const int32_t* start, const int32_t* index, const double* value,
+               int iterations, bool pock_chambolle, std::vector<double>& rs, std::vector<double>& cs, const RowMap& R,
+               bool par) {
   rs.assign(m, 1.0);
   cs.assign(n, 1.0);
   std::vector<double> rmax(m), cmax(n);
   // Infinity-norm equilibration passes.
   for (int it = 0; it < iterations; ++it) {
-    std::fill(rmax.begin(), rmax.end(), 0.0);
+#pragma omp parallel for schedule(static) if (par)
     for (int32_t j = 0; j < n; ++j) {
       double c = 0;
-      for (int32_t q = start[j]; q < start[j + 1]; ++q) {
-        const double a = std::fabs(value[q]) * cs[j] * rs[index[q]];
-        c = smax(c, a);
-        rmax[index[q]] = smax(rmax[index[q]], a);
-      }
+      for (int32_t q = start[j]; q < start[j + 1]; ++q) c = smax(c, std::fabs(value[q]) * cs[j] * rs[index[q]]);
       cmax[j] = c;
     }
+#pragma omp parallel for schedule(static) if (par)
+    for (int32_t i = 0; i < m; ++i) {
+      double r = 0;
+      for (int32_t e = R.ptr[i]; e < R.ptr[i + 1]; ++e)
+        r = smax(r, std::fabs(value[R.pos[e]]) * cs[R.col[e]] * rs[i]);
+      rmax[i] = r;
+    }
+#pragma omp parallel for schedule(static) if (par)
     for (int32_t i = 0; i < m; ++i)
       if (rmax[i] > 0) rs[i] /= std::sqrt(rmax[i]);
+#pragma omp parallel for schedule(static) if (par)
     for (int32_t j = 0; j < n; ++j)
       if (cmax[j] > 0) cs[j] /= std::sqrt(cmax[j]);
   }
   // Pock-Chambolle step with alpha = 1 (row / column 1-norms).
   if (pock_chambolle) {
     std::vector<double> rsum(m, 0.0), csum(n, 0.0);
-    for (int32_t j = 0; j < n; ++j)
-      for (int32_t q = start[j]; q < start[j + 1]; ++q) {
-        const double a = std::fabs(value[q]) * cs[j] * rs[index[q]];
-        csum[j] += a;
-        rsum[index[q]] += a;
-      }
+#pragma omp parallel for schedule(static) if (par)
+    for (int32_t j = 0; j < n; ++j) {
+      double c = 0.0;
+      for (int32_t q = start[j]; q < start[j + 1]; ++q) c += std::fabs(value[q]) * cs[j] * rs[index[q]];
+      csum[j] = c;
+    }
+#pragma omp parallel for schedule(static) if (par)
+    for (int32_t i = 0; i < m; ++i) {
+      double r = 0.0;
+      for (int32_t e = R.ptr[i]; e < R.ptr[i + 1]; ++e) r += std::fabs(value[R.pos[e]]) * cs[R.col[e]] * rs[i];
+      rsum[i] = r;
+    }
+#pragma omp parallel for schedule(static) if (par)
     for (int32_t i = 0; i < m; ++i)
       if (rsum[i] > 0) rs[i] /= std::sqrt(rsum[i]);
+#pragma omp parallel for schedule(static) if (par)
     for (int32_t j = 0; j < n; ++j)
       if (csum[j] > 0) cs[j] /= std::sqrt(csum[j]);
   }
   for (auto& v : rs) v = pow2_round(v);
   for (auto& v : cs) v = pow2_round(v);
+}
+
+}  // namespace
+
+void ruiz_scaling(int32_t m, int32_t n, const int32_t* start, const int32_t* index, const double* value,
+                  int iterations, bool pock_chambolle, std::vector<double>& rs, std::vector<double>& cs,
+                  bool parallel) {
+  ruiz_impl(m, n, start, index, value, iterations, pock_chambolle, rs, cs, row_map(m, n, start, index),
+            parallel && start[n] >= kParallelNnz);
 }
 
 // ||A||_2 estimate: 40 steps of x <- A^T A x / ||A^T A x|| and sqrt of the
@@ -118,14 +153,17 @@ Prepared prepare(int32_t m, int32_t n, const int32_t* start, const int32_t* inde
   P.m = m;
   P.offset = offset;
   const int32_t nnz = start[n];
+  const bool par = opt.parallel && nnz >= kParallelNnz;
+  const RowMap rm = row_map(m, n, start, index);
   if (opt.ruiz_iterations > 0 && nnz > 0) {
-    ruiz_scaling(m, n, start, index, value, opt.ruiz_iterations, opt.pock_chambolle, P.R, P.Cs);
+    ruiz_impl(m, n, start, index, value, opt.ruiz_iterations, opt.pock_chambolle, P.R, P.Cs, rm, par);
   } else {
     P.R.assign(m, 1.0);
     P.Cs.assign(n, 1.0);
   }
   // A <- diag(R) A diag(Cs) (src/lp/scaling.cpp:28-32); exact, the factors are powers of two.
   std::vector<double> sval(nnz);
+#pragma omp parallel for schedule(static) if (par)
   for (int32_t j = 0; j < n; ++j)
     for (int32_t q = start[j]; q < start[j + 1]; ++q) sval[q] = value[q] * (P.R[index[q]] * P.Cs[j]);
   if (opt.rescale) {
@@ -147,7 +185,15 @@ Prepared prepare(int32_t m, int32_t n, const int32_t* start, const int32_t* inde
     P.gamma = 1.0 + std::sqrt(cn);
     P.beta = 1.0 + std::sqrt(bn);
   }
-  P.A = csr_from_csc(m, n, start, index, sval.data());
+  {
+    P.A.rows = m;
+    P.A.cols = n;
+    P.A.ptr = rm.ptr;
+    P.A.idx = rm.col;
+    P.A.val.resize(nnz);
+#pragma omp parallel for schedule(static) if (par)
+    for (int32_t e = 0; e < nnz; ++e) P.A.val[e] = sval[rm.pos[e]];
+  }
   // CSR of A^T is the (scaled) CSC of A.
   P.AT.rows = n;
   P.AT.cols = m;

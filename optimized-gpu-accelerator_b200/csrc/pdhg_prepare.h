@@ -37,6 +37,10 @@ struct PrepareOptions {
   bool pock_chambolle = true;
   bool rescale = true;
   bool norm_on_host = true;  // false: normA is left 0 for the caller to estimate (on the device)
+  // run the element-wise passes on host threads (OpenMP); every result is
+  // the same as the sequential passes' (maxima are order-free, every sum
+  // keeps its order).  Off when the caller already prepares LPs in parallel.
+  bool parallel = true;
 };
 
 // A given in CSC (start/index/value) with m rows and n columns.
@@ -45,7 +49,8 @@ Prepared prepare(int32_t m, int32_t n, const int32_t* start, const int32_t* inde
                  const PrepareOptions& opt);
 
 void ruiz_scaling(int32_t m, int32_t n, const int32_t* start, const int32_t* index, const double* value,
-                  int iterations, bool pock_chambolle, std::vector<double>& row_scale, std::vector<double>& col_scale);
+                  int iterations, bool pock_chambolle, std::vector<double>& row_scale, std::vector<double>& col_scale,
+                  bool parallel = false);
 
 double power_iteration(int32_t m, int32_t n, const int32_t* start, const int32_t* index, const double* value,
                        int iters);

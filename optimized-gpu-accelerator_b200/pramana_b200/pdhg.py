@@ -165,11 +165,18 @@ def _cases_struct(cases, n, m):
     return arr, keep
 
 
+_DEVICE_NAME: list[str] = []
+
+
 def _device_name() -> str:
-    try:
-        return gpuInfoJson().get("name", "")
-    except Exception:  # noqa: BLE001 - informational only
-        return ""
+    """The GPU's name for PdhgStats.device, queried once per process (the
+    query reads every device property, which is not free on a solve path)."""
+    if not _DEVICE_NAME:
+        try:
+            _DEVICE_NAME.append(gpuInfoJson().get("name", ""))
+        except Exception:  # noqa: BLE001 - informational only
+            return ""
+    return _DEVICE_NAME[0]
 
 
 def _results(lp: Model, res, x, y, k, stats) -> list[PdhgResult]:
