@@ -62,13 +62,15 @@ enum {
 /* Arithmetic of the iterates. */
 enum {
   B2P_PRECISION_FP64 = 0, /* plain form: FP64 everywhere, iterate parity with the reference */
-  /* mixed form (single LP in the resident form): operator values, iterates
-   * and their updates in FP32 with FP64-accumulated row sums; check sums,
-   * termination, restarts and primal weight in FP64.  A point that meets the
-   * tolerance in FP32 is re-measured in FP64 before it is returned; when that
+  /* mixed form: operator values and iterates stored in FP32, row sums of
+   * exact FP32 products in FP64; check sums, termination, restarts and
+   * primal weight in FP64.  A single LP (resident form) whose FP32 point meets
+   * the tolerance is re-measured in FP64 before it is returned; when that
    * fails, or the FP32 run stalls, the solve continues in FP64 from the FP32
-   * point (the FP64 polish).  Batches and LPs too large for the resident form
-   * run in FP64. */
+   * point (the FP64 polish).  A batch (num_cases > 1) runs in FP32 until
+   * every case has met the tolerance there or stalled, then re-measures all
+   * cases in FP64: those that pass terminate, the rest continue in FP64.  A
+   * single LP too large for the resident form runs in FP64. */
   B2P_PRECISION_MIXED = 1
 };
 

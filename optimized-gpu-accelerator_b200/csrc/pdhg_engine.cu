@@ -30,6 +30,7 @@
 #include "pdhg_host_common.h"
 #include "pdhg_kernels.cuh"
 #include "pdhg_prepare.h"
+#include "pdhg_batch32.cuh"
 #include "pdhg_resident.cuh"
 #include "pdhg_sched.h"
 #include "pdhg_spmv.cuh"
@@ -151,8 +152,9 @@ struct Engine {
   int32_t* h_mask = nullptr;
 
   // ---- graphs and profiling ----
-  std::map<int, cudaGraphExec_t> graphs;
-  std::map<int, cudaGraph_t> graph_defs;
+  std::map<int, cudaGraphExec_t> graphs, graphs32;  // per interval length; FP32 phase of a batch
+  std::map<int, cudaGraph_t> graph_defs, graph_defs32;
+  bool mixed_batch = false;  // mixed form of a batch (k > 1): FP32 k-interleaved kernels
   bool profiling = false;
   std::vector<cudaEvent_t> prof_ev;  // 4 per iteration of the longest interval
   int64_t prof_launches[3] = {0, 0, 0};
@@ -185,6 +187,8 @@ struct Engine {
   ~Engine() {
     for (auto& g : graphs) cudaGraphExecDestroy(g.second);
     for (auto& g : graph_defs) cudaGraphDestroy(g.second);
+    for (auto& g : graphs32) cudaGraphExecDestroy(g.second);
+    for (auto& g : graph_defs32) cudaGraphDestroy(g.second);
     for (auto e : prof_ev) cudaEventDestroy(e);
     if (ev_start) cudaEventDestroy(ev_start);
     if (ev_stop) cudaEventDestroy(ev_stop);
@@ -303,8 +307,9 @@ struct Engine {
       setup_resident(sms);
       stats.graph_seconds += seconds_since(tk);
     }
+    mixed_batch = k > 1 && opt.precision == B2P_PRECISION_MIXED;
     stats.kernel_mode = (resident || mixed) ? B2P_KERNELS_RESIDENT : B2P_KERNELS_FUSED;
-    stats.precision_used = mixed ? B2P_PRECISION_MIXED : B2P_PRECISION_FP64;
+    stats.precision_used = (mixed || mixed_batch) ? B2P_PRECISION_MIXED : B2P_PRECISION_FP64;
     for (int s = 0; s < NSLOT; ++s) v[s] = dalloc<double>(row_slot(s) ? mk : nk);
     auto put = [&](int s, const std::vector<double>& h) {
       if (!h.empty())
@@ -333,7 +338,7 @@ struct Engine {
     B2P_CUDA(cudaMallocHost(&h_sums, sizeof(double) * k * kNumSums));
     B2P_CUDA(cudaMallocHost(&h_steps, sizeof(double) * 2 * k));
     B2P_CUDA(cudaMallocHost(&h_mask, sizeof(int32_t) * k));
-    if (mixed) setup_mixed();
+    if (mixed || mixed_batch) setup_mixed();
     // AX = A x0 on the device (pdhg.cpp:540-545), kept as the restart point of every solve.
     if (m > 0) {
       k_spmv<<<blocks(static_cast<int64_t>(m) * k), kBlock, 0, stream>>>(m, k, viewA(), v[XINIT], v[AXINIT]);
@@ -439,10 +444,11 @@ struct Engine {
     std::vector<float> av(P.A.val.begin(), P.A.val.end()), tv(P.AT.val.begin(), P.AT.val.end());
     a_val32 = upload(av);
     t_val32 = upload(tv);
-    for (int q = 0; q < NSLOT32; ++q) v32[q] = dalloc<float>(q >= Y32 && q != C32 && q != LO32 && q != UP32 ? m : n);
+    for (int q = 0; q < NSLOT32; ++q)
+      v32[q] = dalloc<float>(static_cast<size_t>(q >= Y32 && q != C32 && q != LO32 && q != UP32 ? m : n) * k);
     const int src[5] = {C, LO, UP, RL, RU}, dst[5] = {C32, LO32, UP32, RL32, RU32};
     for (int q = 0; q < 5; ++q) {
-      const int64_t len = row_slot(src[q]) ? m : n;
+      const int64_t len = static_cast<int64_t>(row_slot(src[q]) ? m : n) * k;
       if (len) k_convert<double, float><<<blocks(len), kBlock, 0, stream>>>(len, v[src[q]], v32[dst[q]]);
     }
     B2P_CUDA(cudaGetLastError());
@@ -521,7 +527,7 @@ struct Engine {
   void state_to_fp32() {
     const int pairs[6][2] = {{X, X32}, {X0, X032}, {Y, Y32}, {Y0, Y032}, {AX, AX32}, {AX0, AX032}};
     for (auto& pr : pairs) {
-      const int64_t len = row_slot(pr[0]) ? m : n;
+      const int64_t len = static_cast<int64_t>(row_slot(pr[0]) ? m : n) * k;
       if (len) k_convert<double, float><<<blocks(len), kBlock, 0, stream>>>(len, v[pr[0]], v32[pr[1]]);
     }
     B2P_CUDA(cudaGetLastError());
@@ -529,9 +535,10 @@ struct Engine {
 
   // x+, y+ of the FP32 phase in FP64, and A x+ recomputed in FP64.
   void fp32_point_to_fp64() {
-    if (n) k_convert<float, double><<<blocks(n), kBlock, 0, stream>>>(n, v32[XP32], v[XP]);
-    if (m) k_convert<float, double><<<blocks(m), kBlock, 0, stream>>>(m, v32[YP32], v[YP]);
-    if (m) k_spmv<<<blocks(m), kBlock, 0, stream>>>(m, 1, viewA(), v[XP], v[AXP]);
+    const int64_t nk = static_cast<int64_t>(n) * k, mk = static_cast<int64_t>(m) * k;
+    if (nk) k_convert<float, double><<<blocks(nk), kBlock, 0, stream>>>(nk, v32[XP32], v[XP]);
+    if (mk) k_convert<float, double><<<blocks(mk), kBlock, 0, stream>>>(mk, v32[YP32], v[YP]);
+    if (mk) k_spmv<<<blocks(mk), kBlock, 0, stream>>>(m, k, viewA(), v[XP], v[AXP]);
     B2P_CUDA(cudaGetLastError());
     launches += 3;
   }
@@ -539,14 +546,14 @@ struct Engine {
   // FP64 check sums of the FP64 point (XP, YP, AXP) into h_sums (the movement
   // norms of this call are not meaningful).
   void verify_fp64() {
-    if (n) k_spmv<<<blocks(n), kBlock, 0, stream>>>(n, 1, viewAT(), v[YP], v[ATYP]);
-    k_check_rows<<<dim3(g_rows, 1), kBlock, 0, stream>>>(m, 1, v[AXP], v[RL], v[RU], v[YP], v[Y], v[Y0], d_rfac,
+    if (n) k_spmv<<<blocks(static_cast<int64_t>(n) * k), kBlock, 0, stream>>>(n, k, viewAT(), v[YP], v[ATYP]);
+    k_check_rows<<<dim3(g_rows, k), kBlock, 0, stream>>>(m, k, v[AXP], v[RL], v[RU], v[YP], v[Y], v[Y0], d_rfac,
                                                          d_prow);
-    k_check_cols<<<dim3(g_cols, 1), kBlock, 0, stream>>>(n, 1, viewAT(), v[YP], v[ATYP], v[XP], v[X], v[X0], v[C],
+    k_check_cols<<<dim3(g_cols, k), kBlock, 0, stream>>>(n, k, viewAT(), v[YP], v[ATYP], v[XP], v[X], v[X0], v[C],
                                                          v[LO], v[UP], d_cfac, d_pcol);
-    k_check_finalize<<<1, kBlock, 0, stream>>>(1, g_rows, g_cols, d_prow, d_pcol, d_sums, d_it_base, 0);
+    k_check_finalize<<<k, kBlock, 0, stream>>>(k, g_rows, g_cols, d_prow, d_pcol, d_sums, d_it_base, 0);
     B2P_CUDA(cudaGetLastError());
-    B2P_CUDA(cudaMemcpyAsync(h_sums, d_sums, sizeof(double) * kNumSums, cudaMemcpyDeviceToHost, stream));
+    B2P_CUDA(cudaMemcpyAsync(h_sums, d_sums, sizeof(double) * k * kNumSums, cudaMemcpyDeviceToHost, stream));
     B2P_CUDA(cudaStreamSynchronize(stream));
     launches += 5;
   }
@@ -554,7 +561,7 @@ struct Engine {
   // Continue in FP64 from the FP32 phase's x+, y+ as from a restart.
   void switch_to_fp64() {
     fp32_point_to_fp64();
-    const int64_t nn = n, mm = m;
+    const int64_t nn = static_cast<int64_t>(n) * k, mm = static_cast<int64_t>(m) * k;
     if (nn) {
       B2P_CUDA(cudaMemcpyAsync(v[X], v[XP], sizeof(double) * nn, cudaMemcpyDeviceToDevice, stream));
       B2P_CUDA(cudaMemcpyAsync(v[X0], v[XP], sizeof(double) * nn, cudaMemcpyDeviceToDevice, stream));
@@ -565,7 +572,7 @@ struct Engine {
       B2P_CUDA(cudaMemcpyAsync(v[AX], v[AXP], sizeof(double) * mm, cudaMemcpyDeviceToDevice, stream));
       B2P_CUDA(cudaMemcpyAsync(v[AX0], v[AXP], sizeof(double) * mm, cudaMemcpyDeviceToDevice, stream));
     }
-    k_restart_clock<<<1, 32, 0, stream>>>(1, d_it_base, d_restart_at);
+    k_restart_clock<<<(k + 127) / 128, 128, 0, stream>>>(k, d_it_base, d_restart_at);
     B2P_CUDA(cudaGetLastError());
     ++launches;
     phase32 = false;
@@ -763,13 +770,56 @@ struct Engine {
     enqueue_check_tail(L, nullptr);
   }
 
+  CsrView32 viewA32() const { return CsrView32{dA_ptr, dA_idx, a_val32, m}; }
+  CsrView32 viewAT32() const { return CsrView32{dT_ptr, dT_idx, t_val32, n}; }
+
+  // One check interval of the FP32 phase of a batch (mixed form, k > 1).
+  void enqueue_interval32(int L) {
+    const double rho = opt.reflection;
+    const int64_t nk = static_cast<int64_t>(n) * k, mk = static_cast<int64_t>(m) * k;
+    const unsigned gp = blocks(nk), gd = blocks(mk);
+    const CsrView32 A = viewA32(), AT = viewAT32();
+    float* const* w = v32;
+    for (int l = 0; l < L; ++l) {
+      const bool last = l == L - 1;
+      const IterClock ck{d_it_base, d_restart_at, l};
+      if (nk) {
+        if (last)
+          k_primal32<false><<<gp, kBlock, 0, stream>>>(n, k, AT, w[Y32], w[C32], w[LO32], w[UP32], w[X32], w[XP32],
+                                                       w[X032], d_tau, ck, rho);
+        else
+          k_primal32<true><<<gp, kBlock, 0, stream>>>(n, k, AT, w[Y32], w[C32], w[LO32], w[UP32], w[X32], w[XP32],
+                                                      w[X032], d_tau, ck, rho);
+      }
+      if (mk) {
+        if (last)
+          k_dual32<false><<<gd, kBlock, 0, stream>>>(m, k, A, w[XP32], w[RL32], w[RU32], w[Y32], w[YP32], w[Y032],
+                                                     w[AX32], w[AXP32], w[AX032], d_sigma, ck, rho);
+        else
+          k_dual32<true><<<gd, kBlock, 0, stream>>>(m, k, A, w[XP32], w[RL32], w[RU32], w[Y32], w[YP32], w[Y032],
+                                                    w[AX32], w[AXP32], w[AX032], d_sigma, ck, rho);
+      }
+      B2P_CUDA(cudaGetLastError());
+    }
+    const IterClock ck{d_it_base, d_restart_at, L - 1};
+    k_check_rows32<<<dim3(g_rows, k), kBlock, 0, stream>>>(m, k, w[AXP32], v[RL], v[RU], w[YP32], w[Y32], w[Y032],
+                                                           d_rfac, d_prow);
+    k_check_cols32<<<dim3(g_cols, k), kBlock, 0, stream>>>(n, k, AT, w[YP32], w[XP32], w[X32], w[X032], v[C], v[LO],
+                                                           v[UP], d_cfac, d_pcol);
+    k_halpern_all32<<<blocks(nk + mk), kBlock, 0, stream>>>(n, m, k, w[X32], w[XP32], w[X032], w[Y32], w[YP32],
+                                                           w[Y032], w[AX32], w[AXP32], w[AX032], ck, rho);
+    k_check_finalize<<<k, kBlock, 0, stream>>>(k, g_rows, g_cols, d_prow, d_pcol, d_sums, d_it_base, L);
+    B2P_CUDA(cudaGetLastError());
+    B2P_CUDA(cudaMemcpyAsync(h_sums, d_sums, sizeof(double) * k * kNumSums, cudaMemcpyDeviceToHost, stream));
+  }
+
   int64_t launches_per_interval(int L) const {
     return static_cast<int64_t>(L) * ((n ? 1 : 0) + (m ? 1 : 0)) + 4 + (k == 1 && n ? 1 : 0);
   }
 
   void run_interval(int L) {
     if (profiling) ensure_prof_events(L);
-    if (phase32 || resident) {
+    if ((phase32 && !mixed_batch) || resident) {
       if (phase32)
         launch_resident32(L);
       else
@@ -778,14 +828,18 @@ struct Engine {
       bytes_down += static_cast<int64_t>(sizeof(double) * kNumSums + sizeof(int32_t));
       return;
     }
+    const bool fp32 = phase32 && mixed_batch;
+    auto& gexec = fp32 ? graphs32 : graphs;
+    auto& gdefs = fp32 ? graph_defs32 : graph_defs;
     if (opt.use_graphs && !profiling) {
-      auto it = graphs.find(L);
-      if (it == graphs.end()) {
+      auto it = gexec.find(L);
+      if (it == gexec.end()) {
         const auto tg = Clock::now();
         cudaGraph_t g;
         B2P_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         try {
-          enqueue_interval(L);
+          if (fp32) enqueue_interval32(L);
+          else enqueue_interval(L);
         } catch (...) {
           cudaStreamEndCapture(stream, &g);
           if (g) cudaGraphDestroy(g);
@@ -794,11 +848,13 @@ struct Engine {
         B2P_CUDA(cudaStreamEndCapture(stream, &g));
         cudaGraphExec_t ge;
         B2P_CUDA(cudaGraphInstantiate(&ge, g, 0));
-        graph_defs[L] = g;
-        it = graphs.emplace(L, ge).first;
+        gdefs[L] = g;
+        it = gexec.emplace(L, ge).first;
         stats.graph_seconds += seconds_since(tg);
       }
       B2P_CUDA(cudaGraphLaunch(it->second, stream));
+    } else if (fp32) {
+      enqueue_interval32(L);
     } else {
       enqueue_interval(L);
     }
@@ -808,6 +864,7 @@ struct Engine {
 
   void collect_profile(int L) {
     if (!profiling) return;
+    if (phase32 && mixed_batch) return;  // the FP32 batch kernels are not profiled per class
     if (phase32 || resident) {
       float ms = 0;
       B2P_CUDA(cudaEventElapsedTime(&ms, prof_ev[0], prof_ev[1]));
@@ -852,8 +909,12 @@ struct Engine {
     prof_launches[0] = prof_launches[1] = prof_launches[2] = 0;
     prof_ms[0] = prof_ms[1] = prof_ms[2] = 0;
     reset_state(omega);
-    phase32 = mixed;
+    phase32 = mixed || mixed_batch;
     if (phase32) state_to_fp32();
+    // mixed batch: per case, reached the tolerance in FP32 / stalled there
+    std::vector<char> conv32(k, 0), stall32(k, 0);
+    std::vector<double> best32v(k, INFINITY);
+    std::vector<int> stale32v(k, 0);
     stats.fp32_iterations = 0;
     double best32 = INFINITY;  // mixed form: best FP32-phase KKT and checks since it improved
     int stale32 = 0;
@@ -894,7 +955,7 @@ struct Engine {
       const int L = static_cast<int>(std::min<int64_t>(cE, opt.max_iterations - it));
       run_interval(L);
       B2P_CUDA(cudaStreamSynchronize(stream));
-      if ((resident || phase32) && *h_error)
+      if ((resident || (phase32 && !mixed_batch)) && *h_error)
         throw Error(B2P_ERR_CUDA, "resident kernel: grid barrier timed out (kernel left the interval)");
       collect_profile(L);
       if (phase32) stats.fp32_iterations += L;
@@ -902,7 +963,69 @@ struct Engine {
       ++checks;
       bool anyRestart = false, fetched = false;
       for (int b = 0; b < k; ++b) h_mask[b] = 0;
-      if (phase32) {
+      if (phase32 && mixed_batch) {
+        // Mixed form of a batch: each case's FP32 point is measured in FP64
+        // arithmetic against the FP64 data; when every live case has met the
+        // tolerance there or stalled (no 10% gain in kStallChecks checks),
+        // the whole batch is re-measured from its FP64 point: cases that
+        // pass terminate, the others continue in FP64 from that point as
+        // from a restart.
+        bool ready = true;
+        for (int b = 0; b < k; ++b) {
+          if (done[b]) continue;
+          const double* s = h_sums + static_cast<size_t>(b) * kNumSums;
+          const double pobj = s[CS_POBJ] * scaleObj, dobj = (s[CS_ROW_DOBJ] + s[CS_COL_DOBJ]) * scaleObj;
+          const double relP = std::sqrt(s[CS_ROW_RES2]) / (1.0 + rhsNorm[b]);
+          const double relD = std::sqrt(s[CS_COL_RES2]) / (1.0 + cNorm[b]);
+          const double gap = std::fabs(pobj - dobj) / (1.0 + std::fabs(pobj) + std::fabs(dobj));
+          const double kkt32 = smax(relP, smax(relD, gap));
+          if (relP <= opt.tolerance && relD <= opt.tolerance && gap <= opt.tolerance) {
+            conv32[b] = 1;
+          } else if (kkt32 < 0.9 * best32v[b]) {
+            best32v[b] = kkt32;
+            stale32v[b] = 0;
+          } else if (++stale32v[b] >= kStallChecks) {
+            stall32[b] = 1;
+          }
+          if (!conv32[b] && !stall32[b]) ready = false;
+        }
+        if (ready) {
+          fp32_point_to_fp64();
+          verify_fp64();
+          bool fetched64 = false;
+          for (int b = 0; b < k; ++b) {
+            if (done[b]) continue;
+            const double* s = h_sums + static_cast<size_t>(b) * kNumSums;
+            const double pobj = s[CS_POBJ] * scaleObj, dobj = (s[CS_ROW_DOBJ] + s[CS_COL_DOBJ]) * scaleObj;
+            const double relP = std::sqrt(s[CS_ROW_RES2]) / (1.0 + rhsNorm[b]);
+            const double relD = std::sqrt(s[CS_COL_RES2]) / (1.0 + cNorm[b]);
+            const double gap = std::fabs(pobj - dobj) / (1.0 + std::fabs(pobj) + std::fabs(dobj));
+            if (relP <= opt.tolerance && relD <= opt.tolerance && gap <= opt.tolerance) {
+              if (!fetched64) {
+                download_iterates(xs, ys);
+                fetched64 = true;
+              }
+              extract(b, B2P_STATUS_OPTIMAL, smax(relP, smax(relD, gap)), pobj, dobj, it);
+              done[b] = 1;
+              --remaining;
+            }
+          }
+          if (remaining == 0) break;
+          switch_to_fp64();
+          for (int b = 0; b < k; ++b) {
+            fpRestart[b] = fpPrev[b] = INFINITY;
+            sinceRestart[b] = 0;
+          }
+          stats.restarts++;
+          if (expired()) {
+            expiredStop = true;
+            break;
+          }
+          ++it;
+          continue;
+        }
+      }
+      if (phase32 && !mixed_batch) {
         // Mixed form (k == 1): an FP32 point that meets the tolerance is
         // re-measured in FP64; failing that, or after kStallChecks checks
         // without a 10% gain, the solve continues in FP64 from this point.

@@ -18,6 +18,7 @@ import pytest
 import lp_cases
 from pramana_b200 import generators as G
 from pramana_b200 import pdhg
+from pramana_b200.model import Model
 from pramana_b200.model import LpCase, Model
 
 pytestmark = pytest.mark.gpu
@@ -331,12 +332,45 @@ def test_mixed_precision_meets_tolerance_in_fp64(which, tol):
     assert abs(r.objective - ref.objective) <= 10 * tol * (1 + abs(ref.objective))
 
 
-def test_mixed_falls_back_to_fp64_for_batches():
+def _case_model(lp, cs):
+    return Model(**{**lp.__dict__, **{f: getattr(cs, f) for f in ("row_lower", "row_upper", "col_lower", "col_upper")
+                                      if getattr(cs, f) is not None},
+                    "col_cost": cs.cost if cs.cost is not None else lp.col_cost})
+
+
+@pytest.mark.parametrize("which", ["random", "family"])
+def test_mixed_precision_batch_meets_tolerance_in_fp64(which):
+    """Mixed form of a batch (k-interleaved FP32 kernels): every case returns
+    Optimal, its KKT recomputed on the host in FP64 meets the tolerance, and
+    its objective stays within a few tolerances of the plain FP64 batch's."""
+    if which == "random":
+        lp = G.random_lp(400, 800, 4.0, 240, 13)
+        cases = lp_cases.mixed_cases(lp, 8)
+    else:
+        from pramana_b200 import warmstart as W
+        fam = W.RefineryFamily(seed=5, periods=2, regions=1, units=4, streams=4, properties=2, scale_exponent=0.0)
+        lp = fam.base
+        cases = [fam.case(p) for p in fam.sample(32, 4)]
+    tol = 1e-6
+    with pdhg.Engine(lp, opts(tolerance=tol, precision=MIXED, maxIterations=400000), cases) as e:
+        rs = e.solve()
+        st = e.last_stats
+    assert st.precision_used == MIXED and st.fp32_iterations > 0
+    ref = pdhg.solvePdhgBatch(lp, cases, opts(tolerance=tol, maxIterations=400000))
+    for cs, r, q in zip(cases, rs, ref):
+        assert r.status == "Optimal" and q.status == "Optimal"
+        relP, relD, gap = _host_kkt(_case_model(lp, cs), r.x, r.rowDual)
+        assert max(relP, relD, gap) <= tol * (1 + 1e-6)
+        assert abs(r.objective - q.objective) <= 10 * tol * (1 + abs(q.objective))
+
+
+def test_mixed_batch_iteration_limit_returns_fp64_measure():
     lp = G.random_lp(150, 300, 4.0, 90, 13)
     cases = lp_cases.cost_sweep_cases(lp, 3)
-    st = pdhg.PdhgStats()
-    rs = pdhg.solvePdhgBatch(lp, cases, opts(tolerance=1e-6, precision=MIXED), batchStats=st)
-    assert all(r.status == "Optimal" for r in rs)
+    rs = pdhg.solvePdhgBatch(lp, cases, opts(tolerance=1e-12, precision=MIXED, maxIterations=300))
+    for cs, r in zip(cases, rs):
+        assert r.status == "IterationLimit"
+        assert abs(r.relativeKkt - max(_host_kkt(_case_model(lp, cs), r.x, r.rowDual))) <= 1e-6 * (1 + r.relativeKkt)
 
 
 @pytest.mark.parametrize("mode", FORMS)
