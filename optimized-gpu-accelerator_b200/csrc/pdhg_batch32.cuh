@@ -47,6 +47,7 @@ __global__ void __launch_bounds__(kBlock) k_primal32(int32_t n, int32_t k, CsrVi
   int64_t j;
   int b;
   split(t, k, j, b);
+  pdl_wait();
   const double aty = row_dot32(AT, y, j, k, b);
   const double xv = x[t];
   double v = __dsub_rn(xv, __dmul_rn(tau[b], __dsub_rn(static_cast<double>(c[t]), aty)));
@@ -55,6 +56,7 @@ __global__ void __launch_bounds__(kBlock) k_primal32(int32_t n, int32_t k, CsrVi
   v = (u < v) ? u : v;
   xp[t] = static_cast<float>(v);
   if (HALPERN) x[t] = static_cast<float>(halpern_step(xv, v, static_cast<double>(x0[t]), halpern_lambda(ck, b), rho));
+  pdl_launch_dependents();
 }
 
 template <bool HALPERN>
@@ -69,6 +71,7 @@ __global__ void __launch_bounds__(kBlock) k_dual32(int32_t m, int32_t k, CsrView
   int64_t i;
   int b;
   split(t, k, i, b);
+  pdl_wait();
   const double axpv = row_dot32(A, xp, i, k, b);
   const double s = sigma[b], yv = y[t], axv = ax[t];
   const double v = __dsub_rn(yv, __dmul_rn(s, __dsub_rn(__dmul_rn(2.0, axpv), axv)));
@@ -84,6 +87,7 @@ __global__ void __launch_bounds__(kBlock) k_dual32(int32_t m, int32_t k, CsrView
     y[t] = static_cast<float>(halpern_step(yv, ypv, static_cast<double>(y0[t]), lam, rho));
     ax[t] = static_cast<float>(halpern_step(axv, axpv, static_cast<double>(ax0[t]), lam, rho));
   }
+  pdl_launch_dependents();
 }
 
 // Halpern steps of x, y and Ax at a check iteration (after the reductions).

@@ -750,19 +750,21 @@ struct Engine {
       if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 0], stream));
       if (nk) {
         if (last)
-          k_primal<false><<<gp, kBlock, 0, stream>>>(n, k, AT, v[Y], v[C], v[LO], v[UP], v[X], v[XP], v[X0], d_tau, ck, rho);
+          launch(k_primal<false>, gp, stream, true, n, k, AT, v[Y], v[C], v[LO], v[UP], v[X], v[XP], v[X0], d_tau, ck,
+                 rho);
         else
-          k_primal<true><<<gp, kBlock, 0, stream>>>(n, k, AT, v[Y], v[C], v[LO], v[UP], v[X], v[XP], v[X0], d_tau, ck, rho);
+          launch(k_primal<true>, gp, stream, true, n, k, AT, v[Y], v[C], v[LO], v[UP], v[X], v[XP], v[X0], d_tau, ck,
+                 rho);
       }
       if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 1], stream));
       if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 2], stream));
       if (mk) {
         if (last)
-          k_dual<false><<<gd, kBlock, 0, stream>>>(m, k, A, v[XP], v[RL], v[RU], v[Y], v[YP], v[Y0], v[AX], v[AXP],
-                                                  v[AX0], d_sigma, ck, rho);
+          launch(k_dual<false>, gd, stream, true, m, k, A, v[XP], v[RL], v[RU], v[Y], v[YP], v[Y0], v[AX], v[AXP],
+                 v[AX0], d_sigma, ck, rho);
         else
-          k_dual<true><<<gd, kBlock, 0, stream>>>(m, k, A, v[XP], v[RL], v[RU], v[Y], v[YP], v[Y0], v[AX], v[AXP],
-                                                 v[AX0], d_sigma, ck, rho);
+          launch(k_dual<true>, gd, stream, true, m, k, A, v[XP], v[RL], v[RU], v[Y], v[YP], v[Y0], v[AX], v[AXP],
+                 v[AX0], d_sigma, ck, rho);
       }
       if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 3], stream));
       B2P_CUDA(cudaGetLastError());
@@ -785,19 +787,19 @@ struct Engine {
       const IterClock ck{d_it_base, d_restart_at, l};
       if (nk) {
         if (last)
-          k_primal32<false><<<gp, kBlock, 0, stream>>>(n, k, AT, w[Y32], w[C32], w[LO32], w[UP32], w[X32], w[XP32],
-                                                       w[X032], d_tau, ck, rho);
+          launch(k_primal32<false>, gp, stream, true, n, k, AT, w[Y32], w[C32], w[LO32], w[UP32], w[X32], w[XP32],
+                 w[X032], d_tau, ck, rho);
         else
-          k_primal32<true><<<gp, kBlock, 0, stream>>>(n, k, AT, w[Y32], w[C32], w[LO32], w[UP32], w[X32], w[XP32],
-                                                      w[X032], d_tau, ck, rho);
+          launch(k_primal32<true>, gp, stream, true, n, k, AT, w[Y32], w[C32], w[LO32], w[UP32], w[X32], w[XP32],
+                 w[X032], d_tau, ck, rho);
       }
       if (mk) {
         if (last)
-          k_dual32<false><<<gd, kBlock, 0, stream>>>(m, k, A, w[XP32], w[RL32], w[RU32], w[Y32], w[YP32], w[Y032],
-                                                     w[AX32], w[AXP32], w[AX032], d_sigma, ck, rho);
+          launch(k_dual32<false>, gd, stream, true, m, k, A, w[XP32], w[RL32], w[RU32], w[Y32], w[YP32], w[Y032],
+                 w[AX32], w[AXP32], w[AX032], d_sigma, ck, rho);
         else
-          k_dual32<true><<<gd, kBlock, 0, stream>>>(m, k, A, w[XP32], w[RL32], w[RU32], w[Y32], w[YP32], w[Y032],
-                                                    w[AX32], w[AXP32], w[AX032], d_sigma, ck, rho);
+          launch(k_dual32<true>, gd, stream, true, m, k, A, w[XP32], w[RL32], w[RU32], w[Y32], w[YP32], w[Y032],
+                 w[AX32], w[AXP32], w[AX032], d_sigma, ck, rho);
       }
       B2P_CUDA(cudaGetLastError());
     }

@@ -42,6 +42,12 @@ enum CheckSum : int {
   CS_AX2 = 9        // sum (x+ - x0)^2                           (diff2(XP, X0))
 };
 
+// Programmatic dependent launch: a kernel launched with the PDL attribute
+// waits here for the previous kernel's memory before reading what it wrote,
+// and lets the next kernel start its launch once its own stores are issued.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
 struct CsrView {
   const int32_t* __restrict__ ptr;
   const int32_t* __restrict__ idx;
@@ -108,6 +114,7 @@ static __global__ void __launch_bounds__(kBlock) k_primal(int32_t n, int32_t k, 
   int64_t j;
   int b;
   split(t, k, j, b);
+  pdl_wait();
   const double aty = row_dot(AT, y, j, k, b);
   const double xv = x[t];
   // x+ = proj_[lo,up](x - tau (c - A^T y))          (src/pdhg/pdhg.cpp:116-125)
@@ -117,6 +124,7 @@ static __global__ void __launch_bounds__(kBlock) k_primal(int32_t n, int32_t k, 
   v = (u < v) ? u : v;
   xp[t] = v;
   if (HALPERN) x[t] = halpern_step(xv, v, x0[t], halpern_lambda(ck, b), rho);
+  pdl_launch_dependents();
 }
 
 template <bool HALPERN>
@@ -131,6 +139,7 @@ static __global__ void __launch_bounds__(kBlock) k_dual(int32_t m, int32_t k, Cs
   int64_t i;
   int b;
   split(t, k, i, b);
+  pdl_wait();
   const double axpv = row_dot(A, xp, i, k, b);
   const double axv = ax[t], yv = y[t];
   // v = y - sigma (2 A x+ - A x);  y+ = v + sigma proj_[L,U](-v / sigma)   (src/pdhg/pdhg.cpp:126-137)
@@ -148,6 +157,7 @@ static __global__ void __launch_bounds__(kBlock) k_dual(int32_t m, int32_t k, Cs
     y[t] = halpern_step(yv, ypv, y0[t], lam, rho);
     ax[t] = halpern_step(axv, axpv, ax0[t], lam, rho);
   }
+  pdl_launch_dependents();
 }
 
 // Halpern steps of x, y and Ax at a check iteration (after the reductions).

@@ -47,8 +47,6 @@ struct RowBins {
   int32_t g;             // lanes per short row
 };
 
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" :::); }
 
 // Several LPs solved together as one block-diagonal operator: inst[row] is
 // the row's instance, done[instance] != 0 once that instance has terminated
