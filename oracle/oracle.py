@@ -216,6 +216,23 @@ def certify(lp, x, y, tol=(1e-6, 1e-6, 1e-6)) -> dict:
     return d
 
 
+def simplex(lp, x=None, y=None) -> dict:
+    """The reference's simplex (ref build): crossover from (x, y) when given,
+    else a solve from scratch.  Returns status name, objective, iterations."""
+    h = _load("ref")
+    out = np.zeros(3)
+    xa = None if x is None else np.ascontiguousarray(x, dtype=np.float64)
+    ya = None if y is None else np.ascontiguousarray(y, dtype=np.float64)
+    rc = h.ref_simplex(C.c_int(lp.num_rows), C.c_int(lp.num_cols), _ip(lp.start), _ip(lp.index), _dp(lp.value),
+                       _dp(lp.col_cost), _dp(lp.col_lower), _dp(lp.col_upper), _dp(lp.row_lower), _dp(lp.row_upper),
+                       C.c_double(lp.obj_offset), _dp(xa) if xa is not None else None,
+                       _dp(ya) if ya is not None else None, _dp(out))
+    if rc != 0:
+        raise RuntimeError("simplex failed")
+    return {"status": STATUS_NAMES.get(int(out[0]), str(int(out[0]))), "objective": out[1],
+            "iterations": int(out[2])}
+
+
 def ruiz(lp, lib: str = "oracle", iterations: int = 10, pock_chambolle: bool = True):
     h = _load(lib)
     fn = h.oracle_ruiz_scaling if lib == "oracle" else h.ref_ruiz_scaling

@@ -9,6 +9,8 @@
 //   - pramana::safeDualBound, the outward-rounded Neumaier-Shcherbina bound
 //                                          (src/cert/certifier.h:93)
 //   - pramana::ruizScaling                 (src/lp/scaling.cpp:97-139)
+//   - pramana::crossover (src/lp/crossover.cpp) from a primal-dual point, and
+//     the dual simplex from scratch (src/lp/simplex.cpp), for the handoff
 //   - pramana::certify of an OPTIMAL LP claim (src/cert/certifier.cpp:208-380)
 //     and its constraint-implied column bounds (Propagator, src/mip/propagate.cpp)
 // The GPU path of the reference is switched off (PRAMANA_DISABLE_GPU) so that
@@ -22,7 +24,9 @@
 
 #include "cert/certifier.h"
 #include "core/model.h"
+#include "lp/crossover.h"
 #include "lp/scaling.h"
+#include "lp/simplex.h"
 #include "mip/propagate.h"
 #include "pdhg/pdhg.h"
 #include "util/log.h"
@@ -261,6 +265,27 @@ int ref_certify_lp(int m, int n, const int* start, const int* index, const doubl
     }
     out[7] = c.maxDualViolation;
     out[8] = c.costPerturbation;
+    return 0;
+  } catch (std::exception& e) {
+    gErr = e.what();
+    return 1;
+  }
+}
+
+// Simplex from a basis guessed at (x, y) (crossover) when x != NULL, else from
+// scratch.  out: status, objective (incl. offset), simplex iterations.
+int ref_simplex(int m, int n, const int* start, const int* index, const double* value, const double* cost,
+                const double* colLower, const double* colUpper, const double* rowLower, const double* rowUpper,
+                double offset, const double* x, const double* y, double* out) {
+  try {
+    Log::setLevel(LogLevel::Error);
+    Model lp = buildModel(m, n, start, index, value, cost, colLower, colUpper, rowLower, rowUpper, offset);
+    SimplexOptions so;
+    LpResult r = x ? crossover(lp, std::vector<double>(x, x + n), std::vector<double>(y, y + m), so, nullptr)
+                   : solveLpSimplex(lp, so, nullptr);
+    out[0] = static_cast<double>(r.status);
+    out[1] = r.objective;
+    out[2] = static_cast<double>(r.stats.iterations);
     return 0;
   } catch (std::exception& e) {
     gErr = e.what();
