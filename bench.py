@@ -283,45 +283,56 @@ MULTI_METRIC = "time-to-1e-6 rel KKT (s) of a batch of uneven LPs in one multi-L
 
 def run_multi(args, rank, world):
     """--workload multi: independent LPs of uneven size (config-2 generator,
-    nnz log-uniform) in one multi-LP run; with --profile-iters, a fixed
-    iteration count for the per-iteration bandwidth only."""
+    nnz log-uniform) in one multi-LP run per GPU; under torchrun the LPs are
+    sharded across the GPUs, balanced by nonzeros, with no communication until
+    the results are gathered.  With --profile-iters, a fixed iteration count for
+    the per-iteration bandwidth only."""
     import torch
 
+    from pramana_b200 import _lib
     from pramana_b200 import generators as G
     from pramana_b200 import pdhg
+    from pramana_b200.shard import gather, max_over_ranks, partition
 
-    if world > 1 and rank != 0:
-        return 0
-    torch.cuda.set_device(0)
-    lps = G.uneven_family(args.instances, 1e4, args.nnz_hi, seed=4)
-    nnz = sum(lp.nnz for lp in lps)
-    m = sum(lp.num_rows for lp in lps)
-    n = sum(lp.num_cols for lp in lps)
-    alg = 24 * nnz + 4 * (m + n + 2 * len(lps)) + 16 * (m + n)  # both CSR SpMVs, FP64 (SURVEY 8d model)
-    # what the fused kernels must move: both SpMVs plus the primal (c, l, u, x, x0 read; x, x+ written)
-    # and dual (L, U, y, y0, Ax, Ax0 read; y, y+, Ax, Ax+ written) vector streams
-    fused = 24 * nnz + 4 * (m + n + 2 * len(lps)) + 8 * (m + n) + 56 * n + 80 * m
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank if world > 1 else 0)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev_id = torch.cuda.current_device()
+    sizes = G.uneven_family_sizes(args.instances, 1e4, args.nnz_hi, seed=4)
+    mine = partition(sizes, world)[rank] if world > 1 else list(range(args.instances))
+    lps = G.uneven_family(args.instances, 1e4, args.nnz_hi, seed=4, only=mine)
     fixed = args.profile_iters > 0
     po = pdhg.PdhgOptions(tolerance=1e-30 if fixed else TOL, maxIterations=args.profile_iters if fixed else 1000000,
-                          spmvSchedule=["auto", "binned", "tiled", "tuned"].index(args.schedule))
-    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device="cuda:0")
+                          spmvSchedule=["auto", "binned", "tiled", "tuned"].index(args.schedule), device=dev_id)
+    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{dev_id}")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
     runs = []
     for s in range(args.warmup + args.steps):
         flush.zero_()
-        torch.cuda.synchronize()
+        barrier()
         st = pdhg.PdhgStats()
         t0 = time.perf_counter()
-        rs = pdhg.solvePdhgMulti(lps, po, batchStats=st)
+        rs = pdhg.solvePdhgMulti(lps, po, batchStats=st) if lps else []
         wall = time.perf_counter() - t0
+        barrier()
         if s >= args.warmup:
-            raw = pdhg.solvePdhgMulti.last_stats
-            runs.append((st.kernelSeconds, wall, st.iterations, rs, raw.kernel_launches, raw.bytes_uploaded,
-                         raw.bytes_downloaded, raw.lanes_per_row_a, raw.lanes_per_row_at))
+            raw = pdhg.solvePdhgMulti.last_stats if lps else _lib.B2pStats()
+            runs.append((st.kernelSeconds if lps else 0.0, wall, st.iterations, rs, raw.kernel_launches,
+                         raw.bytes_uploaded, raw.bytes_downloaded, raw.lanes_per_row_a, raw.lanes_per_row_at,
+                         raw.schedule_a, raw.schedule_at))
     dev = statistics.mean(r[0] for r in runs)
     wall = statistics.mean(r[1] for r in runs)
-    its = runs[-1][2]
     rs = runs[-1][3]
-    per_it = dev / max(1, its)
+
     # work actually done: each LP's bytes per iteration times its own iteration count
     # (terminated LPs drop out of the schedule)
     def lp_bytes(lp, fused_model):
@@ -329,11 +340,17 @@ def run_multi(args, rank, world):
         if fused_model:
             base += -8 * (lp.num_rows + lp.num_cols) + 56 * lp.num_cols + 80 * lp.num_rows
         return base
-    done_alg = sum(lp_bytes(lp, False) * r.iterations for lp, r in zip(lps, rs))
-    done_fused = sum(lp_bytes(lp, True) * r.iterations for lp, r in zip(lps, rs))
-    peak, peak_kind = measured_peak()
+
+    local = {i: {"status": r.status, "iterations": r.iterations, "alg": lp_bytes(lp, False) * r.iterations,
+                 "fused": lp_bytes(lp, True) * r.iterations, "nnz": lp.nnz, "m": lp.num_rows, "n": lp.num_cols}
+             for i, lp, r in zip(mine, lps, rs)}
+    if dist is not None:
+        dev, wall = max_over_ranks([dev, wall], device=f"cuda:{dev_id}")
+        merged = gather(local)
+    else:
+        merged = local
     seq = None
-    if not fixed and args.per_instance_sample > 0:
+    if rank == 0 and world == 1 and not fixed and args.per_instance_sample > 0:
         # sequential plain FP64 single-LP solves of a sample, extrapolated by nonzeros
         import numpy as np
         pick = np.random.default_rng(0).choice(len(lps), size=min(args.per_instance_sample, len(lps)), replace=False)
@@ -344,34 +361,46 @@ def run_multi(args, rank, world):
             pdhg.solvePdhg(lps[i], pdhg.PdhgOptions(tolerance=TOL, precision=0))
             t_s += time.perf_counter() - t0
             nnz_s += lps[i].nnz
+        total_nnz = sum(v["nnz"] for v in merged.values())
         seq = {"members_timed": len(pick), "seconds_timed": t_s,
-               "seconds_extrapolated": t_s * nnz / max(1, nnz_s),
+               "seconds_extrapolated": t_s * total_nnz / max(1, nnz_s),
                "extrapolation": "wall time of one-at-a-time solves x (batch nnz / sample nnz)"}
-    line = {"metric": MULTI_METRIC, "value": dev, "unit": "s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": dev * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)", "workload": "multi",
-            "config": {"workload": f"{len(lps)} config-2-generator LPs, nnz log-uniform [1e4, {args.nnz_hi:g}], "
-                                   f"seeds 4..{3 + len(lps)}: {m} rows, {n} cols, {nnz} nnz in total",
-                       "to": "fixed iterations" if fixed else f"rel KKT {TOL:g} per LP",
-                       "lanes_per_row": [runs[-1][7], runs[-1][8]], "schedule_requested": args.schedule,
-                       "schedule_used": [pdhg.solvePdhgMulti.last_stats.schedule_a,
-                                         pdhg.solvePdhgMulti.last_stats.schedule_at],
-                       "l2": "flushed before each step; the operators (24 B/nnz per iteration) exceed L2"},
-            "iterations": its, "optimal": sum(r.status == "Optimal" for r in rs),
-            "e2e": {"value": wall, "unit": "s", "h2d_bytes_per_step": int(runs[-1][5]),
-                    "d2h_bytes_per_step": int(runs[-1][6])},
-            "gpu_launches": runs[-1][4],
-            "sequential_fp64": seq,
-            "speedup_vs_sequential": (seq["seconds_extrapolated"] / wall) if seq else None,
-            "roofline": {"bound": "hbm", "kernel": "fused primal + dual kernels (+ checks every 64)",
-                         "achieved": done_alg / dev / 1e9, "peak": peak, "unit": "GB/s",
-                         "frac": done_alg / dev / 1e9 / peak, "peak_source": peak_kind,
-                         "algorithmic_bytes": done_alg, "fused_model_bytes": done_fused,
-                         "fused_model_frac": done_fused / dev / 1e9 / peak,
-                         "full_batch_algorithmic_bytes_per_iteration": alg,
-                         "full_batch_fused_bytes_per_iteration": fused, "us_per_iteration": per_it * 1e6,
-                         "unit_of_work": "the whole loop: every LP's SpMV bytes x its own iterations / device time"}}
-    print(json.dumps(line))
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        nnz = sum(v["nnz"] for v in merged.values())
+        m = sum(v["m"] for v in merged.values())
+        n = sum(v["n"] for v in merged.values())
+        done_alg = sum(v["alg"] for v in merged.values())
+        done_fused = sum(v["fused"] for v in merged.values())
+        its = max(v["iterations"] for v in merged.values())
+        line = {"metric": MULTI_METRIC, "value": dev, "unit": "s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": dev * 1e3, "higher_is_better": False,
+                "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded generator)", "workload": "multi",
+                "config": {"workload": f"{args.instances} config-2-generator LPs, nnz log-uniform [1e4, {args.nnz_hi:g}], "
+                                       f"seeds 4..{3 + args.instances}: {m} rows, {n} cols, {nnz} nnz in total",
+                           "to": "fixed iterations" if fixed else f"rel KKT {TOL:g} per LP",
+                           "parallelism": f"LPs sharded over {world} GPUs by nonzeros" if world > 1 else "single GPU",
+                           "lanes_per_row": [runs[-1][7], runs[-1][8]], "schedule_requested": args.schedule,
+                           "schedule_used": [runs[-1][9], runs[-1][10]],
+                           "l2": "flushed before each step; the operators (24 B/nnz per iteration) exceed L2"},
+                "iterations": its, "optimal": sum(v["status"] == "Optimal" for v in merged.values()),
+                "e2e": {"value": wall, "unit": "s", "h2d_bytes_per_step": int(runs[-1][5]),
+                        "d2h_bytes_per_step": int(runs[-1][6])},
+                "gpu_launches": runs[-1][4],
+                "sequential_fp64": seq,
+                "speedup_vs_sequential": (seq["seconds_extrapolated"] / wall) if seq else None,
+                "roofline": {"bound": "hbm", "kernel": "fused primal + dual kernels (+ checks every 64)",
+                             "achieved": done_alg / dev / 1e9, "peak": peak * world, "unit": "GB/s",
+                             "frac": done_alg / dev / 1e9 / (peak * world), "peak_source": peak_kind,
+                             "algorithmic_bytes": done_alg, "fused_model_bytes": done_fused,
+                             "fused_model_frac": done_fused / dev / 1e9 / (peak * world),
+                             "unit_of_work": "the whole loop: every LP's SpMV bytes x its own iterations / device "
+                                             "time (max over GPUs); peak = per-GPU peak x GPUs"}}
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 

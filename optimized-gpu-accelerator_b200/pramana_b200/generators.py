@@ -243,16 +243,22 @@ def config3(seed: int = 3) -> Model:
     return refinery_lp(seed=seed, name=f"c3_s{seed}")
 
 
-def uneven_family(count: int, nnz_lo: float = 1e4, nnz_hi: float = 2e6, seed: int = 4) -> list[Model]:
+def uneven_family_sizes(count: int, nnz_lo: float = 1e4, nnz_hi: float = 2e6, seed: int = 4) -> np.ndarray:
+    """The nonzero counts uneven_family draws (for partitioning before building)."""
+    rng = np.random.default_rng(seed)
+    return np.exp(rng.uniform(np.log(nnz_lo), np.log(nnz_hi), size=count))
+
+
+def uneven_family(count: int, nnz_lo: float = 1e4, nnz_hi: float = 2e6, seed: int = 4, only=None) -> list[Model]:
     """Batched uneven workload: `count` LPs of the config-2 generator, instance i
     with seed `seed` + i and a nonzero count drawn log-uniform from
     [nnz_lo, nnz_hi] (m = nnz / 12.8 rows, n = 2m columns, 6.4 nonzeros per
-    column, 1% of the rows holding 10% of the nonzeros)."""
-    rng = np.random.default_rng(seed)
-    nnz = np.exp(rng.uniform(np.log(nnz_lo), np.log(nnz_hi), size=count))
+    column, 1% of the rows holding 10% of the nonzeros).  `only`: build just
+    these instance indices (in that order)."""
+    nnz = uneven_family_sizes(count, nnz_lo, nnz_hi, seed)
     out = []
-    for i, z in enumerate(nnz):
-        m = max(10, int(round(z / 12.8)))
+    for i in (range(count) if only is None else only):
+        m = max(10, int(round(nnz[i] / 12.8)))
         out.append(random_lp(m, 2 * m, 6.4, int(0.6 * m), seed + i, heavy_row_frac=0.01, heavy_nnz_frac=0.10,
                              name=f"c4_s{seed + i}"))
     return out
