@@ -130,12 +130,32 @@ typedef struct b2p_options {
   int32_t kernel_mode;
   /* SpMV schedule of the multi-LP engine's fused kernels, per operator:
    * B2P_SCHEDULE_BINNED (rows binned by length, lanes per short row),
-   * B2P_SCHEDULE_TILED (TMA-staged tiles of short rows, for operators far
-   * larger than L2), B2P_SCHEDULE_TUNED (the autotuner times every binned
-   * lane count and the tiles on the device and keeps the fastest), or
+   * B2P_SCHEDULE_TILED (warp tiles of up to 32 short rows whose entries one
+   * warp loads coalesced), B2P_SCHEDULE_TUNED (the autotuner times every
+   * binned lane count and the tiles on the device and keeps the fastest), or
    * B2P_SCHEDULE_AUTO (TUNED from 2^20 nonzeros on, BINNED below). */
   int32_t spmv_schedule;
+  /* Multi-LP engine form (B2P_MULTI_*): the block-diagonal form (every LP's
+   * rows in the same fused kernels, host decisions at each check, one CUDA
+   * graph per check interval) or the CTA form (one thread block runs one LP's
+   * whole loop, decisions included, in a single launch).  B2P_MULTI_AUTO
+   * picks the CTA form when every LP fits one block's shared memory. */
+  int32_t multi_form;
+  /* CTA form: bytes of shared memory one LP may use (0 = the device's
+   * per-block maximum); an LP that does not fit keeps its operators, or all
+   * of its data, in global memory. */
+  int32_t cta_smem_limit;
+  /* CTA form: threads per block (128, 256 or 512; 0 = autotuned with the
+   * kernel variant). */
+  int32_t cta_threads;
+  /* CTA form: kernel variant (B2P_CTA_*; 0 = autotuned): the general kernel
+   * (any LP size, three storage tiers) or the owner kernel, whose threads
+   * each own 1 or 2 rows and columns and keep their state in registers (LPs
+   * with max(m, n) <= 2 x threads whose data fit in shared memory). */
+  int32_t cta_kernel;
 } b2p_options;
+enum { B2P_MULTI_AUTO = 0, B2P_MULTI_GRID = 1, B2P_MULTI_CTA = 2 };
+enum { B2P_CTA_AUTO = 0, B2P_CTA_GENERAL = 1, B2P_CTA_OWNER1 = 2, B2P_CTA_OWNER2 = 3 };
 
 enum { B2P_SCHEDULE_AUTO = 0, B2P_SCHEDULE_BINNED = 1, B2P_SCHEDULE_TILED = 2, B2P_SCHEDULE_TUNED = 3 };
 
@@ -165,6 +185,13 @@ typedef struct b2p_stats {
   int32_t schedule_a, schedule_at;            /* multi-LP: B2P_SCHEDULE_BINNED or _TILED per operator */
   double autotune_seconds;                    /* multi-LP: time the autotuner took (part of setup) */
   int32_t streaming_a, streaming_at;          /* multi-LP binned schedules: evict-first streaming loads */
+  int32_t multi_form;                         /* multi-LP: B2P_MULTI_GRID or B2P_MULTI_CTA */
+  int32_t cta_threads;                        /* CTA form: threads per block (autotuned) */
+  int64_t cta_smem_bytes;                     /* CTA form: dynamic shared memory per block */
+  int32_t cta_lps_smem;                       /* CTA form: LPs held wholly in shared memory */
+  int32_t cta_lps_vectors;                    /* CTA form: LPs with only their iterates in shared memory */
+  int32_t cta_owned_per_thread;               /* CTA form: rows and columns each thread owns (0 = general kernel) */
+  int32_t pad2;
 } b2p_stats;
 
 /* Replaces pramana::PdhgResult (src/pdhg/pdhg.h:58-65) minus the vectors,

@@ -21,17 +21,22 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <numeric>
 #include <thread>
 #include <vector>
 
 #include "pdhg_host_common.h"
 #include "pdhg_kernels.cuh"
 #include "pdhg_prepare.h"
+#include "pdhg_cta.cuh"
 #include "pdhg_sched.h"
 #include "pdhg_spmv.cuh"
 #include "pdhg_tiled.cuh"
 
 namespace b2p {
+
+// Instantiated owner-kernel variants: (threads per block, elements per thread).
+#define B2P_OWNER_VARIANTS(X) X(128, 1) X(256, 1) X(512, 1) X(128, 2) X(256, 2) X(512, 2)
 
 constexpr int kSegRows = 2048;  // rows (or columns) per check-reduction block
 
@@ -255,6 +260,19 @@ struct MultiEngine {
   std::vector<std::vector<double>> xs, ys;  // per instance, original space
   int64_t launches = 0, bytes_up = 0, bytes_down = 0;
   int compactions = 0;
+  // CTA form (pdhg_cta.cuh): one block per LP
+  bool cta = false;
+  // kernel variant: threads per block and elements owned per thread (0: the
+  // general kernel, run_lp; 1 or 2: the owner kernel, run_owner)
+  int cta_nt = 256, cta_r = 0;
+  int64_t cta_smem = 0;        // general kernel: largest LP's tier bytes
+  int64_t cta_owner_smem = 0;  // owner kernel: largest LP's bytes (0: not every LP fits)
+  int32_t cta_max_dim = 0;     // largest max(m, n)
+  std::vector<CtaLp> cta_lps;
+  CtaLp* d_lps = nullptr;
+  int32_t* d_order = nullptr;
+  CtaOut* d_out = nullptr;
+  int32_t* h_stop = nullptr;  // host-mapped stop flag
 
   template <class T>
   T* dalloc(size_t count) {
@@ -297,6 +315,7 @@ struct MultiEngine {
     if (h_steps) cudaFreeHost(h_steps);
     if (h_mask) cudaFreeHost(h_mask);
     if (h_done) cudaFreeHost(h_done);
+    if (h_stop) cudaFreeHost(h_stop);
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -449,6 +468,27 @@ struct MultiEngine {
     d_restart_at = dalloc<int64_t>(K);
     d_done = dalloc<int32_t>(K);
     d_mask = dalloc<int32_t>(K);
+    if (M > 0) {
+      k_spmv<<<blocks(M), kBlock, 0, stream>>>(M, 1, viewA(), v[MXINIT], v[MAXINIT]);
+      B2P_CUDA(cudaGetLastError());
+    }
+    inst_nnz.assign(K, 0);
+    for (int b = 0; b < K; ++b) inst_nnz[b] = static_cast<int64_t>(P[b].A.val.size());
+    cta = choose_cta();
+    if (cta)
+      setup_cta(A, AT);
+    else
+      setup_grid(A, AT, annz);
+    B2P_CUDA(cudaStreamSynchronize(stream));
+    stats.upload_seconds = seconds_since(tx);
+    stats.setup_seconds = seconds_since(t0);
+    stats.kernel_mode = B2P_KERNELS_FUSED;
+    stats.precision_used = B2P_PRECISION_FP64;
+  }
+
+  // Block-diagonal form: check tables, fused-kernel schedules, autotuner.
+  void setup_grid(const HostCsr& A, const HostCsr& AT, int64_t annz) {
+    stats.multi_form = B2P_MULTI_GRID;
     // segmented check tables
     auto seg = [&](const std::vector<int64_t>& off, SegTable& tab, int32_t*& dofs, int& g) {
       std::vector<int32_t> inst, beg, end, bo(K + 1, 0);
@@ -488,13 +528,7 @@ struct MultiEngine {
     ltT = hbT.long_thr;
     hA_ptr = A.ptr;
     hT_ptr = AT.ptr;
-    inst_nnz.assign(K, 0);
-    for (int b = 0; b < K; ++b) inst_nnz[b] = static_cast<int64_t>(P[b].A.val.size());
     sched_nnz = annz;
-    if (M > 0) {
-      k_spmv<<<blocks(M), kBlock, 0, stream>>>(M, 1, viewA(), v[MXINIT], v[MAXINIT]);
-      B2P_CUDA(cudaGetLastError());
-    }
     const bool tune = opt.spmv_schedule == B2P_SCHEDULE_TUNED ||
                       (opt.spmv_schedule == B2P_SCHEDULE_AUTO && annz >= (int64_t(1) << 20));
     if (opt.spmv_schedule == B2P_SCHEDULE_TILED) {
@@ -509,11 +543,251 @@ struct MultiEngine {
     stats.schedule_at = tilesT.on ? B2P_SCHEDULE_TILED : B2P_SCHEDULE_BINNED;
     stats.streaming_a = !tilesA.on && streamA;
     stats.streaming_at = !tilesT.on && streamT;
+  }
+
+  // ---- CTA form (pdhg_cta.cuh) ----
+
+  // Static shared memory of k_lp_cta (reduction buffers) is below this.
+  static constexpr int64_t kCtaStaticReserve = 2048;
+
+  // Shared memory one block may give its LP: the device's opt-in per-block
+  // maximum less the kernel's static buffers, or the caller's limit.
+  int64_t cta_budget() const {
+    int optin = 0;
+    B2P_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    int64_t b = static_cast<int64_t>(optin) - kCtaStaticReserve;
+    if (opt.cta_smem_limit > 0) b = std::min<int64_t>(b, opt.cta_smem_limit);
+    return std::max<int64_t>(b, 0);
+  }
+  int cta_tier(int b, int64_t budget) const {
+    const Prepared& p = P[b];
+    const int64_t nnz = static_cast<int64_t>(p.A.val.size());
+    if (cta_tier_bytes(kCtaAll, p.m, p.n, nnz) <= budget) return kCtaAll;
+    if (cta_tier_bytes(kCtaVectors, p.m, p.n, nnz) <= budget) return kCtaVectors;
+    return kCtaGlobal;
+  }
+  // AUTO: the CTA form when every LP fits wholly in one block's shared memory.
+  bool choose_cta() const {
+    if (opt.multi_form == B2P_MULTI_GRID) return false;
+    if (opt.multi_form == B2P_MULTI_CTA) return true;
+    if (opt.multi_form != B2P_MULTI_AUTO) throw Error(B2P_ERR_INVALID, "unknown multi_form");
+    const int64_t budget = cta_budget();
+    for (int b = 0; b < K; ++b)
+      if (cta_tier(b, budget) != kCtaAll) return false;
+    return true;
+  }
+
+  void setup_cta(const HostCsr& A, const HostCsr& AT) {
+    stats.multi_form = B2P_MULTI_CTA;
+    const int64_t budget = cta_budget();
+    cta_lps.resize(K);
+    cta_smem = 0;
+    int n_all = 0, n_vec = 0;
+    for (int b = 0; b < K; ++b) {
+      const Prepared& p = P[b];
+      CtaLp& c = cta_lps[b];
+      c.roff = static_cast<int32_t>(roff[b]);
+      c.coff = static_cast<int32_t>(coff[b]);
+      c.m = p.m;
+      c.n = p.n;
+      c.a_beg = A.ptr[roff[b]];
+      c.t_beg = AT.ptr[coff[b]];
+      c.nnz = static_cast<int32_t>(p.A.val.size());
+      c.tier = cta_tier(b, budget);
+      c.eta = eta[b];
+      c.omega0 = omega0[b];
+      c.cnorm = cNorm[b];
+      c.rhsnorm = rhsNorm[b];
+      c.scale_obj = p.beta * p.gamma;
+      cta_smem = std::max(cta_smem, cta_tier_bytes(c.tier, p.m, p.n, c.nnz));
+      cta_owner_smem = std::max(cta_owner_smem, cta_owner_bytes(p.m, p.n, c.nnz));
+      cta_max_dim = std::max(cta_max_dim, std::max(p.m, p.n));
+      n_all += c.tier == kCtaAll;
+      n_vec += c.tier == kCtaVectors;
+    }
+    if (cta_owner_smem > budget) cta_owner_smem = 0;
+    // largest LPs first, so that the small ones fill in behind them
+    std::vector<int32_t> order(K);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return inst_nnz[x] > inst_nnz[y]; });
+    d_lps = upload(cta_lps);
+    d_order = upload(order);
+    d_out = dalloc<CtaOut>(K);
+    B2P_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&h_stop), sizeof(int32_t), cudaHostAllocMapped));
+    *h_stop = 0;
+    const int smem = static_cast<int>(cta_smem), osmem = static_cast<int>(cta_owner_smem);
+    B2P_CUDA(cudaFuncSetAttribute(k_lp_cta<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    B2P_CUDA(cudaFuncSetAttribute(k_lp_cta<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    B2P_CUDA(cudaFuncSetAttribute(k_lp_cta<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+#define B2P_OWNER_ATTR(NT, R) \
+  B2P_CUDA(cudaFuncSetAttribute(k_lp_owner<NT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, osmem));
+    B2P_OWNER_VARIANTS(B2P_OWNER_ATTR)
+#undef B2P_OWNER_ATTR
+    tune_cta();
+    stats.cta_threads = cta_nt;
+    stats.cta_owned_per_thread = cta_r;
+    stats.cta_smem_bytes = cta_r ? cta_owner_smem : cta_smem;
+    stats.cta_lps_smem = n_all;
+    stats.cta_lps_vectors = n_vec;
+  }
+
+  CtaArgs cta_args(double tol, int64_t max_it) const {
+    CtaArgs a;
+    a.lps = d_lps;
+    a.order = d_order;
+    a.out = d_out;
+    a.A = viewA();
+    a.AT = viewAT();
+    a.c = v[MC], a.lo = v[MLO], a.up = v[MUP], a.rl = v[MRL], a.ru = v[MRU];
+    a.rfac = d_rfac, a.cfac = d_cfac;
+    a.xinit = v[MXINIT], a.yinit = v[MYINIT], a.axinit = v[MAXINIT];
+    a.x = v[MX], a.xp = v[MXP], a.x0 = v[MX0];
+    a.y = v[MY], a.yp = v[MYP], a.y0 = v[MY0];
+    a.ax = v[MAX], a.axp = v[MAXP], a.ax0 = v[MAX0];
+    a.tol = tol;
+    a.rho = opt.reflection;
+    a.max_it = max_it;
+    a.check_every = opt.check_every;
+    a.stop = h_stop;
+    return a;
+  }
+
+  void launch_cta(int nt, int r, const CtaArgs& a) {
+    const unsigned grid = static_cast<unsigned>(K);
+    if (r == 0) {
+      const size_t smem = static_cast<size_t>(cta_smem);
+      if (nt == 128)
+        k_lp_cta<128><<<grid, 128, smem, stream>>>(a);
+      else if (nt == 256)
+        k_lp_cta<256><<<grid, 256, smem, stream>>>(a);
+      else
+        k_lp_cta<512><<<grid, 512, smem, stream>>>(a);
+    } else {
+      const size_t smem = static_cast<size_t>(cta_owner_smem);
+      bool launched = false;
+#define B2P_OWNER_LAUNCH(NT, R)                                 \
+  if (!launched && nt == NT && r == R) {                        \
+    k_lp_owner<NT, R><<<grid, NT, smem, stream>>>(a);           \
+    launched = true;                                            \
+  }
+      B2P_OWNER_VARIANTS(B2P_OWNER_LAUNCH)
+#undef B2P_OWNER_LAUNCH
+      if (!launched) throw Error(B2P_ERR_INVALID, "no such CTA kernel variant");
+    }
+    B2P_CUDA(cudaGetLastError());
+  }
+
+  // Kernel variants that can run this batch: the general kernel at 128, 256
+  // and 512 threads, and the owner kernel where every LP's rows and columns
+  // fit R per thread and its data fits in shared memory.
+  std::vector<std::pair<int, int>> cta_candidates() const {
+    const int want = opt.cta_kernel;  // B2P_CTA_*
+    if (want < B2P_CTA_AUTO || want > B2P_CTA_OWNER2) throw Error(B2P_ERR_INVALID, "unknown cta_kernel");
+    std::vector<std::pair<int, int>> c;
+    if (want == B2P_CTA_AUTO || want == B2P_CTA_GENERAL)
+      for (const int nt : {128, 256, 512})
+        if (opt.cta_threads == 0 || opt.cta_threads == nt) c.emplace_back(nt, 0);
+    if (cta_owner_smem > 0 && want != B2P_CTA_GENERAL) {
+#define B2P_OWNER_CAND(NT, R)                                                                        \
+  if ((opt.cta_threads == 0 || opt.cta_threads == NT) && cta_max_dim <= NT * R &&                    \
+      (want == B2P_CTA_AUTO || want == B2P_CTA_OWNER1 + R - 1))                                      \
+    c.emplace_back(NT, R);
+      B2P_OWNER_VARIANTS(B2P_OWNER_CAND)
+#undef B2P_OWNER_CAND
+    }
+    if (c.empty()) throw Error(B2P_ERR_INVALID, "no CTA kernel variant fits these LPs and options");
+    return c;
+  }
+
+  // Variant choice: each candidate runs every LP for five check intervals
+  // (tolerance -1: no LP stops early), twice, and the fastest is kept.
+  void tune_cta() {
+    const auto t0 = Clock::now();
+    if (opt.cta_threads != 0 && opt.cta_threads != 128 && opt.cta_threads != 256 && opt.cta_threads != 512)
+      throw Error(B2P_ERR_INVALID, "cta_threads must be 128, 256 or 512");
+    const std::vector<std::pair<int, int>> cands = cta_candidates();
+    cta_nt = cands.front().first;
+    cta_r = cands.front().second;
+    const int64_t probe = std::min<int64_t>(opt.max_iterations, 5 * static_cast<int64_t>(opt.check_every));
+    if (probe <= 0 || cands.size() == 1) return;
+    cudaEvent_t e0, e1;
+    B2P_CUDA(cudaEventCreate(&e0));
+    B2P_CUDA(cudaEventCreate(&e1));
+    double best = INFINITY;
+    for (const auto& v : cands) {
+      launch_cta(v.first, v.second, cta_args(-1.0, 1));  // first launch of this kernel: module load
+      for (int rep = 0; rep < 2; ++rep) {
+        B2P_CUDA(cudaEventRecord(e0, stream));
+        launch_cta(v.first, v.second, cta_args(-1.0, probe));
+        B2P_CUDA(cudaEventRecord(e1, stream));
+        B2P_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        B2P_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) {
+          best = ms;
+          cta_nt = v.first;
+          cta_r = v.second;
+        }
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    stats.autotune_seconds = seconds_since(t0);
+  }
+
+  // The whole solve is one launch; the host only watches the deadline and
+  // the cancel flag and raises the mapped stop flag (read at every check).
+  void solve_cta(Clock::time_point deadline_start) {
+    const auto t_solve = Clock::now();
+    results.assign(K, b2p_result{});
+    xs.assign(K, {});
+    ys.assign(K, {});
+    *reinterpret_cast<volatile int32_t*>(h_stop) = 0;
+    B2P_CUDA(cudaEventRecord(ev_start, stream));
+    launch_cta(cta_nt, cta_r, cta_args(opt.tolerance, opt.max_iterations));
+    B2P_CUDA(cudaEventRecord(ev_stop, stream));
+    launches = 1;
+    if (opt.time_limit <= 0 && !opt.cancel_flag) {
+      B2P_CUDA(cudaEventSynchronize(ev_stop));
+    } else {
+      bool raised = false;
+      for (;;) {
+        const cudaError_t q = cudaEventQuery(ev_stop);
+        if (q == cudaSuccess) break;
+        if (q != cudaErrorNotReady) B2P_CUDA(q);
+        const bool expired = (opt.cancel_flag && *opt.cancel_flag) ||
+                             (opt.time_limit > 0 && seconds_since(deadline_start) >= opt.time_limit);
+        if (expired && !raised) {
+          *reinterpret_cast<volatile int32_t*>(h_stop) = 1;
+          raised = true;
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(100));
+      }
+    }
+    float ms = 0;
+    B2P_CUDA(cudaEventElapsedTime(&ms, ev_start, ev_stop));
+    stats.kernel_seconds = ms / 1000.0;
+    std::vector<CtaOut> out(K);
+    std::vector<double> xp(N), yp(M);
+    B2P_CUDA(cudaMemcpyAsync(out.data(), d_out, sizeof(CtaOut) * K, cudaMemcpyDeviceToHost, stream));
+    if (N) B2P_CUDA(cudaMemcpyAsync(xp.data(), v[MXP], sizeof(double) * N, cudaMemcpyDeviceToHost, stream));
+    if (M) B2P_CUDA(cudaMemcpyAsync(yp.data(), v[MYP], sizeof(double) * M, cudaMemcpyDeviceToHost, stream));
     B2P_CUDA(cudaStreamSynchronize(stream));
-    stats.upload_seconds = seconds_since(tx);
-    stats.setup_seconds = seconds_since(t0);
-    stats.kernel_mode = B2P_KERNELS_FUSED;
-    stats.precision_used = B2P_PRECISION_FP64;
+    bytes_down += static_cast<int64_t>(sizeof(CtaOut) * K + sizeof(double) * (static_cast<int64_t>(N) + M));
+    int64_t its = 0;
+    stats.restarts = 0;
+    for (int b = 0; b < K; ++b) {
+      const CtaOut& o = out[b];
+      store_result(b, o.status, o.rel_kkt, o.pobj, o.dobj, o.iterations, xp.data() + coff[b], yp.data() + roff[b]);
+      its = std::max<int64_t>(its, o.iterations + (o.status == B2P_STATUS_OPTIMAL ? 1 : 0));
+      stats.restarts += o.restarts;
+    }
+    stats.iterations = its;
+    stats.primal_weight = K ? out[0].omega : 1.0;
+    stats.solve_seconds = seconds_since(t_solve);
+    stats.kernel_launches = launches;
+    stats.bytes_uploaded = bytes_up;
+    stats.bytes_downloaded = bytes_down;
   }
 
   // Warm starts of some instances (original space); others keep the cold start.
@@ -901,6 +1175,13 @@ struct MultiEngine {
       B2P_CUDA(cudaMemcpyAsync(yp.data(), v[MYP] + roff[b], sizeof(double) * p.m, cudaMemcpyDeviceToHost, stream));
     B2P_CUDA(cudaStreamSynchronize(stream));
     bytes_down += static_cast<int64_t>(sizeof(double) * (p.n + p.m));
+    store_result(b, status, relKkt, pobj, dobj, it, xp.data(), yp.data());
+  }
+
+  // Unscaled answer of instance b from its scaled x+ and y+ (src/pdhg/pdhg.cpp:668-680).
+  void store_result(int b, int status, double relKkt, double pobj, double dobj, int64_t it, const double* xp,
+                    const double* yp) {
+    const Prepared& p = P[b];
     xs[b].resize(p.n);
     ys[b].resize(p.m);
     for (int32_t j = 0; j < p.n; ++j) xs[b][j] = xp[j] * p.Cs[j] * p.beta;
@@ -916,6 +1197,10 @@ struct MultiEngine {
   // runPdhg's loop for every instance at once (src/pdhg/pdhg.cpp:560-687).
   void solve(Clock::time_point deadline_start) {
     B2P_CUDA(cudaSetDevice(device));
+    if (cta) {
+      solve_cta(deadline_start);
+      return;
+    }
     const auto t_solve = Clock::now();
     launches = 0;
     reset_state();

@@ -21,6 +21,8 @@ PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 KERNELS_AUTO, KERNELS_FUSED, KERNELS_RESIDENT = 0, 1, 2
 SCHEDULE_AUTO, SCHEDULE_BINNED, SCHEDULE_TILED, SCHEDULE_TUNED = 0, 1, 2, 3
+MULTI_AUTO, MULTI_GRID, MULTI_CTA = 0, 1, 2
+CTA_AUTO, CTA_GENERAL, CTA_OWNER1, CTA_OWNER2 = 0, 1, 2, 3
 
 dptr = C.POINTER(C.c_double)
 iptr = C.POINTER(C.c_int32)
@@ -44,7 +46,8 @@ class B2pOptions(C.Structure):
                 ("log_interval", C.c_int32), ("device", C.c_int32), ("time_limit", C.c_double),
                 ("cancel_flag", C.POINTER(C.c_int32)), ("precision", C.c_int32), ("use_graphs", C.c_int32),
                 ("lanes_per_row_a", C.c_int32), ("lanes_per_row_at", C.c_int32), ("short_row_rounds", C.c_int32),
-                ("kernel_mode", C.c_int32), ("spmv_schedule", C.c_int32)]
+                ("kernel_mode", C.c_int32), ("spmv_schedule", C.c_int32), ("multi_form", C.c_int32),
+                ("cta_smem_limit", C.c_int32), ("cta_threads", C.c_int32), ("cta_kernel", C.c_int32)]
 
 
 class B2pStats(C.Structure):
@@ -58,7 +61,9 @@ class B2pStats(C.Structure):
                 ("resident_blocks", C.c_int32), ("resident_smem_bytes", C.c_int64), ("precision_used", C.c_int32),
                 ("pad1", C.c_int32), ("fp32_iterations", C.c_int64), ("schedule_a", C.c_int32),
                 ("schedule_at", C.c_int32), ("autotune_seconds", C.c_double), ("streaming_a", C.c_int32),
-                ("streaming_at", C.c_int32)]
+                ("streaming_at", C.c_int32), ("multi_form", C.c_int32), ("cta_threads", C.c_int32),
+                ("cta_smem_bytes", C.c_int64), ("cta_lps_smem", C.c_int32), ("cta_lps_vectors", C.c_int32),
+                ("cta_owned_per_thread", C.c_int32), ("pad2", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_ if not f.startswith("pad")}

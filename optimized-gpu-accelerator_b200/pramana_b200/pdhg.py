@@ -48,6 +48,10 @@ class PdhgOptions:
     shortRowRounds: int = 0
     kernelMode: int = _lib.KERNELS_AUTO   # KERNELS_FUSED / KERNELS_RESIDENT to force a form
     spmvSchedule: int = _lib.SCHEDULE_AUTO  # multi-LP SpMV schedule (SCHEDULE_BINNED / _TILED / _TUNED)
+    multiForm: int = _lib.MULTI_AUTO  # multi-LP engine form (MULTI_GRID / MULTI_CTA)
+    ctaSmemLimit: int = 0  # CTA form: shared-memory bytes one LP may use (0 = device maximum)
+    ctaThreads: int = 0  # CTA form: threads per block (128 / 256 / 512; 0 = autotuned)
+    ctaKernel: int = _lib.CTA_AUTO  # CTA form: CTA_GENERAL / CTA_OWNER1 / CTA_OWNER2 (0 = autotuned)
 
     def to_c(self, cancel_flag=None) -> _lib.B2pOptions:
         if not self.useGpu:
@@ -71,6 +75,10 @@ class PdhgOptions:
         o.short_row_rounds = int(self.shortRowRounds)
         o.kernel_mode = int(self.kernelMode)
         o.spmv_schedule = int(self.spmvSchedule)
+        o.multi_form = int(self.multiForm)
+        o.cta_smem_limit = int(self.ctaSmemLimit)
+        o.cta_threads = int(self.ctaThreads)
+        o.cta_kernel = int(self.ctaKernel)
         if cancel_flag is not None:
             o.cancel_flag = C.cast(cancel_flag, C.POINTER(C.c_int32))
         return o
@@ -228,10 +236,11 @@ def solvePdhgBatch(base: Model, cases: list[LpCase], opts: PdhgOptions | None = 
 
 
 def solvePdhgMulti(lps: list[Model], opts: PdhgOptions | None = None, batchStats: PdhgStats | None = None,
-                   starts: list | None = None) -> list[PdhgResult]:
+                   starts: list | None = None, cancel_flag=None) -> list[PdhgResult]:
     """Independent LPs of different sizes solved together on the GPU, each with
     the reference's algorithm (no counterpart in the reference).  starts[b] =
-    (x, y) warm-starts LP b (None entries: cold start)."""
+    (x, y) warm-starts LP b (None entries: cold start); cancel_flag: a ctypes
+    int32 array whose element 0 stops the solve when set."""
     if not lps:
         return []
     opts = opts or PdhgOptions()
@@ -249,7 +258,7 @@ def solvePdhgMulti(lps: list[Model], opts: PdhgOptions | None = None, batchStats
     yp = (_lib.dptr * k)(*[a.ctypes.data_as(_lib.dptr) for a in ys])
     res = (_lib.B2pResult * k)()
     st = _lib.B2pStats()
-    o = opts.to_c()
+    o = opts.to_c(cancel_flag)
     xst = yst = None
     if starts is not None:
         sx = [None if s is None or s[0] is None else np.ascontiguousarray(s[0], dtype=np.float64) for s in starts]

@@ -1,0 +1,211 @@
+"""The CTA form of the multi-LP engine (one thread block runs one LP's whole
+PDHG loop, restart and termination decisions included): every LP must follow
+the reference algorithm as if solved alone -- iterates against the oracle at
+fixed iteration counts in each storage tier, and to convergence."""
+import ctypes as C
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from pramana_b200 import _lib
+from pramana_b200 import generators as G
+from pramana_b200 import pdhg
+from pramana_b200 import warmstart as W
+from test_gpu_multi import family
+from test_gpu_parity import _host_kkt, assert_close, opts
+
+pytestmark = pytest.mark.gpu
+
+CTA = dict(multiForm=_lib.MULTI_CTA)
+
+
+def _stats():
+    return pdhg.solvePdhgMulti.last_stats
+
+
+@pytest.mark.parametrize("iters", [1, 64, 1000])
+def test_cta_fixed_iterations_vs_oracle(oracle_mod, iters):
+    lps = family()
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-30, maxIterations=iters, **CTA))
+    st = _stats()
+    assert st.multi_form == _lib.MULTI_CTA and st.kernel_launches == 1
+    for lp, r in zip(lps, rs):
+        assert_close(r, oracle_mod.solve(lp, "oracle", tolerance=1e-30, max_iterations=iters))
+
+
+@pytest.mark.parametrize("limit,tiers", [(0, None), (64 * 1024, None), (1, (0, 0))])
+def test_cta_storage_tiers_vs_oracle(oracle_mod, limit, tiers):
+    """Shared-memory limits that move LPs between the three storage tiers
+    (all in shared memory / iterates only / global memory)."""
+    lps = family()
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-30, maxIterations=300, ctaSmemLimit=limit, **CTA))
+    st = _stats()
+    if tiers is not None:
+        assert (st.cta_lps_smem, st.cta_lps_vectors) == tiers
+    else:
+        assert st.cta_lps_smem >= 1
+    for lp, r in zip(lps, rs):
+        assert_close(r, oracle_mod.solve(lp, "oracle", tolerance=1e-30, max_iterations=300))
+
+
+def test_cta_mixed_tiers_counts():
+    lps = family()
+    pdhg.solvePdhgMulti(lps, opts(tolerance=1e-30, maxIterations=10, ctaSmemLimit=64 * 1024, **CTA))
+    st = _stats()
+    # the 2000 x 4000 LP (25.6k nonzeros) keeps only nothing / its iterates in 64 KB
+    assert st.cta_lps_smem + st.cta_lps_vectors < len(lps)
+    assert st.cta_smem_bytes <= 64 * 1024
+
+
+def test_cta_converged_vs_oracle(oracle_mod):
+    lps = family()
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, maxIterations=200000, **CTA))
+    for lp, r in zip(lps, rs):
+        o = oracle_mod.solve(lp, "oracle", tolerance=1e-6, max_iterations=200000)
+        assert r.status == "Optimal" and o.status == 1
+        assert abs(r.iterations - o.iterations) <= 4 * 64
+        assert abs(r.objective - o.objective) <= 1e-5 * (1 + abs(o.objective))
+        if lp.num_rows:
+            assert max(_host_kkt(lp, r.x, r.rowDual)) <= 1e-6 * (1 + 1e-6)
+
+
+def test_cta_iteration_limit_reports_every_instance(oracle_mod):
+    lps = family()
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-30, maxIterations=100, **CTA))
+    for lp, r in zip(lps, rs):
+        o = oracle_mod.solve(lp, "oracle", tolerance=1e-30, max_iterations=100)
+        assert r.status == {1: "Optimal", 6: "IterationLimit"}[o.status] and r.iterations == o.iterations
+
+
+def test_cta_matches_grid_form():
+    """Both forms run the same algorithm; to 1e-6 they agree on status,
+    iteration counts (within a few checks) and objectives."""
+    lps = family()
+    a = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, **CTA))
+    b = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, multiForm=_lib.MULTI_GRID))
+    assert _stats().multi_form == _lib.MULTI_GRID
+    for ra, rb in zip(a, b):
+        assert ra.status == rb.status == "Optimal"
+        assert abs(ra.iterations - rb.iterations) <= 4 * 64
+        assert abs(ra.objective - rb.objective) <= 1e-5 * (1 + abs(rb.objective))
+
+
+def test_cta_warm_start():
+    lps = family()[:6]
+    cold = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, **CTA))
+    starts = [(r.x, r.rowDual) if b % 2 == 0 else None for b, r in enumerate(cold)]
+    warm = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, **CTA), starts=starts)
+    for b, (c, w) in enumerate(zip(cold, warm)):
+        assert w.status == "Optimal"
+        if b % 2 == 0:
+            assert w.iterations <= 64
+        else:
+            assert w.iterations == c.iterations
+
+
+def test_cta_time_limit_and_cancel():
+    lps = [G.random_lp(300, 600, 4.0, 180, 50 + i) for i in range(4)]
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-30, maxIterations=100_000_000, timeLimit=0.2, **CTA))
+    assert all(r.status == "TimeLimit" and 0 < r.iterations < 100_000_000 for r in rs)
+    flag = (C.c_int32 * 1)(0)
+
+    def cancel():
+        time.sleep(0.2)
+        flag[0] = 1
+
+    th = threading.Thread(target=cancel)
+    th.start()
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-30, maxIterations=100_000_000, **CTA), cancel_flag=flag)
+    th.join()
+    assert all(r.status == "TimeLimit" for r in rs)
+
+
+def test_cta_auto_picks_cta_for_small_family():
+    fam = W.RefineryFamily(seed=5, periods=2, regions=1, units=4, streams=4, properties=2, scale_exponent=0.0)
+    params = fam.sample(64, seed=11)
+    lps = [fam.instance(p) for p in params]
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6))
+    st = _stats()
+    assert st.multi_form == _lib.MULTI_CTA and st.cta_lps_smem == len(lps)
+    assert st.cta_threads in (128, 256, 512)
+    g = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, multiForm=_lib.MULTI_GRID))
+    for lp, a, b in zip(lps, rs, g):
+        assert a.status == b.status == "Optimal"
+        assert max(_host_kkt(lp, a.x, a.rowDual)) <= 1e-6 * (1 + 1e-6)
+        assert abs(a.objective - b.objective) <= 1e-5 * (1 + abs(b.objective))
+
+
+def test_cta_uneven_batch_not_auto():
+    """AUTO keeps the block-diagonal form when an LP does not fit in one
+    block's shared memory."""
+    lps = G.uneven_family(4, 1e4, 3e4, seed=3)
+    pdhg.solvePdhgMulti(lps, opts(tolerance=1e-30, maxIterations=64))
+    assert _stats().multi_form == _lib.MULTI_GRID
+
+
+# ---- owner kernel (each thread owns 1 or 2 rows and columns) ----
+
+def small_family():
+    """LPs of at most 500 rows / columns, including one whose rows are all
+    empty, one without rows and a refinery family member."""
+    import lp_cases
+    from pramana_b200.model import Model
+    lps = [G.random_lp(m, 2 * m, 4.0, int(0.6 * m), 300 + i) for i, m in enumerate([40, 250, 120, 7])]
+    lps.append(lp_cases.edge_lp(5))
+    n = 5
+    lps.append(Model(num_rows=0, num_cols=n, start=np.zeros(n + 1), index=[], value=[], col_cost=[1, -1, 2, 0, 3],
+                     col_lower=np.zeros(n), col_upper=np.full(n, 4.0), row_lower=[], row_upper=[]))
+    fam = W.RefineryFamily(seed=5, periods=2, regions=1, units=4, streams=4, properties=2, scale_exponent=0.0)
+    lps.append(fam.instance(fam.sample(1, seed=3)[0]))
+    return lps
+
+
+@pytest.mark.parametrize("kernel,threads", [(_lib.CTA_OWNER1, 512), (_lib.CTA_OWNER2, 256), (_lib.CTA_OWNER2, 512),
+                                            (_lib.CTA_GENERAL, 128)])
+@pytest.mark.parametrize("iters", [1, 64, 1000])
+def test_owner_kernel_fixed_iterations_vs_oracle(oracle_mod, kernel, threads, iters):
+    lps = small_family()
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-30, maxIterations=iters, ctaKernel=kernel, ctaThreads=threads,
+                                       **CTA))
+    st = _stats()
+    assert st.cta_threads == threads
+    assert st.cta_owned_per_thread == {_lib.CTA_OWNER1: 1, _lib.CTA_OWNER2: 2, _lib.CTA_GENERAL: 0}[kernel]
+    for lp, r in zip(lps, rs):
+        assert_close(r, oracle_mod.solve(lp, "oracle", tolerance=1e-30, max_iterations=iters))
+
+
+def test_owner_and_general_kernels_agree_bitwise():
+    """Same arithmetic element by element and the same reductions' inputs:
+    the two kernels' answers are identical to convergence."""
+    lps = small_family()
+    a = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, ctaKernel=_lib.CTA_OWNER2, ctaThreads=256, **CTA))
+    b = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, ctaKernel=_lib.CTA_GENERAL, ctaThreads=256, **CTA))
+    for ra, rb in zip(a, b):
+        assert ra.status == rb.status == "Optimal"
+        assert ra.iterations == rb.iterations
+        assert np.array_equal(ra.x, rb.x) and np.array_equal(ra.rowDual, rb.rowDual)
+
+
+def test_owner_kernel_refused_when_too_large():
+    lps = small_family()
+    with pytest.raises(Exception):
+        pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, ctaKernel=_lib.CTA_OWNER1, ctaThreads=128, **CTA))
+
+
+def test_owner_kernel_converged_and_warm(oracle_mod):
+    lps = small_family()
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, ctaKernel=_lib.CTA_OWNER2, **CTA))
+    for lp, r in zip(lps, rs):
+        o = oracle_mod.solve(lp, "oracle", tolerance=1e-6, max_iterations=200000)
+        assert r.status == "Optimal" and o.status == 1
+        assert abs(r.iterations - o.iterations) <= 4 * 64
+        if lp.num_rows:
+            assert max(_host_kkt(lp, r.x, r.rowDual)) <= 1e-6 * (1 + 1e-6)
+    starts = [(r.x, r.rowDual) for r in rs]
+    warm = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, ctaKernel=_lib.CTA_OWNER2, **CTA), starts=starts)
+    ref = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, ctaKernel=_lib.CTA_GENERAL, **CTA), starts=starts)
+    for r, w, g in zip(rs, warm, ref):
+        assert w.status == "Optimal" and w.iterations <= r.iterations
+        assert w.iterations == g.iterations and np.array_equal(w.x, g.x)
