@@ -203,7 +203,7 @@ def run_family(args, rank, world):
     opts = pdhg.PdhgOptions(tolerance=TOL, maxIterations=200000, precision=0)
     t0 = time.perf_counter()
     P_train = fam.sample(args.train, 100)
-    tr = W.solve_family(fam, P_train, opts, batch=args.batch)
+    tr = W.solve_family(fam, P_train, opts, batch=args.batch, engine=args.engine)
     gen_s = time.perf_counter() - t0
     ok = tr.status == 1
     lw = W.LearnedWarmStart(fam, seed=1)
@@ -212,7 +212,7 @@ def run_family(args, rank, world):
     nn = W.NearestWarmStart(fam).fit(P_train[ok], tr.X[ok], tr.Y[ok])
     strategies = {"cold": None, "nearest": nn, "learned": lw}
     for w in range(args.warmup):  # untimed warm-up batches
-        W.solve_warm(fam, fam.sample(args.batch, 900 + w), lw, opts, batch=args.batch)
+        W.solve_warm(fam, fam.sample(args.batch, 900 + w), lw, opts, batch=args.batch, engine=args.engine)
     acc = {k: {"seconds": [], "solve_seconds": [], "iterations": [], "certified": [], "fallback": [], "kkt": []}
            for k in strategies}
     with ClockSampler(0) as clk:
@@ -221,7 +221,7 @@ def run_family(args, rank, world):
             for name, pred in strategies.items():
                 torch.cuda.synchronize()
                 t1 = time.perf_counter()
-                r, cert, redo = W.solve_warm(fam, P, pred, opts, batch=args.batch)
+                r, cert, redo = W.solve_warm(fam, P, pred, opts, batch=args.batch, engine=args.engine)
                 wall = time.perf_counter() - t1
                 a = acc[name]
                 a["seconds"].append(wall)
@@ -263,6 +263,8 @@ def run_family(args, rank, world):
                                    f"({FAMILY_SIZE}), 16 parameters; {args.train} training members, "
                                    f"{args.steps} x {args.batch} held-out members, to rel KKT {TOL:g}",
                        "step": "one held-out batch solved and certified per strategy",
+                       "engine": {"multi": "multi-LP engine (AUTO form: one thread block per member)",
+                                  "batch": "shared-A batch engine (k-interleaved cases)"}[args.engine],
                        "network": lw.widths, "pca_rank": lw.rank, "pca_explained": lw.basis.explained,
                        "l2": "inputs re-uploaded per batch; the batch state (~4 MB) is L2-resident"},
             "strategies": out,
@@ -419,6 +421,8 @@ def main():
                     help="multi: SpMV schedule of the multi-LP kernels")
     ap.add_argument("--train", type=int, default=32768, help="family: training members")
     ap.add_argument("--batch", type=int, default=1024, help="family: members per batched solve")
+    ap.add_argument("--engine", choices=["multi", "batch"], default="multi",
+                    help="family: multi-LP engine (one block per member) or the shared-A batch engine")
     ap.add_argument("--epochs", type=int, default=200, help="family: MLP training epochs")
     ap.add_argument("--per-instance-sample", type=int, default=16,
                     help="family: members solved one at a time for the per-instance FP64 baseline")

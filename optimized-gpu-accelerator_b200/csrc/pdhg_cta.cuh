@@ -223,7 +223,10 @@ __device__ __forceinline__ void copy_in(T* __restrict__ dst, const T* __restrict
 }
 
 // Left-to-right row sum over entries [p, e) of (idx, val) against the local
-// vector v (index minus `shift`).
+// vector v (index minus `shift`): s = ((0 + a0 v0) + a1 v1) + ...  (A version
+// that issued the loads of 4 or 8 entries before their additions measured
+// slower: the block is bound by shared-memory wavefronts -- scattered row
+// starts and gathers -- not by load latency.)
 __device__ __forceinline__ double row_sum(int p, const int e, const int32_t* __restrict__ idx,
                                           const double* __restrict__ val, const double* __restrict__ v, int shift) {
   double s = 0.0;

@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <numeric>
 #include <thread>
 #include <vector>
@@ -700,7 +701,10 @@ struct MultiEngine {
   }
 
   // Variant choice: each candidate runs every LP for five check intervals
-  // (tolerance -1: no LP stops early), twice, and the fastest is kept.
+  // (tolerance -1: no LP stops early), twice, and the fastest is kept.  The
+  // choice is remembered for the process per batch shape (device, LP count,
+  // largest dimension, shared-memory sizes, nonzeros, options), so repeated
+  // batches of one family pay for it once.
   void tune_cta() {
     const auto t0 = Clock::now();
     if (opt.cta_threads != 0 && opt.cta_threads != 128 && opt.cta_threads != 256 && opt.cta_threads != 512)
@@ -710,6 +714,21 @@ struct MultiEngine {
     cta_r = cands.front().second;
     const int64_t probe = std::min<int64_t>(opt.max_iterations, 5 * static_cast<int64_t>(opt.check_every));
     if (probe <= 0 || cands.size() == 1) return;
+    int64_t total_nnz = 0;
+    for (const CtaLp& c : cta_lps) total_nnz += c.nnz;
+    const std::vector<int64_t> key{device, K, cta_max_dim, cta_smem, cta_owner_smem, total_nnz, opt.cta_threads,
+                                   opt.cta_kernel, opt.check_every};
+    static std::mutex mu;
+    static std::map<std::vector<int64_t>, std::pair<int, int>> chosen;
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      const auto it = chosen.find(key);
+      if (it != chosen.end()) {
+        cta_nt = it->second.first;
+        cta_r = it->second.second;
+        return;
+      }
+    }
     cudaEvent_t e0, e1;
     B2P_CUDA(cudaEventCreate(&e0));
     B2P_CUDA(cudaEventCreate(&e1));
@@ -732,6 +751,10 @@ struct MultiEngine {
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      chosen[key] = {cta_nt, cta_r};
+    }
     stats.autotune_seconds = seconds_since(t0);
   }
 
