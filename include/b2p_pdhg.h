@@ -153,6 +153,12 @@ typedef struct b2p_options {
    * each own 1 or 2 rows and columns and keep their state in registers (LPs
    * with max(m, n) <= 2 x threads whose data fit in shared memory). */
   int32_t cta_kernel;
+  /* FP64 batches (k > 1 cases sharing A): variant of the two per-iteration
+   * kernels -- 0 = timed on the device when the batch's vectors far exceed L2
+   * (plain otherwise); 1..4 force (cases per thread, evict-first streamed
+   * vectors) = (1, no), (2, no), (1, yes), (2, yes). */
+  int32_t batch_variant;
+  int32_t pad_options;
 } b2p_options;
 enum { B2P_MULTI_AUTO = 0, B2P_MULTI_GRID = 1, B2P_MULTI_CTA = 2 };
 enum { B2P_CTA_AUTO = 0, B2P_CTA_GENERAL = 1, B2P_CTA_OWNER1 = 2, B2P_CTA_OWNER2 = 3 };
@@ -184,7 +190,7 @@ typedef struct b2p_stats {
   int64_t fp32_iterations;                    /* mixed form: iterations run in FP32 */
   int32_t schedule_a, schedule_at;            /* multi-LP: B2P_SCHEDULE_BINNED or _TILED per operator */
   double autotune_seconds;                    /* multi-LP: time the autotuner took (part of setup) */
-  int32_t streaming_a, streaming_at;          /* multi-LP binned schedules: evict-first streaming loads */
+  int32_t streaming_a, streaming_at;          /* multi-LP binned schedules, FP64 batches: evict-first streaming loads */
   int32_t multi_form;                         /* multi-LP: B2P_MULTI_GRID or B2P_MULTI_CTA */
   int32_t cta_threads;                        /* CTA form: threads per block (autotuned) */
   int64_t cta_smem_bytes;                     /* CTA form: dynamic shared memory per block */
@@ -192,6 +198,7 @@ typedef struct b2p_stats {
   int32_t cta_lps_vectors;                    /* CTA form: LPs with only their iterates in shared memory */
   int32_t cta_owned_per_thread;               /* CTA form: rows and columns each thread owns (0 = general kernel) */
   int32_t pad2;
+  int32_t cases_per_thread_at, cases_per_thread_a; /* FP64 batches: cases per thread of the A^T / A kernels */
 } b2p_stats;
 
 /* Replaces pramana::PdhgResult (src/pdhg/pdhg.h:58-65) minus the vectors,

@@ -155,6 +155,8 @@ struct Engine {
   std::map<int, cudaGraphExec_t> graphs, graphs32;  // per interval length; FP32 phase of a batch
   std::map<int, cudaGraph_t> graph_defs, graph_defs32;
   bool mixed_batch = false;  // mixed form of a batch (k > 1): FP32 k-interleaved kernels
+  bool batch_stream_p = false, batch_stream_d = false;  // evict-first streamed vectors (tuned per kernel)
+  int batch_cpt_p = 1, batch_cpt_d = 1;  // cases per thread of the primal / dual batch kernels (tuned)
   bool profiling = false;
   std::vector<cudaEvent_t> prof_ev;  // 4 per iteration of the longest interval
   int64_t prof_launches[3] = {0, 0, 0};
@@ -344,6 +346,7 @@ struct Engine {
       k_spmv<<<blocks(static_cast<int64_t>(m) * k), kBlock, 0, stream>>>(m, k, viewA(), v[XINIT], v[AXINIT]);
       B2P_CUDA(cudaGetLastError());
     }
+    tune_batch();
     B2P_CUDA(cudaStreamSynchronize(stream));
     transfer_seconds = seconds_since(tx);
     stats.upload_seconds = transfer_seconds;
@@ -734,38 +737,111 @@ struct Engine {
     B2P_CUDA(cudaMemcpyAsync(h_sums, d_sums, sizeof(double) * k * kNumSums, cudaMemcpyDeviceToHost, stream));
   }
 
+  // FP64 batch kernels (k > 1) of one iteration.
+  void enqueue_batch_primal(bool halpern, bool streamed, const IterClock& ck, int cpt) {
+    const double rho = opt.reflection;
+    const unsigned gp = blocks(static_cast<int64_t>(n) * ((k + cpt - 1) / cpt));
+    const CsrView AT = viewAT();
+#define B2P_BP(H, ST, CP) \
+  launch(k_primal<H, ST, CP>, gp, stream, true, n, k, AT, v[Y], v[C], v[LO], v[UP], v[X], v[XP], v[X0], d_tau, ck, rho)
+#define B2P_BP2(H, ST) \
+  if (cpt == 2) B2P_BP(H, ST, 2); else B2P_BP(H, ST, 1);
+    if (halpern) {
+      if (streamed) { B2P_BP2(true, true) } else { B2P_BP2(true, false) }
+    } else {
+      if (streamed) { B2P_BP2(false, true) } else { B2P_BP2(false, false) }
+    }
+#undef B2P_BP2
+#undef B2P_BP
+  }
+  void enqueue_batch_dual(bool halpern, bool streamed, const IterClock& ck, int cpt) {
+    const double rho = opt.reflection;
+    const unsigned gd = blocks(static_cast<int64_t>(m) * ((k + cpt - 1) / cpt));
+    const CsrView A = viewA();
+#define B2P_BD(H, ST, CP)                                                                                           \
+  launch(k_dual<H, ST, CP>, gd, stream, true, m, k, A, v[XP], v[RL], v[RU], v[Y], v[YP], v[Y0], v[AX], v[AXP], \
+         v[AX0], d_sigma, ck, rho)
+#define B2P_BD2(H, ST) \
+  if (cpt == 2) B2P_BD(H, ST, 2); else B2P_BD(H, ST, 1);
+    if (halpern) {
+      if (streamed) { B2P_BD2(true, true) } else { B2P_BD2(true, false) }
+    } else {
+      if (streamed) { B2P_BD2(false, true) } else { B2P_BD2(false, false) }
+    }
+#undef B2P_BD2
+#undef B2P_BD
+  }
+
+  // FP64 batch kernel variants: forced by the options, or, for batches whose
+  // vectors far exceed L2 (k (m + n) >= 2^22 elements), each kernel is timed
+  // with one and with two cases per thread, with cached and with evict-first
+  // streamed vectors (one warm-up, three timed launches each, from the
+  // starting state), and the fastest is kept per kernel.
+  void tune_batch() {
+    if (opt.batch_variant < 0 || opt.batch_variant > 4) throw Error(B2P_ERR_INVALID, "batch_variant must be 0..4");
+    if (k <= 1 || mixed_batch) return;
+    if (opt.batch_variant > 0) {
+      batch_cpt_p = batch_cpt_d = (opt.batch_variant == 2 || opt.batch_variant == 4) ? 2 : 1;
+      batch_stream_p = batch_stream_d = opt.batch_variant >= 3;
+    } else if (static_cast<int64_t>(n + m) * k >= (int64_t(1) << 22)) {
+      time_batch_variants();
+    }
+    stats.streaming_at = batch_stream_p;
+    stats.streaming_a = batch_stream_d;
+    stats.cases_per_thread_at = batch_cpt_p;
+    stats.cases_per_thread_a = batch_cpt_d;
+  }
+
+  void time_batch_variants() {
+    const auto t0 = Clock::now();
+    std::vector<double> omega;
+    reset_state(omega);
+    cudaEvent_t e0, e1;
+    B2P_CUDA(cudaEventCreate(&e0));
+    B2P_CUDA(cudaEventCreate(&e1));
+    const IterClock ck{d_it_base, d_restart_at, 0};
+    auto timed = [&](auto&& enq) {
+      enq();
+      B2P_CUDA(cudaEventRecord(e0, stream));
+      for (int r = 0; r < 3; ++r) enq();
+      B2P_CUDA(cudaEventRecord(e1, stream));
+      B2P_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      B2P_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      return static_cast<double>(ms);
+    };
+    double best_p = INFINITY, best_d = INFINITY;
+    for (const int cpt : {1, 2})
+      for (int st = 0; st < 2; ++st) {
+        if (n) {
+          const double t = timed([&] { enqueue_batch_primal(true, st != 0, ck, cpt); });
+          if (t < best_p) best_p = t, batch_stream_p = st != 0, batch_cpt_p = cpt;
+        }
+        if (m) {
+          const double t = timed([&] { enqueue_batch_dual(true, st != 0, ck, cpt); });
+          if (t < best_d) best_d = t, batch_stream_d = st != 0, batch_cpt_d = cpt;
+        }
+      }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    stats.autotune_seconds = seconds_since(t0);
+  }
+
   // Enqueues one check interval of L iterations on the stream (captured or not).
   void enqueue_interval(int L) {
     if (k == 1) {
       enqueue_interval_single(L);
       return;
     }
-    const double rho = opt.reflection;
     const int64_t nk = static_cast<int64_t>(n) * k, mk = static_cast<int64_t>(m) * k;
-    const unsigned gp = blocks(nk), gd = blocks(mk);
-    const CsrView A = viewA(), AT = viewAT();
     for (int l = 0; l < L; ++l) {
       const bool last = l == L - 1;
       const IterClock ck{d_it_base, d_restart_at, l};
       if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 0], stream));
-      if (nk) {
-        if (last)
-          launch(k_primal<false>, gp, stream, true, n, k, AT, v[Y], v[C], v[LO], v[UP], v[X], v[XP], v[X0], d_tau, ck,
-                 rho);
-        else
-          launch(k_primal<true>, gp, stream, true, n, k, AT, v[Y], v[C], v[LO], v[UP], v[X], v[XP], v[X0], d_tau, ck,
-                 rho);
-      }
+      if (nk) enqueue_batch_primal(!last, batch_stream_p, ck, batch_cpt_p);
       if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 1], stream));
       if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 2], stream));
-      if (mk) {
-        if (last)
-          launch(k_dual<false>, gd, stream, true, m, k, A, v[XP], v[RL], v[RU], v[Y], v[YP], v[Y0], v[AX], v[AXP],
-                 v[AX0], d_sigma, ck, rho);
-        else
-          launch(k_dual<true>, gd, stream, true, m, k, A, v[XP], v[RL], v[RU], v[Y], v[YP], v[Y0], v[AX], v[AXP],
-                 v[AX0], d_sigma, ck, rho);
-      }
+      if (mk) enqueue_batch_dual(!last, batch_stream_d, ck, batch_cpt_d);
       if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 3], stream));
       B2P_CUDA(cudaGetLastError());
     }

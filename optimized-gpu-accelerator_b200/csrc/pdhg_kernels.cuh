@@ -103,60 +103,141 @@ __device__ __forceinline__ void split(int64_t t, int k, int64_t& row, int& b) {
 
 // ---- per-iteration kernels ------------------------------------------------
 
-template <bool HALPERN>
-static __global__ void __launch_bounds__(kBlock) k_primal(int32_t n, int32_t k, CsrView AT, const double* __restrict__ y,
-                                                   const double* __restrict__ c, const double* __restrict__ lo,
-                                                   const double* __restrict__ up, double* __restrict__ x,
-                                                   double* __restrict__ xp, const double* __restrict__ x0,
-                                                   const double* __restrict__ tau, IterClock ck, double rho) {
+// Loads and stores of vectors that one kernel touches once per element: with
+// STREAM they are evict-first (ld.global.cs / st.global.cs), so that L2 keeps
+// the vector the other kernel gathers (y for k_primal, x+ for k_dual).
+template <bool STREAM>
+__device__ __forceinline__ double ld_vec(const double* p) {
+  return STREAM ? __ldcs(p) : *p;
+}
+template <bool STREAM>
+__device__ __forceinline__ void st_vec(double* p, double v) {
+  if (STREAM)
+    __stcs(p, v);
+  else
+    *p = v;
+}
+
+// Left-to-right row sums of CPT cases of one row at once (cases b[q], valid
+// when b[q] < k): the row's index and value are loaded once per entry and the
+// CPT gathers are independent, so a thread keeps CPT loads in flight.
+template <int CPT>
+__device__ __forceinline__ void row_dot_cases(const CsrView& M, const double* __restrict__ x, int64_t row, int k,
+                                              const int (&b)[CPT], double (&s)[CPT]) {
+  int p = __ldg(M.ptr + row);
+  const int e = __ldg(M.ptr + row + 1);
+#pragma unroll
+  for (int q = 0; q < CPT; ++q) s[q] = 0.0;
+#pragma unroll 4
+  for (; p < e; ++p) {
+    const int64_t base = static_cast<int64_t>(__ldg(M.idx + p)) * k;
+    const double a = __ldg(M.val + p);
+#pragma unroll
+    for (int q = 0; q < CPT; ++q)
+      if (b[q] < k) s[q] = __dadd_rn(s[q], __dmul_rn(a, __ldg(x + base + b[q])));
+  }
+}
+
+// Batch kernels (k > 1 cases sharing A, k-interleaved vectors): thread t takes
+// row t / kh and the cases t % kh + q kh, q < CPT (kh = ceil(k / CPT)).
+// k_primal : aty = A^T y (row j of A^T), x+ = proj(x - tau (c - aty)),
+//            Halpern step of x                    (spmvT + primalStep + halpern x)
+// k_dual   : ax+ = A x+ (row i of A), y+ = v + sigma proj(-v/sigma),
+//            Halpern steps of y and Ax            (spmv + dualStep + halpern y, Ax)
+// The vectors a kernel reads but the kernel it may overlap (programmatic
+// dependent launch) does not write are loaded before griddepcontrol.wait, so
+// their latency overlaps the previous kernel's tail and this kernel's
+// gathers.  (k_restart and k_halpern_all, which write x, x0, y, y0, Ax and
+// A x0, do not trigger early: a kernel that follows them starts only when
+// they have completed.)
+template <bool HALPERN, bool STREAM = false, int CPT = 1>
+static __global__ void __launch_bounds__(kBlock, 8 / CPT)
+    k_primal(int32_t n, int32_t k, CsrView AT, const double* __restrict__ y, const double* __restrict__ c,
+             const double* __restrict__ lo, const double* __restrict__ up, double* __restrict__ x,
+             double* __restrict__ xp, const double* __restrict__ x0, const double* __restrict__ tau, IterClock ck,
+             double rho) {
+  const int kh = (k + CPT - 1) / CPT;
   const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= static_cast<int64_t>(n) * k) return;
-  int64_t j;
-  int b;
-  split(t, k, j, b);
+  if (t >= static_cast<int64_t>(n) * kh) return;
+  const int64_t j = t / kh;
+  int b[CPT];
+#pragma unroll
+  for (int q = 0; q < CPT; ++q) b[q] = static_cast<int>(t - j * kh) + q * kh;
+  double xv[CPT], cv[CPT], l[CPT], u[CPT], x0v[CPT];
+#pragma unroll
+  for (int q = 0; q < CPT; ++q)
+    if (b[q] < k) {
+      const int64_t e = j * k + b[q];
+      xv[q] = ld_vec<STREAM>(x + e);
+      cv[q] = ld_vec<STREAM>(c + e);
+      l[q] = ld_vec<STREAM>(lo + e);
+      u[q] = ld_vec<STREAM>(up + e);
+      x0v[q] = HALPERN ? ld_vec<STREAM>(x0 + e) : 0.0;
+    }
   pdl_wait();
-  const double aty = row_dot(AT, y, j, k, b);
-  const double xv = x[t];
-  // x+ = proj_[lo,up](x - tau (c - A^T y))          (src/pdhg/pdhg.cpp:116-125)
-  double v = __dsub_rn(xv, __dmul_rn(tau[b], __dsub_rn(c[t], aty)));
-  const double l = lo[t], u = up[t];
-  v = (v < l) ? l : v;
-  v = (u < v) ? u : v;
-  xp[t] = v;
-  if (HALPERN) x[t] = halpern_step(xv, v, x0[t], halpern_lambda(ck, b), rho);
+  double aty[CPT];
+  row_dot_cases<CPT>(AT, y, j, k, b, aty);
+#pragma unroll
+  for (int q = 0; q < CPT; ++q)
+    if (b[q] < k) {
+      const int64_t e = j * k + b[q];
+      // x+ = proj_[lo,up](x - tau (c - A^T y))          (src/pdhg/pdhg.cpp:116-125)
+      double v = __dsub_rn(xv[q], __dmul_rn(tau[b[q]], __dsub_rn(cv[q], aty[q])));
+      v = (v < l[q]) ? l[q] : v;
+      v = (u[q] < v) ? u[q] : v;
+      xp[e] = v;  // gathered by k_dual: kept in L2
+      if (HALPERN) st_vec<STREAM>(x + e, halpern_step(xv[q], v, x0v[q], halpern_lambda(ck, b[q]), rho));
+    }
   pdl_launch_dependents();
 }
 
-template <bool HALPERN>
-static __global__ void __launch_bounds__(kBlock) k_dual(int32_t m, int32_t k, CsrView A, const double* __restrict__ xp,
-                                                 const double* __restrict__ rl, const double* __restrict__ ru,
-                                                 double* __restrict__ y, double* __restrict__ yp,
-                                                 const double* __restrict__ y0, double* __restrict__ ax,
-                                                 double* __restrict__ axp, const double* __restrict__ ax0,
-                                                 const double* __restrict__ sigma, IterClock ck, double rho) {
+template <bool HALPERN, bool STREAM = false, int CPT = 1>
+static __global__ void __launch_bounds__(kBlock, 8 / CPT)
+    k_dual(int32_t m, int32_t k, CsrView A, const double* __restrict__ xp, const double* __restrict__ rl,
+           const double* __restrict__ ru, double* __restrict__ y, double* __restrict__ yp,
+           const double* __restrict__ y0, double* __restrict__ ax, double* __restrict__ axp,
+           const double* __restrict__ ax0, const double* __restrict__ sigma, IterClock ck, double rho) {
+  const int kh = (k + CPT - 1) / CPT;
   const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= static_cast<int64_t>(m) * k) return;
-  int64_t i;
-  int b;
-  split(t, k, i, b);
+  if (t >= static_cast<int64_t>(m) * kh) return;
+  const int64_t i = t / kh;
+  int b[CPT];
+#pragma unroll
+  for (int q = 0; q < CPT; ++q) b[q] = static_cast<int>(t - i * kh) + q * kh;
+  double axv[CPT], yv[CPT], l[CPT], u[CPT], y0v[CPT], ax0v[CPT];
+#pragma unroll
+  for (int q = 0; q < CPT; ++q)
+    if (b[q] < k) {
+      const int64_t e = i * k + b[q];
+      axv[q] = ld_vec<STREAM>(ax + e);
+      yv[q] = ld_vec<STREAM>(y + e);
+      l[q] = ld_vec<STREAM>(rl + e);
+      u[q] = ld_vec<STREAM>(ru + e);
+      y0v[q] = HALPERN ? ld_vec<STREAM>(y0 + e) : 0.0;
+      ax0v[q] = HALPERN ? ld_vec<STREAM>(ax0 + e) : 0.0;
+    }
   pdl_wait();
-  const double axpv = row_dot(A, xp, i, k, b);
-  const double axv = ax[t], yv = y[t];
-  // v = y - sigma (2 A x+ - A x);  y+ = v + sigma proj_[L,U](-v / sigma)   (src/pdhg/pdhg.cpp:126-137)
-  const double s = sigma[b];
-  const double v = __dsub_rn(yv, __dmul_rn(s, __dsub_rn(__dmul_rn(2.0, axpv), axv)));
-  double w = __ddiv_rn(-v, s);
-  const double l = rl[t], u = ru[t];
-  w = (w < l) ? l : w;
-  w = (u < w) ? u : w;
-  const double ypv = __dadd_rn(v, __dmul_rn(s, w));
-  axp[t] = axpv;
-  yp[t] = ypv;
-  if (HALPERN) {
-    const double lam = halpern_lambda(ck, b);
-    y[t] = halpern_step(yv, ypv, y0[t], lam, rho);
-    ax[t] = halpern_step(axv, axpv, ax0[t], lam, rho);
-  }
+  double axpv[CPT];
+  row_dot_cases<CPT>(A, xp, i, k, b, axpv);
+#pragma unroll
+  for (int q = 0; q < CPT; ++q)
+    if (b[q] < k) {
+      const int64_t e = i * k + b[q];
+      // v = y - sigma (2 A x+ - A x);  y+ = v + sigma proj_[L,U](-v / sigma)   (src/pdhg/pdhg.cpp:126-137)
+      const double s = sigma[b[q]];
+      const double v = __dsub_rn(yv[q], __dmul_rn(s, __dsub_rn(__dmul_rn(2.0, axpv[q]), axv[q])));
+      double w = __ddiv_rn(-v, s);
+      w = (w < l[q]) ? l[q] : w;
+      w = (u[q] < w) ? u[q] : w;
+      const double ypv = __dadd_rn(v, __dmul_rn(s, w));
+      st_vec<STREAM>(axp + e, axpv[q]);
+      st_vec<STREAM>(yp + e, ypv);
+      if (HALPERN) {
+        const double lam = halpern_lambda(ck, b[q]);
+        y[e] = halpern_step(yv[q], ypv, y0v[q], lam, rho);  // gathered by k_primal: kept in L2
+        st_vec<STREAM>(ax + e, halpern_step(axv[q], axpv[q], ax0v[q], lam, rho));
+      }
+    }
   pdl_launch_dependents();
 }
 

@@ -47,7 +47,8 @@ class B2pOptions(C.Structure):
                 ("cancel_flag", C.POINTER(C.c_int32)), ("precision", C.c_int32), ("use_graphs", C.c_int32),
                 ("lanes_per_row_a", C.c_int32), ("lanes_per_row_at", C.c_int32), ("short_row_rounds", C.c_int32),
                 ("kernel_mode", C.c_int32), ("spmv_schedule", C.c_int32), ("multi_form", C.c_int32),
-                ("cta_smem_limit", C.c_int32), ("cta_threads", C.c_int32), ("cta_kernel", C.c_int32)]
+                ("cta_smem_limit", C.c_int32), ("cta_threads", C.c_int32), ("cta_kernel", C.c_int32),
+                ("batch_variant", C.c_int32), ("pad_options", C.c_int32)]
 
 
 class B2pStats(C.Structure):
@@ -63,7 +64,8 @@ class B2pStats(C.Structure):
                 ("schedule_at", C.c_int32), ("autotune_seconds", C.c_double), ("streaming_a", C.c_int32),
                 ("streaming_at", C.c_int32), ("multi_form", C.c_int32), ("cta_threads", C.c_int32),
                 ("cta_smem_bytes", C.c_int64), ("cta_lps_smem", C.c_int32), ("cta_lps_vectors", C.c_int32),
-                ("cta_owned_per_thread", C.c_int32), ("pad2", C.c_int32)]
+                ("cta_owned_per_thread", C.c_int32), ("pad2", C.c_int32),
+                ("cases_per_thread_at", C.c_int32), ("cases_per_thread_a", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_ if not f.startswith("pad")}
