@@ -374,7 +374,8 @@ def run_sweep(args, rank, world):
             "reference_model_gbs": ref_model / (t_dev / iters) / 1e9,
             "tuned": {"streamed_vectors_primal": bool(st.streaming_at), "streamed_vectors_dual": bool(st.streaming_a),
                       "cases_per_thread_primal": int(st.cases_per_thread_at),
-                      "cases_per_thread_dual": int(st.cases_per_thread_a)},
+                      "cases_per_thread_dual": int(st.cases_per_thread_a),
+                      "warp_rows_primal": bool(st.warp_rows_at), "warp_rows_dual": bool(st.warp_rows_a)},
             "e2e": {"value": t_e2e, "unit": "s per batch call (host arrays)", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "single_case_ms_per_iteration": t_single * 1e3,

@@ -156,7 +156,9 @@ typedef struct b2p_options {
   /* FP64 batches (k > 1 cases sharing A): variant of the two per-iteration
    * kernels -- 0 = timed on the device when the batch's vectors far exceed L2
    * (plain otherwise); 1..4 force (cases per thread, evict-first streamed
-   * vectors) = (1, no), (2, no), (1, yes), (2, yes). */
+   * vectors) = (1, no), (2, no), (1, yes), (2, yes); 5..8 the same with whole
+   * warps per row (row entries loaded once per warp and shared by shuffle)
+   * where k / cases per thread is a multiple of 32. */
   int32_t batch_variant;
   int32_t pad_options;
 } b2p_options;
@@ -199,6 +201,7 @@ typedef struct b2p_stats {
   int32_t cta_owned_per_thread;               /* CTA form: rows and columns each thread owns (0 = general kernel) */
   int32_t pad2;
   int32_t cases_per_thread_at, cases_per_thread_a; /* FP64 batches: cases per thread of the A^T / A kernels */
+  int32_t warp_rows_at, warp_rows_a;          /* FP64 batches: whole warps per row, entries shared by shuffle */
 } b2p_stats;
 
 /* Replaces pramana::PdhgResult (src/pdhg/pdhg.h:58-65) minus the vectors,

@@ -157,6 +157,7 @@ struct Engine {
   bool mixed_batch = false;  // mixed form of a batch (k > 1): FP32 k-interleaved kernels
   bool batch_stream_p = false, batch_stream_d = false;  // evict-first streamed vectors (tuned per kernel)
   int batch_cpt_p = 1, batch_cpt_d = 1;  // cases per thread of the primal / dual batch kernels (tuned)
+  bool batch_wr_p = false, batch_wr_d = false;  // whole warps per row, entries passed by shuffle (tuned)
   bool profiling = false;
   std::vector<cudaEvent_t> prof_ev;  // 4 per iteration of the longest interval
   int64_t prof_launches[3] = {0, 0, 0};
@@ -738,14 +739,21 @@ struct Engine {
   }
 
   // FP64 batch kernels (k > 1) of one iteration.
-  void enqueue_batch_primal(bool halpern, bool streamed, const IterClock& ck, int cpt) {
+  void enqueue_batch_primal(bool halpern, bool streamed, const IterClock& ck, int cpt, bool wr) {
     const double rho = opt.reflection;
     const unsigned gp = blocks(static_cast<int64_t>(n) * ((k + cpt - 1) / cpt));
     const CsrView AT = viewAT();
-#define B2P_BP(H, ST, CP) \
-  launch(k_primal<H, ST, CP>, gp, stream, true, n, k, AT, v[Y], v[C], v[LO], v[UP], v[X], v[XP], v[X0], d_tau, ck, rho)
-#define B2P_BP2(H, ST) \
-  if (cpt == 2) B2P_BP(H, ST, 2); else B2P_BP(H, ST, 1);
+#define B2P_BP(H, ST, CP, WR)                                                                                   \
+  launch(k_primal<H, ST, CP, WR>, gp, stream, true, n, k, AT, v[Y], v[C], v[LO], v[UP], v[X], v[XP], v[X0], d_tau, \
+         ck, rho)
+#define B2P_BP2(H, ST)                \
+  if (cpt == 2) {                     \
+    if (wr) B2P_BP(H, ST, 2, true);   \
+    else B2P_BP(H, ST, 2, false);     \
+  } else {                            \
+    if (wr) B2P_BP(H, ST, 1, true);   \
+    else B2P_BP(H, ST, 1, false);     \
+  }
     if (halpern) {
       if (streamed) { B2P_BP2(true, true) } else { B2P_BP2(true, false) }
     } else {
@@ -754,15 +762,21 @@ struct Engine {
 #undef B2P_BP2
 #undef B2P_BP
   }
-  void enqueue_batch_dual(bool halpern, bool streamed, const IterClock& ck, int cpt) {
+  void enqueue_batch_dual(bool halpern, bool streamed, const IterClock& ck, int cpt, bool wr) {
     const double rho = opt.reflection;
     const unsigned gd = blocks(static_cast<int64_t>(m) * ((k + cpt - 1) / cpt));
     const CsrView A = viewA();
-#define B2P_BD(H, ST, CP)                                                                                           \
-  launch(k_dual<H, ST, CP>, gd, stream, true, m, k, A, v[XP], v[RL], v[RU], v[Y], v[YP], v[Y0], v[AX], v[AXP], \
+#define B2P_BD(H, ST, CP, WR)                                                                                        \
+  launch(k_dual<H, ST, CP, WR>, gd, stream, true, m, k, A, v[XP], v[RL], v[RU], v[Y], v[YP], v[Y0], v[AX], v[AXP], \
          v[AX0], d_sigma, ck, rho)
-#define B2P_BD2(H, ST) \
-  if (cpt == 2) B2P_BD(H, ST, 2); else B2P_BD(H, ST, 1);
+#define B2P_BD2(H, ST)                \
+  if (cpt == 2) {                     \
+    if (wr) B2P_BD(H, ST, 2, true);   \
+    else B2P_BD(H, ST, 2, false);     \
+  } else {                            \
+    if (wr) B2P_BD(H, ST, 1, true);   \
+    else B2P_BD(H, ST, 1, false);     \
+  }
     if (halpern) {
       if (streamed) { B2P_BD2(true, true) } else { B2P_BD2(true, false) }
     } else {
@@ -774,15 +788,18 @@ struct Engine {
 
   // FP64 batch kernel variants: forced by the options, or, for batches whose
   // vectors far exceed L2 (k (m + n) >= 2^22 elements), each kernel is timed
-  // with one and with two cases per thread, with cached and with evict-first
-  // streamed vectors (one warm-up, three timed launches each, from the
-  // starting state), and the fastest is kept per kernel.
+  // with one and with two cases per thread, with and (when k / cases per
+  // thread is a multiple of 32) without per-lane index loads, with cached and
+  // with evict-first streamed vectors (one warm-up, three timed launches
+  // each, from the starting state), and the fastest is kept per kernel.
   void tune_batch() {
-    if (opt.batch_variant < 0 || opt.batch_variant > 4) throw Error(B2P_ERR_INVALID, "batch_variant must be 0..4");
+    if (opt.batch_variant < 0 || opt.batch_variant > 8) throw Error(B2P_ERR_INVALID, "batch_variant must be 0..8");
     if (k <= 1 || mixed_batch) return;
     if (opt.batch_variant > 0) {
-      batch_cpt_p = batch_cpt_d = (opt.batch_variant == 2 || opt.batch_variant == 4) ? 2 : 1;
-      batch_stream_p = batch_stream_d = opt.batch_variant >= 3;
+      const int v0 = (opt.batch_variant - 1) % 4 + 1;
+      batch_cpt_p = batch_cpt_d = (v0 == 2 || v0 == 4) ? 2 : 1;
+      batch_stream_p = batch_stream_d = v0 >= 3;
+      batch_wr_p = batch_wr_d = opt.batch_variant > 4 && warp_rows(batch_cpt_p);
     } else if (static_cast<int64_t>(n + m) * k >= (int64_t(1) << 22)) {
       time_batch_variants();
     }
@@ -790,7 +807,12 @@ struct Engine {
     stats.streaming_a = batch_stream_d;
     stats.cases_per_thread_at = batch_cpt_p;
     stats.cases_per_thread_a = batch_cpt_d;
+    stats.warp_rows_at = batch_wr_p;
+    stats.warp_rows_a = batch_wr_d;
   }
+
+  // Whole warps per row: k / cpt (rounded up) a multiple of 32.
+  bool warp_rows(int cpt) const { return ((k + cpt - 1) / cpt) % 32 == 0; }
 
   void time_batch_variants() {
     const auto t0 = Clock::now();
@@ -812,14 +834,17 @@ struct Engine {
     };
     double best_p = INFINITY, best_d = INFINITY;
     for (const int cpt : {1, 2})
-      for (int st = 0; st < 2; ++st) {
-        if (n) {
-          const double t = timed([&] { enqueue_batch_primal(true, st != 0, ck, cpt); });
-          if (t < best_p) best_p = t, batch_stream_p = st != 0, batch_cpt_p = cpt;
-        }
-        if (m) {
-          const double t = timed([&] { enqueue_batch_dual(true, st != 0, ck, cpt); });
-          if (t < best_d) best_d = t, batch_stream_d = st != 0, batch_cpt_d = cpt;
+      for (int wr = 0; wr < 2; ++wr) {
+        if (wr && !warp_rows(cpt)) continue;
+        for (int st = 0; st < 2; ++st) {
+          if (n) {
+            const double t = timed([&] { enqueue_batch_primal(true, st != 0, ck, cpt, wr != 0); });
+            if (t < best_p) best_p = t, batch_stream_p = st != 0, batch_cpt_p = cpt, batch_wr_p = wr != 0;
+          }
+          if (m) {
+            const double t = timed([&] { enqueue_batch_dual(true, st != 0, ck, cpt, wr != 0); });
+            if (t < best_d) best_d = t, batch_stream_d = st != 0, batch_cpt_d = cpt, batch_wr_d = wr != 0;
+          }
         }
       }
     cudaEventDestroy(e0);
@@ -838,10 +863,10 @@ struct Engine {
       const bool last = l == L - 1;
       const IterClock ck{d_it_base, d_restart_at, l};
       if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 0], stream));
-      if (nk) enqueue_batch_primal(!last, batch_stream_p, ck, batch_cpt_p);
+      if (nk) enqueue_batch_primal(!last, batch_stream_p, ck, batch_cpt_p, batch_wr_p);
       if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 1], stream));
       if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 2], stream));
-      if (mk) enqueue_batch_dual(!last, batch_stream_d, ck, batch_cpt_d);
+      if (mk) enqueue_batch_dual(!last, batch_stream_d, ck, batch_cpt_d, batch_wr_d);
       if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 3], stream));
       B2P_CUDA(cudaGetLastError());
     }

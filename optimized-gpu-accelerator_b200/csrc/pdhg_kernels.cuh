@@ -120,26 +120,51 @@ __device__ __forceinline__ void st_vec(double* p, double v) {
 
 // Left-to-right row sums of CPT cases of one row at once (cases b[q], valid
 // when b[q] < k): the row's index and value are loaded once per entry and the
-// CPT gathers are independent, so a thread keeps CPT loads in flight.
-template <int CPT>
+// CPT gathers are independent, so a thread keeps CPT loads in flight.  With
+// WARPROW (every lane of the warp on the same row: k / CPT a multiple of 32)
+// the lanes load 32 of the row's entries at a time, coalesced, and pass each
+// entry's index and value by shuffle, so a gather waits on no index load.
+template <int CPT, bool WARPROW>
 __device__ __forceinline__ void row_dot_cases(const CsrView& M, const double* __restrict__ x, int64_t row, int k,
                                               const int (&b)[CPT], double (&s)[CPT]) {
   int p = __ldg(M.ptr + row);
   const int e = __ldg(M.ptr + row + 1);
 #pragma unroll
   for (int q = 0; q < CPT; ++q) s[q] = 0.0;
+  if (WARPROW) {
+    const int lane = threadIdx.x & 31;
+    for (; p < e; p += 32) {
+      const int cnt = (e - p) < 32 ? (e - p) : 32;  // the same in every lane
+      int my_idx = 0;
+      double my_val = 0.0;
+      if (lane < cnt) {
+        my_idx = __ldg(M.idx + p + lane);
+        my_val = __ldg(M.val + p + lane);
+      }
 #pragma unroll 4
-  for (; p < e; ++p) {
-    const int64_t base = static_cast<int64_t>(__ldg(M.idx + p)) * k;
-    const double a = __ldg(M.val + p);
+      for (int r = 0; r < cnt; ++r) {
+        const int64_t base = static_cast<int64_t>(__shfl_sync(0xffffffffu, my_idx, r)) * k;
+        const double a = __shfl_sync(0xffffffffu, my_val, r);
 #pragma unroll
-    for (int q = 0; q < CPT; ++q)
-      if (b[q] < k) s[q] = __dadd_rn(s[q], __dmul_rn(a, __ldg(x + base + b[q])));
+        for (int q = 0; q < CPT; ++q)
+          if (b[q] < k) s[q] = __dadd_rn(s[q], __dmul_rn(a, __ldg(x + base + b[q])));
+      }
+    }
+  } else {
+#pragma unroll 4
+    for (; p < e; ++p) {
+      const int64_t base = static_cast<int64_t>(__ldg(M.idx + p)) * k;
+      const double a = __ldg(M.val + p);
+#pragma unroll
+      for (int q = 0; q < CPT; ++q)
+        if (b[q] < k) s[q] = __dadd_rn(s[q], __dmul_rn(a, __ldg(x + base + b[q])));
+    }
   }
 }
 
 // Batch kernels (k > 1 cases sharing A, k-interleaved vectors): thread t takes
-// row t / kh and the cases t % kh + q kh, q < CPT (kh = ceil(k / CPT)).
+// row t / kh and the cases t % kh + q kh, q < CPT (kh = ceil(k / CPT));
+// WARPROW requires kh to be a multiple of 32 (whole warps per row).
 // k_primal : aty = A^T y (row j of A^T), x+ = proj(x - tau (c - aty)),
 //            Halpern step of x                    (spmvT + primalStep + halpern x)
 // k_dual   : ax+ = A x+ (row i of A), y+ = v + sigma proj(-v/sigma),
@@ -150,7 +175,7 @@ __device__ __forceinline__ void row_dot_cases(const CsrView& M, const double* __
 // gathers.  (k_restart and k_halpern_all, which write x, x0, y, y0, Ax and
 // A x0, do not trigger early: a kernel that follows them starts only when
 // they have completed.)
-template <bool HALPERN, bool STREAM = false, int CPT = 1>
+template <bool HALPERN, bool STREAM = false, int CPT = 1, bool WARPROW = false>
 static __global__ void __launch_bounds__(kBlock, 8 / CPT)
     k_primal(int32_t n, int32_t k, CsrView AT, const double* __restrict__ y, const double* __restrict__ c,
              const double* __restrict__ lo, const double* __restrict__ up, double* __restrict__ x,
@@ -176,7 +201,7 @@ static __global__ void __launch_bounds__(kBlock, 8 / CPT)
     }
   pdl_wait();
   double aty[CPT];
-  row_dot_cases<CPT>(AT, y, j, k, b, aty);
+  row_dot_cases<CPT, WARPROW>(AT, y, j, k, b, aty);
 #pragma unroll
   for (int q = 0; q < CPT; ++q)
     if (b[q] < k) {
@@ -191,7 +216,7 @@ static __global__ void __launch_bounds__(kBlock, 8 / CPT)
   pdl_launch_dependents();
 }
 
-template <bool HALPERN, bool STREAM = false, int CPT = 1>
+template <bool HALPERN, bool STREAM = false, int CPT = 1, bool WARPROW = false>
 static __global__ void __launch_bounds__(kBlock, 8 / CPT)
     k_dual(int32_t m, int32_t k, CsrView A, const double* __restrict__ xp, const double* __restrict__ rl,
            const double* __restrict__ ru, double* __restrict__ y, double* __restrict__ yp,
@@ -218,7 +243,7 @@ static __global__ void __launch_bounds__(kBlock, 8 / CPT)
     }
   pdl_wait();
   double axpv[CPT];
-  row_dot_cases<CPT>(A, xp, i, k, b, axpv);
+  row_dot_cases<CPT, WARPROW>(A, xp, i, k, b, axpv);
 #pragma unroll
   for (int q = 0; q < CPT; ++q)
     if (b[q] < k) {

@@ -65,7 +65,8 @@ class B2pStats(C.Structure):
                 ("streaming_at", C.c_int32), ("multi_form", C.c_int32), ("cta_threads", C.c_int32),
                 ("cta_smem_bytes", C.c_int64), ("cta_lps_smem", C.c_int32), ("cta_lps_vectors", C.c_int32),
                 ("cta_owned_per_thread", C.c_int32), ("pad2", C.c_int32),
-                ("cases_per_thread_at", C.c_int32), ("cases_per_thread_a", C.c_int32)]
+                ("cases_per_thread_at", C.c_int32), ("cases_per_thread_a", C.c_int32),
+                ("warp_rows_at", C.c_int32), ("warp_rows_a", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_ if not f.startswith("pad")}

@@ -1,6 +1,6 @@
 """Variants of the FP64 batch kernels (k cases sharing A, k-interleaved
 vectors): one or two cases per thread, cached or evict-first streamed
-vectors.  Every variant does each case's arithmetic in the same order, so all
+vectors, row entries loaded per lane or once per warp and shared by shuffle.  Every variant does each case's arithmetic in the same order, so all
 of them follow the oracle's batch run exactly and agree with one another bit
 for bit; the tuner's choice on a batch larger than L2 is one of them."""
 import numpy as np
@@ -28,15 +28,29 @@ def test_batch_variant_vs_oracle(oracle_mod, variant, which):
         assert_close(g, o)
 
 
+@pytest.mark.parametrize("variant", [5, 6, 7, 8])
+@pytest.mark.parametrize("iters", [1, 64, 500])
+def test_warp_row_variant_vs_oracle(oracle_mod, variant, iters):
+    """k = 64: k / cases per thread is a multiple of 32, so whole warps share
+    a row and its entries come by shuffle."""
+    lp = G.random_lp(150, 300, 4.0, 90, 13)
+    cases = lp_cases.mixed_cases(lp, 64)
+    stats = pdhg.PdhgStats()
+    gs = pdhg.solvePdhgBatch(lp, cases, opts(tolerance=1e-30, maxIterations=iters, batchVariant=variant))
+    os_ = oracle_mod.solve(lp, "oracle", cases=cases, tolerance=1e-30, max_iterations=iters)
+    for g, o in zip(gs, os_):
+        assert_close(g, o)
+
+
 def test_batch_variants_agree_bitwise_and_tuner_runs():
     """A batch whose vectors exceed L2 (k (m + n) >= 2^22): the tuned run and
     every forced variant give identical iterates at a fixed iteration count."""
     lp = G.random_lp(20000, 40000, 4.0, 12000, 21)
-    k = 71
+    k = 128
     rng = np.random.default_rng(4)
     cases = [lp_cases.LpCase(cost=lp.col_cost * (1.0 + 0.05 * rng.standard_normal(lp.num_cols))) for _ in range(k)]
     runs = {}
-    for variant in [0, 1, 2, 3, 4]:
+    for variant in [0, 1, 2, 3, 4, 5, 6, 7, 8]:
         stats = pdhg.PdhgStats()
         rs = pdhg.solvePdhgBatch(lp, cases, opts(tolerance=1e-30, maxIterations=300, batchVariant=variant),
                                  batchStats=stats)
