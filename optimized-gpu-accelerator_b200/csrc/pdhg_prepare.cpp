@@ -1,5 +1,8 @@
 #include "pdhg_prepare.h"
 
+#include <omp.h>
+
+#include <algorithm>
 #include <cmath>
 
 namespace b2p {
@@ -23,21 +26,72 @@ struct RowMap {
   std::vector<int32_t> ptr, col, pos;
 };
 
-RowMap row_map(int32_t m, int32_t n, const int32_t* start, const int32_t* index) {
+RowMap row_map(int32_t m, int32_t n, const int32_t* start, const int32_t* index, bool par) {
   RowMap r;
   const int32_t nnz = start[n];
   r.ptr.assign(static_cast<size_t>(m) + 1, 0);
   r.col.resize(nnz);
   r.pos.resize(nnz);
-  for (int32_t q = 0; q < nnz; ++q) r.ptr[index[q] + 1]++;
+  int T = par ? omp_get_max_threads() : 1;
+  // per-thread row counters: T x m integers, capped at 2^26
+  if (T > 1 && static_cast<int64_t>(T) * m > (int64_t(1) << 26))
+    T = static_cast<int>(std::max<int64_t>(1, (int64_t(1) << 26) / std::max<int32_t>(m, 1)));
+  if (T <= 1 || m == 0) {
+    for (int32_t q = 0; q < nnz; ++q) r.ptr[index[q] + 1]++;
+    for (int32_t i = 0; i < m; ++i) r.ptr[i + 1] += r.ptr[i];
+    std::vector<int32_t> next(r.ptr.begin(), r.ptr.end() - 1);
+    for (int32_t j = 0; j < n; ++j)
+      for (int32_t q = start[j]; q < start[j + 1]; ++q) {
+        const int32_t e = next[index[q]]++;
+        r.col[e] = j;
+        r.pos[e] = q;
+      }
+    return r;
+  }
+  // Parallel stable counting sort: thread t takes a run of whole columns
+  // (balanced by entries); its entries of row i go after those of threads
+  // < t, in column order, so the result equals the sequential one.
+  std::vector<int32_t> cbeg(static_cast<size_t>(T) + 1);
+  for (int t = 0; t <= T; ++t) {
+    const int64_t target = static_cast<int64_t>(nnz) * t / T;
+    cbeg[t] = static_cast<int32_t>(std::lower_bound(start, start + n, target) - start);
+  }
+  cbeg[T] = n;
+  std::vector<int32_t> cnt(static_cast<size_t>(T) * m, 0);
+#pragma omp parallel num_threads(T)
+  {
+    const int t = omp_get_thread_num();
+    int32_t* c = cnt.data() + static_cast<size_t>(t) * m;
+    for (int32_t q = start[cbeg[t]]; q < start[cbeg[t + 1]]; ++q) c[index[q]]++;
+  }
+#pragma omp parallel for schedule(static) num_threads(T)
+  for (int32_t i = 0; i < m; ++i) {
+    int32_t tot = 0;
+    for (int t = 0; t < T; ++t) tot += cnt[static_cast<size_t>(t) * m + i];
+    r.ptr[i + 1] = tot;
+  }
   for (int32_t i = 0; i < m; ++i) r.ptr[i + 1] += r.ptr[i];
-  std::vector<int32_t> next(r.ptr.begin(), r.ptr.end() - 1);
-  for (int32_t j = 0; j < n; ++j)
-    for (int32_t q = start[j]; q < start[j + 1]; ++q) {
-      const int32_t e = next[index[q]]++;
-      r.col[e] = j;
-      r.pos[e] = q;
+#pragma omp parallel for schedule(static) num_threads(T)
+  for (int32_t i = 0; i < m; ++i) {
+    int32_t off = r.ptr[i];
+    for (int t = 0; t < T; ++t) {
+      int32_t& c = cnt[static_cast<size_t>(t) * m + i];
+      const int32_t k = c;
+      c = off;
+      off += k;
     }
+  }
+#pragma omp parallel num_threads(T)
+  {
+    const int t = omp_get_thread_num();
+    int32_t* cur = cnt.data() + static_cast<size_t>(t) * m;
+    for (int32_t j = cbeg[t]; j < cbeg[t + 1]; ++j)
+      for (int32_t q = start[j]; q < start[j + 1]; ++q) {
+        const int32_t e = cur[index[q]]++;
+        r.col[e] = j;
+        r.pos[e] = q;
+      }
+  }
   return r;
 }
 
@@ -58,6 +112,11 @@ void ruiz_impl(int32_t m, int32_t n, const int32_t* start, const int32_t* index,
   rs.assign(m, 1.0);
   cs.assign(n, 1.0);
   std::vector<double> rmax(m), cmax(n);
+  // |A| in row order, once: the row passes then read it sequentially
+  const int32_t nnz = start[n];
+  std::vector<double> rabs(nnz);
+#pragma omp parallel for schedule(static) if (par)
+  for (int32_t e = 0; e < nnz; ++e) rabs[e] = std::fabs(value[R.pos[e]]);
   // Infinity-norm equilibration passes.
   for (int it = 0; it < iterations; ++it) {
 #pragma omp parallel for schedule(static) if (par)
@@ -69,8 +128,7 @@ void ruiz_impl(int32_t m, int32_t n, const int32_t* start, const int32_t* index,
 #pragma omp parallel for schedule(static) if (par)
     for (int32_t i = 0; i < m; ++i) {
       double r = 0;
-      for (int32_t e = R.ptr[i]; e < R.ptr[i + 1]; ++e)
-        r = smax(r, std::fabs(value[R.pos[e]]) * cs[R.col[e]] * rs[i]);
+      for (int32_t e = R.ptr[i]; e < R.ptr[i + 1]; ++e) r = smax(r, rabs[e] * cs[R.col[e]] * rs[i]);
       rmax[i] = r;
     }
 #pragma omp parallel for schedule(static) if (par)
@@ -92,7 +150,7 @@ void ruiz_impl(int32_t m, int32_t n, const int32_t* start, const int32_t* index,
 #pragma omp parallel for schedule(static) if (par)
     for (int32_t i = 0; i < m; ++i) {
       double r = 0.0;
-      for (int32_t e = R.ptr[i]; e < R.ptr[i + 1]; ++e) r += std::fabs(value[R.pos[e]]) * cs[R.col[e]] * rs[i];
+      for (int32_t e = R.ptr[i]; e < R.ptr[i + 1]; ++e) r += rabs[e] * cs[R.col[e]] * rs[i];
       rsum[i] = r;
     }
 #pragma omp parallel for schedule(static) if (par)
@@ -111,8 +169,8 @@ void ruiz_impl(int32_t m, int32_t n, const int32_t* start, const int32_t* index,
 void ruiz_scaling(int32_t m, int32_t n, const int32_t* start, const int32_t* index, const double* value,
                   int iterations, bool pock_chambolle, std::vector<double>& rs, std::vector<double>& cs,
                   bool parallel) {
-  ruiz_impl(m, n, start, index, value, iterations, pock_chambolle, rs, cs, row_map(m, n, start, index),
-            parallel && start[n] >= kParallelNnz);
+  const bool par = parallel && start[n] >= kParallelNnz;
+  ruiz_impl(m, n, start, index, value, iterations, pock_chambolle, rs, cs, row_map(m, n, start, index, par), par);
 }
 
 // ||A||_2 estimate: 40 steps of x <- A^T A x / ||A^T A x|| and sqrt of the
@@ -154,7 +212,7 @@ Prepared prepare(int32_t m, int32_t n, const int32_t* start, const int32_t* inde
   P.offset = offset;
   const int32_t nnz = start[n];
   const bool par = opt.parallel && nnz >= kParallelNnz;
-  const RowMap rm = row_map(m, n, start, index);
+  RowMap rm = row_map(m, n, start, index, par);
   if (opt.ruiz_iterations > 0 && nnz > 0) {
     ruiz_impl(m, n, start, index, value, opt.ruiz_iterations, opt.pock_chambolle, P.R, P.Cs, rm, par);
   } else {
@@ -188,23 +246,27 @@ Prepared prepare(int32_t m, int32_t n, const int32_t* start, const int32_t* inde
   {
     P.A.rows = m;
     P.A.cols = n;
-    P.A.ptr = rm.ptr;
-    P.A.idx = rm.col;
     P.A.val.resize(nnz);
 #pragma omp parallel for schedule(static) if (par)
     for (int32_t e = 0; e < nnz; ++e) P.A.val[e] = sval[rm.pos[e]];
+    P.A.ptr = std::move(rm.ptr);
+    P.A.idx = std::move(rm.col);
   }
   // CSR of A^T is the (scaled) CSC of A.
   P.AT.rows = n;
   P.AT.cols = m;
-  P.AT.ptr.assign(start, start + n + 1);
-  P.AT.idx.assign(index, index + nnz);
-  P.AT.val = sval;
+  P.AT.ptr.resize(static_cast<size_t>(n) + 1);
+  P.AT.idx.resize(nnz);
+#pragma omp parallel for schedule(static) if (par)
+  for (int32_t j = 0; j <= n; ++j) P.AT.ptr[j] = start[j];
+#pragma omp parallel for schedule(static) if (par)
+  for (int32_t q = 0; q < nnz; ++q) P.AT.idx[q] = index[q];
+  P.AT.val = std::move(sval);
   P.rfac.resize(m);
   P.cfac.resize(n);
   for (int32_t i = 0; i < m; ++i) P.rfac[i] = P.beta / P.R[i];
   for (int32_t j = 0; j < n; ++j) P.cfac[j] = P.gamma / P.Cs[j];
-  if (opt.norm_on_host) P.normA = power_iteration(m, n, start, index, sval.data(), 40) * 1.01;
+  if (opt.norm_on_host) P.normA = power_iteration(m, n, start, index, P.AT.val.data(), 40) * 1.01;
   return P;
 }
 
