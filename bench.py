@@ -280,6 +280,95 @@ def run_family(args, rank, world):
     return 0
 
 
+ROUTER_METRIC = "held-out geo-mean regret of the B200-calibrated engine router (time of chosen engine / fastest)"
+
+
+def router_instances():
+    """Seeded LPs from four generator families (the calibration set)."""
+    from pramana_b200 import generators as G
+    out = []
+    for i, m in enumerate([100, 200, 400, 800, 1500, 3000, 6000]):
+        for d in (3.0, 6.0):
+            out.append(("random", f"random_m{m}_d{d:g}", G.random_lp(m, 2 * m, d, int(0.6 * m), 500 + 10 * i + int(d))))
+    for i, m in enumerate([500, 1000, 2000, 4000, 8000]):
+        out.append(("skewed", f"skewed_m{m}", G.random_lp(m, 2 * m, 6.4, int(0.6 * m), 700 + i, heavy_row_frac=0.01,
+                                                          heavy_nnz_frac=0.1)))
+    for i, (T, R_, U, S, Q, e) in enumerate([(1, 1, 2, 3, 2, 0.0), (2, 1, 4, 4, 2, 0.0), (3, 1, 4, 4, 2, 0.0),
+                                             (2, 2, 4, 6, 3, 0.0), (4, 2, 6, 6, 3, 0.0), (1, 1, 2, 3, 2, 1.0),
+                                             (2, 1, 4, 4, 2, 1.0), (3, 2, 4, 6, 3, 1.0)]):
+        out.append(("refinery", f"refinery_{T}x{R_}x{U}x{S}x{Q}_e{e:g}",
+                    G.refinery_lp(periods=T, regions=R_, units=U, streams=S, properties=Q, pools=10, seed=900 + i,
+                                  scale_exponent=e)))
+    for i, lp in enumerate(G.uneven_family(6, 1e4, 6e4, seed=11)):
+        out.append(("uneven", f"uneven_{i}_nnz{lp.nnz}", lp))
+    return out
+
+
+def run_router(args, rank, world):
+    """--workload router: every LP of the calibration set solved by the four
+    engines the router chooses between -- this library's GPU PDHG through the
+    public call ("pdhg-gpu") and the reference's CPU engines on this host's
+    cores (dual simplex, interior point with crossover, CPU PDHG; oracle/_ref)
+    -- with a time limit; the router's log-linear model is fitted on these
+    timings, validated on held-out LPs, and written in Router::load's format."""
+    import torch
+
+    from oracle import oracle as O
+    from pramana_b200 import pdhg
+    from pramana_b200 import router as R
+
+    if world > 1 and rank != 0:
+        return 0
+    torch.cuda.set_device(0)
+    if not O.available("ref"):
+        print(json.dumps({"workload": "router", "unavailable": "oracle/_ref/libpramana_ref.so was not built"}))
+        return 0
+    threads = os.cpu_count() or 1
+    O.set_ref_threads(threads)
+    limit = args.router_limit
+    tol = 1e-6
+    insts = router_instances()
+    pdhg.solvePdhg(insts[0][2], pdhg.PdhgOptions(tolerance=tol))  # module load, pools
+    records, rows = [], []
+    for fam, name, lp in insts:
+        times, stats = {}, {}
+        # the reference's CPU PDHG wrapper sets PRAMANA_DISABLE_GPU (C setenv) to
+        # keep the reference off the GPU; this engine honours the variable too
+        os.unsetenv("PRAMANA_DISABLE_GPU")
+        t0 = time.perf_counter()
+        r = pdhg.solvePdhg(lp, pdhg.PdhgOptions(tolerance=tol, timeLimit=limit))
+        t = time.perf_counter() - t0
+        times["pdhg-gpu"], stats["pdhg-gpu"] = (t if r.status == "Optimal" else None), r.status
+        t0 = time.perf_counter()
+        o = O.solve(lp, "ref", tolerance=tol, time_limit=limit)
+        t = time.perf_counter() - t0
+        times["pdhg-cpu"], stats["pdhg-cpu"] = (t if o.status == 1 else None), int(o.status)
+        for e in ("dual", "ipm"):
+            s = O.timed_solve(lp, e, limit)
+            times[e], stats[e] = (s["seconds"] if s["status"] == "Optimal" else None), s["status"]
+        rec = R.Record(name=name, family=fam, features=R.features(lp), times=times, limit=limit, statuses=stats)
+        records.append(rec)
+        rows.append({"instance": name, "family": fam, **{f"t_{e}": times[e] for e in R.ENGINES},
+                     **{f"status_{e}": stats[e] for e in R.ENGINES}, **rec.features})
+    val = R.validate(records, tolerance=tol)
+    W = R.fit(records)
+    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
+    R.write_model(os.path.join(ROOT, "gpurun_out", "router_model_b200.json"), W, len(records),
+                  note=f"fitted on {len(records)} seeded LPs timed on one B200 and {threads} host threads; "
+                       f"time limit {limit:g} s, rel KKT {tol:g} for the PDHG engines")
+    with open(os.path.join(ROOT, "gpurun_out", "router_runs.json"), "w") as fh:
+        json.dump(rows, fh, indent=1)
+    line = {"metric": ROUTER_METRIC, "value": val["router_held_out"]["geo_mean_regret"], "unit": "x",
+            "n_gpus": 1, "steps": 1, "warmup": 1, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded)", "workload": "router",
+            "config": {"workload": f"{len(records)} LPs from 4 generator families (random, skewed, refinery, "
+                                   f"uneven config-2), 4 engines each, time limit {limit:g} s, 5-fold held-out",
+                       "host_threads": threads},
+            "validation": val, "weights": W}
+    print(json.dumps(line))
+    return 0
+
+
 SWEEP_METRIC = "HBM GB/s of the batched PDHG kernels: 256-case crude-price sweep of the full refinery LP (shared A)"
 
 
@@ -522,7 +611,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-sample-iters", type=int, default=CPU_SAMPLE_ITERS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["lp", "family", "multi", "sweep"], default="lp")
+    ap.add_argument("--workload", choices=["lp", "family", "multi", "sweep", "router"], default="lp")
+    ap.add_argument("--router-limit", type=float, default=3.0, help="router: time limit per engine and LP (s)")
     ap.add_argument("--cases", type=int, default=256, help="sweep: cases in the shared-A batch")
     ap.add_argument("--sweep-iters", type=int, default=640, help="sweep: PDHG iterations per step")
     ap.add_argument("--instances", type=int, default=256, help="multi: LPs in the batch")
@@ -554,6 +644,8 @@ def main():
         return run_multi(args, rank, world)
     if args.workload == "sweep":
         return run_sweep(args, rank, world)
+    if args.workload == "router":
+        return run_router(args, rank, world)
 
     import torch
     dist = None

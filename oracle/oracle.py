@@ -256,3 +256,54 @@ def csr_mult(ptr, idx, val, x, rows, k=1):
     out = np.zeros(rows * k)
     h.oracle_csr_mult(C.c_int(rows), C.c_int(k), _ip(ptr), _ip(idx), _dp(val), _dp(x), _dp(out))
     return out
+
+
+# ---- the reference's router and CPU engines (ref build), for the router calibration ----
+
+ROUTER_ENGINES = ["dual", "ipm", "pdhg-cpu", "pdhg-gpu"]
+
+
+def _lp_args(lp):
+    return (C.c_int(lp.num_rows), C.c_int(lp.num_cols), _ip(lp.start), _ip(lp.index), _dp(lp.value),
+            _dp(lp.col_cost), _dp(lp.col_lower), _dp(lp.col_upper), _dp(lp.row_lower), _dp(lp.row_upper))
+
+
+def router_features(lp) -> dict:
+    """computeFeatures (src/router/router.cpp:64-95) of the reference."""
+    h = _load("ref")
+    out = np.zeros(10)
+    if h.ref_router_features(*_lp_args(lp), _dp(out)) != 0:
+        raise RuntimeError("router_features failed")
+    keys = ["rows", "cols", "nnz", "avg_row_nnz", "max_row_nnz", "coefficient_range", "equality_row_fraction",
+            "free_column_fraction", "is_mip", "is_qp"]
+    return dict(zip(keys, out.tolist()))
+
+
+def router_decide(lp, model_path=None, gpu: bool = True, tolerance: float = 1e-6) -> dict:
+    """Router::decide (src/router/router.cpp:163-207) with the weights in
+    `model_path` (Router::load) or the built-in priors."""
+    h = _load("ref")
+    eng = C.c_int(-1)
+    loaded = C.c_int(0)
+    pred = np.zeros(4)
+    path = None if model_path is None else str(model_path).encode()
+    rc = h.ref_router_decide(*_lp_args(lp), C.c_char_p(path), C.c_int(int(gpu)), C.c_double(tolerance),
+                             C.byref(eng), _dp(pred), C.byref(loaded))
+    if rc != 0:
+        raise RuntimeError("router_decide failed")
+    return {"engine": ROUTER_ENGINES[eng.value] if eng.value >= 0 else None, "predicted": pred.tolist(),
+            "loaded": bool(loaded.value)}
+
+
+def timed_solve(lp, engine: str, time_limit: float) -> dict:
+    """A solve from scratch by the reference's dual simplex ("dual") or
+    interior-point method ("ipm") under a time limit."""
+    h = _load("ref")
+    out = np.zeros(4)
+    which = {"dual": 0, "ipm": 1}[engine]
+    rc = h.ref_timed_solve(C.c_int(which), *_lp_args(lp), C.c_double(lp.obj_offset), C.c_double(time_limit),
+                           _dp(out))
+    if rc != 0:
+        raise RuntimeError("timed_solve failed")
+    return {"status": STATUS_NAMES.get(int(out[0]), str(int(out[0]))), "objective": out[1], "seconds": out[2],
+            "iterations": int(out[3])}

@@ -13,6 +13,9 @@
 //     the dual simplex from scratch (src/lp/simplex.cpp), for the handoff
 //   - pramana::certify of an OPTIMAL LP claim (src/cert/certifier.cpp:208-380)
 //     and its constraint-implied column bounds (Propagator, src/mip/propagate.cpp)
+//   - the router's features and decision (src/router/router.cpp) and timed
+//     solves by the dual simplex and the interior-point method (src/ipm/ipm.cpp),
+//     the CPU engines a router calibration compares the GPU engine with
 // The GPU path of the reference is switched off (PRAMANA_DISABLE_GPU) so that
 // loading this library never brings up a CUDA context or NVRTC.
 #include <cstdint>
@@ -24,11 +27,13 @@
 
 #include "cert/certifier.h"
 #include "core/model.h"
+#include "ipm/ipm.h"
 #include "lp/crossover.h"
 #include "lp/scaling.h"
 #include "lp/simplex.h"
 #include "mip/propagate.h"
 #include "pdhg/pdhg.h"
+#include "router/router.h"
 #include "util/log.h"
 #include "util/parallel.h"
 #include "util/timer.h"
@@ -303,6 +308,84 @@ int ref_ruiz_scaling(int m, int n, const int* start, const int* index, const dou
     ScalingResult s = ruizScaling(A, iterations, pockChambolle != 0);
     std::memcpy(rowScale, s.rowScale.data(), sizeof(double) * m);
     std::memcpy(colScale, s.colScale.data(), sizeof(double) * n);
+    return 0;
+  } catch (std::exception& e) {
+    gErr = e.what();
+    return 1;
+  }
+}
+
+// computeFeatures (src/router/router.cpp:64-95): out = m, n, nnz, avg row nnz,
+// max row nnz, coefficient range, equality-row fraction, free-column
+// fraction, is_mip, is_qp.
+int ref_router_features(int m, int n, const int* start, const int* index, const double* value, const double* cost,
+                        const double* colLower, const double* colUpper, const double* rowLower,
+                        const double* rowUpper, double* out) {
+  try {
+    Model lp = buildModel(m, n, start, index, value, cost, colLower, colUpper, rowLower, rowUpper, 0.0);
+    const RouterFeatures f = computeFeatures(lp);
+    const double v[10] = {f.m, f.n, f.nnz, f.avgRowNnz, f.maxRowNnz, f.coeffRange, f.eqFraction, f.freeFraction,
+                          f.isMip ? 1.0 : 0.0, f.isQp ? 1.0 : 0.0};
+    std::memcpy(out, v, sizeof(v));
+    return 0;
+  } catch (std::exception& e) {
+    gErr = e.what();
+    return 1;
+  }
+}
+
+// Router::decide (src/router/router.cpp:163-207) with the weights of
+// `model_path` (Router::load) or, when it is NULL or does not load, the
+// built-in priors.  engine = index into dual, ipm, pdhg-cpu, pdhg-gpu;
+// pred = the four predicted seconds; loaded = whether the file loaded.
+int ref_router_decide(int m, int n, const int* start, const int* index, const double* value, const double* cost,
+                      const double* colLower, const double* colUpper, const double* rowLower,
+                      const double* rowUpper, const char* model_path, int gpu, double tolerance, int* engine,
+                      double* pred, int* loaded) {
+  try {
+    Log::setLevel(LogLevel::Error);
+    Model lp = buildModel(m, n, start, index, value, cost, colLower, colUpper, rowLower, rowUpper, 0.0);
+    Router r;
+    *loaded = model_path ? (r.load(model_path) ? 1 : 0) : 0;
+    const RouterDecision d = r.decide(lp, gpu != 0, tolerance);
+    const auto& names = Router::engines();
+    *engine = -1;
+    for (size_t e = 0; e < names.size(); ++e)
+      if (names[e] == d.engine) *engine = static_cast<int>(e);
+    pred[0] = d.predictedDual;
+    pred[1] = d.predictedIpm;
+    pred[2] = d.predictedPdhgCpu;
+    pred[3] = d.predictedPdhgGpu;
+    return 0;
+  } catch (std::exception& e) {
+    gErr = e.what();
+    return 1;
+  }
+}
+
+// A timed solve from scratch by the reference's dual simplex (engine 0) or
+// interior-point method with crossover (engine 1) under a time limit:
+// out = status, objective, seconds, iterations.
+int ref_timed_solve(int engine, int m, int n, const int* start, const int* index, const double* value,
+                    const double* cost, const double* colLower, const double* colUpper, const double* rowLower,
+                    const double* rowUpper, double offset, double time_limit, double* out) {
+  try {
+    Log::setLevel(LogLevel::Error);
+    Model lp = buildModel(m, n, start, index, value, cost, colLower, colUpper, rowLower, rowUpper, offset);
+    Deadline dl(time_limit);
+    Timer t;
+    if (engine == 0) {
+      const LpResult r = solveLpSimplex(lp, SimplexOptions{}, time_limit > 0 ? &dl : nullptr);
+      out[0] = static_cast<double>(r.status);
+      out[1] = r.objective;
+      out[3] = static_cast<double>(r.stats.iterations);
+    } else {
+      const IpmResult r = solveIpm(lp, IpmOptions{}, time_limit > 0 ? &dl : nullptr);
+      out[0] = static_cast<double>(r.status);
+      out[1] = r.objective;
+      out[3] = static_cast<double>(r.stats.iterations);
+    }
+    out[2] = t.seconds();
     return 0;
   } catch (std::exception& e) {
     gErr = e.what();
