@@ -378,33 +378,37 @@ struct MultiEngine {
     A.cols = N;
     AT.rows = N;
     AT.cols = M;
-    A.ptr.reserve(static_cast<size_t>(M) + 1);
-    AT.ptr.reserve(static_cast<size_t>(N) + 1);
-    A.ptr.push_back(0);
-    AT.ptr.push_back(0);
-    A.idx.reserve(annz);
-    A.val.reserve(annz);
-    AT.idx.reserve(annz);
-    AT.val.reserve(annz);
+    std::vector<int64_t> aoff(K + 1, 0);  // first entry of LP b in the concatenated operators
+    for (int b = 0; b < K; ++b) aoff[b + 1] = aoff[b] + static_cast<int64_t>(P[b].A.val.size());
+    A.ptr.resize(static_cast<size_t>(M) + 1);
+    AT.ptr.resize(static_cast<size_t>(N) + 1);
+    A.ptr[0] = 0;
+    AT.ptr[0] = 0;
+    A.idx.resize(annz);
+    A.val.resize(annz);
+    AT.idx.resize(annz);
+    AT.val.resize(annz);
     std::vector<int32_t> rinst(M), cinst(N);
     std::vector<double> rfac(M), cfac(N), c(N), lo(N), up(N), rl(M), ru(M), x0(N);
     cNorm.assign(K, 0);
     rhsNorm.assign(K, 0);
     omega0.assign(K, 1.0);
     eta.assign(K, 0);
-    for (int b = 0; b < K; ++b) {
+    // every LP fills its own ranges: on all host threads, with the same values
+    // as one pass in LP order
+    auto fill = [&](int b) {
       const Prepared& p = P[b];
       const b2p_lp& l = lps[b];
-      const int32_t base_a = A.ptr.back(), base_t = AT.ptr.back();
-      for (int32_t i = 0; i < p.m; ++i) A.ptr.push_back(base_a + p.A.ptr[i + 1]);
+      const int32_t base = static_cast<int32_t>(aoff[b]);
+      for (int32_t i = 0; i < p.m; ++i) A.ptr[roff[b] + i + 1] = base + p.A.ptr[i + 1];
       for (size_t q = 0; q < p.A.idx.size(); ++q) {
-        A.idx.push_back(static_cast<int32_t>(coff[b]) + p.A.idx[q]);
-        A.val.push_back(p.A.val[q]);
+        A.idx[aoff[b] + q] = static_cast<int32_t>(coff[b]) + p.A.idx[q];
+        A.val[aoff[b] + q] = p.A.val[q];
       }
-      for (int32_t j = 0; j < p.n; ++j) AT.ptr.push_back(base_t + p.AT.ptr[j + 1]);
+      for (int32_t j = 0; j < p.n; ++j) AT.ptr[coff[b] + j + 1] = base + p.AT.ptr[j + 1];
       for (size_t q = 0; q < p.AT.idx.size(); ++q) {
-        AT.idx.push_back(static_cast<int32_t>(roff[b]) + p.AT.idx[q]);
-        AT.val.push_back(p.AT.val[q]);
+        AT.idx[aoff[b] + q] = static_cast<int32_t>(roff[b]) + p.AT.idx[q];
+        AT.val[aoff[b] + q] = p.AT.val[q];
       }
       // scaled case vectors (src/pdhg/pdhg.cpp:466-481, 506-530), k = 1 per instance
       double s = 0;
@@ -438,6 +442,15 @@ struct MultiEngine {
       }
       if (cn > 1e-20 && bn > 1e-20) omega0[b] = std::sqrt(cn) / std::sqrt(bn);
       eta[b] = 0.998 / p.normA;
+    };
+    {
+      std::atomic<int> nextb{0};
+      std::vector<std::thread> fillers;
+      for (int t = 0; t < nth; ++t)
+        fillers.emplace_back([&] {
+          for (int b; (b = nextb.fetch_add(1)) < K;) fill(b);
+        });
+      for (auto& th : fillers) th.join();
     }
     // ---- device ----
     const auto tx = Clock::now();
