@@ -196,18 +196,21 @@ __global__ void k_ns_sum(int32_t k, int64_t len, const double* __restrict__ term
   bound[b] = inf_terms[b] > 0 ? -INFINITY : lb;
 }
 
-// Device buffers and the stream of one call, released on every exit path.
+// Device buffers and the stream of one call, released on every exit path;
+// the buffers come from the device's stream-ordered pool (no cudaMalloc /
+// cudaFree per call).
 struct NsBuffers {
+  int dev;
   cudaStream_t s;
   std::vector<void*> p;
   ~NsBuffers() {
-    for (void* q : p) cudaFree(q);
+    for (void* q : p) cudaFreeAsync(q, s);
     cudaStreamDestroy(s);
   }
   template <class T>
   T* put(const T* h, size_t count) {
     void* d = nullptr;
-    B2P_CUDA(cudaMalloc(&d, std::max<size_t>(count, 1) * sizeof(T)));
+    B2P_CUDA(cudaMallocFromPoolAsync(&d, std::max<size_t>(count, 1) * sizeof(T), device_pool(dev), s));
     p.push_back(d);
     if (h && count) B2P_CUDA(cudaMemcpyAsync(d, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
     return static_cast<T*>(d);
@@ -253,7 +256,7 @@ extern "C" int b2p_safe_dual_bound(const b2p_lp* lp, const b2p_case* cases, int3
     B2P_CUDA(cudaSetDevice(dev));
     cudaStream_t s = nullptr;
     B2P_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    NsBuffers r{s, {}};
+    NsBuffers r{dev, s, {}};
     const CsrView AT{r.put(lp->start, static_cast<size_t>(n) + 1), r.put(lp->index, nnz), r.put(lp->value, nnz), n};
     const double* dy = r.put(row_dual, static_cast<size_t>(k) * m);
     const double* dc = r.put(c.data(), c.size());

@@ -161,15 +161,19 @@ inline void enqueue_kkt(cudaStream_t stream, int32_t m, int32_t n, int32_t k, Cs
 
 namespace {
 
+// Device buffers of one call, from the device's stream-ordered pool (freed
+// blocks stay cached for the next call; no cudaMalloc / cudaFree per call).
 struct DeviceBuffers {
+  int dev;
+  cudaStream_t stream;
   std::vector<void*> ptrs;
   ~DeviceBuffers() {
-    for (void* p : ptrs) cudaFree(p);
+    for (void* p : ptrs) cudaFreeAsync(p, stream);
   }
   template <class T>
   T* put(const T* h, size_t count, cudaStream_t s) {
     void* p = nullptr;
-    B2P_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+    B2P_CUDA(cudaMallocFromPoolAsync(&p, std::max<size_t>(count, 1) * sizeof(T), device_pool(dev), s));
     ptrs.push_back(p);
     if (h && count) B2P_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
     return static_cast<T*>(p);
@@ -237,7 +241,7 @@ extern "C" int b2p_kkt_residual(const b2p_lp* lp, const b2p_case* cases, int32_t
       cudaStream_t s;
       ~StreamGuard() { cudaStreamDestroy(s); }
     } sg{s};
-    DeviceBuffers buf;
+    DeviceBuffers buf{dev, s, {}};
     const CsrView A{buf.put(aptr.data(), aptr.size(), s), buf.put(aidx.data(), aidx.size(), s),
                     buf.put(aval.data(), aval.size(), s), m};
     const CsrView AT{buf.put(lp->start, static_cast<size_t>(n) + 1, s), buf.put(lp->index, nnz, s),
