@@ -207,6 +207,56 @@ __global__ void __launch_bounds__(kBlock) k_restart_multi(int32_t n, int32_t m, 
   }
 }
 
+// ---- ||A|| of every LP at once (powerIteration, src/pdhg/pdhg.cpp:404-422) ----
+// The block-diagonal A x and A^T y are CSR row sums in increasing column
+// order -- the addition order of the reference's scatter products -- and each
+// LP's ||z|| is summed by one thread in index order, so every LP's estimate is
+// bit-identical to its own sequential power iteration.
+
+// x_j = 1 / sqrt(n_b) for the columns of LP b; LPs without entries are done
+// from the start with ||A|| = 1.
+__global__ void k_pi_init(int32_t N, int32_t K, const int32_t* __restrict__ cinst, const int32_t* __restrict__ coff,
+                          const int64_t* __restrict__ lp_nnz, double* __restrict__ x, int32_t* __restrict__ done,
+                          double* __restrict__ s) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t < N) {
+    const int b = cinst[t];
+    const int32_t nb = coff[b + 1] - coff[b];
+    x[t] = __ddiv_rn(1.0, __dsqrt_rn(static_cast<double>(nb > 1 ? nb : 1)));
+  }
+  if (t < K) {
+    done[t] = lp_nnz[t] == 0 ? 1 : 0;
+    s[t] = 1.0;
+  }
+}
+
+// One thread per LP: nz = sqrt(sum z_j^2) in index order; nz == 0 ends the
+// LP's iteration with ||A|| = 1, else s = sqrt(nz).
+__global__ void k_pi_norm(int32_t K, const int32_t* __restrict__ coff, const double* __restrict__ z,
+                          int32_t* __restrict__ done, double* __restrict__ nz_out, double* __restrict__ s) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= K || done[b]) return;
+  double acc = 0.0;
+  for (int32_t j = coff[b]; j < coff[b + 1]; ++j) acc = __dadd_rn(acc, __dmul_rn(z[j], z[j]));
+  const double nz = __dsqrt_rn(acc);
+  nz_out[b] = nz;
+  if (nz == 0.0) {
+    done[b] = 1;
+    s[b] = 1.0;
+  } else {
+    s[b] = __dsqrt_rn(nz);
+  }
+}
+
+// x = z / nz of the column's LP (LPs that are done keep their x).
+__global__ void k_pi_scale(int32_t N, const int32_t* __restrict__ cinst, const int32_t* __restrict__ done,
+                           const double* __restrict__ nz, const double* __restrict__ z, double* __restrict__ x) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= N) return;
+  const int b = cinst[t];
+  if (!done[b]) x[t] = __ddiv_rn(z[t], nz[b]);
+}
+
 namespace {
 
 enum MSlot : int { MX, MXP, MX0, MC, MLO, MUP, MXINIT, MATYP, MNCOL, MY = MNCOL, MYP, MY0, MAX, MAXP, MAX0, MRL, MRU,
@@ -338,7 +388,7 @@ struct MultiEngine {
     po.ruiz_iterations = opt.ruiz_iterations;
     po.pock_chambolle = opt.pock_chambolle != 0;
     po.rescale = opt.rescale_objective_and_bounds != 0;
-    po.norm_on_host = true;
+    po.norm_on_host = false;  // ||A|| of every LP on the device below
     po.parallel = false;  // the LPs themselves are prepared on all host threads
     std::atomic<int> next{0};
     const int nth = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), static_cast<unsigned>(K)));
@@ -441,7 +491,6 @@ struct MultiEngine {
         if (finite_bound(ru[t]) && ru[t] != rl[t]) bn += ru[t] * ru[t];
       }
       if (cn > 1e-20 && bn > 1e-20) omega0[b] = std::sqrt(cn) / std::sqrt(bn);
-      eta[b] = 0.998 / p.normA;
     };
     {
       std::atomic<int> nextb{0};
@@ -464,6 +513,8 @@ struct MultiEngine {
     d_cfac = upload(cfac);
     d_rinst = upload(rinst);
     d_cinst = upload(cinst);
+    device_power_iterations(40);
+    for (int b = 0; b < K; ++b) eta[b] = 0.998 / P[b].normA;
     for (int q = 0; q < MNSLOT; ++q) v[q] = dalloc<double>(q >= MY ? M : N);
     auto put = [&](int q, const std::vector<double>& h) {
       if (!h.empty()) B2P_CUDA(cudaMemcpyAsync(v[q], h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
@@ -498,6 +549,43 @@ struct MultiEngine {
     stats.setup_seconds = seconds_since(t0);
     stats.kernel_mode = B2P_KERNELS_FUSED;
     stats.precision_used = B2P_PRECISION_FP64;
+  }
+
+  // ||A|| of every LP on the device (1.01 x the power-iteration estimate, as
+  // prepare() computes on the host), bit-identical to the host's.
+  void device_power_iterations(int iters) {
+    if (M == 0 || N == 0) {
+      for (int b = 0; b < K; ++b) P[b].normA = 1.0 * 1.01;
+      return;
+    }
+    std::vector<int32_t> co(K + 1);
+    for (int b = 0; b <= K; ++b) co[b] = static_cast<int32_t>(coff[b]);
+    int32_t* d_co = upload(co);
+    int64_t* d_nnz = upload(inst_nnz_of_lps());
+    double* dx = dalloc<double>(N);
+    double* dy = dalloc<double>(M);
+    double* dz = dalloc<double>(N);
+    double* d_nz = dalloc<double>(K);
+    double* d_s = dalloc<double>(K);
+    int32_t* d_pdone = dalloc<int32_t>(K);
+    const unsigned kb = static_cast<unsigned>((K + kBlock - 1) / kBlock);
+    k_pi_init<<<blocks(std::max<int64_t>(N, K)), kBlock, 0, stream>>>(N, K, d_cinst, d_co, d_nnz, dx, d_pdone, d_s);
+    for (int it = 0; it < iters; ++it) {
+      k_spmv<<<blocks(M), kBlock, 0, stream>>>(M, 1, viewA(), dx, dy);
+      k_spmv<<<blocks(N), kBlock, 0, stream>>>(N, 1, viewAT(), dy, dz);
+      k_pi_norm<<<kb, kBlock, 0, stream>>>(K, d_co, dz, d_pdone, d_nz, d_s);
+      k_pi_scale<<<blocks(N), kBlock, 0, stream>>>(N, d_cinst, d_pdone, d_nz, dz, dx);
+    }
+    B2P_CUDA(cudaGetLastError());
+    std::vector<double> s(K);
+    B2P_CUDA(cudaMemcpyAsync(s.data(), d_s, sizeof(double) * K, cudaMemcpyDeviceToHost, stream));
+    B2P_CUDA(cudaStreamSynchronize(stream));
+    for (int b = 0; b < K; ++b) P[b].normA = s[b] * 1.01;
+  }
+  std::vector<int64_t> inst_nnz_of_lps() const {
+    std::vector<int64_t> v(K);
+    for (int b = 0; b < K; ++b) v[b] = static_cast<int64_t>(P[b].A.val.size());
+    return v;
   }
 
   // Block-diagonal form: check tables, fused-kernel schedules, autotuner.

@@ -209,3 +209,20 @@ def test_owner_kernel_converged_and_warm(oracle_mod):
     for r, w, g in zip(rs, warm, ref):
         assert w.status == "Optimal" and w.iterations <= r.iterations
         assert w.iterations == g.iterations and np.array_equal(w.x, g.x)
+
+
+@pytest.mark.parametrize("iters", [1, 2, 63, 64])
+@pytest.mark.parametrize("kernel", [_lib.CTA_GENERAL, _lib.CTA_OWNER2])
+def test_cta_iterates_bit_identical_to_oracle(oracle_mod, iters, kernel):
+    """The CTA kernels sum every row left to right, as the reference does, and
+    each LP's ||A|| (the device power iteration over the whole batch) equals
+    its own sequential estimate bit for bit: up to the first check (whose
+    sums are reduced in another order) the iterates are the oracle's
+    exactly, for every LP of the batch."""
+    lps = [G.random_lp(m, 2 * m, 4.0, int(0.6 * m), 600 + i) for i, m in enumerate([30, 100, 250, 450])]
+    fam = W.RefineryFamily(seed=5, periods=2, regions=1, units=4, streams=4, properties=2, scale_exponent=0.0)
+    lps.append(fam.instance(fam.sample(1, seed=8)[0]))
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-30, maxIterations=iters, ctaKernel=kernel, **CTA))
+    for lp, r in zip(lps, rs):
+        o = oracle_mod.solve(lp, "oracle", tolerance=1e-30, max_iterations=iters)
+        assert np.array_equal(r.x, o.x) and np.array_equal(r.rowDual, o.y)
