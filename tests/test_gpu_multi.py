@@ -64,7 +64,7 @@ def test_multi_warm_start():
             assert w.iterations == c.iterations
 
 
-# ---- SpMV schedules of the multi-LP engine: TMA-staged tiles and the autotuner ----
+# ---- SpMV schedules of the multi-LP engine: warp tiles and the autotuner ----
 
 from pramana_b200 import _lib  # noqa: E402
 
@@ -97,8 +97,8 @@ def test_tiled_rows_sum_in_reference_order(oracle_mod, iters):
 
 
 def test_tiled_many_tiles_per_cta_matches_binned():
-    """~3M nonzeros: several tiles per persistent CTA (double-buffered bulk
-    copies), long rows on the binned path beside them."""
+    """~3M nonzeros: many warp tiles per launch, long rows on the binned
+    path as leading blocks of the same launch."""
     lps = G.uneven_family(8, 2e5, 6e5, seed=11)
     kw = dict(tolerance=1e-30, maxIterations=200)
     rb = pdhg.solvePdhgMulti(lps, opts(spmvSchedule=_lib.SCHEDULE_BINNED, **kw))
