@@ -527,7 +527,10 @@ def run_multi(args, rank, world):
             raw = pdhg.solvePdhgMulti.last_stats if lps else _lib.B2pStats()
             runs.append((st.kernelSeconds if lps else 0.0, wall, st.iterations, rs, raw.kernel_launches,
                          raw.bytes_uploaded, raw.bytes_downloaded, raw.lanes_per_row_a, raw.lanes_per_row_at,
-                         raw.schedule_a, raw.schedule_at))
+                         raw.schedule_a, raw.schedule_at,
+                         {"setup_s": raw.setup_seconds, "host_preparation_s": raw.prepare_seconds,
+                          "uploads_schedules_autotune_s": raw.upload_seconds, "autotune_s": raw.autotune_seconds,
+                          "graphs_s": raw.graph_seconds, "loop_s": raw.solve_seconds}))
     dev = statistics.mean(r[0] for r in runs)
     wall = statistics.mean(r[1] for r in runs)
     rs = runs[-1][3]
@@ -586,6 +589,7 @@ def run_multi(args, rank, world):
                 "iterations": its, "optimal": sum(v["status"] == "Optimal" for v in merged.values()),
                 "e2e": {"value": wall, "unit": "s", "h2d_bytes_per_step": int(runs[-1][5]),
                         "d2h_bytes_per_step": int(runs[-1][6])},
+                "setup": runs[-1][11],
                 "gpu_launches": runs[-1][4],
                 "sequential_fp64": seq,
                 "speedup_vs_sequential": (seq["seconds_extrapolated"] / wall) if seq else None,
