@@ -207,6 +207,15 @@ __global__ void __launch_bounds__(kBlock) k_restart_multi(int32_t n, int32_t m, 
   }
 }
 
+// idx[q] += off[b] for the entries q of LP b (block b): LP-local indices of
+// the concatenated operator become global ones.
+__global__ void k_offset_segments(const int64_t* __restrict__ seg, const int32_t* __restrict__ off,
+                                  int32_t* __restrict__ idx) {
+  const int b = blockIdx.x;
+  const int32_t o = off[b];
+  for (int64_t q = seg[b] + threadIdx.x; q < seg[b + 1]; q += blockDim.x) idx[q] += o;
+}
+
 // ---- ||A|| of every LP at once (powerIteration, src/pdhg/pdhg.cpp:404-422) ----
 // The block-diagonal A x and A^T y are CSR row sums in increasing column
 // order -- the addition order of the reference's scatter products -- and each
@@ -339,15 +348,6 @@ struct MultiEngine {
     bytes_up += static_cast<int64_t>(h.size() * sizeof(T));
     return d;
   }
-  // operator index / value arrays carry kTilePad zero entries past the end
-  template <class T>
-  T* upload_padded(const std::vector<T>& h) {
-    T* d = dalloc<T>(h.size() + kTilePad);
-    B2P_CUDA(cudaMemsetAsync(d + h.size(), 0, kTilePad * sizeof(T), stream));
-    if (!h.empty()) B2P_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
-    bytes_up += static_cast<int64_t>(h.size() * sizeof(T));
-    return d;
-  }
   static unsigned blocks(int64_t len) { return static_cast<unsigned>(std::max<int64_t>(1, (len + kBlock - 1) / kBlock)); }
   CsrView viewA() const { return CsrView{dA_ptr, dA_idx, dA_val, M}; }
   CsrView viewAT() const { return CsrView{dT_ptr, dT_idx, dT_val, N}; }
@@ -434,10 +434,6 @@ struct MultiEngine {
     AT.ptr.resize(static_cast<size_t>(N) + 1);
     A.ptr[0] = 0;
     AT.ptr[0] = 0;
-    A.idx.resize(annz);
-    A.val.resize(annz);
-    AT.idx.resize(annz);
-    AT.val.resize(annz);
     std::vector<int32_t> rinst(M), cinst(N);
     std::vector<double> rfac(M), cfac(N), c(N), lo(N), up(N), rl(M), ru(M), x0(N);
     cNorm.assign(K, 0);
@@ -451,15 +447,7 @@ struct MultiEngine {
       const b2p_lp& l = lps[b];
       const int32_t base = static_cast<int32_t>(aoff[b]);
       for (int32_t i = 0; i < p.m; ++i) A.ptr[roff[b] + i + 1] = base + p.A.ptr[i + 1];
-      for (size_t q = 0; q < p.A.idx.size(); ++q) {
-        A.idx[aoff[b] + q] = static_cast<int32_t>(coff[b]) + p.A.idx[q];
-        A.val[aoff[b] + q] = p.A.val[q];
-      }
       for (int32_t j = 0; j < p.n; ++j) AT.ptr[coff[b] + j + 1] = base + p.AT.ptr[j + 1];
-      for (size_t q = 0; q < p.AT.idx.size(); ++q) {
-        AT.idx[aoff[b] + q] = static_cast<int32_t>(roff[b]) + p.AT.idx[q];
-        AT.val[aoff[b] + q] = p.AT.val[q];
-      }
       // scaled case vectors (src/pdhg/pdhg.cpp:466-481, 506-530), k = 1 per instance
       double s = 0;
       for (int32_t j = 0; j < p.n; ++j) s += l.col_cost[j] * l.col_cost[j];
@@ -504,11 +492,41 @@ struct MultiEngine {
     // ---- device ----
     const auto tx = Clock::now();
     dA_ptr = upload(A.ptr);
-    dA_idx = upload_padded(A.idx);
-    dA_val = upload_padded(A.val);
+    // Each LP's index and value arrays go straight to their ranges of the
+    // concatenated device operators (no host copy of the whole batch); the
+    // row / column offsets of the indices are added on the device.
+    dA_idx = dalloc<int32_t>(static_cast<size_t>(annz) + kTilePad);
+    dA_val = dalloc<double>(static_cast<size_t>(annz) + kTilePad);
+    dT_idx = dalloc<int32_t>(static_cast<size_t>(annz) + kTilePad);
+    dT_val = dalloc<double>(static_cast<size_t>(annz) + kTilePad);
+    B2P_CUDA(cudaMemsetAsync(dA_idx + annz, 0, kTilePad * sizeof(int32_t), stream));
+    B2P_CUDA(cudaMemsetAsync(dA_val + annz, 0, kTilePad * sizeof(double), stream));
+    B2P_CUDA(cudaMemsetAsync(dT_idx + annz, 0, kTilePad * sizeof(int32_t), stream));
+    B2P_CUDA(cudaMemsetAsync(dT_val + annz, 0, kTilePad * sizeof(double), stream));
+    for (int b = 0; b < K; ++b) {
+      const Prepared& p = P[b];
+      const size_t e = p.A.val.size();
+      if (!e) continue;
+      B2P_CUDA(cudaMemcpyAsync(dA_idx + aoff[b], p.A.idx.data(), e * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
+      B2P_CUDA(cudaMemcpyAsync(dA_val + aoff[b], p.A.val.data(), e * sizeof(double), cudaMemcpyHostToDevice, stream));
+      B2P_CUDA(cudaMemcpyAsync(dT_idx + aoff[b], p.AT.idx.data(), e * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
+      B2P_CUDA(cudaMemcpyAsync(dT_val + aoff[b], p.AT.val.data(), e * sizeof(double), cudaMemcpyHostToDevice, stream));
+    }
+    bytes_up += 24 * annz;
+    {
+      std::vector<int32_t> co(K), ro(K);
+      for (int b = 0; b < K; ++b) {
+        co[b] = static_cast<int32_t>(coff[b]);
+        ro[b] = static_cast<int32_t>(roff[b]);
+      }
+      const int64_t* d_aoff = upload(aoff);
+      const int32_t* d_co = upload(co);
+      const int32_t* d_ro = upload(ro);
+      k_offset_segments<<<K, kBlock, 0, stream>>>(d_aoff, d_co, dA_idx);
+      k_offset_segments<<<K, kBlock, 0, stream>>>(d_aoff, d_ro, dT_idx);
+      B2P_CUDA(cudaGetLastError());
+    }
     dT_ptr = upload(AT.ptr);
-    dT_idx = upload_padded(AT.idx);
-    dT_val = upload_padded(AT.val);
     d_rfac = upload(rfac);
     d_cfac = upload(cfac);
     d_rinst = upload(rinst);
