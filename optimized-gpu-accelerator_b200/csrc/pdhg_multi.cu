@@ -1104,8 +1104,52 @@ struct MultiEngine {
   // every binned schedule (1..32 lanes per short row, with cached or
   // evict-first streaming loads) and the tile schedule on the device, from the
   // solve's starting state, and keep the fastest.
+  // The choice per operator: binned (lanes per short row, streaming) or tiles
+  // (capped or not).  Remembered for the process per batch shape, so repeated
+  // solves of a batch (or of batches of one family) time the candidates once.
+  struct SchedChoice {
+    int g = 1;
+    bool streaming = false, tiles = false, capped = false;
+  };
+  void apply_choice(const HostCsr& Op, int32_t rows, const SchedChoice& c, RowBins& bins, TileSched& tiles,
+                    bool& streaming, const std::vector<int32_t>& ptr, const std::vector<int64_t>& off) {
+    if (c.tiles) {
+      tiles = device_tiles(ptr, off, nullptr);
+      tiles.capped = c.capped;
+    } else {
+      tiles.on = false;
+      streaming = c.streaming;
+      bins = device_bins(make_bins(Op, wave, c.g, rounds), rows);
+    }
+  }
+  static SchedChoice choice_of(const RowBins& bins, const TileSched& tiles, bool streaming) {
+    SchedChoice c;
+    c.g = bins.g;
+    c.streaming = streaming;
+    c.tiles = tiles.on;
+    c.capped = tiles.capped;
+    return c;
+  }
+
   void autotune(const HostCsr& A, const HostCsr& AT) {
     const auto t0 = Clock::now();
+    int64_t annz = static_cast<int64_t>(hA_ptr.empty() ? 0 : hA_ptr.back());
+    const std::vector<int64_t> key{device, K, M, N, annz, opt.spmv_schedule, rounds, opt.lanes_per_row_a,
+                                   opt.lanes_per_row_at};
+    static std::mutex mu;
+    static std::map<std::vector<int64_t>, std::pair<SchedChoice, SchedChoice>> chosen;
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      const auto it = chosen.find(key);
+      if (it != chosen.end()) {
+        apply_choice(AT, N, it->second.first, binsT, tilesT, streamT, hT_ptr, coff);
+        apply_choice(A, M, it->second.second, binsA, tilesA, streamA, hA_ptr, roff);
+        ltA = binsA.long_thr;
+        ltT = binsT.long_thr;
+        stats.autotune_seconds = seconds_since(t0);
+        return;
+      }
+    }
     reset_state();
     cudaEvent_t e0, e1;
     B2P_CUDA(cudaEventCreate(&e0));
@@ -1164,6 +1208,10 @@ struct MultiEngine {
     ltT = binsT.long_thr;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      chosen[key] = {choice_of(binsT, tilesT, streamT), choice_of(binsA, tilesA, streamA)};
+    }
     stats.autotune_seconds = seconds_since(t0);
   }
 
