@@ -200,10 +200,10 @@ struct Engine {
       for (void* p : allocs) cudaFreeAsync(p, stream);
       cudaStreamSynchronize(stream);
     }
-    if (h_sums) cudaFreeHost(h_sums);
-    if (h_steps) cudaFreeHost(h_steps);
-    if (h_mask) cudaFreeHost(h_mask);
-    if (h_error) cudaFreeHost(h_error);
+    PinnedCache::put(h_sums, sizeof(double) * k * kNumSums);
+    PinnedCache::put(h_steps, sizeof(double) * 2 * k);
+    PinnedCache::put(h_mask, sizeof(int32_t) * k);
+    PinnedCache::put(h_error, sizeof(int32_t));
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -338,9 +338,9 @@ struct Engine {
     d_prow = dalloc<double>(static_cast<size_t>(k) * g_rows * kRowSums);
     d_pcol = dalloc<double>(static_cast<size_t>(k) * g_cols * kRowSums);
     d_sums = dalloc<double>(static_cast<size_t>(k) * kNumSums);
-    B2P_CUDA(cudaMallocHost(&h_sums, sizeof(double) * k * kNumSums));
-    B2P_CUDA(cudaMallocHost(&h_steps, sizeof(double) * 2 * k));
-    B2P_CUDA(cudaMallocHost(&h_mask, sizeof(int32_t) * k));
+    h_sums = static_cast<double*>(PinnedCache::get(sizeof(double) * k * kNumSums));
+    h_steps = static_cast<double*>(PinnedCache::get(sizeof(double) * 2 * k));
+    h_mask = static_cast<int32_t*>(PinnedCache::get(sizeof(int32_t) * k));
     if (mixed || mixed_batch) setup_mixed();
     // AX = A x0 on the device (pdhg.cpp:540-545), kept as the restart point of every solve.
     if (m > 0) {
@@ -368,11 +368,12 @@ struct Engine {
     std::vector<double> hx(n, 1.0 / std::sqrt(static_cast<double>(n > 1 ? n : 1)));
     B2P_CUDA(cudaMemcpyAsync(dx, hx.data(), sizeof(double) * n, cudaMemcpyHostToDevice, stream));
     double* hz = nullptr;
-    B2P_CUDA(cudaMallocHost(&hz, sizeof(double) * n));
+    hz = static_cast<double*>(PinnedCache::get(sizeof(double) * n));
     struct PinnedGuard {
       double* p;
-      ~PinnedGuard() { cudaFreeHost(p); }
-    } guard{hz};
+      size_t bytes;
+      ~PinnedGuard() { PinnedCache::put(p, bytes); }
+    } guard{hz, sizeof(double) * n};
     double s = 1;
     for (int it = 0; it < iters; ++it) {
       k_spmv<<<blocks(m), kBlock, 0, stream>>>(m, 1, viewA(), dx, dy);
@@ -433,7 +434,8 @@ struct Engine {
     d_rb = upload(rb);
     d_sync = dalloc<unsigned>(4);
     d_rpartial = dalloc<double>(static_cast<size_t>(nb) * kNumSums);
-    B2P_CUDA(cudaMallocHost(&h_error, sizeof(int32_t)));
+    h_error = static_cast<int32_t*>(PinnedCache::get(sizeof(int32_t)));
+    *h_error = 0;
     res_blocks = nb;
     res_smem = ok64 ? need64 : 0;
     res_smem32 = ok32 ? need32 : 0;

@@ -13,6 +13,7 @@
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "../../include/b2p_pdhg.h"
 
@@ -85,6 +86,66 @@ inline cudaMemPool_t device_pool(int dev) {
   pools.emplace(dev, pool);
   return pool;
 }
+
+// Page-locked host buffers, cached for the process: cudaMallocHost pins
+// pages and cudaFreeHost unpins them (and waits for the device), at a cost
+// that varies with the host's load, so the engines take their small pinned
+// buffers (check sums, step sizes, masks, power-iteration vectors) from here
+// and give them back.  Buffers come in power-of-two sizes from 256 bytes; up
+// to kPinnedKeepBytes of freed buffers are kept, the rest are freed.
+constexpr size_t kPinnedKeepBytes = size_t(256) << 20;
+
+class PinnedCache {
+ public:
+  static void* get(size_t bytes) {
+    const size_t cls = size_class(bytes);
+    {
+      std::lock_guard<std::mutex> lock(mu());
+      auto& fl = lists()[cls];
+      if (!fl.empty()) {
+        void* p = fl.back();
+        fl.pop_back();
+        kept() -= cls;
+        return p;
+      }
+    }
+    void* p = nullptr;
+    B2P_CUDA(cudaMallocHost(&p, cls));
+    return p;
+  }
+  static void put(void* p, size_t bytes) {
+    if (!p) return;
+    const size_t cls = size_class(bytes);
+    {
+      std::lock_guard<std::mutex> lock(mu());
+      if (kept() + cls <= kPinnedKeepBytes) {
+        lists()[cls].push_back(p);
+        kept() += cls;
+        return;
+      }
+    }
+    cudaFreeHost(p);
+  }
+
+ private:
+  static size_t size_class(size_t bytes) {
+    size_t c = 256;
+    while (c < bytes) c <<= 1;
+    return c;
+  }
+  static std::mutex& mu() {
+    static std::mutex m;
+    return m;
+  }
+  static std::map<size_t, std::vector<void*>>& lists() {
+    static std::map<size_t, std::vector<void*>> l;
+    return l;
+  }
+  static size_t& kept() {
+    static size_t k = 0;
+    return k;
+  }
+};
 
 // Ordinal of the sm_100 device to use: `requested`, else PRAMANA_GPU_DEVICE,
 // else 0 (src/gpu/cuda_driver.cpp:223); PRAMANA_DISABLE_GPU disables the

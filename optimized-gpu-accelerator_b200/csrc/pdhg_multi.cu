@@ -362,10 +362,10 @@ struct MultiEngine {
       for (void* p : allocs) cudaFreeAsync(p, stream);
       cudaStreamSynchronize(stream);
     }
-    if (h_sums) cudaFreeHost(h_sums);
-    if (h_steps) cudaFreeHost(h_steps);
-    if (h_mask) cudaFreeHost(h_mask);
-    if (h_done) cudaFreeHost(h_done);
+    PinnedCache::put(h_sums, sizeof(double) * K * kNumSums);
+    PinnedCache::put(h_steps, sizeof(double) * 2 * K);
+    PinnedCache::put(h_mask, sizeof(int32_t) * K);
+    PinnedCache::put(h_done, sizeof(int32_t) * K);
     if (h_stop) cudaFreeHost(h_stop);
     if (stream) cudaStreamDestroy(stream);
   }
@@ -630,10 +630,10 @@ struct MultiEngine {
     d_prow = dalloc<double>(static_cast<size_t>(std::max(1, g_rows)) * kRowSums);
     d_pcol = dalloc<double>(static_cast<size_t>(std::max(1, g_cols)) * kRowSums);
     d_sums = dalloc<double>(static_cast<size_t>(K) * kNumSums);
-    B2P_CUDA(cudaMallocHost(&h_sums, sizeof(double) * K * kNumSums));
-    B2P_CUDA(cudaMallocHost(&h_steps, sizeof(double) * 2 * K));
-    B2P_CUDA(cudaMallocHost(&h_mask, sizeof(int32_t) * K));
-    B2P_CUDA(cudaMallocHost(&h_done, sizeof(int32_t) * K));
+    h_sums = static_cast<double*>(PinnedCache::get(sizeof(double) * K * kNumSums));
+    h_steps = static_cast<double*>(PinnedCache::get(sizeof(double) * 2 * K));
+    h_mask = static_cast<int32_t*>(PinnedCache::get(sizeof(int32_t) * K));
+    h_done = static_cast<int32_t*>(PinnedCache::get(sizeof(int32_t) * K));
     // fused-kernel schedules of the concatenated operators
     int per_sm = 0, sms = 0;
     B2P_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dual_binned<4, true, true>, kBlock, 0));
