@@ -216,6 +216,55 @@ __global__ void k_offset_segments(const int64_t* __restrict__ seg, const int32_t
   for (int64_t q = seg[b] + threadIdx.x; q < seg[b + 1]; q += blockDim.x) idx[q] += o;
 }
 
+// ---- Ruiz equilibration and the Pock-Chambolle step on the device
+// (src/lp/scaling.cpp:97-139) over the block-diagonal operator: the rows and
+// columns of different LPs never meet, so this is every LP's own scaling.
+// Each row / column quantity is the host's expression, evaluated in its
+// order ((|a| * c_j) * r_i; maxima are order-free; the 1-norms are summed by
+// one thread in the row's or column's entry order), so the factors are
+// bit-identical to the host's.
+
+// out[r] = max over the entries of row r of (|a| * cscale[col]) * rscale[r]
+// (ROWS: a row of A, scales (rs, cs)); for A^T the roles of the two scale
+// vectors swap, and the product keeps the host's order: (|a| * cs_j) * rs_i.
+template <bool SUM>
+__global__ void k_ruiz_rows(int32_t rows, const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                            const double* __restrict__ val, const double* __restrict__ own,
+                            const double* __restrict__ other, bool own_is_row, double* __restrict__ out) {
+  const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  const double so = own[r];
+  double acc = 0.0;
+  for (int32_t q = ptr[r]; q < ptr[r + 1]; ++q) {
+    const double a = fabs(val[q]);
+    // host order: (|a| * cs[j]) * rs[i]
+    const double t = own_is_row ? __dmul_rn(__dmul_rn(a, other[idx[q]]), so) : __dmul_rn(__dmul_rn(a, so), other[idx[q]]);
+    if (SUM)
+      acc = __dadd_rn(acc, t);
+    else
+      acc = (acc < t) ? t : acc;
+  }
+  out[r] = acc;
+}
+
+// s[i] /= sqrt(q[i]) where q[i] > 0.
+__global__ void k_ruiz_update(int32_t len, const double* __restrict__ q, double* __restrict__ s) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < len && q[i] > 0) s[i] = __ddiv_rn(s[i], __dsqrt_rn(q[i]));
+}
+
+// a = a * (own[r] * other[idx]) for the entries of row r: the scaled operator
+// value[q] * (R[i] * Cs[j]) (src/lp/scaling.cpp:28-32); for A^T, own = Cs and
+// other = R, and the factor is still R[i] * Cs[j].
+__global__ void k_scale_rows(int32_t rows, const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+                             const double* __restrict__ own, const double* __restrict__ other,
+                             double* __restrict__ val) {
+  const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  const double so = own[r];
+  for (int32_t q = ptr[r]; q < ptr[r + 1]; ++q) val[q] = __dmul_rn(val[q], __dmul_rn(so, other[idx[q]]));
+}
+
 // ---- ||A|| of every LP at once (powerIteration, src/pdhg/pdhg.cpp:404-422) ----
 // The block-diagonal A x and A^T y are CSR row sums in increasing column
 // order -- the addition order of the reference's scatter products -- and each
@@ -382,14 +431,8 @@ struct MultiEngine {
     B2P_CUDA(cudaEventCreate(&ev_stop));
     K = num;
     const auto t0 = Clock::now();
-    // ---- host preparation of every instance, on all host threads ----
+    // ---- host preparation of every instance (structure only), on all host threads ----
     P.resize(K);
-    PrepareOptions po;
-    po.ruiz_iterations = opt.ruiz_iterations;
-    po.pock_chambolle = opt.pock_chambolle != 0;
-    po.rescale = opt.rescale_objective_and_bounds != 0;
-    po.norm_on_host = false;  // ||A|| of every LP on the device below
-    po.parallel = false;  // the LPs themselves are prepared on all host threads
     std::atomic<int> next{0};
     const int nth = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), static_cast<unsigned>(K)));
     std::vector<std::thread> pool;
@@ -399,8 +442,8 @@ struct MultiEngine {
         try {
           for (int b; (b = next.fetch_add(1)) < K;) {
             const b2p_lp& l = lps[b];
-            P[b] = prepare(l.num_rows, l.num_cols, l.start, l.index, l.value, l.col_cost, l.row_lower, l.row_upper,
-                           l.obj_offset, po);
+            // structure and raw values; the scaling runs on the device below
+            P[b] = prepare_structure(l.num_rows, l.num_cols, l.start, l.index, l.value, l.obj_offset, false);
           }
         } catch (std::exception& e) {
           errs[t] = e.what();
@@ -442,12 +485,24 @@ struct MultiEngine {
     eta.assign(K, 0);
     // every LP fills its own ranges: on all host threads, with the same values
     // as one pass in LP order
-    auto fill = [&](int b) {
+    auto parallel_lps = [&](auto&& f) {
+      std::atomic<int> nextb{0};
+      std::vector<std::thread> workers;
+      for (int t = 0; t < nth; ++t)
+        workers.emplace_back([&] {
+          for (int b; (b = nextb.fetch_add(1)) < K;) f(b);
+        });
+      for (auto& th : workers) th.join();
+    };
+    parallel_lps([&](int b) {
       const Prepared& p = P[b];
-      const b2p_lp& l = lps[b];
       const int32_t base = static_cast<int32_t>(aoff[b]);
       for (int32_t i = 0; i < p.m; ++i) A.ptr[roff[b] + i + 1] = base + p.A.ptr[i + 1];
       for (int32_t j = 0; j < p.n; ++j) AT.ptr[coff[b] + j + 1] = base + p.AT.ptr[j + 1];
+    });
+    auto fill = [&](int b) {
+      const Prepared& p = P[b];
+      const b2p_lp& l = lps[b];
       // scaled case vectors (src/pdhg/pdhg.cpp:466-481, 506-530), k = 1 per instance
       double s = 0;
       for (int32_t j = 0; j < p.n; ++j) s += l.col_cost[j] * l.col_cost[j];
@@ -480,15 +535,6 @@ struct MultiEngine {
       }
       if (cn > 1e-20 && bn > 1e-20) omega0[b] = std::sqrt(cn) / std::sqrt(bn);
     };
-    {
-      std::atomic<int> nextb{0};
-      std::vector<std::thread> fillers;
-      for (int t = 0; t < nth; ++t)
-        fillers.emplace_back([&] {
-          for (int b; (b = nextb.fetch_add(1)) < K;) fill(b);
-        });
-      for (auto& th : fillers) th.join();
-    }
     // ---- device ----
     const auto tx = Clock::now();
     dA_ptr = upload(A.ptr);
@@ -527,6 +573,31 @@ struct MultiEngine {
       B2P_CUDA(cudaGetLastError());
     }
     dT_ptr = upload(AT.ptr);
+    // ---- scaling on the device (Ruiz + Pock-Chambolle), rounding and the
+    // rescaling constants on the host, the scaled operators on the device ----
+    const auto ts = Clock::now();
+    {
+      std::vector<double> rs(M, 1.0), cs(N, 1.0);
+      if (opt.ruiz_iterations > 0 && annz > 0) device_ruiz(opt.ruiz_iterations, opt.pock_chambolle != 0, rs, cs);
+      const bool rescale = opt.rescale_objective_and_bounds != 0;
+      parallel_lps([&](int b) {
+        const b2p_lp& l = lps[b];
+        finish_scaling(P[b], rs.data() + roff[b], cs.data() + coff[b], l.col_cost, l.row_lower, l.row_upper,
+                       rescale);
+      });
+      std::vector<double> R(M), Cs(N);
+      for (int b = 0; b < K; ++b) {
+        std::copy(P[b].R.begin(), P[b].R.end(), R.begin() + roff[b]);
+        std::copy(P[b].Cs.begin(), P[b].Cs.end(), Cs.begin() + coff[b]);
+      }
+      const double* dR = upload(R);
+      const double* dC = upload(Cs);
+      if (M > 0) k_scale_rows<<<blocks(M), kBlock, 0, stream>>>(M, dA_ptr, dA_idx, dR, dC, dA_val);
+      if (N > 0) k_scale_rows<<<blocks(N), kBlock, 0, stream>>>(N, dT_ptr, dT_idx, dC, dR, dT_val);
+      B2P_CUDA(cudaGetLastError());
+    }
+    stats.prepare_seconds += seconds_since(ts);
+    parallel_lps(fill);
     d_rfac = upload(rfac);
     d_cfac = upload(cfac);
     d_rinst = upload(rinst);
@@ -567,6 +638,35 @@ struct MultiEngine {
     stats.setup_seconds = seconds_since(t0);
     stats.kernel_mode = B2P_KERNELS_FUSED;
     stats.precision_used = B2P_PRECISION_FP64;
+  }
+
+  // Unrounded Ruiz (+ Pock-Chambolle) factors of every LP on the device,
+  // from the raw operators (ruiz_impl in pdhg_prepare.cpp is the host form).
+  void device_ruiz(int iterations, bool pock_chambolle, std::vector<double>& rs, std::vector<double>& cs) {
+    double* d_rs = dalloc<double>(M);
+    double* d_cs = dalloc<double>(N);
+    double* d_rq = dalloc<double>(M);
+    double* d_cq = dalloc<double>(N);
+    B2P_CUDA(cudaMemcpyAsync(d_rs, rs.data(), sizeof(double) * M, cudaMemcpyHostToDevice, stream));
+    B2P_CUDA(cudaMemcpyAsync(d_cs, cs.data(), sizeof(double) * N, cudaMemcpyHostToDevice, stream));
+    auto pass = [&](bool sum) {
+      // columns: (|a| * cs_j) * rs_i over A^T's row j; rows: (|a| * cs_j) * rs_i over A's row i
+      if (sum) {
+        k_ruiz_rows<true><<<blocks(N), kBlock, 0, stream>>>(N, dT_ptr, dT_idx, dT_val, d_cs, d_rs, false, d_cq);
+        k_ruiz_rows<true><<<blocks(M), kBlock, 0, stream>>>(M, dA_ptr, dA_idx, dA_val, d_rs, d_cs, true, d_rq);
+      } else {
+        k_ruiz_rows<false><<<blocks(N), kBlock, 0, stream>>>(N, dT_ptr, dT_idx, dT_val, d_cs, d_rs, false, d_cq);
+        k_ruiz_rows<false><<<blocks(M), kBlock, 0, stream>>>(M, dA_ptr, dA_idx, dA_val, d_rs, d_cs, true, d_rq);
+      }
+      k_ruiz_update<<<blocks(M), kBlock, 0, stream>>>(M, d_rq, d_rs);
+      k_ruiz_update<<<blocks(N), kBlock, 0, stream>>>(N, d_cq, d_cs);
+    };
+    for (int it = 0; it < iterations; ++it) pass(false);
+    if (pock_chambolle) pass(true);
+    B2P_CUDA(cudaGetLastError());
+    B2P_CUDA(cudaMemcpyAsync(rs.data(), d_rs, sizeof(double) * M, cudaMemcpyDeviceToHost, stream));
+    B2P_CUDA(cudaMemcpyAsync(cs.data(), d_cs, sizeof(double) * N, cudaMemcpyDeviceToHost, stream));
+    B2P_CUDA(cudaStreamSynchronize(stream));
   }
 
   // ||A|| of every LP on the device (1.01 x the power-iteration estimate, as

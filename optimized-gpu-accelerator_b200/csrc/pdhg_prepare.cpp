@@ -7,8 +7,6 @@
 
 namespace b2p {
 
-namespace {
-
 // Power-of-two rounding of a scale factor (src/lp/scaling.cpp:9-14): the
 // nearest 2^e with |e| <= 60, so that scaling and unscaling are exact.
 double pow2_round(double v) {
@@ -17,6 +15,8 @@ double pow2_round(double v) {
   e = e < -60 ? -60 : (e > 60 ? 60 : e);
   return std::ldexp(1.0, e);
 }
+
+namespace {
 
 // Row-major view of a CSC matrix: for every row, its entries by increasing
 // column -- the order SparseMatrix::transpose produces
@@ -268,6 +268,63 @@ Prepared prepare(int32_t m, int32_t n, const int32_t* start, const int32_t* inde
   for (int32_t j = 0; j < n; ++j) P.cfac[j] = P.gamma / P.Cs[j];
   if (opt.norm_on_host) P.normA = power_iteration(m, n, start, index, P.AT.val.data(), 40) * 1.01;
   return P;
+}
+
+Prepared prepare_structure(int32_t m, int32_t n, const int32_t* start, const int32_t* index, const double* value,
+                           double offset, bool parallel) {
+  Prepared P;
+  P.n = n;
+  P.m = m;
+  P.offset = offset;
+  const int32_t nnz = start[n];
+  const bool par = parallel && nnz >= kParallelNnz;
+  RowMap rm = row_map(m, n, start, index, par);
+  P.R.assign(m, 1.0);
+  P.Cs.assign(n, 1.0);
+  P.A.rows = m;
+  P.A.cols = n;
+  P.A.val.resize(nnz);
+#pragma omp parallel for schedule(static) if (par)
+  for (int32_t e = 0; e < nnz; ++e) P.A.val[e] = value[rm.pos[e]];
+  P.A.ptr = std::move(rm.ptr);
+  P.A.idx = std::move(rm.col);
+  P.AT.rows = n;
+  P.AT.cols = m;
+  P.AT.ptr.assign(start, start + n + 1);
+  P.AT.idx.assign(index, index + nnz);
+  P.AT.val.assign(value, value + nnz);
+  return P;
+}
+
+void finish_scaling(Prepared& P, const double* rs, const double* cs, const double* cost, const double* row_lower,
+                    const double* row_upper, bool rescale) {
+  const int32_t m = P.m, n = P.n;
+  for (int32_t i = 0; i < m; ++i) P.R[i] = pow2_round(rs[i]);
+  for (int32_t j = 0; j < n; ++j) P.Cs[j] = pow2_round(cs[j]);
+  P.beta = P.gamma = 1.0;
+  if (rescale) {
+    double cn = 0, bn = 0;
+    for (int32_t j = 0; j < n; ++j) {
+      const double t = cost[j] * P.Cs[j];
+      cn += t * t;
+    }
+    for (int32_t i = 0; i < m; ++i) {
+      if (finite_bound(row_lower[i])) {
+        const double t = row_lower[i] * P.R[i];
+        bn += t * t;
+      }
+      if (finite_bound(row_upper[i]) && row_upper[i] != row_lower[i]) {
+        const double t = row_upper[i] * P.R[i];
+        bn += t * t;
+      }
+    }
+    P.gamma = 1.0 + std::sqrt(cn);
+    P.beta = 1.0 + std::sqrt(bn);
+  }
+  P.rfac.resize(m);
+  P.cfac.resize(n);
+  for (int32_t i = 0; i < m; ++i) P.rfac[i] = P.beta / P.R[i];
+  for (int32_t j = 0; j < n; ++j) P.cfac[j] = P.gamma / P.Cs[j];
 }
 
 }  // namespace b2p

@@ -48,6 +48,21 @@ Prepared prepare(int32_t m, int32_t n, const int32_t* start, const int32_t* inde
                  const double* cost, const double* row_lower, const double* row_upper, double offset,
                  const PrepareOptions& opt);
 
+// Structure-only preparation (scaling done elsewhere, e.g. on the device):
+// A (CSR, from the same stable counting sort) and A^T (= the CSC) with the
+// raw values, R = Cs = 1, no rescaling constants yet.
+Prepared prepare_structure(int32_t m, int32_t n, const int32_t* start, const int32_t* index, const double* value,
+                           double offset, bool parallel);
+
+// Completes a structure-only preparation from the unrounded Ruiz factors
+// (rs, cs): their power-of-two rounding (src/lp/scaling.cpp:9-14), beta and
+// gamma (src/pdhg/pdhg.cpp:440-452) and the factors of the check.  The
+// operators' values are left to the caller.
+void finish_scaling(Prepared& P, const double* rs, const double* cs, const double* cost, const double* row_lower,
+                    const double* row_upper, bool rescale);
+
+double pow2_round(double v);
+
 void ruiz_scaling(int32_t m, int32_t n, const int32_t* start, const int32_t* index, const double* value,
                   int iterations, bool pock_chambolle, std::vector<double>& row_scale, std::vector<double>& col_scale,
                   bool parallel = false);
