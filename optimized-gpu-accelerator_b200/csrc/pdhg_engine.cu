@@ -30,6 +30,7 @@
 #include "pdhg_host_common.h"
 #include "pdhg_kernels.cuh"
 #include "pdhg_prepare.h"
+#include "pdhg_scale.cuh"
 #include "pdhg_batch32.cuh"
 #include "pdhg_resident.cuh"
 #include "pdhg_sched.h"
@@ -231,13 +232,26 @@ struct Engine {
     m = lp->num_rows;
     const auto t0 = Clock::now();
 
-    PrepareOptions po;
-    po.ruiz_iterations = opt.ruiz_iterations;
-    po.pock_chambolle = opt.pock_chambolle != 0;
-    po.rescale = opt.rescale_objective_and_bounds != 0;
-    po.norm_on_host = false;  // estimated on the device below, bit-identically
-    P = prepare(m, n, lp->start, lp->index, lp->value, lp->col_cost, lp->row_lower, lp->row_upper, lp->obj_offset,
-                po);
+    // Structure (the CSR of A) on host threads; the scaling (Ruiz,
+    // Pock-Chambolle, the scaled operators) and ||A|| on the device, the
+    // power-of-two rounding and beta / gamma on the host -- bit-identical to
+    // the host's prepare() (pdhg_scale.cuh).
+    P = prepare_structure(m, n, lp->start, lp->index, lp->value, lp->obj_offset, true);
+    const auto tx = Clock::now();
+    dA_ptr = upload(P.A.ptr);
+    dA_idx = upload(P.A.idx);
+    dA_val = upload(P.A.val);
+    dT_ptr = upload(P.AT.ptr);
+    dT_idx = upload(P.AT.idx);
+    dT_val = upload(P.AT.val);
+    {
+      std::vector<double> rs(m, 1.0), cs(n, 1.0);
+      if (opt.ruiz_iterations > 0 && !P.A.val.empty())
+        device_ruiz_factors(stream, device, viewA(), viewAT(), opt.ruiz_iterations, opt.pock_chambolle != 0, rs, cs);
+      finish_scaling(P, rs.data(), cs.data(), lp->col_cost, lp->row_lower, lp->row_upper,
+                     opt.rescale_objective_and_bounds != 0);
+      device_scale_operators(stream, device, viewA(), viewAT(), dA_val, dT_val, P.R, P.Cs);
+    }
     stats.prepare_seconds = seconds_since(t0);
 
     // Case data in scaled space, k-interleaved (src/pdhg/pdhg.cpp:466-481, 506-530).
@@ -282,13 +296,6 @@ struct Engine {
     }
 
     // ---- device state (GpuBackend::init, src/pdhg/pdhg.cpp:238-277) ----
-    const auto tx = Clock::now();
-    dA_ptr = upload(P.A.ptr);
-    dA_idx = upload(P.A.idx);
-    dA_val = upload(P.A.val);
-    dT_ptr = upload(P.AT.ptr);
-    dT_idx = upload(P.AT.idx);
-    dT_val = upload(P.AT.val);
     const auto tn = Clock::now();
     P.normA = device_power_iteration(40) * 1.01;
     stats.prepare_seconds += seconds_since(tn);
@@ -447,9 +454,14 @@ struct Engine {
 
   // FP32 copies of the operators and case vectors for the mixed form.
   void setup_mixed() {
-    std::vector<float> av(P.A.val.begin(), P.A.val.end()), tv(P.AT.val.begin(), P.AT.val.end());
-    a_val32 = upload(av);
-    t_val32 = upload(tv);
+    // FP32 copies of the scaled operators, rounded to nearest on the device
+    const int64_t nnz = static_cast<int64_t>(P.A.val.size());
+    a_val32 = dalloc<float>(static_cast<size_t>(nnz));
+    t_val32 = dalloc<float>(static_cast<size_t>(nnz));
+    if (nnz) {
+      k_convert<double, float><<<blocks(nnz), kBlock, 0, stream>>>(nnz, dA_val, a_val32);
+      k_convert<double, float><<<blocks(nnz), kBlock, 0, stream>>>(nnz, dT_val, t_val32);
+    }
     for (int q = 0; q < NSLOT32; ++q)
       v32[q] = dalloc<float>(static_cast<size_t>(q >= Y32 && q != C32 && q != LO32 && q != UP32 ? m : n) * k);
     const int src[5] = {C, LO, UP, RL, RU}, dst[5] = {C32, LO32, UP32, RL32, RU32};

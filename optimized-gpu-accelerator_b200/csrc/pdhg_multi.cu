@@ -29,6 +29,7 @@
 #include "pdhg_host_common.h"
 #include "pdhg_kernels.cuh"
 #include "pdhg_prepare.h"
+#include "pdhg_scale.cuh"
 #include "pdhg_cta.cuh"
 #include "pdhg_sched.h"
 #include "pdhg_spmv.cuh"
@@ -214,55 +215,6 @@ __global__ void k_offset_segments(const int64_t* __restrict__ seg, const int32_t
   const int b = blockIdx.x;
   const int32_t o = off[b];
   for (int64_t q = seg[b] + threadIdx.x; q < seg[b + 1]; q += blockDim.x) idx[q] += o;
-}
-
-// ---- Ruiz equilibration and the Pock-Chambolle step on the device
-// (src/lp/scaling.cpp:97-139) over the block-diagonal operator: the rows and
-// columns of different LPs never meet, so this is every LP's own scaling.
-// Each row / column quantity is the host's expression, evaluated in its
-// order ((|a| * c_j) * r_i; maxima are order-free; the 1-norms are summed by
-// one thread in the row's or column's entry order), so the factors are
-// bit-identical to the host's.
-
-// out[r] = max over the entries of row r of (|a| * cscale[col]) * rscale[r]
-// (ROWS: a row of A, scales (rs, cs)); for A^T the roles of the two scale
-// vectors swap, and the product keeps the host's order: (|a| * cs_j) * rs_i.
-template <bool SUM>
-__global__ void k_ruiz_rows(int32_t rows, const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                            const double* __restrict__ val, const double* __restrict__ own,
-                            const double* __restrict__ other, bool own_is_row, double* __restrict__ out) {
-  const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (r >= rows) return;
-  const double so = own[r];
-  double acc = 0.0;
-  for (int32_t q = ptr[r]; q < ptr[r + 1]; ++q) {
-    const double a = fabs(val[q]);
-    // host order: (|a| * cs[j]) * rs[i]
-    const double t = own_is_row ? __dmul_rn(__dmul_rn(a, other[idx[q]]), so) : __dmul_rn(__dmul_rn(a, so), other[idx[q]]);
-    if (SUM)
-      acc = __dadd_rn(acc, t);
-    else
-      acc = (acc < t) ? t : acc;
-  }
-  out[r] = acc;
-}
-
-// s[i] /= sqrt(q[i]) where q[i] > 0.
-__global__ void k_ruiz_update(int32_t len, const double* __restrict__ q, double* __restrict__ s) {
-  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i < len && q[i] > 0) s[i] = __ddiv_rn(s[i], __dsqrt_rn(q[i]));
-}
-
-// a = a * (own[r] * other[idx]) for the entries of row r: the scaled operator
-// value[q] * (R[i] * Cs[j]) (src/lp/scaling.cpp:28-32); for A^T, own = Cs and
-// other = R, and the factor is still R[i] * Cs[j].
-__global__ void k_scale_rows(int32_t rows, const int32_t* __restrict__ ptr, const int32_t* __restrict__ idx,
-                             const double* __restrict__ own, const double* __restrict__ other,
-                             double* __restrict__ val) {
-  const int64_t r = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (r >= rows) return;
-  const double so = own[r];
-  for (int32_t q = ptr[r]; q < ptr[r + 1]; ++q) val[q] = __dmul_rn(val[q], __dmul_rn(so, other[idx[q]]));
 }
 
 // ---- ||A|| of every LP at once (powerIteration, src/pdhg/pdhg.cpp:404-422) ----
@@ -578,7 +530,8 @@ struct MultiEngine {
     const auto ts = Clock::now();
     {
       std::vector<double> rs(M, 1.0), cs(N, 1.0);
-      if (opt.ruiz_iterations > 0 && annz > 0) device_ruiz(opt.ruiz_iterations, opt.pock_chambolle != 0, rs, cs);
+      if (opt.ruiz_iterations > 0 && annz > 0)
+        device_ruiz_factors(stream, device, viewA(), viewAT(), opt.ruiz_iterations, opt.pock_chambolle != 0, rs, cs);
       const bool rescale = opt.rescale_objective_and_bounds != 0;
       parallel_lps([&](int b) {
         const b2p_lp& l = lps[b];
@@ -590,11 +543,7 @@ struct MultiEngine {
         std::copy(P[b].R.begin(), P[b].R.end(), R.begin() + roff[b]);
         std::copy(P[b].Cs.begin(), P[b].Cs.end(), Cs.begin() + coff[b]);
       }
-      const double* dR = upload(R);
-      const double* dC = upload(Cs);
-      if (M > 0) k_scale_rows<<<blocks(M), kBlock, 0, stream>>>(M, dA_ptr, dA_idx, dR, dC, dA_val);
-      if (N > 0) k_scale_rows<<<blocks(N), kBlock, 0, stream>>>(N, dT_ptr, dT_idx, dC, dR, dT_val);
-      B2P_CUDA(cudaGetLastError());
+      device_scale_operators(stream, device, viewA(), viewAT(), dA_val, dT_val, R, Cs);
     }
     stats.prepare_seconds += seconds_since(ts);
     parallel_lps(fill);
@@ -638,35 +587,6 @@ struct MultiEngine {
     stats.setup_seconds = seconds_since(t0);
     stats.kernel_mode = B2P_KERNELS_FUSED;
     stats.precision_used = B2P_PRECISION_FP64;
-  }
-
-  // Unrounded Ruiz (+ Pock-Chambolle) factors of every LP on the device,
-  // from the raw operators (ruiz_impl in pdhg_prepare.cpp is the host form).
-  void device_ruiz(int iterations, bool pock_chambolle, std::vector<double>& rs, std::vector<double>& cs) {
-    double* d_rs = dalloc<double>(M);
-    double* d_cs = dalloc<double>(N);
-    double* d_rq = dalloc<double>(M);
-    double* d_cq = dalloc<double>(N);
-    B2P_CUDA(cudaMemcpyAsync(d_rs, rs.data(), sizeof(double) * M, cudaMemcpyHostToDevice, stream));
-    B2P_CUDA(cudaMemcpyAsync(d_cs, cs.data(), sizeof(double) * N, cudaMemcpyHostToDevice, stream));
-    auto pass = [&](bool sum) {
-      // columns: (|a| * cs_j) * rs_i over A^T's row j; rows: (|a| * cs_j) * rs_i over A's row i
-      if (sum) {
-        k_ruiz_rows<true><<<blocks(N), kBlock, 0, stream>>>(N, dT_ptr, dT_idx, dT_val, d_cs, d_rs, false, d_cq);
-        k_ruiz_rows<true><<<blocks(M), kBlock, 0, stream>>>(M, dA_ptr, dA_idx, dA_val, d_rs, d_cs, true, d_rq);
-      } else {
-        k_ruiz_rows<false><<<blocks(N), kBlock, 0, stream>>>(N, dT_ptr, dT_idx, dT_val, d_cs, d_rs, false, d_cq);
-        k_ruiz_rows<false><<<blocks(M), kBlock, 0, stream>>>(M, dA_ptr, dA_idx, dA_val, d_rs, d_cs, true, d_rq);
-      }
-      k_ruiz_update<<<blocks(M), kBlock, 0, stream>>>(M, d_rq, d_rs);
-      k_ruiz_update<<<blocks(N), kBlock, 0, stream>>>(N, d_cq, d_cs);
-    };
-    for (int it = 0; it < iterations; ++it) pass(false);
-    if (pock_chambolle) pass(true);
-    B2P_CUDA(cudaGetLastError());
-    B2P_CUDA(cudaMemcpyAsync(rs.data(), d_rs, sizeof(double) * M, cudaMemcpyDeviceToHost, stream));
-    B2P_CUDA(cudaMemcpyAsync(cs.data(), d_cs, sizeof(double) * N, cudaMemcpyDeviceToHost, stream));
-    B2P_CUDA(cudaStreamSynchronize(stream));
   }
 
   // ||A|| of every LP on the device (1.01 x the power-iteration estimate, as
