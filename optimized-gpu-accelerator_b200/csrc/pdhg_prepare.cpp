@@ -166,13 +166,6 @@ void ruiz_impl(int32_t m, int32_t n, const int32_t* start, const int32_t* index,
 
 }  // namespace
 
-void ruiz_scaling(int32_t m, int32_t n, const int32_t* start, const int32_t* index, const double* value,
-                  int iterations, bool pock_chambolle, std::vector<double>& rs, std::vector<double>& cs,
-                  bool parallel) {
-  const bool par = parallel && start[n] >= kParallelNnz;
-  ruiz_impl(m, n, start, index, value, iterations, pock_chambolle, rs, cs, row_map(m, n, start, index, par), par);
-}
-
 // ||A||_2 estimate: 40 steps of x <- A^T A x / ||A^T A x|| and sqrt of the
 // last norm (src/pdhg/pdhg.cpp:404-422), with the scatter-order products of
 // SparseMatrix::multiply / multiplyTranspose (src/core/sparse.cpp:67-82).

@@ -63,10 +63,6 @@ void finish_scaling(Prepared& P, const double* rs, const double* cs, const doubl
 
 double pow2_round(double v);
 
-void ruiz_scaling(int32_t m, int32_t n, const int32_t* start, const int32_t* index, const double* value,
-                  int iterations, bool pock_chambolle, std::vector<double>& row_scale, std::vector<double>& col_scale,
-                  bool parallel = false);
-
 double power_iteration(int32_t m, int32_t n, const int32_t* start, const int32_t* index, const double* value,
                        int iters);
 
