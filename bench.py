@@ -352,11 +352,11 @@ def run_router(args, rank, world):
                      **{f"status_{e}": stats[e] for e in R.ENGINES}, **rec.features})
     val = R.validate(records, tolerance=tol)
     W = R.fit(records)
-    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-    R.write_model(os.path.join(ROOT, "gpurun_out", "router_model_b200.json"), W, len(records),
+    os.makedirs(args.router_out, exist_ok=True)
+    R.write_model(os.path.join(args.router_out, "router_model_b200.json"), W, len(records),
                   note=f"fitted on {len(records)} seeded LPs timed on one B200 and {threads} host threads; "
                        f"time limit {limit:g} s, rel KKT {tol:g} for the PDHG engines")
-    with open(os.path.join(ROOT, "gpurun_out", "router_runs.json"), "w") as fh:
+    with open(os.path.join(args.router_out, "router_runs.json"), "w") as fh:
         json.dump(rows, fh, indent=1)
     line = {"metric": ROUTER_METRIC, "value": val["router_held_out"]["geo_mean_regret"], "unit": "x",
             "n_gpus": 1, "steps": 1, "warmup": 1, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
@@ -617,6 +617,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["lp", "family", "multi", "sweep", "router"], default="lp")
     ap.add_argument("--router-limit", type=float, default=3.0, help="router: time limit per engine and LP (s)")
+    ap.add_argument("--router-out", default="router_calibration",
+                    help="router: folder for the fitted model and the per-LP timings")
     ap.add_argument("--cases", type=int, default=256, help="sweep: cases in the shared-A batch")
     ap.add_argument("--sweep-iters", type=int, default=640, help="sweep: PDHG iterations per step")
     ap.add_argument("--instances", type=int, default=256, help="multi: LPs in the batch")
