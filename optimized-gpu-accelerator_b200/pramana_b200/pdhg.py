@@ -144,7 +144,9 @@ def _lp_struct(lp: Model):
     keep = []
 
     def p(a, ctype):
-        a = np.ascontiguousarray(a)
+        # a no-op for the arrays Model already holds; a copy if a field was
+        # replaced by one of another dtype after construction
+        a = np.ascontiguousarray(a, dtype=np.int32 if ctype is C.c_int32 else np.float64)
         keep.append(a)
         return a.ctypes.data_as(C.POINTER(ctype))
 

@@ -157,6 +157,28 @@ def solve(lp, lib: str = "oracle", cases=None, **opts) -> list[OracleResult] | O
     return out if cases is not None else out[0]
 
 
+def load_mps(path: str, presolve: bool = True):
+    """The LP that the reference's solve() hands to its LP engines for an MPS
+    file: read by its own reader, in minimisation form and, with presolve,
+    reduced by its Presolver (src/api/solver.cpp:251, 302-333; ref build).
+    Returns (Model, rows removed, columns removed)."""
+    from pramana_b200.model import Model
+    h = _load("ref")
+    dims = np.zeros(5, dtype=np.int32)
+    off = C.c_double()
+    if h.ref_load_mps(path.encode(), C.c_int(1 if presolve else 0), _ip(dims), C.byref(off)) != 0:
+        h.ref_last_error.restype = C.c_char_p
+        raise RuntimeError("reference MPS load failed: " + h.ref_last_error().decode())
+    m, n, nnz = int(dims[0]), int(dims[1]), int(dims[2])
+    start, index = np.zeros(n + 1, dtype=np.int32), np.zeros(nnz, dtype=np.int32)
+    value, cost, cl, cu = np.zeros(nnz), np.zeros(n), np.zeros(n), np.zeros(n)
+    rl, ru = np.zeros(m), np.zeros(m)
+    h.ref_model_arrays(_ip(start), _ip(index), _dp(value), _dp(cost), _dp(cl), _dp(cu), _dp(rl), _dp(ru))
+    lp = Model(num_rows=m, num_cols=n, start=start, index=index, value=value, col_cost=cost, col_lower=cl,
+               col_upper=cu, row_lower=rl, row_upper=ru, obj_offset=off.value, name=os.path.basename(path))
+    return lp, int(dims[3]), int(dims[4])
+
+
 def safe_dual_bound(lp, y, col_lower=None, col_upper=None, full: bool = False):
     """The reference's outward-rounded Neumaier-Shcherbina bound (needs the ref
     build), plus the objective offset; with full=True the whole SafeBoundResult

@@ -16,6 +16,9 @@
 //   - the router's features and decision (src/router/router.cpp) and timed
 //     solves by the dual simplex and the interior-point method (src/ipm/ipm.cpp),
 //     the CPU engines a router calibration compares the GPU engine with
+//   - the LP that solve() hands to its LP engines for an MPS file: readMps
+//     (src/io/mps.cpp), minimisation form, Presolver (src/presolve/presolve.cpp),
+//     the inputs of the reference's published PDHG runs
 // The GPU path of the reference is switched off (PRAMANA_DISABLE_GPU) so that
 // loading this library never brings up a CUDA context or NVRTC.
 #include <cstdint>
@@ -27,12 +30,14 @@
 
 #include "cert/certifier.h"
 #include "core/model.h"
+#include "io/mps.h"
 #include "ipm/ipm.h"
 #include "lp/crossover.h"
 #include "lp/scaling.h"
 #include "lp/simplex.h"
 #include "mip/propagate.h"
 #include "pdhg/pdhg.h"
+#include "presolve/presolve.h"
 #include "router/router.h"
 #include "util/log.h"
 #include "util/parallel.h"
@@ -62,6 +67,8 @@ Model buildModel(int m, int n, const int* start, const int* index, const double*
   lp.colType.assign(n, VarType::Continuous);
   return lp;
 }
+
+Model gLoaded;  // the model of the last ref_load_mps, until ref_model_arrays copies it out
 
 std::vector<double> vecOrEmpty(const double* p, int len) {
   return p ? std::vector<double>(p, p + len) : std::vector<double>();
@@ -391,6 +398,53 @@ int ref_timed_solve(int engine, int m, int n, const int* start, const int* index
     gErr = e.what();
     return 1;
   }
+}
+
+// The LP that pramana::solve hands to an LP engine for the MPS file at
+// `path` (src/api/solver.cpp:251, 302-333): readMps, Model::toMinimization
+// and, when `presolve` is set, Presolver::run(minModel, mip) whose reduced
+// model is used when the status is Reduced or Empty.  dims = m, n, nnz,
+// rows removed, columns removed; the arrays follow from ref_model_arrays.
+int ref_load_mps(const char* path, int presolve, int* dims, double* offset) {
+  try {
+    Log::setLevel(LogLevel::Error);
+    const Model input = readMps(path);
+    input.validate();
+    const Model minModel = input.toMinimization();
+    gLoaded = minModel;
+    dims[3] = dims[4] = 0;
+    if (presolve) {
+      Presolver pre;
+      const PresolveStatus ps = pre.run(minModel, input.isMip());
+      if (ps == PresolveStatus::Reduced || ps == PresolveStatus::Empty) {
+        gLoaded = pre.reduced();
+        dims[3] = pre.stats().rowsRemoved;
+        dims[4] = pre.stats().colsRemoved;
+      }
+    }
+    dims[0] = gLoaded.numRows();
+    dims[1] = gLoaded.numCols();
+    dims[2] = gLoaded.A.nnz();
+    *offset = gLoaded.objOffset;
+    return 0;
+  } catch (std::exception& e) {
+    gErr = e.what();
+    return 1;
+  }
+}
+
+int ref_model_arrays(int* start, int* index, double* value, double* cost, double* colLower, double* colUpper,
+                     double* rowLower, double* rowUpper) {
+  const Model& lp = gLoaded;
+  std::memcpy(start, lp.A.start.data(), sizeof(int) * lp.A.start.size());
+  std::memcpy(index, lp.A.index.data(), sizeof(int) * lp.A.index.size());
+  std::memcpy(value, lp.A.value.data(), sizeof(double) * lp.A.value.size());
+  std::memcpy(cost, lp.colCost.data(), sizeof(double) * lp.colCost.size());
+  std::memcpy(colLower, lp.colLower.data(), sizeof(double) * lp.colLower.size());
+  std::memcpy(colUpper, lp.colUpper.data(), sizeof(double) * lp.colUpper.size());
+  std::memcpy(rowLower, lp.rowLower.data(), sizeof(double) * lp.rowLower.size());
+  std::memcpy(rowUpper, lp.rowUpper.data(), sizeof(double) * lp.rowUpper.size());
+  return 0;
 }
 
 }  // extern "C"

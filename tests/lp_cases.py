@@ -1,5 +1,7 @@
 """Small deterministic LPs for parity tests (every bound type the PDHG path
 distinguishes, src/pdhg/pdhg.cpp:166-197 and 506-530)."""
+import os
+
 import numpy as np
 
 from pramana_b200.model import LpCase, Model
@@ -185,3 +187,21 @@ def read_mps(path: str) -> Model:
     offset = -rhs.get(obj, 0.0) if obj else 0.0
     return Model(num_rows=m, num_cols=n, start=start, index=rr, value=vv, col_cost=c, col_lower=lo, col_upper=up,
                  row_lower=rl, row_upper=ru, obj_offset=offset, name=path)
+
+
+GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+PLANS = ("plan_6x4", "plan_10x12", "plan_20x12", "plan_20x52", "plan_30x52", "plan_40x104")
+
+
+def load_plan(name: str):
+    """A refinery planning LP of the reference's published PDHG runs, as
+    solve() hands it to solvePdhg (presolved, minimisation form), and the
+    published telemetry of those runs keyed by run ("pdhg-cpu_raw1e-4",
+    "pdhg-gpu_raw1e-4", "pdhg-gpu_raw1e-6"); fixtures made by
+    tests/golden/make_plan_golden.py."""
+    import json
+    d = np.load(os.path.join(GOLDEN_DIR, name + ".npz"))
+    lp = Model(num_rows=int(d["num_rows"]), num_cols=int(d["num_cols"]), start=d["start"], index=d["index"],
+               value=d["value"], col_cost=d["col_cost"], col_lower=d["col_lower"], col_upper=d["col_upper"],
+               row_lower=d["row_lower"], row_upper=d["row_upper"], obj_offset=float(d["obj_offset"]), name=name)
+    return lp, json.loads(str(d["published"]))

@@ -143,3 +143,39 @@ def test_afiro_batch_pin(oracle_mod):
                       method="highs")
         assert r.status == 1
         assert abs(r.objective - (ref.fun + lp.obj_offset)) <= 1e-5 * (1 + abs(ref.fun))
+
+
+# ---- the reference's published PDHG runs on its refinery planning models ----
+# (results/gpu/plan_*.pdhg-{cpu,gpu}_raw1e-{4,6}.json: solve() -> presolve ->
+# solvePdhg on the reduced LP; fixtures by tests/golden/make_plan_golden.py)
+
+PLAN_RUNS_CPU = [(p, "pdhg-cpu_raw1e-4") for p in lp_cases.PLANS[:5]] + \
+                [(p, "pdhg-gpu_raw1e-6") for p in lp_cases.PLANS[:2]]
+
+
+@pytest.mark.parametrize("plan,run", PLAN_RUNS_CPU)
+def test_oracle_reproduces_published_plan_runs(oracle_mod, plan, run):
+    """The C restatement reproduces the reference's published runs: the same
+    iteration and restart counts (the reference's GPU and CPU runs agree on
+    them) and the same spectral-norm estimate, bit for bit; against its
+    published CPU runs (16 threads, whose chunked reductions round a few sums
+    differently from one thread on the larger plans) the objective within
+    1e-12 and the relative KKT within 1e-9 relative, bit-identical on the
+    smaller plans; against its GPU runs (another summation order over 16k+
+    iterations) within 1e-12 and 1e-7."""
+    lp, pub = lp_cases.load_plan(plan)
+    p = pub[run]
+    r = oracle_mod.solve(lp, "oracle", tolerance=p["tolerance"])
+    st = oracle_mod.solve.last_stats
+    assert r.status == 1
+    assert st["iterations"] == p["iterations"] and st["restarts"] == p["restarts"]
+    assert st["spectral_norm"] == p["spectral_norm_estimate"]
+    if "cpu" in run:
+        assert abs(r.relative_kkt - p["relative_kkt"]) <= 1e-9 * p["relative_kkt"]
+        assert abs(r.objective - p["objective"]) <= 1e-12 * abs(p["objective"])
+        assert abs(st["primal_weight"] - p["primal_weight"]) <= 1e-12 * p["primal_weight"]
+        if plan in ("plan_6x4", "plan_10x12", "plan_20x12"):
+            assert r.objective == p["objective"] and r.relative_kkt == p["relative_kkt"]
+    else:
+        assert abs(r.relative_kkt - p["relative_kkt"]) <= 1e-7 * p["relative_kkt"]
+        assert abs(r.objective - p["objective"]) <= 1e-12 * abs(p["objective"])
