@@ -1,4 +1,4 @@
-"""Regenerates the refinery-plan fixtures in this folder: the LPs of the
+"""Regenerates the refinery-plan fixtures in plans/: the LPs of the
 reference's published PDHG runs, with the figures it published for them.
 
 The reference ships generated refinery planning models (data/gen/plan_*.mps)
@@ -53,7 +53,8 @@ def main():
             published[run]["device"] = t["pdhg"].get("device", "")
         d["published"] = json.dumps(published)
         d["rows_removed"] = rows_removed
-        np.savez_compressed(os.path.join(HERE, name + ".npz"), **d)
+        os.makedirs(os.path.join(HERE, "plans"), exist_ok=True)
+        np.savez_compressed(os.path.join(HERE, "plans", name + ".npz"), **d)
         print(name, lp.num_rows, lp.num_cols, len(lp.value),
               {r: (p["iterations"], p["restarts"]) for r, p in published.items()})
 

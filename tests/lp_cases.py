@@ -200,7 +200,7 @@ def load_plan(name: str):
     "pdhg-gpu_raw1e-4", "pdhg-gpu_raw1e-6"); fixtures made by
     tests/golden/make_plan_golden.py."""
     import json
-    d = np.load(os.path.join(GOLDEN_DIR, name + ".npz"))
+    d = np.load(os.path.join(GOLDEN_DIR, "plans", name + ".npz"))
     lp = Model(num_rows=int(d["num_rows"]), num_cols=int(d["num_cols"]), start=d["start"], index=d["index"],
                value=d["value"], col_cost=d["col_cost"], col_lower=d["col_lower"], col_upper=d["col_upper"],
                row_lower=d["row_lower"], row_upper=d["row_upper"], obj_offset=float(d["obj_offset"]), name=name)
