@@ -190,7 +190,7 @@ def read_mps(path: str) -> Model:
 
 
 GOLDEN_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-PLANS = ("plan_6x4", "plan_10x12", "plan_20x12", "plan_20x52", "plan_30x52", "plan_40x104")
+PLANS = ("plan_6x4", "plan_10x12", "plan_20x12", "plan_20x52", "plan_30x52", "plan_40x104", "plan_60x156")
 
 
 def load_plan(name: str):
