@@ -454,6 +454,61 @@ def run_plan(args, rank, world):
     return 0
 
 
+def run_families(args, rank, world):
+    """--workload families: the batched-PDHG leg of the reference's published
+    repeated-solve experiment (compareFamilyStrategies; tests/golden/families/,
+    made by tests/golden/make_family_golden.py): per family, K crude-price or
+    crude-availability cases of a refinery plan in one solvePdhgBatch call
+    (1e-6, at most 200,000 iterations) from host arrays, then the
+    outward-rounded dual bound over constraint-implied column bounds for every
+    solved case, timed together as the reference times its strategy; the
+    published figures of the same runs (other hardware) ride along."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import lp_cases
+    from pramana_b200 import pdhg
+
+    torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    rows = {}
+    launches = 0
+    with ClockSampler(dev) as clk:
+        for fam in lp_cases.FAMILIES:
+            lp, cases, exact, pub = lp_cases.load_family(fam)
+            po = pdhg.PdhgOptions(tolerance=1e-6, maxIterations=200000, device=dev)
+            times = []
+            for s in range(args.warmup + args.steps):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                st = pdhg.PdhgStats()
+                rs = pdhg.solvePdhgBatch(lp, cases, po, batchStats=st)
+                cert = lp_cases.family_certified(lp, cases, rs, pdhg.safeDualBound, pdhg.impliedBounds)
+                if s >= args.warmup:
+                    times.append(time.perf_counter() - t0)
+                    launches += st.kernelLaunches
+            solved = [b for b, r in enumerate(rs) if r.status == "Optimal"]
+            err = max((abs(rs[b].objective - exact[b]) / max(1.0, abs(exact[b])) for b in solved), default=0.0)
+            rows[fam] = {"seconds": statistics.mean(times), "kernel_seconds": st.kernelSeconds,
+                         "iterations": st.iterations, "cases": len(cases), "solved": len(solved), "certified": cert,
+                         "max_relative_error": err,
+                         "published_gpu": {k: pub["gpu"][k] for k in ("seconds", "iterations", "solved", "certified",
+                                                                      "max_relative_error")},
+                         "published_cpu_seconds": pub["cpu"]["seconds"], "published_device": pub["device"]}
+    total = sum(r["seconds"] for r in rows.values())
+    line = {"metric": "seconds per batched family solve + safe bounds (reference's repeated-solve experiment)",
+            "value": total, "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "the reference's refinery plans and published parameter grids",
+            "workload": "families",
+            "config": {"workload": "4 published families: plan_10x12 CR03 price / availability (64 cases each), "
+                                   "plan_20x12 CR07 price (64), plan_20x52 CR05 availability (32); 1e-6, "
+                                   "200,000 iterations at most; value = sum over the families"},
+            "families": rows, "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": None}
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def run_sweep(args, rank, world):
     """--workload sweep: 256 cases of the full-size refinery LP (the config-3
     generator: 42,072 rows, 97,344 columns, 748,910 nonzeros, rows and columns
@@ -697,7 +752,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-sample-iters", type=int, default=CPU_SAMPLE_ITERS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["lp", "family", "multi", "sweep", "router", "plan"], default="lp")
+    ap.add_argument("--workload", choices=["lp", "family", "multi", "sweep", "router", "plan", "families"],
+                    default="lp")
     ap.add_argument("--plan", default="plan_60x156", help="plan: which refinery plan of the published runs")
     ap.add_argument("--plan-tol", type=float, default=1e-4, help="plan: relative KKT tolerance (1e-4 or 1e-6)")
     ap.add_argument("--router-limit", type=float, default=3.0, help="router: time limit per engine and LP (s)")
@@ -738,6 +794,8 @@ def main():
         return run_router(args, rank, world)
     if args.workload == "plan":
         return run_plan(args, rank, world)
+    if args.workload == "families":
+        return run_families(args, rank, world)
 
     import torch
     dist = None

@@ -179,6 +179,15 @@ def load_mps(path: str, presolve: bool = True):
     return lp, int(dims[3]), int(dims[4])
 
 
+def loaded_column(name: str):
+    """(index of column `name`, was the file a maximisation) for the model of
+    the last load_mps (ref build)."""
+    h = _load("ref")
+    was_max = C.c_int()
+    j = h.ref_loaded_column(name.encode(), C.byref(was_max))
+    return int(j), bool(was_max.value)
+
+
 def safe_dual_bound(lp, y, col_lower=None, col_upper=None, full: bool = False):
     """The reference's outward-rounded Neumaier-Shcherbina bound (needs the ref
     build), plus the objective offset; with full=True the whole SafeBoundResult

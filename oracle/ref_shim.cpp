@@ -68,7 +68,8 @@ Model buildModel(int m, int n, const int* start, const int* index, const double*
   return lp;
 }
 
-Model gLoaded;  // the model of the last ref_load_mps, until ref_model_arrays copies it out
+Model gLoaded;          // the model of the last ref_load_mps, until ref_model_arrays copies it out
+bool gLoadedMax = false;  // whether that file's objective sense was maximise
 
 std::vector<double> vecOrEmpty(const double* p, int len) {
   return p ? std::vector<double>(p, p + len) : std::vector<double>();
@@ -412,6 +413,7 @@ int ref_load_mps(const char* path, int presolve, int* dims, double* offset) {
     input.validate();
     const Model minModel = input.toMinimization();
     gLoaded = minModel;
+    gLoadedMax = input.sense == ObjSense::Maximize;
     dims[3] = dims[4] = 0;
     if (presolve) {
       Presolver pre;
@@ -431,6 +433,15 @@ int ref_load_mps(const char* path, int presolve, int* dims, double* offset) {
     gErr = e.what();
     return 1;
   }
+}
+
+// Column of the last loaded model named `name` (-1 if none) and whether the
+// file was a maximisation (its costs are negated in the loaded model).
+int ref_loaded_column(const char* name, int* was_max) {
+  *was_max = gLoadedMax ? 1 : 0;
+  for (size_t j = 0; j < gLoaded.colNames.size(); ++j)
+    if (gLoaded.colNames[j] == name) return static_cast<int>(j);
+  return -1;
 }
 
 int ref_model_arrays(int* start, int* index, double* value, double* cost, double* colLower, double* colUpper,

@@ -205,3 +205,54 @@ def load_plan(name: str):
                value=d["value"], col_cost=d["col_cost"], col_lower=d["col_lower"], col_upper=d["col_upper"],
                row_lower=d["row_lower"], row_upper=d["row_upper"], obj_offset=float(d["obj_offset"]), name=name)
     return lp, json.loads(str(d["published"]))
+
+
+FAMILIES = ("plan_10x12_BUY_CR03_0_cost", "plan_10x12_BUY_CR03_0_upper", "plan_20x12_BUY_CR07_3_cost",
+            "plan_20x52_BUY_CR05_10_upper")
+
+
+def load_family(name: str):
+    """The batched-PDHG leg of the reference's published repeated-solve
+    experiment (compareFamilyStrategies, src/parametric/parametric.cpp:483-527):
+    the model in minimisation form without presolve, its K cases (one column's
+    cost or upper bound set to each theta, withParameter + toMinimization,
+    :77-98), the exact optimum of every case and the published figures;
+    fixtures made by tests/golden/make_family_golden.py."""
+    import json
+    d = np.load(os.path.join(GOLDEN_DIR, "families", name + ".npz"))
+    lp = Model(num_rows=int(d["num_rows"]), num_cols=int(d["num_cols"]), start=d["start"], index=d["index"],
+               value=d["value"], col_cost=d["col_cost"], col_lower=d["col_lower"], col_upper=d["col_upper"],
+               row_lower=d["row_lower"], row_upper=d["row_upper"], obj_offset=float(d["obj_offset"]), name=name)
+    col, kind, was_max = int(d["column"]), str(d["kind"]), bool(d["was_max"])
+    cases = []
+    for th in d["thetas"]:
+        if kind == "cost":
+            c = lp.col_cost.copy()
+            c[col] = -th if was_max else th
+            cases.append(LpCase(cost=c))
+        else:
+            u = lp.col_upper.copy()
+            u[col] = th
+            cases.append(LpCase(col_upper=u))
+    return lp, cases, np.asarray(d["exact_objective"]), json.loads(str(d["published"]))
+
+
+def family_certified(lp, cases, results, safe_bound, implied_bounds):
+    """The reference's count of certified cases (parametric.cpp:508-523): the
+    outward-rounded dual bound over constraint-implied column bounds, from the
+    case's row duals, within 1e-4 of its objective.  `safe_bound` and
+    `implied_bounds` are the engine's batched entries."""
+    lo, up = implied_bounds(lp, cases)
+    ok = [r.status == "Optimal" for r in results]
+    cc = []
+    for b, cs in enumerate(cases):
+        cc.append(LpCase(cost=cs.cost, col_lower=lo[b], col_upper=up[b], row_lower=cs.row_lower,
+                         row_upper=cs.row_upper))
+    y = np.concatenate([r.rowDual for r in results])
+    sb = safe_bound(lp, y, cc)
+    n = 0
+    for r, s, good in zip(results, sb, ok):
+        lb = s["bound"] + lp.obj_offset
+        if good and np.isfinite(s["bound"]) and abs(r.objective - lb) <= 1e-4 * (1 + abs(r.objective)):
+            n += 1
+    return n
