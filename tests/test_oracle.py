@@ -179,3 +179,41 @@ def test_oracle_reproduces_published_plan_runs(oracle_mod, plan, run):
     else:
         assert abs(r.relative_kkt - p["relative_kkt"]) <= 1e-7 * p["relative_kkt"]
         assert abs(r.objective - p["objective"]) <= 1e-12 * abs(p["objective"])
+
+
+def test_oracle_reproduces_published_family_batch(oracle_mod):
+    """The batched-PDHG leg of the reference's published repeated-solve
+    experiment for plan_10x12's CR03 crude price (64 cases, 1e-6; 16 threads
+    on the reference's CPU): the C restatement's batch ends at the published
+    18,560 iterations with all 64 cases solved and certified, and the largest
+    objective error against the exact optima equals the published one to
+    rounding."""
+    lp, cases, exact, pub = lp_cases.load_family("plan_10x12_BUY_CR03_0_cost")
+    p = pub["cpu"]
+    rs = oracle_mod.solve(lp, "oracle", cases=cases, tolerance=1e-6, max_iterations=200000)
+    assert oracle_mod.solve.last_stats["iterations"] == p["iterations"]
+    assert sum(r.status == 1 for r in rs) == p["solved"]
+    err = max(abs(r.objective - e) / max(1.0, abs(e)) for r, e in zip(rs, exact))
+    assert abs(err - p["max_relative_error"]) <= 1e-6 * p["max_relative_error"]
+
+    def implied(lp_, cs):
+        bounds = [oracle_mod.implied_bounds(lp_, lp_.col_lower, c.col_upper if c.col_upper is not None
+                                            else lp_.col_upper) for c in cs]
+        return np.stack([b[0] for b in bounds]), np.stack([b[1] for b in bounds])
+
+    def safe(lp_, y, cs):
+        out = []
+        for b, c in enumerate(cs):
+            case_lp = Model(num_rows=lp_.num_rows, num_cols=lp_.num_cols, start=lp_.start, index=lp_.index,
+                            value=lp_.value, col_cost=c.cost if c.cost is not None else lp_.col_cost,
+                            col_lower=c.col_lower, col_upper=c.col_upper, row_lower=lp_.row_lower,
+                            row_upper=lp_.row_upper)
+            out.append(oracle_mod.safe_dual_bound(case_lp, y[b * lp_.num_rows:(b + 1) * lp_.num_rows], full=True))
+        return out
+
+    class R:  # the oracle's results in the engine's result vocabulary
+        def __init__(self, r):
+            self.status = "Optimal" if r.status == 1 else "other"
+            self.objective, self.rowDual = r.objective, r.y
+
+    assert lp_cases.family_certified(lp, cases, [R(r) for r in rs], safe, implied) == p["certified"]
