@@ -509,6 +509,79 @@ def run_families(args, rank, world):
     return 0
 
 
+def run_calibrate(args, rank, world):
+    """--workload calibrate: the reference's PDHG per-iteration calibration
+    (calibrateBandwidth, src/parametric/parametric.cpp:531-585) on this
+    engine: its six random transportation-like LPs (1e3 to 1e6 rows, 8k to 8M
+    nonzeros; generators.calibration_lp), 512 iterations of the plain FP64
+    form each (tolerance 1e-30), seconds per iteration from the device loop
+    and from the host's loop clock, and the reference's "effective GB/s"
+    (24 nnz + 80 (m + n) bytes per iteration).  The reference's CPU PDHG on
+    this host's cores runs a bounded sample of each instance (cpu_baseline);
+    the published laptop figures (tests/golden/calibration_published.json)
+    ride along."""
+    import torch
+    from pramana_b200 import _lib, pdhg
+    from pramana_b200 import generators as G
+
+    torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    with open(os.path.join(ROOT, "tests", "golden", "calibration_published.json")) as f:
+        pub = json.load(f)
+    iters = 512
+    rows = []
+    launches = 0
+    cpu_rows = []
+    threads = os.cpu_count() or 1
+    with ClockSampler(dev) as clk:
+        for k, scale in enumerate(G.CALIBRATION_SCALES):
+            lp = G.calibration_lp(scale)
+            po = pdhg.PdhgOptions(tolerance=1e-30, maxIterations=iters, device=dev, precision=_lib.PRECISION_FP64)
+            eng = pdhg.Engine(lp, po)
+            dev_t, host_t = [], []
+            for s in range(args.warmup + args.steps):
+                eng.solve()
+                st = eng.last_stats
+                if s >= args.warmup:
+                    dev_t.append(st.kernel_seconds / st.iterations)
+                    host_t.append(st.solve_seconds / st.iterations)
+                    launches += st.kernel_launches
+            eng.close()
+            per = statistics.mean(dev_t)
+            model_bytes = 24.0 * lp.nnz + 80.0 * (lp.num_rows + lp.num_cols)
+            p = pub["scales"][k]
+            rows.append({"rows": lp.num_rows, "cols": lp.num_cols, "nnz": lp.nnz,
+                         "seconds_per_iteration": per, "host_loop_seconds_per_iteration": statistics.mean(host_t),
+                         "effective_GBs": model_bytes / per / 1e9,
+                         "published_gpu_seconds_per_iteration": p["gpu_seconds_per_iteration"],
+                         "published_cpu_seconds_per_iteration": p["cpu_seconds_per_iteration"],
+                         "speedup_vs_published_gpu": p["gpu_seconds_per_iteration"] / per})
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        if O.available("ref"):
+            for scale in G.CALIBRATION_SCALES:
+                lp = G.calibration_lp(scale)
+                n_s = 128 if lp.nnz < 1e6 else 32
+                spi, wall, _ = cpu_reference_sample(lp, n_s, threads)
+                cpu_rows.append({"nnz": lp.nnz, "seconds_per_iteration": spi, "sample_iterations": n_s})
+    big = rows[-1]
+    line = {"metric": "PDHG seconds per iteration, the reference's calibration LPs (largest: 8M nonzeros)",
+            "value": big["seconds_per_iteration"], "unit": "s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": big["seconds_per_iteration"] * iters * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "the reference's calibration generator (SplitMix64 seed 7), restated", "workload": "calibrate",
+            "config": {"workload": "6 random transportation-like LPs, 1e3..1e6 rows, 512 iterations each; "
+                                   "value = the 1e6-row instance"},
+            "scales": rows, "published_hardware": {"gpu": pub["gpu"], "cpu_threads": pub["cpu_threads"]},
+            "gpu_launches": launches, "clocks": clk.summary(),
+            "cpu_baseline": ({"value": cpu_rows[-1]["seconds_per_iteration"], "unit": "s", "cores": threads,
+                              "kind": "reference", "sample": "per scale: " + json.dumps(cpu_rows)}
+                             if cpu_rows else None)}
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def run_sweep(args, rank, world):
     """--workload sweep: 256 cases of the full-size refinery LP (the config-3
     generator: 42,072 rows, 97,344 columns, 748,910 nonzeros, rows and columns
@@ -752,8 +825,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-sample-iters", type=int, default=CPU_SAMPLE_ITERS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["lp", "family", "multi", "sweep", "router", "plan", "families"],
-                    default="lp")
+    ap.add_argument("--workload", choices=["lp", "family", "multi", "sweep", "router", "plan", "families",
+                                           "calibrate"], default="lp")
     ap.add_argument("--plan", default="plan_60x156", help="plan: which refinery plan of the published runs")
     ap.add_argument("--plan-tol", type=float, default=1e-4, help="plan: relative KKT tolerance (1e-4 or 1e-6)")
     ap.add_argument("--router-limit", type=float, default=3.0, help="router: time limit per engine and LP (s)")
@@ -796,6 +869,8 @@ def main():
         return run_plan(args, rank, world)
     if args.workload == "families":
         return run_families(args, rank, world)
+    if args.workload == "calibrate":
+        return run_calibrate(args, rank, world)
 
     import torch
     dist = None

@@ -262,3 +262,57 @@ def uneven_family(count: int, nnz_lo: float = 1e4, nnz_hi: float = 2e6, seed: in
         out.append(random_lp(m, 2 * m, 6.4, int(0.6 * m), seed + i, heavy_row_frac=0.01, heavy_nnz_frac=0.10,
                              name=f"c4_s{seed + i}"))
     return out
+
+
+# ---- the reference's per-iteration calibration instances ----------------------
+
+_GOLDEN_GAMMA = np.uint64(0x9E3779B97F4A7C15)
+
+
+def _splitmix64(seed: int, first: int, count: int) -> np.ndarray:
+    """Outputs first .. first+count-1 of the SplitMix64 stream (Steele, Lea and
+    Flood, 2014) started at `seed`: output i mixes seed + (i+1)*gamma with the
+    published finaliser.  The reference's Rng is this generator
+    (src/util/rng.h)."""
+    with np.errstate(over="ignore"):
+        i = np.arange(first + 1, first + count + 1, dtype=np.uint64)
+        z = np.uint64(seed) + i * _GOLDEN_GAMMA
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return z ^ (z >> np.uint64(31))
+
+
+CALIBRATION_SCALES = (1000, 4000, 16000, 64000, 256000, 1000000)
+
+
+def calibration_lp(scale: int) -> Model:
+    """The random transportation-like LP of the reference's PDHG per-iteration
+    calibration (calibrateBandwidth, src/parametric/parametric.cpp:545-563):
+    m = scale rows, n = 2 scale columns, four entries per column at rows
+    below(m) with values 0.5 + uniform(), drawn in column order (row, then
+    value, per entry) from one SplitMix64 stream seeded 7 that runs on across
+    the scales 1e3, 4e3, 1.6e4, 6.4e4, 2.56e5, 1e6 in that order; duplicate
+    entries summed (SparseMatrix::fromTriplets); the costs uniform() - 0.3 are
+    drawn after the entries; 0 <= x <= 10; every row >= 1."""
+    m, n = int(scale), 2 * int(scale)
+    offset = 0
+    for s in CALIBRATION_SCALES[:CALIBRATION_SCALES.index(scale)]:
+        offset += 9 * 2 * s  # 8 draws per column for the entries, 1 for the cost
+    draws = _splitmix64(7, offset, 8 * n)
+    rows = (draws[0::2] % np.uint64(m)).astype(np.int64)
+    vals = 0.5 + (draws[1::2] >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+    cols = np.repeat(np.arange(n, dtype=np.int64), 4)
+    order = np.lexsort((rows, cols))
+    rows, cols, vals = rows[order], cols[order], vals[order]
+    first = np.ones(len(rows), dtype=bool)
+    first[1:] = (rows[1:] != rows[:-1]) | (cols[1:] != cols[:-1])
+    group = np.cumsum(first) - 1
+    merged = np.zeros(int(first.sum()))
+    np.add.at(merged, group, vals)
+    rows, cols = rows[first], cols[first]
+    start = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(np.bincount(cols, minlength=n), out=start[1:])
+    cost = (_splitmix64(7, offset + 8 * n, n) >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0) - 0.3
+    return Model(num_rows=m, num_cols=n, start=start, index=rows, value=merged, col_cost=cost,
+                 col_lower=np.zeros(n), col_upper=np.full(n, 10.0), row_lower=np.ones(m),
+                 row_upper=np.full(m, np.inf), name=f"calib_{scale}")
