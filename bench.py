@@ -153,10 +153,63 @@ def cpu_reference_sample(lp, iters: int, threads: int):
     return st["solve_seconds"] / iters, wall, st
 
 
+def run_reference_gpu(args):
+    """--impl reference --reference-backend gpu: the reference's own GPU
+    backend (its NVRTC-compiled FP64 kernels, compute_90 PTX run through the
+    driver's JIT) on this GPU, full solves of config-2 to 1e-6 (or, with
+    --workload plan, of the plan to --plan-tol): the same-hardware comparison
+    for this engine.  Not the contract's reference arm, which is the CPU."""
+    from oracle import oracle as O
+    if not O.available("ref"):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libpramana_ref.so was not built"}))
+        return 0
+    from pramana_b200 import generators as G
+    O.solve(G.config1(1), "ref", backend="gpu", tolerance=1e-30, max_iterations=1)
+    if O.solve.last_stats["backend"] != "gpu":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's GPU backend did not come up "
+                                                               "(it fell back to its CPU backend)"}))
+        return 0
+    if args.workload == "plan":
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import lp_cases
+        lp, _ = lp_cases.load_plan(args.plan)
+        tol, name = args.plan_tol, f"{args.plan} after presolve, to rel KKT {args.plan_tol:g}"
+    else:
+        lp, tol, name = G.config2(SEED), TOL, workload_config(G.config2(SEED))["workload"]
+    loops, walls, kern = [], [], []
+    for s in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        r = O.solve(lp, "ref", backend="gpu", tolerance=tol)
+        wall = time.perf_counter() - t0
+        st = O.solve.last_stats
+        if st["backend"] != "gpu":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference's GPU backend did not come up "
+                                                                   "(it fell back to its CPU backend)"}))
+            return 0
+        if s >= args.warmup:
+            loops.append(st["solve_seconds"])
+            walls.append(wall)
+            kern.append(st["kernel_seconds"])
+    value = statistics.mean(loops)
+    line = {"metric": METRIC if args.workload != "plan" else f"time to rel KKT {tol:g} (s), reference refinery plan",
+            "value": value, "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "as the engine's arm", "config": {"workload": name},
+            "impl": "reference", "reference_backend": "gpu (the reference's NVRTC kernels, compute_90 PTX, driver JIT)",
+            "iterations": st["iterations"], "restarts": st["restarts"], "relative_kkt": r.relative_kkt,
+            "kernel_seconds": statistics.mean(kern),
+            "e2e": {"value": statistics.mean(walls), "unit": "s", "h2d_bytes_per_step": None,
+                    "d2h_bytes_per_step": None}}
+    print(json.dumps(line))
+    return 0
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's own CPU PDHG on this host's cores."""
     if rank != 0:
         return 0
+    if args.reference_backend == "gpu":
+        return run_reference_gpu(args)
     from pramana_b200 import generators as G
     from oracle import oracle as O
     lp = G.config2(SEED)
@@ -823,6 +876,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--reference-backend", choices=["cpu", "gpu"], default="cpu",
+                    help="reference arm: its CPU PDHG (the contract's arm) or its own GPU backend on this GPU")
     ap.add_argument("--cpu-sample-iters", type=int, default=CPU_SAMPLE_ITERS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["lp", "family", "multi", "sweep", "router", "plan", "families",

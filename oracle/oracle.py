@@ -114,10 +114,12 @@ def default_options(**kw) -> Options:
     return o
 
 
-def solve(lp, lib: str = "oracle", cases=None, **opts) -> list[OracleResult] | OracleResult:
-    """Run solvePdhg (cases is None) or solvePdhgBatch (list of LpCase-like objects)."""
+def solve(lp, lib: str = "oracle", cases=None, backend: str = "cpu", **opts) -> list[OracleResult] | OracleResult:
+    """Run solvePdhg (cases is None) or solvePdhgBatch (list of LpCase-like
+    objects).  backend="gpu" (ref build only) runs the reference's own GPU
+    backend; last_stats["backend"] says which backend the reference used."""
     h = _load(lib)
-    fn = h.oracle_pdhg_solve if lib == "oracle" else h.ref_pdhg_solve
+    fn = h.oracle_pdhg_solve if lib == "oracle" else (h.ref_pdhg_solve_gpu if backend == "gpu" else h.ref_pdhg_solve)
     m, n = lp.num_rows, lp.num_cols
     o = default_options(**opts)
     k = 0 if cases is None else len(cases)
@@ -154,6 +156,11 @@ def solve(lp, lib: str = "oracle", cases=None, **opts) -> list[OracleResult] | O
                         res[b].relative_kkt, x[b * n:(b + 1) * n].copy(), y[b * m:(b + 1) * m].copy())
            for b in range(kk)]
     solve.last_stats = {f: getattr(st, f) for f, _ in Stats._fields_}
+    if lib == "ref":
+        h.ref_last_backend.restype = C.c_char_p
+        h.ref_last_kernel_seconds.restype = C.c_double
+        solve.last_stats["backend"] = h.ref_last_backend().decode()
+        solve.last_stats["kernel_seconds"] = h.ref_last_kernel_seconds()
     return out if cases is not None else out[0]
 
 

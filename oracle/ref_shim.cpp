@@ -119,14 +119,23 @@ void ref_set_threads(int n) {
 int ref_threads() { return ThreadPool::instance().threads(); }
 
 // cost/colLower/... of case b: cases_x[b] (NULL = base model's vector).
-int ref_pdhg_solve(int m, int n, const int* start, const int* index, const double* value, const double* cost,
-                   const double* colLower, const double* colUpper, const double* rowLower, const double* rowUpper,
-                   double offset, int k, const double* const* caseCost, const double* const* caseColLower,
-                   const double* const* caseColUpper, const double* const* caseRowLower,
-                   const double* const* caseRowUpper, const ref_options* o, double* xOut, double* yOut,
-                   ref_case_result* res, ref_stats* st) {
+}  // extern "C"
+
+namespace {
+std::string gBackend;        // backend of the last solve ("cpu" / "gpu")
+double gKernelSeconds = 0;   // its PdhgStats::kernelSeconds
+
+int solve_impl(bool gpu, int m, int n, const int* start, const int* index, const double* value, const double* cost,
+               const double* colLower, const double* colUpper, const double* rowLower, const double* rowUpper,
+               double offset, int k, const double* const* caseCost, const double* const* caseColLower,
+               const double* const* caseColUpper, const double* const* caseRowLower,
+               const double* const* caseRowUpper, const ref_options* o, double* xOut, double* yOut,
+               ref_case_result* res, ref_stats* st) {
   try {
-    setenv("PRAMANA_DISABLE_GPU", "1", 1);
+    if (gpu)
+      unsetenv("PRAMANA_DISABLE_GPU");
+    else
+      setenv("PRAMANA_DISABLE_GPU", "1", 1);
     Log::setLevel(LogLevel::Error);
     Model lp = buildModel(m, n, start, index, value, cost, colLower, colUpper, rowLower, rowUpper, offset);
     PdhgOptions po;
@@ -137,7 +146,7 @@ int ref_pdhg_solve(int m, int n, const int* start, const int* index, const doubl
     po.pockChambolle = o->pock_chambolle != 0;
     po.rescaleObjectiveAndBounds = o->rescale != 0;
     po.reflection = o->reflection;
-    po.useGpu = false;
+    po.useGpu = gpu;
     Deadline dl(o->time_limit);
     std::vector<PdhgResult> rr;
     PdhgStats bst;
@@ -177,12 +186,45 @@ int ref_pdhg_solve(int m, int n, const int* start, const int* index, const doubl
       st->dual_residual = bst.dualResidual;
       st->gap = bst.gap;
     }
+    gBackend = bst.backend;
+    gKernelSeconds = bst.kernelSeconds;
     return 0;
   } catch (std::exception& e) {
     gErr = e.what();
     return 1;
   }
 }
+}  // namespace
+
+extern "C" {
+
+// solvePdhg / solvePdhgBatch on the reference's multithreaded CpuBackend.
+int ref_pdhg_solve(int m, int n, const int* start, const int* index, const double* value, const double* cost,
+                   const double* colLower, const double* colUpper, const double* rowLower, const double* rowUpper,
+                   double offset, int k, const double* const* caseCost, const double* const* caseColLower,
+                   const double* const* caseColUpper, const double* const* caseRowLower,
+                   const double* const* caseRowUpper, const ref_options* o, double* xOut, double* yOut,
+                   ref_case_result* res, ref_stats* st) {
+  return solve_impl(false, m, n, start, index, value, cost, colLower, colUpper, rowLower, rowUpper, offset, k,
+                    caseCost, caseColLower, caseColUpper, caseRowLower, caseRowUpper, o, xOut, yOut, res, st);
+}
+
+// The same on the reference's own GpuBackend (its NVRTC-compiled kernels,
+// src/pdhg/kernels.cpp, through its driver-API context), where a GPU and
+// NVRTC are present; the reference falls back to its CPU backend otherwise,
+// which ref_last_backend reports.
+int ref_pdhg_solve_gpu(int m, int n, const int* start, const int* index, const double* value, const double* cost,
+                       const double* colLower, const double* colUpper, const double* rowLower,
+                       const double* rowUpper, double offset, int k, const double* const* caseCost,
+                       const double* const* caseColLower, const double* const* caseColUpper,
+                       const double* const* caseRowLower, const double* const* caseRowUpper, const ref_options* o,
+                       double* xOut, double* yOut, ref_case_result* res, ref_stats* st) {
+  return solve_impl(true, m, n, start, index, value, cost, colLower, colUpper, rowLower, rowUpper, offset, k,
+                    caseCost, caseColLower, caseColUpper, caseRowLower, caseRowUpper, o, xOut, yOut, res, st);
+}
+
+const char* ref_last_backend() { return gBackend.c_str(); }
+double ref_last_kernel_seconds() { return gKernelSeconds; }
 
 // Outward-rounded lower bound on min c^T x over the given boxes, valid for any y.
 // extra (optional): maxDualInfeasibility, rowProjection, costPerturbation
