@@ -169,6 +169,8 @@ def run_reference_gpu(args):
         print(json.dumps({"impl": "reference", "unavailable": "the reference's GPU backend did not come up "
                                                                "(it fell back to its CPU backend)"}))
         return 0
+    if args.workload in ("families", "calibrate"):
+        return run_reference_gpu_sets(args, O, G)
     if args.workload == "plan":
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import lp_cases
@@ -201,6 +203,43 @@ def run_reference_gpu(args):
             "e2e": {"value": statistics.mean(walls), "unit": "s", "h2d_bytes_per_step": None,
                     "d2h_bytes_per_step": None}}
     print(json.dumps(line))
+    return 0
+
+
+def run_reference_gpu_sets(args, O, G):
+    """The reference's GPU backend on the published families (one batched
+    solve per family, 1e-6, 200,000 iterations at most) or on the six
+    calibration LPs (512 iterations each): loop seconds, wall seconds and
+    iterations per item, for the same-hardware comparison."""
+    items = []
+    if args.workload == "families":
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import lp_cases
+        for fam in lp_cases.FAMILIES:
+            lp, cases, _, _ = lp_cases.load_family(fam)
+            loops, walls = [], []
+            for s in range(args.warmup + args.steps):
+                t0 = time.perf_counter()
+                rs = O.solve(lp, "ref", cases=cases, backend="gpu", tolerance=1e-6, max_iterations=200000)
+                if s >= args.warmup:
+                    walls.append(time.perf_counter() - t0)
+                    loops.append(O.solve.last_stats["solve_seconds"])
+            items.append({"family": fam, "loop_seconds": statistics.mean(loops), "wall_seconds": statistics.mean(walls),
+                          "iterations": O.solve.last_stats["iterations"],
+                          "solved": sum(r.status == 1 for r in rs), "backend": O.solve.last_stats["backend"]})
+    else:
+        for scale in G.CALIBRATION_SCALES:
+            lp = G.calibration_lp(scale)
+            per = []
+            for s in range(args.warmup + args.steps):
+                O.solve(lp, "ref", backend="gpu", tolerance=1e-30, max_iterations=512)
+                st = O.solve.last_stats
+                if s >= args.warmup:
+                    per.append(st["solve_seconds"] / st["iterations"])
+            items.append({"nnz": lp.nnz, "seconds_per_iteration": statistics.mean(per), "backend": st["backend"]})
+    print(json.dumps({"impl": "reference", "reference_backend": "gpu (the reference's NVRTC kernels, compute_90 PTX, "
+                                                               "driver JIT)", "workload": args.workload,
+                      "steps": args.steps, "warmup": args.warmup, "items": items}))
     return 0
 
 
