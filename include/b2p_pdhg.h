@@ -179,9 +179,11 @@ typedef struct b2p_stats {
   double transfer_seconds; /* host<->device copies */
   int64_t bytes_uploaded, bytes_downloaded, kernel_launches;
   double spectral_norm;
-  /* setup breakdown: host preparation (scaling, CSR, ||A||), allocations and
-   * uploads, and kernel set-up (schedules, resident-form set-up, capture and
-   * instantiation of the CUDA graphs) */
+  /* setup breakdown: prepare = the CSR of A on host threads, then the upload
+   * of A and A^T, the scaling and the ||A|| estimate on the device; upload =
+   * everything after the host structure (uploads, device scaling, case
+   * vectors; overlaps prepare); graph = kernel set-up (schedules,
+   * resident-form set-up, capture and instantiation of the CUDA graphs) */
   double prepare_seconds, upload_seconds, graph_seconds;
   int32_t lanes_per_row_a, lanes_per_row_at; /* schedule used */
   int32_t kernel_mode;                        /* B2P_KERNELS_FUSED or B2P_KERNELS_RESIDENT (batches: FUSED) */
