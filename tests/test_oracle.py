@@ -150,7 +150,7 @@ def test_afiro_batch_pin(oracle_mod):
 # solvePdhg on the reduced LP; fixtures by tests/golden/make_plan_golden.py)
 
 PLAN_RUNS_CPU = [(p, "pdhg-cpu_raw1e-4") for p in lp_cases.PLANS[:5]] + \
-                [(p, "pdhg-gpu_raw1e-6") for p in lp_cases.PLANS[:2]]
+                [(p, "pdhg-gpu_raw1e-6") for p in lp_cases.PLANS[:3]]
 
 
 @pytest.mark.parametrize("plan,run", PLAN_RUNS_CPU)
