@@ -292,8 +292,10 @@ def calibration_lp(scale: int) -> Model:
     below(m) with values 0.5 + uniform(), drawn in column order (row, then
     value, per entry) from one SplitMix64 stream seeded 7 that runs on across
     the scales 1e3, 4e3, 1.6e4, 6.4e4, 2.56e5, 1e6 in that order; duplicate
-    entries summed (SparseMatrix::fromTriplets); the costs uniform() - 0.3 are
-    drawn after the entries; 0 <= x <= 10; every row >= 1."""
+    entries summed (SparseMatrix::fromTriplets; a pair sums identically in
+    either order, a rare triple may differ from the reference's unstable sort
+    in the last bit); the costs uniform() - 0.3 are drawn after the entries;
+    0 <= x <= 10; every row >= 1."""
     m, n = int(scale), 2 * int(scale)
     offset = 0
     for s in CALIBRATION_SCALES[:CALIBRATION_SCALES.index(scale)]:
