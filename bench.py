@@ -30,6 +30,16 @@ MLP trained on the GPU, then --steps held-out batches of --batch members
 solved to certified relative KKT 1e-6 from a cold start, from the nearest
 training solution and from the network's prediction, plus plain FP64
 single-LP solves of a sample of members (the per-instance baseline).
+
+Other workloads (each prints its own line; see their functions):
+  multi      uneven batch of config-2-generator LPs through the multi-LP engine
+  sweep      256 crude-price cases of the full refinery LP as a shared-A batch
+  router     the router's per-engine timings and the refitted model
+  plan       the reference's headline refinery plan (plan_60x156) to 1e-4 / 1e-6
+  families   the batched leg of the reference's published repeated-solve runs
+  calibrate  the reference's six per-iteration calibration LPs
+``--impl reference --reference-backend gpu`` times the reference's own GPU
+backend on this GPU (config-2, or --workload plan / families / calibrate).
 """
 from __future__ import annotations
 
