@@ -23,3 +23,25 @@ def test_calibration_instances_have_published_sizes(k):
     assert (lp.num_rows, lp.num_cols, lp.nnz) == (pub["rows"], pub["cols"], pub["nnz"])
     assert np.all(np.diff(lp.start) <= 4) and np.all(lp.value >= 0.5)
     assert np.all(lp.col_cost >= -0.3) and np.all(lp.col_cost < 0.7)
+
+
+REF_SRC = "/root/reference/src"
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_SRC), reason="reference sources not present")
+def test_splitmix_stream_matches_reference_rng(tmp_path):
+    """The restated stream equals the reference's own Rng (src/util/rng.h,
+    compiled here as the checker) draw for draw, from the start and from an
+    offset, for the seeds its calibration (7) and certifier test (1) use."""
+    import subprocess
+    src = tmp_path / "rng.cpp"
+    src.write_text('#include <cstdio>\n#include <initializer_list>\n#include "util/rng.h"\n'
+                   'int main(){for(unsigned long long s : {7ull, 1ull}){'
+                   'pramana::Rng r(s); for(int i = 0; i < 40; ++i) std::printf("%llu\\n", '
+                   '(unsigned long long)r.next());}}\n')
+    exe = tmp_path / "rng"
+    subprocess.run(["g++", "-std=c++17", f"-I{REF_SRC}", str(src), "-o", str(exe)], check=True)
+    ref = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    ours = [int(v) for seed in (7, 1) for v in G._splitmix64(seed, 0, 40)]
+    assert ours == ref
+    assert [int(v) for v in G._splitmix64(7, 25, 15)] == ref[25:40]
