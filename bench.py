@@ -465,6 +465,8 @@ def run_router(args, rank, world):
             "dtype": "f64", "data": "synthetic (seeded)", "workload": "router",
             "config": {"workload": f"{len(records)} LPs from 4 generator families (random, skewed, refinery, "
                                    f"uneven config-2), 4 engines each, time limit {limit:g} s, 5-fold held-out",
+                       "timing": "a calibration pass, not a repeated bench: each LP solved once per engine (as "
+                                 "the reference's router fitting times them), after one warm-up solve",
                        "host_threads": threads},
             "validation": val, "weights": W}
     print(json.dumps(line))
