@@ -89,3 +89,19 @@ def test_info_json_is_valid(engine_lib):
     engine_lib.b2p_gpu_info_json(buf, need + 1)
     d = json.loads(buf.value.decode())
     assert {"available", "name", "reason", "compute_capability", "multiprocessors"} <= set(d)
+
+
+def test_host_side_argument_checks():
+    """Wrong-length case vectors, duals and points are refused on the host,
+    before any device work."""
+    from pramana_b200 import pdhg
+    from pramana_b200.model import LpCase
+    lp = G.random_lp(20, 40, 3.0, 10, 1)
+    with pytest.raises(ValueError):
+        pdhg.solvePdhgBatch(lp, [LpCase(cost=np.ones(lp.num_cols - 1))])
+    with pytest.raises(ValueError):
+        pdhg.safeDualBound(lp, np.zeros(lp.num_rows + 1))
+    with pytest.raises(ValueError):
+        pdhg.certifyLp(lp, np.zeros(lp.num_cols), np.zeros(lp.num_rows - 1))
+    with pytest.raises(ValueError):
+        pdhg.kktResidual(lp, np.zeros(lp.num_cols + 2), np.zeros(lp.num_rows))
