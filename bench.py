@@ -179,7 +179,7 @@ def run_reference_gpu(args):
         print(json.dumps({"impl": "reference", "unavailable": "the reference's GPU backend did not come up "
                                                                "(it fell back to its CPU backend)"}))
         return 0
-    if args.workload in ("families", "calibrate"):
+    if args.workload in ("families", "calibrate", "sweep"):
         return run_reference_gpu_sets(args, O, G)
     if args.workload == "plan":
         sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -218,9 +218,10 @@ def run_reference_gpu(args):
 
 def run_reference_gpu_sets(args, O, G):
     """The reference's GPU backend on the published families (one batched
-    solve per family, 1e-6, 200,000 iterations at most) or on the six
-    calibration LPs (512 iterations each): loop seconds, wall seconds and
-    iterations per item, for the same-hardware comparison."""
+    solve per family, 1e-6, 200,000 iterations at most), on the six
+    calibration LPs (512 iterations each) or on the 256-case refinery price
+    sweep (--sweep-iters iterations of its solvePdhgBatch): loop seconds, wall
+    seconds and iterations per item, for the same-hardware comparison."""
     items = []
     if args.workload == "families":
         sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -237,6 +238,22 @@ def run_reference_gpu_sets(args, O, G):
             items.append({"family": fam, "loop_seconds": statistics.mean(loops), "wall_seconds": statistics.mean(walls),
                           "iterations": O.solve.last_stats["iterations"],
                           "solved": sum(r.status == 1 for r in rs), "backend": O.solve.last_stats["backend"]})
+    elif args.workload == "sweep":
+        import numpy as np
+        from pramana_b200 import warmstart as W
+        fam = W.RefineryFamily(seed=5)
+        rng = np.random.default_rng(9)
+        levels = np.linspace(40.0, 120.0, args.cases)
+        prices = np.stack([rng.permutation(levels) for _ in range(fam.crudes)], axis=1)
+        cases = [fam.case(p) for p in np.hstack([prices, np.ones((args.cases, fam.num_params - fam.crudes))])]
+        per = []
+        for s in range(args.warmup + args.steps):
+            O.solve(fam.base, "ref", cases=cases, backend="gpu", tolerance=1e-4, max_iterations=args.sweep_iters)
+            st = O.solve.last_stats
+            if s >= args.warmup:
+                per.append(st["solve_seconds"] / st["iterations"])
+        items.append({"cases": args.cases, "iterations": st["iterations"], "seconds_per_iteration": statistics.mean(per),
+                      "backend": st["backend"]})
     else:
         for scale in G.CALIBRATION_SCALES:
             lp = G.calibration_lp(scale)
