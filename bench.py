@@ -20,7 +20,8 @@ maximum over ranks.
 
 ``--impl reference`` times the reference's own multithreaded CPU PDHG
 (oracle/_ref/libpramana_ref.so, built from the reference sources) on the
-host's cores, on a bounded sample of the same solve.
+host's cores: every timed step is one full solve of the same LP to the same
+tolerance (the warm-up steps are short samples).
 
 ``--workload family`` runs the learned-warm-start workload instead: a
 164 x 324 refinery-planning LP family with 16 parameters (6 crude prices
@@ -62,15 +63,14 @@ CPU_SAMPLE_ITERS = 4096
 REF_ITERS_TO_TOL = 20288  # loop iterations of the reference CPU PDHG on this LP to 1e-6 (20,287 reported + 1)
 
 
-def workload_config(lp, extra=None):
-    cfg = {"workload": f"config-2 random LP m={lp.num_rows} n={lp.num_cols} nnz={lp.nnz} "
-                       f"(1% rows hold 10% nnz), seed {SEED}, to rel KKT {TOL:g}",
-           "form": "mixed precision (plain FP64 form timed beside it)", "check_every": 64,
-           "l2": "flushed before every step (512 MiB device write); the LP itself (~20 MB/iteration) is L2-resident "
-                 "within a solve"}
-    if extra:
-        cfg.update(extra)
-    return cfg
+def workload_config(lp, world=1):
+    """The workload both arms print, identical for the engine and the reference."""
+    return {"workload": f"config-2 random LP m={lp.num_rows} n={lp.num_cols} nnz={lp.nnz} "
+                        f"(1% rows hold 10% nnz), seed {SEED}, to rel KKT {TOL:g}",
+            "form": "mixed precision (plain FP64 form timed beside it)", "check_every": 64,
+            "l2": "flushed before every step (512 MiB device write); the LP itself (~20 MB/iteration) is L2-resident "
+                  "within a solve",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
 
 
 class ClockSampler:
@@ -163,6 +163,17 @@ def cpu_reference_sample(lp, iters: int, threads: int):
     return st["solve_seconds"] / iters, wall, st
 
 
+def cpu_reference_solve(lp, threads: int):
+    """One full solve of the reference CPU PDHG (oracle/_ref) to TOL from the
+    host arrays: (loop seconds, wall seconds, result, stats)."""
+    from oracle import oracle as O
+    O.set_ref_threads(threads)
+    t0 = time.perf_counter()
+    r = O.solve(lp, "ref", tolerance=TOL)
+    wall = time.perf_counter() - t0
+    return O.solve.last_stats["solve_seconds"], wall, r, O.solve.last_stats
+
+
 def run_reference_gpu(args):
     """--impl reference --reference-backend gpu: the reference's own GPU
     backend (its NVRTC-compiled FP64 kernels, compute_90 PTX run through the
@@ -246,13 +257,14 @@ def run_reference_gpu_sets(args, O, G):
         levels = np.linspace(40.0, 120.0, args.cases)
         prices = np.stack([rng.permutation(levels) for _ in range(fam.crudes)], axis=1)
         cases = [fam.case(p) for p in np.hstack([prices, np.ones((args.cases, fam.num_params - fam.crudes))])]
-        per = []
+        per, its = [], []
         for s in range(args.warmup + args.steps):
             O.solve(fam.base, "ref", cases=cases, backend="gpu", tolerance=1e-4, max_iterations=args.sweep_iters)
             st = O.solve.last_stats
             if s >= args.warmup:
                 per.append(st["solve_seconds"] / st["iterations"])
-        items.append({"cases": args.cases, "iterations": st["iterations"], "seconds_per_iteration": statistics.mean(per),
+                its.append(st["iterations"])
+        items.append({"cases": args.cases, "iterations_per_step": its, "seconds_per_iteration": statistics.mean(per),
                       "backend": st["backend"]})
     else:
         for scale in G.CALIBRATION_SCALES:
@@ -271,11 +283,14 @@ def run_reference_gpu_sets(args, O, G):
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the reference's own CPU PDHG on this host's cores."""
+    """--impl reference: the reference's own CPU PDHG on this host's cores,
+    every timed step one full solve of the same LP to the same tolerance."""
     if rank != 0:
         return 0
     if args.reference_backend == "gpu":
         return run_reference_gpu(args)
+    if args.steps < 1:
+        raise SystemExit("--steps must be >= 1")
     from pramana_b200 import generators as G
     from oracle import oracle as O
     lp = G.config2(SEED)
@@ -283,19 +298,24 @@ def run_reference(args, rank, world):
     if not O.available("ref"):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libpramana_ref.so was not built"}))
         return 0
-    per_iter = []
-    for s in range(args.warmup + args.steps):
-        spi, wall, st = cpu_reference_sample(lp, args.cpu_sample_iters, threads)
-        if s >= args.warmup:
-            per_iter.append(spi)
-    spi = statistics.mean(per_iter)
-    value = spi * REF_ITERS_TO_TOL
-    sample = (f"first {args.cpu_sample_iters} of the {REF_ITERS_TO_TOL} PDHG iterations the reference needs on this "
-              f"LP, per step; value = mean s/iteration x {REF_ITERS_TO_TOL}")
+    # warm-up: bounded samples (thread pool, page cache); timed: full solves
+    for _ in range(args.warmup):
+        cpu_reference_sample(lp, 512, threads)
+    loops, walls, its = [], [], []
+    for _ in range(args.steps):
+        loop, wall, r, st = cpu_reference_solve(lp, threads)
+        assert r.status == 1, r.status
+        loops.append(loop)
+        walls.append(wall)
+        its.append(r.iterations)
+    value = statistics.mean(loops)
+    sample = (f"{args.steps} full solves to rel KKT {TOL:g} ({its[-1]} iterations each), loop time; the "
+              f"{args.warmup} warm-up steps are 512-iteration samples")
     line = {"metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-            "config": workload_config(lp), "impl": "reference",
+            "config": workload_config(lp, world), "impl": "reference",
+            "run": {"iterations": its[-1], "relative_kkt": r.relative_kkt, "wall_seconds": statistics.mean(walls)},
             "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -974,6 +994,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.steps < 1:
+        ap.error("--steps must be >= 1")
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -1095,36 +1117,50 @@ def main():
             h2d, d2h = r.stats.bytesUploaded, r.stats.bytesDownloaded
     t_e2e = statistics.mean(e2e_times)
 
+    # ---- e2e of the plain FP64 form through the same call ----
+    e2e_plain = []
+    for s in range(args.warmup + args.steps):
+        flush.zero_()
+        barrier()
+        t0 = time.perf_counter()
+        r = pdhg.solvePdhg(lp, po_plain)
+        t1 = time.perf_counter()
+        if s >= args.warmup:
+            e2e_plain.append(t1 - t0)
+    t_e2e_plain = statistics.mean(e2e_plain)
+
     if dist is not None:
-        tt = torch.tensor([t_dev, t_e2e, t_plain], dtype=torch.float64, device=f"cuda:{dev}")
+        tt = torch.tensor([t_dev, t_e2e, t_plain, t_e2e_plain], dtype=torch.float64, device=f"cuda:{dev}")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_dev, t_e2e, t_plain = tt.tolist()
+        t_dev, t_e2e, t_plain, t_e2e_plain = tt.tolist()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
         if O.available("ref"):
             threads = os.cpu_count() or 1
-            spi, wall, _ = cpu_reference_sample(lp, args.cpu_sample_iters, threads)
-            cpu = {"value": spi * REF_ITERS_TO_TOL, "unit": "s", "cores": threads, "kind": "reference",
-                   "sample": f"first {args.cpu_sample_iters} of {REF_ITERS_TO_TOL} iterations of the same LP "
-                             f"({wall:.1f} s), scaled by iteration count"}
+            loop, wall, rr, _ = cpu_reference_solve(lp, threads)
+            cpu = {"value": loop, "unit": "s", "cores": threads, "kind": "reference",
+                   "sample": f"one full solve of the same LP to rel KKT {TOL:g} ({rr.iterations} iterations, "
+                             f"{wall:.1f} s wall), loop time"}
 
     if rank == 0:
         line = {"metric": METRIC, "value": t_dev, "unit": "s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_dev * 1e3, "higher_is_better": False, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32 iterates, f64 checks and polish",
                 "data": "synthetic (seeded generator)",
-                "config": workload_config(lp, {"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                                               "iterations": iters, "fp32_iterations": fp32_iters,
-                                               "kernel_form": form, "chosen_form": "mixed precision"}),
+                "config": workload_config(lp, world),
+                "run": {"iterations": iters, "fp32_iterations": fp32_iters, "kernel_form": form,
+                        "chosen_form": "mixed precision"},
                 "forms": {
                     "mixed": {"value": t_dev, "iterations": iters, "fp32_iterations": fp32_iters,
                               "relative_kkt_fp64": r_mixed.relativeKkt,
                               "objective_rel_diff_vs_fp64": abs(r_mixed.objective - r_plain.objective)
                               / (1 + abs(r_plain.objective))},
                     "plain_fp64": {"value": t_plain, "iterations": r_plain.iterations,
-                                   "relative_kkt": r_plain.relativeKkt}},
+                                   "relative_kkt": r_plain.relativeKkt,
+                                   "e2e": {"value": t_e2e_plain, "unit": "s", "h2d_bytes_per_step": h2d,
+                                           "d2h_bytes_per_step": d2h}}},
                 "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches,
                 "spmv_gbs": spmv_total_bytes / spmv_total_s / 1e9,

@@ -21,7 +21,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle_pdhg.so")
 REF_SO = os.path.join(HERE, "_ref", "libpramana_ref.so")
-REFERENCE_SRC = "/root/reference"
+# The reference tree, present only where the checkers are built (never on the
+# GPU box): PRAMANA_REFERENCE names it, else the build container's copy.
+REFERENCE_SRC = os.environ.get("PRAMANA_REFERENCE", "/root/reference")
 
 STATUS_NAMES = {0: "NotSolved", 1: "Optimal", 5: "TimeLimit", 6: "IterationLimit"}
 

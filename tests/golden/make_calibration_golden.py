@@ -12,7 +12,7 @@ import json
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference"
+REF = os.environ.get("PRAMANA_REFERENCE", "/root/reference")
 
 
 def main():

@@ -34,7 +34,7 @@ sys.path[:0] = [ROOT, os.path.join(ROOT, "optimized-gpu-accelerator_b200")]
 from oracle import oracle as O  # noqa: E402
 from pramana_b200.model import Model  # noqa: E402
 
-REF = "/root/reference"
+REF = os.environ.get("PRAMANA_REFERENCE", "/root/reference")
 FAMILIES = ("plan_10x12_BUY_CR03_0_cost", "plan_10x12_BUY_CR03_0_upper", "plan_20x12_BUY_CR07_3_cost",
             "plan_20x52_BUY_CR05_10_upper")
 

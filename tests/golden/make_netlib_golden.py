@@ -21,7 +21,7 @@ sys.path[:0] = [ROOT, os.path.join(ROOT, "optimized-gpu-accelerator_b200")]
 from oracle import oracle as O  # noqa: E402
 from pramana_b200.model import Model  # noqa: E402
 
-REF = "/root/reference"
+REF = os.environ.get("PRAMANA_REFERENCE", "/root/reference")
 
 
 def arrays(lp):

@@ -38,7 +38,7 @@ sys.path[:0] = [ROOT, os.path.join(ROOT, "optimized-gpu-accelerator_b200")]
 
 from oracle import oracle as O  # noqa: E402
 
-REF = "/root/reference"
+REF = os.environ.get("PRAMANA_REFERENCE", "/root/reference")
 PLANS = ("plan_6x4", "plan_10x12", "plan_20x12", "plan_20x52", "plan_30x52", "plan_40x104", "plan_60x156")
 RUNS = ("pdhg-cpu_raw1e-4", "pdhg-gpu_raw1e-4", "pdhg-gpu_raw1e-6")
 FIELDS = ("iterations", "restarts", "relative_kkt", "relative_primal_residual", "relative_dual_residual",

@@ -34,3 +34,21 @@ def test_reference_gpu_arm_without_gpu_is_unavailable(oracle_mod):
                        capture_output=True, text=True, check=True, timeout=600)
     line = json.loads([x for x in r.stdout.splitlines() if x.startswith("{")][-1])
     assert line["impl"] == "reference" and "unavailable" in line
+
+
+def test_reference_arm_times_full_solves_of_the_same_config(oracle_mod):
+    """The reference arm's line carries the engine arm's config dict verbatim,
+    and its timed step is a whole solve to the tolerance, not a scaled sample."""
+    if not oracle_mod.available("ref"):
+        pytest.skip("reference build absent")
+    sys.path.insert(0, ROOT)
+    import bench
+    from pramana_b200 import generators as G
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "3"], capture_output=True, text=True, check=True, timeout=900)
+    line = json.loads([x for x in r.stdout.splitlines() if x.startswith("{")][-1])
+    assert line["impl"] == "reference"
+    assert line["config"] == bench.workload_config(G.config2(bench.SEED), 1)
+    assert line["run"]["relative_kkt"] <= bench.TOL
+    assert line["run"]["iterations"] == bench.REF_ITERS_TO_TOL - 1
+    assert line["value"] == line["cpu_baseline"]["value"] == line["e2e"]["value"]

@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 from pramana_b200 import generators as G
+from oracle import oracle as O
 
 PUBLISHED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "calibration_published.json")
 
@@ -25,7 +26,7 @@ def test_calibration_instances_have_published_sizes(k):
     assert np.all(lp.col_cost >= -0.3) and np.all(lp.col_cost < 0.7)
 
 
-REF_SRC = "/root/reference/src"
+REF_SRC = os.path.join(O.REFERENCE_SRC, "src")
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_SRC), reason="reference sources not present")

@@ -5,9 +5,10 @@ import re
 import subprocess
 
 import pytest
+from oracle import oracle as O
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_SRC = "/root/reference/src"
+REF_SRC = os.path.join(O.REFERENCE_SRC, "src")
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_SRC), reason="reference sources not present")

@@ -11,9 +11,10 @@ import pytest
 import lp_cases
 from pramana_b200 import generators as G
 from pramana_b200.model import Model
+from oracle import oracle as O
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-REF_DATA = "/root/reference/data/netlib"
+REF_DATA = os.path.join(O.REFERENCE_SRC, "data", "netlib")
 
 
 def load_golden(path):
