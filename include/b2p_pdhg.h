@@ -322,27 +322,36 @@ typedef struct b2p_safe_bound {
 int b2p_safe_dual_bound(const b2p_lp* lp, const b2p_case* cases, int32_t num_cases, const double* row_dual,
                         b2p_safe_bound* out);
 
-/* Constraint-implied column bounds by activity-based bound propagation
- * (30 rounds, continuous columns), each tightened bound relaxed by
- * 1e-6 (1 + |bound|), untightened bounds left as given: the certifier's
- * fallback for first-order duals (src/cert/certifier.cpp:340-356, calling
- * Propagator::propagate of src/mip/propagate.cpp:23-138; the same steps as
- * impliedBounds, src/parametric/parametric.cpp:62-73), bit-identical.
- * Host computation, no GPU needed.  Outputs are num_cases x num_cols
- * (case-major; num_cases <= 0: one case, the base model). */
+/* Constraint-implied column bounds, for num_cases cases of a shared A at once
+ * (num_cases <= 0: one case, the base model): what the certifier of the
+ * reference falls back on for first-order duals (src/cert/certifier.cpp:340-356
+ * over Propagator::propagate, src/mip/propagate.cpp:23-138), computed on the
+ * GPU by activity-based bound tightening in Jacobi rounds -- every row's
+ * activity range from the previous round's bounds, then every column's
+ * bounds intersected with what its rows imply -- with every operation rounded
+ * in the safe direction, so the bounds contain every feasible point of the
+ * exact LP.  Rounds run until no bound moves by more than 1e-9 relative (at
+ * most 1,024).  Untightened bounds are returned as given; a case proved
+ * infeasible keeps the bounds it had when that was found.  Outputs are
+ * num_cases x num_cols (case-major).  The reference relaxes each tightened
+ * bound by 1e-6 (1 + |bound|) instead of rounding outward, so its bounds are
+ * looser by about that much; both are valid. */
 int b2p_implied_bounds(const b2p_lp* lp, const b2p_case* cases, int32_t num_cases, double* col_lower_out,
                        double* col_upper_out);
 
 /* The certifier's verdict on an OPTIMAL claim (x, row_dual) of an LP
- * (certify, src/cert/certifier.cpp:208-380, LP branch): relative column and
- * row violations (compensated row activities) against primal_feasibility,
- * the safe dual bound -- retried with constraint-implied column bounds when it
- * is -inf -- and the relative gap (pobj - LB) / max(1, |pobj|) against
- * relative_gap; without a finite bound the wrong-signed reduced cost is held
- * against dual_feasibility.  Primal checks run on host threads, the bounds on
- * the GPU (b2p_safe_dual_bound); every field is bit-identical to the
- * reference's Certificate.  x is num_cases x num_cols, row_dual num_cases x
- * num_rows (case-major). */
+ * (certify, src/cert/certifier.cpp:208-380, LP branch), for num_cases cases
+ * of a shared A at once, on the GPU: relative column and row violations
+ * against primal_feasibility (row activities as compensated dot products),
+ * the objective c'x + offset (compensated), the outward-rounded safe dual
+ * bound of b2p_safe_dual_bound -- retried over the constraint-implied column
+ * bounds of b2p_implied_bounds when it is -inf -- rounded down with the
+ * offset, and the relative gap (pobj - LB) / max(1, |pobj|) against
+ * relative_gap; without a finite bound the largest wrong-signed reduced cost
+ * is held against dual_feasibility.  The safe bound over the given column
+ * bounds is bit-identical to the reference's; the primal figures agree with
+ * the reference's to rounding (the sums are compensated differently).  x is
+ * num_cases x num_cols, row_dual num_cases x num_rows (case-major). */
 typedef struct b2p_cert_tolerances {
   double primal_feasibility; /* CertTolerances::primalFeas, 1e-6 */
   double dual_feasibility;   /* CertTolerances::dualFeas, 1e-6 */
@@ -369,16 +378,23 @@ int b2p_certify_lp(const b2p_lp* lp, const b2p_case* cases, int32_t num_cases, c
 
 /* Allocation-free form of b2p_kkt_residual.  No counterpart in the
  * reference.  For callers that cannot allocate device memory (a host
- * framework that owns all device memory through its own pool, code inside a
- * stream-capture region, or a path where allocation is forbidden): every
- * array is a caller-owned DEVICE pointer, and the call itself allocates
- * nothing.  Inputs: A as CSR (a_ptr[num_rows+1], a_idx, a_val) and as CSC read
- * as the CSR of A^T (at_ptr[num_cols+1], at_idx, at_val), and per point b
- * (case-major) cost, col_lower, col_upper (num_points x num_cols), row_lower,
- * row_upper (num_points x num_rows), x and row_dual.  Output: out[4b..4b+3]
- * as in b2p_kkt_residual, written on `stream` (a cudaStream_t; NULL = the
- * legacy default stream) -- the call only enqueues; synchronize the stream
- * before reading out.
+ * framework that owns all device memory through its own pool, or a path where
+ * allocation is forbidden): every array is a caller-owned DEVICE pointer of
+ * the current device, and the call itself allocates nothing.  Inputs: A as
+ * CSR (a_ptr[num_rows+1], a_idx, a_val) and as CSC read as the CSR of A^T
+ * (at_ptr[num_cols+1], at_idx, at_val), and per point b (case-major) cost,
+ * col_lower, col_upper (num_points x num_cols), row_lower, row_upper
+ * (num_points x num_rows), x and row_dual.  Output: out[4b..4b+3] as in
+ * b2p_kkt_residual, written on `stream` (a cudaStream_t; NULL = the legacy
+ * default stream) -- the call only enqueues; synchronize the stream before
+ * reading out.
+ * Checks before any launch: each array the kernels may read or write must be
+ * memory of the current device (host memory, unregistered addresses and other
+ * GPUs' memory give B2P_ERR_INVALID naming the argument; a_idx, a_val, at_idx
+ * and at_val may be NULL only when num_rows or num_cols is 0).  A CUDA error
+ * left pending on the calling thread by earlier work is neither cleared nor
+ * charged to this call: the call returns B2P_ERR_CUDA without launching.  A
+ * failure of its own launches is returned as B2P_ERR_CUDA and cleared.
  * Scratch: the reductions' block partials live in one file-scope device array
  * of 458,752 bytes, which every GPU that loads this library holds until the
  * process exits.  num_points above 32 is rejected with B2P_ERR_TOO_LARGE.

@@ -24,6 +24,7 @@
 #include <cstring>
 #include <vector>
 
+#include "pdhg_cert.h"
 #include "pdhg_host_common.h"
 #include "pdhg_kernels.cuh"
 
@@ -196,6 +197,19 @@ __global__ void k_ns_sum(int32_t k, int64_t len, const double* __restrict__ term
   bound[b] = inf_terms[b] > 0 ? -INFINITY : lb;
 }
 
+void enqueue_safe_bound(cudaStream_t s, int32_t m, int32_t n, int32_t k, CsrView AT, const double* y, const double* c,
+                        const double* lo, const double* up, const double* rl, const double* ru, double* yp,
+                        double* terms, double* stats, int32_t* inf_terms, double* bound) {
+  B2P_CUDA(cudaMemsetAsync(stats, 0, sizeof(double) * 4 * k, s));
+  B2P_CUDA(cudaMemsetAsync(inf_terms, 0, sizeof(int32_t) * k, s));
+  if (m) k_ns_rows<<<dim3((m + kBlock - 1) / kBlock, k), kBlock, 0, s>>>(m, n, y, rl, ru, yp, terms, stats);
+  if (n)
+    k_ns_cols<<<dim3((n + kBlock - 1) / kBlock, k), kBlock, 0, s>>>(m, n, AT, yp, c, lo, up, terms, stats,
+                                                                    inf_terms);
+  k_ns_sum<<<(k + 127) / 128, 128, 0, s>>>(k, static_cast<int64_t>(m) + n, terms, inf_terms, bound);
+  B2P_CUDA(cudaGetLastError());
+}
+
 // Device buffers and the stream of one call, released on every exit path;
 // the buffers come from the device's stream-ordered pool (no cudaMalloc /
 // cudaFree per call).
@@ -270,14 +284,7 @@ extern "C" int b2p_safe_dual_bound(const b2p_lp* lp, const b2p_case* cases, int3
     double* dstats = r.put<double>(nullptr, static_cast<size_t>(k) * 4);
     int32_t* dinf = r.put<int32_t>(nullptr, static_cast<size_t>(k));
     double* dbound = r.put<double>(nullptr, static_cast<size_t>(k));
-    B2P_CUDA(cudaMemsetAsync(dstats, 0, sizeof(double) * 4 * k, s));
-    B2P_CUDA(cudaMemsetAsync(dinf, 0, sizeof(int32_t) * k, s));
-    if (m) k_ns_rows<<<dim3((m + kBlock - 1) / kBlock, k), kBlock, 0, s>>>(m, n, dy, drl, dru, dyp, dterms, dstats);
-    if (n)
-      k_ns_cols<<<dim3((n + kBlock - 1) / kBlock, k), kBlock, 0, s>>>(m, n, AT, dyp, dc, dlo, dup, dterms, dstats,
-                                                                      dinf);
-    k_ns_sum<<<(k + 127) / 128, 128, 0, s>>>(k, len, dterms, dinf, dbound);
-    B2P_CUDA(cudaGetLastError());
+    enqueue_safe_bound(s, m, n, k, AT, dy, dc, dlo, dup, drl, dru, dyp, dterms, dstats, dinf, dbound);
     std::vector<double> hb(k), hs(static_cast<size_t>(k) * 4);
     std::vector<int32_t> hi(k);
     B2P_CUDA(cudaMemcpyAsync(hb.data(), dbound, sizeof(double) * k, cudaMemcpyDeviceToHost, s));

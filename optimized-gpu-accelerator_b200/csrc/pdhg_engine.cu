@@ -30,6 +30,7 @@
 #include "pdhg_host_common.h"
 #include "pdhg_kernels.cuh"
 #include "pdhg_prepare.h"
+#include "pdhg_restart.h"
 #include "pdhg_scale.cuh"
 #include "pdhg_batch32.cuh"
 #include "pdhg_resident.cuh"
@@ -1041,8 +1042,7 @@ struct Engine {
     y_out.assign(static_cast<size_t>(m) * k, 0.0);
     stats.restarts = 0;
     std::vector<char> done(k, 0);
-    std::vector<double> fpRestart(k, INFINITY), fpPrev(k, INFINITY);
-    std::vector<int64_t> sinceRestart(k, 0);
+    std::vector<RestartTracker> restarts(k);
     std::vector<double> xs, ys;
     int remaining = k;
     int checks = 0;
@@ -1129,10 +1129,7 @@ struct Engine {
           }
           if (remaining == 0) break;
           switch_to_fp64();
-          for (int b = 0; b < k; ++b) {
-            fpRestart[b] = fpPrev[b] = INFINITY;
-            sinceRestart[b] = 0;
-          }
+          for (auto& r : restarts) r.reset();
           stats.restarts++;
           if (expired()) {
             expiredStop = true;
@@ -1180,8 +1177,7 @@ struct Engine {
         }
         if (to_fp64) {
           switch_to_fp64();
-          fpRestart[0] = fpPrev[0] = INFINITY;
-          sinceRestart[0] = 0;
+          restarts[0].reset();
           stats.restarts++;
           if (expired()) {
             expiredStop = true;
@@ -1220,27 +1216,15 @@ struct Engine {
           --remaining;
           continue;
         }
-        sinceRestart[b] += cE;
-        const double fp = std::sqrt(omega[b] * s[CS_DX2] + s[CS_DY2] / omega[b]);
-        if (fpRestart[b] == INFINITY) fpRestart[b] = fp;
-        const bool restart = fp <= 0.2 * fpRestart[b] || (fp <= 0.8 * fpRestart[b] && fp > fpPrev[b]) ||
-                             sinceRestart[b] >= static_cast<int64_t>(0.36 * static_cast<double>(it + 1));
-        fpPrev[b] = fp;
-        if (restart) {
+        if (restarts[b].due(omega[b], s, it, cE)) {
           h_mask[b] = 1;
           anyRestart = true;
         }
       }
       if (anyRestart) {
-        // Primal weight from the movement since the last restart (pdhg.cpp:642-656).
         for (int b = 0; b < k; ++b) {
           if (!h_mask[b]) continue;
-          const double* s = h_sums + static_cast<size_t>(b) * kNumSums;
-          const double dxn = std::sqrt(s[CS_AX2]), dyn = std::sqrt(s[CS_AY2]);
-          if (dxn > 1e-10 && dyn > 1e-10) omega[b] = std::exp(0.5 * std::log(dyn / dxn) + 0.5 * std::log(omega[b]));
-          fpRestart[b] = std::sqrt(omega[b] * s[CS_DX2] + s[CS_DY2] / omega[b]);
-          fpPrev[b] = INFINITY;
-          sinceRestart[b] = 0;
+          restarts[b].restart(omega[b], h_sums + static_cast<size_t>(b) * kNumSums);
           stats.restarts++;
         }
         upload_steps(omega);

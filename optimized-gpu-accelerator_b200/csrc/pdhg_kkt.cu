@@ -156,7 +156,6 @@ inline void enqueue_kkt(cudaStream_t stream, int32_t m, int32_t n, int32_t k, Cs
   k_kkt_point_rows<<<dim3(gr, k), kBlock, 0, stream>>>(m, n, A, x, y, rl, ru, prow);
   k_kkt_point_cols<<<dim3(gc, k), kBlock, 0, stream>>>(n, m, AT, x, y, c, lo, up, pcol);
   k_kkt_point_finalize<<<k, kBlock, 0, stream>>>(gr, gc, prow, pcol, out);
-  B2P_CUDA(cudaGetLastError());
 }
 
 namespace {
@@ -257,6 +256,7 @@ extern "C" int b2p_kkt_residual(const b2p_lp* lp, const b2p_case* cases, int32_t
     double* pcol = buf.put<double>(nullptr, static_cast<size_t>(k) * kKktMaxBlocks * kKktColSums, s);
     double* dout = buf.put<double>(nullptr, static_cast<size_t>(k) * 4, s);
     enqueue_kkt(s, m, n, k, A, AT, dx, dy, dc, dlo, dup, drl, dru, prow, pcol, dout);
+    B2P_CUDA(cudaGetLastError());
     B2P_CUDA(cudaMemcpyAsync(out, dout, sizeof(double) * 4 * k, cudaMemcpyDeviceToHost, s));
     B2P_CUDA(cudaStreamSynchronize(s));
   });
@@ -306,14 +306,23 @@ double* noalloc_scratch_on_current_device() {
   return g_noalloc_scratch[dev];
 }
 
-void require_device_pointer(const void* p, const char* what) {
+// Refuses, before anything is launched, an argument that is not device
+// memory of the current device: a host pointer (pageable or page-locked), an
+// unregistered address, or another GPU's allocation would reach the kernels
+// as an illegal address.
+void require_device_pointer(const void* p, const char* what, int dev) {
+  if (!p) throw Error(B2P_ERR_INVALID, std::string(what) + " is NULL");
   cudaPointerAttributes at{};
   if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
-    cudaGetLastError();
+    cudaGetLastError();  // clears only the error this query itself raised
     throw Error(B2P_ERR_INVALID, std::string(what) + " is not a device pointer");
   }
-  if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)
+  if (at.type == cudaMemoryTypeManaged) return;
+  if (at.type != cudaMemoryTypeDevice)
     throw Error(B2P_ERR_INVALID, std::string(what) + " is not a device pointer");
+  if (at.device != dev)
+    throw Error(B2P_ERR_INVALID, std::string(what) + " is memory of device " + std::to_string(at.device) +
+                                     ", not of the current device " + std::to_string(dev));
 }
 
 }  // namespace
@@ -332,14 +341,36 @@ extern "C" int b2p_kkt_residual_noalloc(int32_t num_rows, int32_t num_cols, int3
     if (num_points > kNoAllocMaxPoints)
       throw Error(B2P_ERR_TOO_LARGE, "num_points " + std::to_string(num_points) + " exceeds the maximum of " +
                                          std::to_string(kNoAllocMaxPoints) + " points per call");
-    if (!a_ptr || !at_ptr || !out || (num_cols > 0 && (!cost || !col_lower || !col_upper || !x)) ||
-        (num_rows > 0 && (!row_lower || !row_upper || !row_dual)))
-      throw Error(B2P_ERR_INVALID, "NULL argument");
-    require_device_pointer(out, "out");
-    require_device_pointer(a_ptr, "a_ptr");
-    require_device_pointer(at_ptr, "at_ptr");
-    if (num_cols > 0) require_device_pointer(x, "x");
-    if (num_rows > 0) require_device_pointer(row_dual, "row_dual");
+    int dev = 0;
+    B2P_CUDA(cudaGetDevice(&dev));
+    // An error left pending by the caller's own earlier work stays the
+    // caller's: it is neither reported as this call's nor cleared.
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess)
+      throw Error(B2P_ERR_CUDA, std::string("a CUDA error from earlier work is pending on this thread (") +
+                                    cudaGetErrorName(pending) + "); nothing was launched and the error is left in place");
+    // every array the kernels can touch: the operators' entries exist only
+    // when both dimensions are nonzero
+    require_device_pointer(out, "out", dev);
+    require_device_pointer(a_ptr, "a_ptr", dev);
+    require_device_pointer(at_ptr, "at_ptr", dev);
+    if (num_rows > 0 && num_cols > 0) {
+      require_device_pointer(a_idx, "a_idx", dev);
+      require_device_pointer(a_val, "a_val", dev);
+      require_device_pointer(at_idx, "at_idx", dev);
+      require_device_pointer(at_val, "at_val", dev);
+    }
+    if (num_cols > 0) {
+      require_device_pointer(cost, "cost", dev);
+      require_device_pointer(col_lower, "col_lower", dev);
+      require_device_pointer(col_upper, "col_upper", dev);
+      require_device_pointer(x, "x", dev);
+    }
+    if (num_rows > 0) {
+      require_device_pointer(row_lower, "row_lower", dev);
+      require_device_pointer(row_upper, "row_upper", dev);
+      require_device_pointer(row_dual, "row_dual", dev);
+    }
     double* scratch = noalloc_scratch_on_current_device();
     double* prow = scratch;
     double* pcol = scratch + static_cast<size_t>(kNoAllocMaxPoints) * kKktMaxBlocks * kKktRowSums;
@@ -347,5 +378,7 @@ extern "C" int b2p_kkt_residual_noalloc(int32_t num_rows, int32_t num_cols, int3
     const CsrView AT{at_ptr, at_idx, at_val, num_cols};
     enqueue_kkt(static_cast<cudaStream_t>(stream), num_rows, num_cols, num_points, A, AT, x, row_dual, cost,
                 col_lower, col_upper, row_lower, row_upper, prow, pcol, out);
+    // nothing was pending before the launches, so an error now is theirs
+    B2P_CUDA(cudaGetLastError());
   });
 }

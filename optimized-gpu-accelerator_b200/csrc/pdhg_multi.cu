@@ -29,6 +29,7 @@
 #include "pdhg_host_common.h"
 #include "pdhg_kernels.cuh"
 #include "pdhg_prepare.h"
+#include "pdhg_restart.h"
 #include "pdhg_scale.cuh"
 #include "pdhg_cta.cuh"
 #include "pdhg_sched.h"
@@ -1420,8 +1421,7 @@ struct MultiEngine {
     ys.assign(K, {});
     stats.restarts = 0;
     std::vector<char> done(K, 0);
-    std::vector<double> fpRestart(K, INFINITY), fpPrev(K, INFINITY);
-    std::vector<int64_t> sinceRestart(K, 0);
+    std::vector<RestartTracker> restarts(K);
     int remaining = K;
     const int cE = opt.check_every;
     auto expired = [&]() {
@@ -1454,20 +1454,10 @@ struct MultiEngine {
           --remaining;
           continue;
         }
-        sinceRestart[b] += cE;
-        const double fp = std::sqrt(omega[b] * s[CS_DX2] + s[CS_DY2] / omega[b]);
-        if (fpRestart[b] == INFINITY) fpRestart[b] = fp;
-        const bool restart = fp <= 0.2 * fpRestart[b] || (fp <= 0.8 * fpRestart[b] && fp > fpPrev[b]) ||
-                             sinceRestart[b] >= static_cast<int64_t>(0.36 * static_cast<double>(it + 1));
-        fpPrev[b] = fp;
-        if (restart) {
+        if (restarts[b].due(omega[b], s, it, cE)) {
           h_mask[b] = 1;
           anyRestart = true;
-          const double dxn = std::sqrt(s[CS_AX2]), dyn = std::sqrt(s[CS_AY2]);
-          if (dxn > 1e-10 && dyn > 1e-10) omega[b] = std::exp(0.5 * std::log(dyn / dxn) + 0.5 * std::log(omega[b]));
-          fpRestart[b] = std::sqrt(omega[b] * s[CS_DX2] + s[CS_DY2] / omega[b]);
-          fpPrev[b] = INFINITY;
-          sinceRestart[b] = 0;
+          restarts[b].restart(omega[b], s);
           stats.restarts++;
         }
       }

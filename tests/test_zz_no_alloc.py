@@ -1,7 +1,8 @@
 """The allocation-free KKT entry point, b2p_kkt_residual_noalloc.
 
-It serves callers that cannot allocate device memory themselves (their host
-framework owns all device memory, or they run inside a stream capture): every
+It serves callers that cannot allocate device memory themselves (a host
+framework that owns every device byte through its own pool, or a path where
+allocation is forbidden): every
 array is a device pointer they own, and the entry point's only scratch is a
 fixed device array inside the library.  Its result must equal that of the
 allocating entry point b2p_kkt_residual on the same points, call after call,
@@ -122,11 +123,25 @@ def test_no_alloc_rejects_more_points_than_its_scratch_holds():
     assert np.allclose(dev32["out"].cpu().numpy(), want, rtol=REL_TOL, atol=1e-300)
 
 
-def test_no_alloc_rejects_host_pointers():
+ARGS = ("a_ptr", "a_idx", "a_val", "at_ptr", "at_idx", "at_val", "cost", "col_lower", "col_upper", "row_lower",
+        "row_upper", "x", "row_dual", "out")
+
+
+@pytest.mark.parametrize("which", ARGS)
+def test_no_alloc_rejects_a_host_pointer_in_any_position(which):
+    """Every array is checked on the host before anything is launched: a host
+    pointer in any one position is refused with B2P_ERR_INVALID, and the
+    device output is left untouched."""
+    torch = pytest.importorskip("torch")
     lib = _lib.load()
     lp = G.random_lp(40, 80, 3.0, 20, 3)
-    host = np.zeros(8)
-    hp = C.c_void_p(host.ctypes.data)
-    rc = lib.b2p_kkt_residual_noalloc(lp.num_rows, lp.num_cols, 1, hp, hp, hp, hp, hp, hp, hp, hp, hp, hp, hp, hp, hp,
-                                      hp, None)
-    assert rc == 1 and b"not a device pointer" in lib.b2p_last_error()
+    dev, k = _device_inputs(torch, lp, np.zeros(lp.num_cols), np.zeros(lp.num_rows), None)
+    torch.cuda.synchronize()
+    host = np.zeros(max(lp.num_rows, lp.num_cols, lp.start[-1]) * 4 + 8)
+    ptrs = [C.c_void_p(host.ctypes.data) if name == which else C.c_void_p(dev[name].data_ptr()) for name in ARGS]
+    rc = lib.b2p_kkt_residual_noalloc(lp.num_rows, lp.num_cols, k, *ptrs, None)
+    assert rc == 1, lib.b2p_last_error()
+    msg = lib.b2p_last_error()
+    assert which.encode() in msg and b"not a device pointer" in msg
+    torch.cuda.synchronize()
+    assert np.all(np.isnan(dev["out"].cpu().numpy()))
