@@ -322,7 +322,15 @@ def run_reference(args, rank, world):
     return 0
 
 
-FAMILY_SIZE = dict(periods=2, regions=1, units=4, streams=4, properties=2, scale_exponent=0.0)
+# Sizes of the refinery-planning family (generators.refinery_lp, unit row and
+# column scales): small 164 x 324 (1,072 nonzeros), medium 1,692 x 3,528
+# (14,982), large 5,064 x 11,376 (57,178).
+FAMILY_SIZES = {
+    "small": dict(periods=2, regions=1, units=4, streams=4, properties=2, scale_exponent=0.0),
+    "medium": dict(periods=6, regions=2, units=6, streams=6, properties=3, pools=12, scale_exponent=0.0),
+    "large": dict(periods=12, regions=2, units=8, streams=8, properties=4, pools=12, scale_exponent=0.0),
+}
+FAMILY_SIZE = FAMILY_SIZES["small"]
 FAMILY_METRIC = "wall time per 1,024-member refinery family batch to certified rel KKT 1e-6 (s), learned warm start"
 
 
@@ -338,8 +346,12 @@ def run_family(args, rank, world):
     if world > 1 and rank != 0:
         return 0
     torch.cuda.set_device(0)
-    fam = W.RefineryFamily(seed=5, **FAMILY_SIZE)
-    opts = pdhg.PdhgOptions(tolerance=TOL, maxIterations=200000, precision=0)
+    size = FAMILY_SIZES[args.family_size]
+    fam = W.RefineryFamily(seed=5, **size)
+    precision = {"fp64": 0, "mixed": 1}[args.precision]
+    # the batched engine's form, and the plain FP64 single-LP form of the per-instance baseline
+    opts = pdhg.PdhgOptions(tolerance=TOL, maxIterations=args.family_max_iters, precision=precision)
+    plain = pdhg.PdhgOptions(tolerance=TOL, maxIterations=args.family_max_iters, precision=0)
     t0 = time.perf_counter()
     P_train = fam.sample(args.train, 100)
     tr = W.solve_family(fam, P_train, opts, batch=args.batch, engine=args.engine)
@@ -377,7 +389,7 @@ def run_family(args, rank, world):
         lp = fam.instance(p)
         torch.cuda.synchronize()
         t1 = time.perf_counter()
-        r = pdhg.solvePdhg(lp, opts)
+        r = pdhg.solvePdhg(lp, plain)
         per.append(time.perf_counter() - t1)
         its1.append(r.iterations)
     per_instance_batch = statistics.mean(per) * args.batch
@@ -396,11 +408,14 @@ def run_family(args, rank, world):
     b = fam.base
     line = {"metric": FAMILY_METRIC, "value": value, "unit": "s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64 PDHG, bf16 MLP with f32 accumulation", "data": "synthetic (seeded)",
+            "vs_baseline": None,
+            "dtype": {"fp64": "f64 PDHG", "mixed": "f32 iterates / f64 checks, re-measure and polish"}[args.precision]
+            + ", bf16 MLP with f32 accumulation", "data": "synthetic (seeded)",
             "workload": "family",
-            "config": {"workload": f"refinery-planning family, {b.num_rows} rows x {b.num_cols} cols, {b.nnz} nnz "
-                                   f"({FAMILY_SIZE}), 16 parameters; {args.train} training members, "
-                                   f"{args.steps} x {args.batch} held-out members, to rel KKT {TOL:g}",
+            "config": {"workload": f"refinery-planning family ({args.family_size}), {b.num_rows} rows x "
+                                   f"{b.num_cols} cols, {b.nnz} nnz ({size}), 16 parameters; {args.train} training "
+                                   f"members, {args.steps} x {args.batch} held-out members, to rel KKT {TOL:g}",
+                       "precision": args.precision,
                        "step": "one held-out batch solved and certified per strategy",
                        "engine": {"multi": "multi-LP engine (AUTO form: one thread block per member)",
                                   "batch": "shared-A batch engine (k-interleaved cases)"}[args.engine],
@@ -982,6 +997,11 @@ def main():
     ap.add_argument("--schedule", choices=["auto", "binned", "tiled", "tuned"], default="auto",
                     help="multi: SpMV schedule of the multi-LP kernels")
     ap.add_argument("--train", type=int, default=32768, help="family: training members")
+    ap.add_argument("--family-size", choices=sorted(FAMILY_SIZES), default="small",
+                    help="family: refinery LP size (small 164 x 324, medium 1,692 x 3,528, large 5,064 x 11,376)")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed",
+                    help="family: arithmetic of the batched solves (the per-instance baseline is plain FP64)")
+    ap.add_argument("--family-max-iters", type=int, default=400000, help="family: iteration limit per member")
     ap.add_argument("--batch", type=int, default=1024, help="family: members per batched solve")
     ap.add_argument("--engine", choices=["multi", "batch"], default="multi",
                     help="family: multi-LP engine (one block per member) or the shared-A batch engine")

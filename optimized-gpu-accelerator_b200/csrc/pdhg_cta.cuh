@@ -24,6 +24,17 @@
 // uniform across the block.  Two variants share this loop: run_lp (any LP
 // size, three storage tiers) and run_owner (max(m, n) <= R * threads: each
 // thread keeps its own rows' and columns' state in registers).
+//
+// Mixed precision (run_lp with T = float): the operator values and the nine
+// iterate / anchor vectors are FP32 -- half the shared memory, so larger LPs
+// keep their iterates on chip -- while every row sum accumulates the exact
+// FP32 x FP32 products in FP64, the updates are evaluated in FP64 from the
+// FP32 operands and rounded once at the store, and the check sums, costs,
+// bounds, scaling factors and every decision stay FP64.  The FP32 run of an LP
+// ends when its FP32 point meets the tolerance, or when its KKT error has not
+// fallen by 10% in `stall_checks` checks; the host then restarts it in FP64
+// from that point (entry_check: the point is measured in FP64 first, and an LP
+// it already satisfies stops there).
 #pragma once
 
 #include <cstdint>
@@ -42,13 +53,25 @@ struct CtaLp {
   int32_t m, n;
   int32_t a_beg, t_beg;  // first entry of its rows in A / in A^T
   int32_t nnz;
-  int32_t tier;
+  int32_t tier;    // storage tier of the FP64 run
+  int32_t tier32;  // storage tier of the FP32 run (mixed precision)
+  // Where the LP's operators sit: its first row pointer in A / in A^T and
+  // the offset its column / row indices carry.  Its own block of the
+  // concatenated operators (roff, coff, coff, roff), or -- for members of a
+  // family that share one A -- the first LP's block (0, 0, 0, 0), which every
+  // block then reads from L2.
+  int32_t aptr_off, tptr_off, ashift, tshift;
+  int32_t pad;
+  int64_t it0;     // iteration the run starts at (> 0: continuing an earlier run)
   double eta;        // 0.998 / ||A||
   double omega0;     // initial primal weight
   double cnorm;      // ||c|| of the original LP
   double rhsnorm;    // ||finite row bounds|| of the original LP
   double scale_obj;  // beta * gamma
 };
+
+// Status of an FP32 run that stalled (host-internal; never returned).
+constexpr int32_t kCtaStalled = 100;
 
 // Per LP result, written by the block when its loop ends.
 struct CtaOut {
@@ -68,19 +91,46 @@ struct CtaArgs {
   // global state (kCtaGlobal LPs iterate here); x+ and y+ of every LP are
   // left in xp and yp when its loop ends
   double *x, *xp, *x0, *y, *yp, *y0, *ax, *axp, *ax0;
+  // FP32 run: the operators' values and the global-tier state in FP32 (its
+  // x+ and y+ still go to xp and yp above, converted)
+  const float *A32, *AT32;
+  float *x32, *xp32, *x032, *y32, *yp32, *y032, *ax32, *axp32, *ax032;
   double tol, rho;
   int64_t max_it;
   int32_t check_every;
+  int32_t entry_check;   // measure the starting point first; stop there if it meets tol
+  int32_t stall_checks;  // > 0: end the run after this many checks without a 10% KKT gain
+  int32_t pad;
   const volatile int32_t* stop;  // host-mapped; nonzero = stop at the next check
 };
 
-// Shared-memory bytes an LP needs in each tier of run_lp (doubles first,
-// then int32).
-__host__ __device__ inline int64_t cta_tier_bytes(int tier, int64_t m, int64_t n, int64_t nnz) {
+template <class T>
+struct CtaState {
+  T *x, *xp, *x0, *y, *yp, *y0, *ax, *axp, *ax0;
+  const T *Av, *Tv;
+};
+__device__ __forceinline__ CtaState<double> cta_state(const CtaArgs& a, double*) {
+  return CtaState<double>{a.x, a.xp, a.x0, a.y, a.yp, a.y0, a.ax, a.axp, a.ax0, a.A.val, a.AT.val};
+}
+__device__ __forceinline__ CtaState<float> cta_state(const CtaArgs& a, float*) {
+  return CtaState<float>{a.x32, a.xp32, a.x032, a.y32, a.yp32, a.y032, a.ax32, a.axp32, a.ax032, a.A32, a.AT32};
+}
+
+// Iterate / anchor vector elements of an LP in shared memory, rounded up so
+// that the FP64 constants after them start on an 8-byte boundary.
+__host__ __device__ inline int64_t cta_vector_elems(int64_t m, int64_t n, int esize) {
+  const int64_t e = 3 * n + 6 * m;
+  return esize == 4 ? (e + 1) / 2 * 2 : e;
+}
+
+// Shared-memory bytes an LP needs in each tier of run_lp with esize-byte
+// iterates and operator values (vectors, FP64 constants, values, int32).
+__host__ __device__ inline int64_t cta_tier_bytes(int tier, int64_t m, int64_t n, int64_t nnz, int esize = 8) {
   if (tier == kCtaGlobal) return 0;
-  const int64_t vec = 8 * (3 * n + 6 * m);
+  const int64_t vec = esize * cta_vector_elems(m, n, esize);
   if (tier == kCtaVectors) return vec;
-  return vec + 8 * (4 * n + 3 * m) + 8 * 2 * nnz + 4 * ((m + 1) + (n + 1) + 2 * nnz);
+  const int64_t vals = (esize * 2 * nnz + 7) / 8 * 8;
+  return vec + 8 * (4 * n + 3 * m) + vals + 4 * ((m + 1) + (n + 1) + 2 * nnz);
 }
 
 // Shared-memory bytes of an LP in run_owner: x+, y, y+ and both operators'
@@ -98,9 +148,12 @@ struct Ctl {
   double rel_p, rel_d, gap, pobj, dobj;
   int64_t since_restart, restart_at;
   int32_t restarts;
-  int32_t status;   // 0 while running, else B2P_STATUS_*
+  int32_t status;   // 0 while running, else B2P_STATUS_* (or kCtaStalled)
   int32_t restart;  // restart at this check
   int32_t stop;     // the stop flag as read at this check
+  double best_kkt;  // FP32 run: smallest KKT error a 10% gain last reached
+  int32_t since_best;
+  int32_t pad;
 };
 
 template <int NT>
@@ -123,6 +176,8 @@ __device__ __forceinline__ void init_ctl(Ctl& c, const CtaLp& L) {
   c.status = 0;
   c.restart = 0;
   c.stop = 0;
+  c.best_kkt = INFINITY;
+  c.since_best = 0;
 }
 
 // The host's decisions at a check from the ten sums (src/pdhg/pdhg.cpp:598-662):
@@ -130,7 +185,7 @@ __device__ __forceinline__ void init_ctl(Ctl& c, const CtaLp& L) {
 // `it` is the index of the check iteration.  Out of line: the exp / log live
 // here, not in the iteration loop's registers.
 __device__ __noinline__ void decide(Ctl& c, const double* tot, double scale_obj, double rhsnorm, double cnorm,
-                                    double eta, int64_t it, double tol, int cE) {
+                                    double eta, int64_t it, double tol, int cE, int stall_checks) {
   const double pobj = tot[CS_POBJ] * scale_obj;
   const double dobj = (tot[CS_ROW_DOBJ] + tot[CS_COL_DOBJ]) * scale_obj;
   const double relP = sqrt(tot[CS_ROW_RES2]) / (1.0 + rhsnorm);
@@ -145,6 +200,16 @@ __device__ __noinline__ void decide(Ctl& c, const double* tot, double scale_obj,
   if (relP <= tol && relD <= tol && gap <= tol) {
     c.status = B2P_STATUS_OPTIMAL;
     return;
+  }
+  if (stall_checks > 0) {
+    const double kkt = fmax(relP, fmax(relD, gap));
+    if (kkt < 0.9 * c.best_kkt) {
+      c.best_kkt = kkt;
+      c.since_best = 0;
+    } else if (++c.since_best >= stall_checks) {
+      c.status = kCtaStalled;
+      return;
+    }
   }
   c.since_restart += cE;
   double omega = c.omega;
@@ -197,7 +262,44 @@ __device__ __forceinline__ void check_decide(double (&s)[kNumSums], Shared<NT>& 
       sh.tot[lane] = t;
     }
     __syncwarp();
-    if (lane == 0) decide(sh.ctl, sh.tot, L.scale_obj, L.rhsnorm, L.cnorm, L.eta, it, a.tol, a.check_every);
+    if (lane == 0)
+      decide(sh.ctl, sh.tot, L.scale_obj, L.rhsnorm, L.cnorm, L.eta, it, a.tol, a.check_every, a.stall_checks);
+  }
+  __syncthreads();
+}
+
+// The termination test alone, on sums of the starting point (entry check):
+// on return every thread sees sh.ctl.status.
+template <int NT>
+__device__ __forceinline__ void entry_decide(double (&s)[kNumSums], Shared<NT>& sh, const CtaArgs& a,
+                                             const CtaLp& L) {
+#pragma unroll
+  for (int q = 0; q < kNumSums; ++q)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s[q] += __shfl_xor_sync(0xffffffffu, s[q], off);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < kNumSums; ++q) sh.w[q][warp] = s[q];
+  __syncthreads();
+  if (warp == 0) {
+    if (lane < kNumSums) {
+      double t = 0.0;
+#pragma unroll
+      for (int w = 0; w < NT / 32; ++w) t += sh.w[lane][w];
+      sh.tot[lane] = t;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      Ctl& c = sh.ctl;
+      const double* tot = sh.tot;
+      c.pobj = tot[CS_POBJ] * L.scale_obj;
+      c.dobj = (tot[CS_ROW_DOBJ] + tot[CS_COL_DOBJ]) * L.scale_obj;
+      c.rel_p = sqrt(tot[CS_ROW_RES2]) / (1.0 + L.rhsnorm);
+      c.rel_d = sqrt(tot[CS_COL_RES2]) / (1.0 + L.cnorm);
+      c.gap = fabs(c.pobj - c.dobj) / (1.0 + fabs(c.pobj) + fabs(c.dobj));
+      if (c.rel_p <= a.tol && c.rel_d <= a.tol && c.gap <= a.tol) c.status = B2P_STATUS_OPTIMAL;
+    }
   }
   __syncthreads();
 }
@@ -217,9 +319,9 @@ __device__ __forceinline__ void write_out(const CtaArgs& a, const Ctl& c, int lp
   a.out[lp] = o;
 }
 
-template <class T>
-__device__ __forceinline__ void copy_in(T* __restrict__ dst, const T* __restrict__ src, int64_t len) {
-  for (int64_t t = threadIdx.x; t < len; t += blockDim.x) dst[t] = src[t];
+template <class T, class S>
+__device__ __forceinline__ void copy_in(T* __restrict__ dst, const S* __restrict__ src, int64_t len) {
+  for (int64_t t = threadIdx.x; t < len; t += blockDim.x) dst[t] = static_cast<T>(src[t]);
 }
 
 // Left-to-right row sum over entries [p, e) of (idx, val) against the local
@@ -227,11 +329,13 @@ __device__ __forceinline__ void copy_in(T* __restrict__ dst, const T* __restrict
 // that issued the loads of 4 or 8 entries before their additions measured
 // slower: the block is bound by shared-memory wavefronts -- scattered row
 // starts and gathers -- not by load latency.)
+template <class T>
 __device__ __forceinline__ double row_sum(int p, const int e, const int32_t* __restrict__ idx,
-                                          const double* __restrict__ val, const double* __restrict__ v, int shift) {
+                                          const T* __restrict__ val, const T* __restrict__ v, int shift) {
   double s = 0.0;
 #pragma unroll 4
-  for (; p < e; ++p) s = __dadd_rn(s, __dmul_rn(val[p], v[idx[p] - shift]));
+  for (; p < e; ++p)
+    s = __dadd_rn(s, __dmul_rn(static_cast<double>(val[p]), static_cast<double>(v[idx[p] - shift])));
   return s;
 }
 
@@ -282,28 +386,31 @@ __device__ __forceinline__ void col_check(double (&s)[kNumSums], double atyp, do
   s[CS_AX2] += d2 * d2;
 }
 
-template <int NT, int TIER>
+template <int NT, int TIER, class T>
 __device__ __forceinline__ void run_lp(const CtaArgs& a, const CtaLp& L, int lp, unsigned char* smem,
                                        Shared<NT>& sh) {
   const int m = L.m, n = L.n, tid = threadIdx.x;
-  double *x, *xp, *x0, *y, *yp, *y0, *ax, *axp, *ax0;
+  const CtaState<T> g = cta_state(a, static_cast<T*>(nullptr));
+  T *x, *xp, *x0, *y, *yp, *y0, *ax, *axp, *ax0;
   const double *c, *lo, *up, *cfac, *rl, *ru, *rfac;
   const int32_t *Ap, *Ai, *Tp, *Ti;
-  const double *Av, *Tv;
+  const T *Av, *Tv;
   if (TIER == kCtaGlobal) {
-    x = a.x + L.coff, xp = a.xp + L.coff, x0 = a.x0 + L.coff;
-    y = a.y + L.roff, yp = a.yp + L.roff, y0 = a.y0 + L.roff;
-    ax = a.ax + L.roff, axp = a.axp + L.roff, ax0 = a.ax0 + L.roff;
+    x = g.x + L.coff, xp = g.xp + L.coff, x0 = g.x0 + L.coff;
+    y = g.y + L.roff, yp = g.yp + L.roff, y0 = g.y0 + L.roff;
+    ax = g.ax + L.roff, axp = g.axp + L.roff, ax0 = g.ax0 + L.roff;
   } else {
-    double* d = reinterpret_cast<double*>(smem);
+    T* d = reinterpret_cast<T*>(smem);
     x = d, xp = x + n, x0 = xp + n;
     y = x0 + n, yp = y + m, y0 = yp + m, ax = y0 + m, axp = ax + m, ax0 = axp + m;
   }
   if (TIER == kCtaAll) {
-    double* d = ax0 + m;
+    double* d = reinterpret_cast<double*>(smem + sizeof(T) * cta_vector_elems(m, n, sizeof(T)));
     double *sc = d, *slo = sc + n, *sup = slo + n, *scf = sup + n, *srl = scf + n, *sru = srl + m, *srf = sru + m;
-    double *sAv = srf + m, *sTv = sAv + L.nnz;
-    int32_t* sAp = reinterpret_cast<int32_t*>(sTv + L.nnz);
+    T *sAv = reinterpret_cast<T*>(srf + m), *sTv = sAv + L.nnz;
+    int32_t* sAp = reinterpret_cast<int32_t*>(smem + sizeof(T) * cta_vector_elems(m, n, sizeof(T)) +
+                                              8 * (4 * static_cast<int64_t>(n) + 3 * m) +
+                                              (sizeof(T) * 2 * static_cast<int64_t>(L.nnz) + 7) / 8 * 8);
     int32_t *sAi = sAp + (m + 1), *sTp = sAi + L.nnz, *sTi = sTp + (n + 1);
     copy_in(sc, a.c + L.coff, n);
     copy_in(slo, a.lo + L.coff, n);
@@ -312,25 +419,25 @@ __device__ __forceinline__ void run_lp(const CtaArgs& a, const CtaLp& L, int lp,
     copy_in(srl, a.rl + L.roff, m);
     copy_in(sru, a.ru + L.roff, m);
     copy_in(srf, a.rfac + L.roff, m);
-    copy_in(sAv, a.A.val + L.a_beg, L.nnz);
-    copy_in(sTv, a.AT.val + L.t_beg, L.nnz);
+    copy_in(sAv, g.Av + L.a_beg, L.nnz);
+    copy_in(sTv, g.Tv + L.t_beg, L.nnz);
     copy_in(sAi, a.A.idx + L.a_beg, L.nnz);
     copy_in(sTi, a.AT.idx + L.t_beg, L.nnz);
-    for (int t = tid; t <= m; t += NT) sAp[t] = a.A.ptr[L.roff + t] - L.a_beg;
-    for (int t = tid; t <= n; t += NT) sTp[t] = a.AT.ptr[L.coff + t] - L.t_beg;
+    for (int t = tid; t <= m; t += NT) sAp[t] = a.A.ptr[L.aptr_off + t] - L.a_beg;
+    for (int t = tid; t <= n; t += NT) sTp[t] = a.AT.ptr[L.tptr_off + t] - L.t_beg;
     c = sc, lo = slo, up = sup, cfac = scf, rl = srl, ru = sru, rfac = srf;
     Ap = sAp, Ai = sAi, Av = sAv, Tp = sTp, Ti = sTi, Tv = sTv;
   } else {
     c = a.c + L.coff, lo = a.lo + L.coff, up = a.up + L.coff, cfac = a.cfac + L.coff;
     rl = a.rl + L.roff, ru = a.ru + L.roff, rfac = a.rfac + L.roff;
-    Ap = a.A.ptr + L.roff, Ai = a.A.idx, Av = a.A.val;
-    Tp = a.AT.ptr + L.coff, Ti = a.AT.idx, Tv = a.AT.val;
+    Ap = a.A.ptr + L.aptr_off, Ai = a.A.idx, Av = g.Av;
+    Tp = a.AT.ptr + L.tptr_off, Ti = a.AT.idx, Tv = g.Tv;
   }
   // starting point (x0 = x = x_init, y0 = y = y_init, A x0)
-  for (int j = tid; j < n; j += NT) x[j] = x0[j] = a.xinit[L.coff + j];
+  for (int j = tid; j < n; j += NT) x[j] = x0[j] = static_cast<T>(a.xinit[L.coff + j]);
   for (int i = tid; i < m; i += NT) {
-    y[i] = y0[i] = a.yinit[L.roff + i];
-    ax[i] = ax0[i] = a.axinit[L.roff + i];
+    y[i] = y0[i] = static_cast<T>(a.yinit[L.roff + i]);
+    ax[i] = ax0[i] = static_cast<T>(a.axinit[L.roff + i]);
   }
   if (tid == 0) init_ctl(sh.ctl, L);
   __syncthreads();
@@ -338,39 +445,56 @@ __device__ __forceinline__ void run_lp(const CtaArgs& a, const CtaLp& L, int lp,
   const double rho = a.rho;
   const int cE = a.check_every;
   double tau = sh.ctl.tau, sigma = sh.ctl.sigma;
-  int64_t restartAt = 0, it = 0;
-  while (it < a.max_it) {
+  int64_t restartAt = L.it0, it = L.it0;
+  if (a.entry_check) {
+    // the starting point measured as it is (x+ = x, y+ = y, A x+ = A x)
+    double s[kNumSums] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = tid; i < m; i += NT) {
+      const double yv = static_cast<double>(y[i]);
+      row_check(s, static_cast<double>(ax[i]), rl[i], ru[i], rfac[i], yv, yv, yv);
+      axp[i] = ax[i];
+      yp[i] = y[i];
+    }
+    for (int j = tid; j < n; j += NT) {
+      const double xv = static_cast<double>(x[j]);
+      col_check(s, row_sum(Tp[j], Tp[j + 1], Ti, Tv, y, L.tshift), c[j], lo[j], up[j], cfac[j], xv, xv, xv);
+      xp[j] = x[j];
+    }
+    entry_decide<NT>(s, sh, a, L);
+    if (sh.ctl.status) it = L.it0 - 1;  // reported as the check iteration that produced the point
+  }
+  while (!sh.ctl.status && it < a.max_it) {
     const int Lint = static_cast<int>((a.max_it - it) < cE ? (a.max_it - it) : cE);
     for (int l = 0; l < Lint; ++l) {
       const bool halpern = l != Lint - 1;
       const double lam = lambda_at(it + l - restartAt);
       // x+ = proj(x - tau (c - A^T y)), Halpern step of x
       for (int j = tid; j < n; j += NT) {
-        const double aty = row_sum(Tp[j], Tp[j + 1], Ti, Tv, y, L.roff);
-        const double xv = x[j];
+        const double aty = row_sum(Tp[j], Tp[j + 1], Ti, Tv, y, L.tshift);
+        const double xv = static_cast<double>(x[j]);
         double v = __dsub_rn(xv, __dmul_rn(tau, __dsub_rn(c[j], aty)));
         const double lj = lo[j], uj = up[j];
         v = (v < lj) ? lj : v;
         v = (uj < v) ? uj : v;
-        xp[j] = v;
-        if (halpern) x[j] = halpern_step(xv, v, x0[j], lam, rho);
+        xp[j] = static_cast<T>(v);
+        if (halpern) x[j] = static_cast<T>(halpern_step(xv, v, static_cast<double>(x0[j]), lam, rho));
       }
       __syncthreads();
       // A x+, y+ = v + sigma proj(-v / sigma), Halpern steps of y and A x
       for (int i = tid; i < m; i += NT) {
-        const double axpv = row_sum(Ap[i], Ap[i + 1], Ai, Av, xp, L.coff);
-        const double axv = ax[i], yv = y[i];
+        const double axpv = row_sum(Ap[i], Ap[i + 1], Ai, Av, xp, L.ashift);
+        const double axv = static_cast<double>(ax[i]), yv = static_cast<double>(y[i]);
         const double v = __dsub_rn(yv, __dmul_rn(sigma, __dsub_rn(__dmul_rn(2.0, axpv), axv)));
         double w = __ddiv_rn(-v, sigma);
         const double li = rl[i], ui = ru[i];
         w = (w < li) ? li : w;
         w = (ui < w) ? ui : w;
         const double ypv = __dadd_rn(v, __dmul_rn(sigma, w));
-        axp[i] = axpv;
-        yp[i] = ypv;
+        axp[i] = static_cast<T>(axpv);
+        yp[i] = static_cast<T>(ypv);
         if (halpern) {
-          y[i] = halpern_step(yv, ypv, y0[i], lam, rho);
-          ax[i] = halpern_step(axv, axpv, ax0[i], lam, rho);
+          y[i] = static_cast<T>(halpern_step(yv, ypv, static_cast<double>(y0[i]), lam, rho));
+          ax[i] = static_cast<T>(halpern_step(axv, axpv, static_cast<double>(ax0[i]), lam, rho));
         }
       }
       __syncthreads();
@@ -380,16 +504,17 @@ __device__ __forceinline__ void run_lp(const CtaArgs& a, const CtaLp& L, int lp,
     const double lam = lambda_at(it + Lint - 1 - restartAt);
     double s[kNumSums] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int i = tid; i < m; i += NT) {
-      const double yc = y[i], yv = yp[i];
-      row_check(s, axp[i], rl[i], ru[i], rfac[i], yv, yc, y0[i]);
-      y[i] = halpern_step(yc, yv, y0[i], lam, rho);
-      ax[i] = halpern_step(ax[i], axp[i], ax0[i], lam, rho);
+      const double yc = static_cast<double>(y[i]), yv = static_cast<double>(yp[i]);
+      const double y0v = static_cast<double>(y0[i]), axpv = static_cast<double>(axp[i]);
+      row_check(s, axpv, rl[i], ru[i], rfac[i], yv, yc, y0v);
+      y[i] = static_cast<T>(halpern_step(yc, yv, y0v, lam, rho));
+      ax[i] = static_cast<T>(halpern_step(static_cast<double>(ax[i]), axpv, static_cast<double>(ax0[i]), lam, rho));
     }
     for (int j = tid; j < n; j += NT) {
-      const double atyp = row_sum(Tp[j], Tp[j + 1], Ti, Tv, yp, L.roff);
-      const double xc = x[j], xpv = xp[j];
-      col_check(s, atyp, c[j], lo[j], up[j], cfac[j], xpv, xc, x0[j]);
-      x[j] = halpern_step(xc, xpv, x0[j], lam, rho);
+      const double atyp = row_sum(Tp[j], Tp[j + 1], Ti, Tv, yp, L.tshift);
+      const double xc = static_cast<double>(x[j]), xpv = static_cast<double>(xp[j]), x0v = static_cast<double>(x0[j]);
+      col_check(s, atyp, c[j], lo[j], up[j], cfac[j], xpv, xc, x0v);
+      x[j] = static_cast<T>(halpern_step(xc, xpv, x0v, lam, rho));
     }
     it += Lint - 1;
     check_decide<NT>(s, sh, a, L, it);
@@ -407,10 +532,10 @@ __device__ __forceinline__ void run_lp(const CtaArgs& a, const CtaLp& L, int lp,
     }
     ++it;
   }
-  // results: x+ and y+ to the engine's arrays, the scalars to out[lp]
-  if (TIER != kCtaGlobal) {
-    for (int j = tid; j < n; j += NT) a.xp[L.coff + j] = xp[j];
-    for (int i = tid; i < m; i += NT) a.yp[L.roff + i] = yp[i];
+  // results: x+ and y+ to the engine's FP64 arrays, the scalars to out[lp]
+  if (TIER != kCtaGlobal || sizeof(T) != sizeof(double)) {
+    for (int j = tid; j < n; j += NT) a.xp[L.coff + j] = static_cast<double>(xp[j]);
+    for (int i = tid; i < m; i += NT) a.yp[L.roff + i] = static_cast<double>(yp[i]);
   }
   write_out<NT>(a, sh.ctl, lp, it);
 }
@@ -435,8 +560,8 @@ __device__ __forceinline__ void run_owner(const CtaArgs& a, const CtaLp& L, int 
   copy_in(Av, a.A.val + L.a_beg, L.nnz);
   copy_in(Tv, a.AT.val + L.t_beg, L.nnz);
   for (int t = tid; t < L.nnz; t += NT) {
-    Ai[t] = a.A.idx[L.a_beg + t] - L.coff;
-    Ti[t] = a.AT.idx[L.t_beg + t] - L.roff;
+    Ai[t] = a.A.idx[L.a_beg + t] - L.ashift;
+    Ti[t] = a.AT.idx[L.t_beg + t] - L.tshift;
   }
   double x[R], x0[R], c[R], lo[R], up[R], xpr[R];
   double y[R], y0[R], ax[R], ax0[R], rl[R], ru[R], ypr[R], axpr[R];
@@ -448,16 +573,16 @@ __device__ __forceinline__ void run_owner(const CtaArgs& a, const CtaLp& L, int 
     x[r] = x0[r] = c[r] = lo[r] = up[r] = xpr[r] = 0.0;
     y[r] = y0[r] = ax[r] = ax0[r] = rl[r] = ru[r] = ypr[r] = axpr[r] = 0.0;
     if (e < n) {
-      tb[r] = a.AT.ptr[L.coff + e] - L.t_beg;
-      te[r] = a.AT.ptr[L.coff + e + 1] - L.t_beg;
+      tb[r] = a.AT.ptr[L.tptr_off + e] - L.t_beg;
+      te[r] = a.AT.ptr[L.tptr_off + e + 1] - L.t_beg;
       x[r] = x0[r] = a.xinit[L.coff + e];
       c[r] = a.c[L.coff + e];
       lo[r] = a.lo[L.coff + e];
       up[r] = a.up[L.coff + e];
     }
     if (e < m) {
-      ab[r] = a.A.ptr[L.roff + e] - L.a_beg;
-      ae[r] = a.A.ptr[L.roff + e + 1] - L.a_beg;
+      ab[r] = a.A.ptr[L.aptr_off + e] - L.a_beg;
+      ae[r] = a.A.ptr[L.aptr_off + e + 1] - L.a_beg;
       y[r] = y0[r] = a.yinit[L.roff + e];
       ax[r] = ax0[r] = a.axinit[L.roff + e];
       rl[r] = a.rl[L.roff + e];
@@ -568,18 +693,20 @@ __device__ __forceinline__ void run_owner(const CtaArgs& a, const CtaLp& L, int 
 
 }  // namespace cta
 
-template <int NT>
+// T = double: the plain FP64 run; T = float: the FP32 run of the mixed form.
+template <int NT, class T = double>
 __global__ void __launch_bounds__(NT) k_lp_cta(CtaArgs a) {
   extern __shared__ __align__(16) unsigned char cta_smem[];
   __shared__ cta::Shared<NT> sh;
   const int lp = a.order[blockIdx.x];
   const CtaLp L = a.lps[lp];
-  if (L.tier == kCtaAll)
-    cta::run_lp<NT, kCtaAll>(a, L, lp, cta_smem, sh);
-  else if (L.tier == kCtaVectors)
-    cta::run_lp<NT, kCtaVectors>(a, L, lp, cta_smem, sh);
+  const int tier = sizeof(T) == sizeof(double) ? L.tier : L.tier32;
+  if (tier == kCtaAll)
+    cta::run_lp<NT, kCtaAll, T>(a, L, lp, cta_smem, sh);
+  else if (tier == kCtaVectors)
+    cta::run_lp<NT, kCtaVectors, T>(a, L, lp, cta_smem, sh);
   else
-    cta::run_lp<NT, kCtaGlobal>(a, L, lp, cta_smem, sh);
+    cta::run_lp<NT, kCtaGlobal, T>(a, L, lp, cta_smem, sh);
 }
 
 template <int NT, int R>

@@ -50,6 +50,19 @@ struct SegTable {
   const int32_t* __restrict__ end;
 };
 
+// x_out = the projection of x onto [lo, up] (the FP64 run's starting point
+// from an FP32 run's x+, whose FP32 rounding may sit just outside a bound).
+__global__ void __launch_bounds__(kBlock) k_clamp_to_bounds(int32_t n, const double* __restrict__ x,
+                                                            const double* __restrict__ lo,
+                                                            const double* __restrict__ up, double* __restrict__ out) {
+  const int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  double v = x[j];
+  v = (v < lo[j]) ? lo[j] : v;
+  v = (up[j] < v) ? up[j] : v;
+  out[j] = v;
+}
+
 // Row part of the check for every live instance (see k_check_rows).
 __global__ void __launch_bounds__(kBlock) k_check_rows_multi(SegTable t, const int32_t* __restrict__ done,
                                                              const double* __restrict__ axp,
@@ -335,6 +348,21 @@ struct MultiEngine {
   int32_t* d_order = nullptr;
   CtaOut* d_out = nullptr;
   int32_t* h_stop = nullptr;  // host-mapped stop flag
+  // Mixed precision in the CTA form: an FP32 run of every LP (operators and
+  // state in FP32), then an FP64 run from each LP's FP32 point.
+  bool mixed = false;
+  // every LP has the same A (members of one family): the CTA form reads the
+  // first LP's copy of the (identically scaled) operators for all of them
+  bool shared_operator = false;
+  float *dA_val32 = nullptr, *dT_val32 = nullptr;
+  float* v32[9] = {};           // global-tier FP32 state: x, x+, x0 (N); y, y+, y0, Ax, Ax+, Ax0 (M)
+  int64_t cta_smem32 = 0;       // FP32 run: largest LP's tier bytes
+  int cta_nt32 = 256;           // FP32 run: threads per block
+  double *d_x2 = nullptr, *d_y2 = nullptr, *d_ax2 = nullptr;  // the FP64 run's starting point
+  CtaLp* d_lps2 = nullptr;
+  int32_t* d_order2 = nullptr;
+  std::vector<int32_t> host_order;  // largest LPs first
+  static constexpr int kStallChecks = 20;  // FP32 run: checks without a 10% KKT gain before it ends
 
   template <class T>
   T* dalloc(size_t count) {
@@ -383,6 +411,7 @@ struct MultiEngine {
     B2P_CUDA(cudaEventCreate(&ev_start));
     B2P_CUDA(cudaEventCreate(&ev_stop));
     K = num;
+    shared_operator = same_operator(lps, num);
     const auto t0 = Clock::now();
     // ---- host preparation of every instance (structure only), on all host threads ----
     P.resize(K);
@@ -590,6 +619,24 @@ struct MultiEngine {
     stats.precision_used = B2P_PRECISION_FP64;
   }
 
+  // Whether all LPs have one A: equal sizes and equal column pointers, row
+  // indices and values (the same arrays, or equal contents).  Scaling
+  // depends on A alone, so their scaled operators are then identical too.
+  static bool same_operator(const b2p_lp* lps, int num) {
+    if (num < 2) return false;
+    const b2p_lp& f = lps[0];
+    const int32_t nnz = f.start[f.num_cols];
+    for (int b = 1; b < num; ++b) {
+      const b2p_lp& l = lps[b];
+      if (l.num_rows != f.num_rows || l.num_cols != f.num_cols || l.start[l.num_cols] != nnz) return false;
+      if (l.start != f.start && std::memcmp(l.start, f.start, sizeof(int32_t) * (f.num_cols + 1)) != 0) return false;
+      if (nnz == 0) continue;
+      if (l.index != f.index && std::memcmp(l.index, f.index, sizeof(int32_t) * nnz) != 0) return false;
+      if (l.value != f.value && std::memcmp(l.value, f.value, sizeof(double) * nnz) != 0) return false;
+    }
+    return true;
+  }
+
   // ||A|| of every LP on the device (1.01 x the power-iteration estimate, as
   // prepare() computes on the host), bit-identical to the host's.
   void device_power_iterations(int iters) {
@@ -700,18 +747,20 @@ struct MultiEngine {
     if (opt.cta_smem_limit > 0) b = std::min<int64_t>(b, opt.cta_smem_limit);
     return std::max<int64_t>(b, 0);
   }
-  int cta_tier(int b, int64_t budget) const {
+  int cta_tier(int b, int64_t budget, int esize = 8) const {
     const Prepared& p = P[b];
     const int64_t nnz = static_cast<int64_t>(p.A.val.size());
-    if (cta_tier_bytes(kCtaAll, p.m, p.n, nnz) <= budget) return kCtaAll;
-    if (cta_tier_bytes(kCtaVectors, p.m, p.n, nnz) <= budget) return kCtaVectors;
+    if (cta_tier_bytes(kCtaAll, p.m, p.n, nnz, esize) <= budget) return kCtaAll;
+    if (cta_tier_bytes(kCtaVectors, p.m, p.n, nnz, esize) <= budget) return kCtaVectors;
     return kCtaGlobal;
   }
-  // AUTO: the CTA form when every LP fits wholly in one block's shared memory.
+  // AUTO: the CTA form when every LP fits wholly in one block's shared memory,
+  // or when all LPs share one A.
   bool choose_cta() const {
     if (opt.multi_form == B2P_MULTI_GRID) return false;
     if (opt.multi_form == B2P_MULTI_CTA) return true;
     if (opt.multi_form != B2P_MULTI_AUTO) throw Error(B2P_ERR_INVALID, "unknown multi_form");
+    if (shared_operator) return true;  // one operator in L2 for every block
     const int64_t budget = cta_budget();
     for (int b = 0; b < K; ++b)
       if (cta_tier(b, budget) != kCtaAll) return false;
@@ -731,16 +780,27 @@ struct MultiEngine {
       c.coff = static_cast<int32_t>(coff[b]);
       c.m = p.m;
       c.n = p.n;
-      c.a_beg = A.ptr[roff[b]];
-      c.t_beg = AT.ptr[coff[b]];
+      if (shared_operator) {
+        c.a_beg = c.t_beg = 0;
+        c.aptr_off = c.tptr_off = c.ashift = c.tshift = 0;
+      } else {
+        c.a_beg = A.ptr[roff[b]];
+        c.t_beg = AT.ptr[coff[b]];
+        c.aptr_off = c.tshift = static_cast<int32_t>(roff[b]);
+        c.tptr_off = c.ashift = static_cast<int32_t>(coff[b]);
+      }
       c.nnz = static_cast<int32_t>(p.A.val.size());
       c.tier = cta_tier(b, budget);
+      c.tier32 = cta_tier(b, budget, 4);
+      c.pad = 0;
+      c.it0 = 0;
       c.eta = eta[b];
       c.omega0 = omega0[b];
       c.cnorm = cNorm[b];
       c.rhsnorm = rhsNorm[b];
       c.scale_obj = p.beta * p.gamma;
       cta_smem = std::max(cta_smem, cta_tier_bytes(c.tier, p.m, p.n, c.nnz));
+      cta_smem32 = std::max(cta_smem32, cta_tier_bytes(c.tier32, p.m, p.n, c.nnz, 4));
       cta_owner_smem = std::max(cta_owner_smem, cta_owner_bytes(p.m, p.n, c.nnz));
       cta_max_dim = std::max(cta_max_dim, std::max(p.m, p.n));
       n_all += c.tier == kCtaAll;
@@ -753,6 +813,7 @@ struct MultiEngine {
     std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return inst_nnz[x] > inst_nnz[y]; });
     d_lps = upload(cta_lps);
     d_order = upload(order);
+    host_order = order;
     d_out = dalloc<CtaOut>(K);
     B2P_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&h_stop), sizeof(int32_t), cudaHostAllocMapped));
     *h_stop = 0;
@@ -764,7 +825,10 @@ struct MultiEngine {
   B2P_CUDA(cudaFuncSetAttribute(k_lp_owner<NT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, osmem));
     B2P_OWNER_VARIANTS(B2P_OWNER_ATTR)
 #undef B2P_OWNER_ATTR
+    mixed = opt.precision == B2P_PRECISION_MIXED;
+    if (mixed) setup_cta_fp32();
     tune_cta();
+    if (mixed) tune_cta_fp32();
     stats.cta_threads = cta_nt;
     stats.cta_owned_per_thread = cta_r;
     stats.cta_smem_bytes = cta_r ? cta_owner_smem : cta_smem;
@@ -785,16 +849,108 @@ struct MultiEngine {
     a.x = v[MX], a.xp = v[MXP], a.x0 = v[MX0];
     a.y = v[MY], a.yp = v[MYP], a.y0 = v[MY0];
     a.ax = v[MAX], a.axp = v[MAXP], a.ax0 = v[MAX0];
+    a.A32 = dA_val32, a.AT32 = dT_val32;
+    a.x32 = v32[0], a.xp32 = v32[1], a.x032 = v32[2];
+    a.y32 = v32[3], a.yp32 = v32[4], a.y032 = v32[5];
+    a.ax32 = v32[6], a.axp32 = v32[7], a.ax032 = v32[8];
     a.tol = tol;
     a.rho = opt.reflection;
     a.max_it = max_it;
     a.check_every = opt.check_every;
+    a.entry_check = 0;
+    a.stall_checks = 0;
+    a.pad = 0;
     a.stop = h_stop;
     return a;
   }
 
-  void launch_cta(int nt, int r, const CtaArgs& a) {
-    const unsigned grid = static_cast<unsigned>(K);
+  // FP32 run of the mixed form: FP32 copies of the scaled operators' values,
+  // FP32 global-tier state, the FP64 run's starting point, kernel attributes.
+  void setup_cta_fp32() {
+    const size_t annz = static_cast<size_t>(inst_nnz_total());
+    dA_val32 = dalloc<float>(annz);
+    dT_val32 = dalloc<float>(annz);
+    if (annz) {
+      k_convert<double, float><<<blocks(static_cast<int64_t>(annz)), kBlock, 0, stream>>>(annz, dA_val, dA_val32);
+      k_convert<double, float><<<blocks(static_cast<int64_t>(annz)), kBlock, 0, stream>>>(annz, dT_val, dT_val32);
+      B2P_CUDA(cudaGetLastError());
+    }
+    for (int q = 0; q < 9; ++q) v32[q] = dalloc<float>(q < 3 ? N : M);
+    d_x2 = dalloc<double>(N);
+    d_y2 = dalloc<double>(M);
+    d_ax2 = dalloc<double>(M);
+    d_lps2 = dalloc<CtaLp>(K);
+    d_order2 = dalloc<int32_t>(K);
+    const int smem = static_cast<int>(cta_smem32);
+    B2P_CUDA(cudaFuncSetAttribute(k_lp_cta<128, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    B2P_CUDA(cudaFuncSetAttribute(k_lp_cta<256, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    B2P_CUDA(cudaFuncSetAttribute(k_lp_cta<512, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  }
+  int64_t inst_nnz_total() const {
+    int64_t t = 0;
+    for (int b = 0; b < K; ++b) t += inst_nnz[b];
+    return t;
+  }
+
+  void launch_cta32(int nt, const CtaArgs& a, unsigned grid) {
+    const size_t smem = static_cast<size_t>(cta_smem32);
+    if (nt == 128)
+      k_lp_cta<128, float><<<grid, 128, smem, stream>>>(a);
+    else if (nt == 256)
+      k_lp_cta<256, float><<<grid, 256, smem, stream>>>(a);
+    else
+      k_lp_cta<512, float><<<grid, 512, smem, stream>>>(a);
+    B2P_CUDA(cudaGetLastError());
+  }
+
+  // Threads per block of the FP32 run: each count runs every LP for five
+  // check intervals, twice; the fastest is kept (remembered per batch shape).
+  void tune_cta_fp32() {
+    const auto t0 = Clock::now();
+    cta_nt32 = opt.cta_threads ? opt.cta_threads : 256;
+    const int64_t probe = std::min<int64_t>(opt.max_iterations, 5 * static_cast<int64_t>(opt.check_every));
+    if (opt.cta_threads != 0 || probe <= 0) return;
+    const std::vector<int64_t> key{device, K, cta_max_dim, cta_smem32, inst_nnz_total(), opt.check_every};
+    static std::mutex mu;
+    static std::map<std::vector<int64_t>, int> chosen;
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      const auto it = chosen.find(key);
+      if (it != chosen.end()) {
+        cta_nt32 = it->second;
+        return;
+      }
+    }
+    cudaEvent_t e0, e1;
+    B2P_CUDA(cudaEventCreate(&e0));
+    B2P_CUDA(cudaEventCreate(&e1));
+    double best = INFINITY;
+    for (const int nt : {128, 256, 512}) {
+      launch_cta32(nt, cta_args(-1.0, 1), static_cast<unsigned>(K));
+      for (int rep = 0; rep < 2; ++rep) {
+        B2P_CUDA(cudaEventRecord(e0, stream));
+        launch_cta32(nt, cta_args(-1.0, probe), static_cast<unsigned>(K));
+        B2P_CUDA(cudaEventRecord(e1, stream));
+        B2P_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        B2P_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) {
+          best = ms;
+          cta_nt32 = nt;
+        }
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    {
+      std::lock_guard<std::mutex> lock(mu);
+      chosen[key] = cta_nt32;
+    }
+    stats.autotune_seconds += seconds_since(t0);
+  }
+
+  void launch_cta(int nt, int r, const CtaArgs& a, int lps = -1) {
+    const unsigned grid = static_cast<unsigned>(lps < 0 ? K : lps);
     if (r == 0) {
       const size_t smem = static_cast<size_t>(cta_smem);
       if (nt == 128)
@@ -828,7 +984,7 @@ struct MultiEngine {
     if (want == B2P_CTA_AUTO || want == B2P_CTA_GENERAL)
       for (const int nt : {128, 256, 512})
         if (opt.cta_threads == 0 || opt.cta_threads == nt) c.emplace_back(nt, 0);
-    if (cta_owner_smem > 0 && want != B2P_CTA_GENERAL) {
+    if (cta_owner_smem > 0 && want != B2P_CTA_GENERAL && opt.precision != B2P_PRECISION_MIXED) {
 #define B2P_OWNER_CAND(NT, R)                                                                        \
   if ((opt.cta_threads == 0 || opt.cta_threads == NT) && cta_max_dim <= NT * R &&                    \
       (want == B2P_CTA_AUTO || want == B2P_CTA_OWNER1 + R - 1))                                      \
@@ -898,24 +1054,24 @@ struct MultiEngine {
     stats.autotune_seconds = seconds_since(t0);
   }
 
-  // The whole solve is one launch; the host only watches the deadline and
-  // the cancel flag and raises the mapped stop flag (read at every check).
+  // The whole solve is one launch (mixed precision: two, the FP32 run of
+  // every LP and the FP64 run from its point); the host only watches the
+  // deadline and the cancel flag and raises the mapped stop flag (read at
+  // every check).
   void solve_cta(Clock::time_point deadline_start) {
     const auto t_solve = Clock::now();
     results.assign(K, b2p_result{});
     xs.assign(K, {});
     ys.assign(K, {});
     *reinterpret_cast<volatile int32_t*>(h_stop) = 0;
-    B2P_CUDA(cudaEventRecord(ev_start, stream));
-    launch_cta(cta_nt, cta_r, cta_args(opt.tolerance, opt.max_iterations));
-    B2P_CUDA(cudaEventRecord(ev_stop, stream));
-    launches = 1;
-    if (opt.time_limit <= 0 && !opt.cancel_flag) {
-      B2P_CUDA(cudaEventSynchronize(ev_stop));
-    } else {
-      bool raised = false;
+    bool raised = false;
+    auto wait_for = [&](cudaEvent_t ev) {
+      if (opt.time_limit <= 0 && !opt.cancel_flag) {
+        B2P_CUDA(cudaEventSynchronize(ev));
+        return;
+      }
       for (;;) {
-        const cudaError_t q = cudaEventQuery(ev_stop);
+        const cudaError_t q = cudaEventQuery(ev);
         if (q == cudaSuccess) break;
         if (q != cudaErrorNotReady) B2P_CUDA(q);
         const bool expired = (opt.cancel_flag && *opt.cancel_flag) ||
@@ -926,26 +1082,94 @@ struct MultiEngine {
         }
         std::this_thread::sleep_for(std::chrono::microseconds(100));
       }
+    };
+    std::vector<CtaOut> out(K), out32;
+    std::vector<char> ran32(K, 0);
+    B2P_CUDA(cudaEventRecord(ev_start, stream));
+    if (!mixed) {
+      launch_cta(cta_nt, cta_r, cta_args(opt.tolerance, opt.max_iterations));
+      B2P_CUDA(cudaEventRecord(ev_stop, stream));
+      launches = 1;
+      wait_for(ev_stop);
+    } else {
+      // FP32 run of every LP
+      CtaArgs a1 = cta_args(opt.tolerance, opt.max_iterations);
+      a1.stall_checks = kStallChecks;
+      launch_cta32(cta_nt32, a1, static_cast<unsigned>(K));
+      B2P_CUDA(cudaEventRecord(ev_stop, stream));
+      wait_for(ev_stop);
+      out32.resize(K);
+      B2P_CUDA(cudaMemcpyAsync(out32.data(), d_out, sizeof(CtaOut) * K, cudaMemcpyDeviceToHost, stream));
+      B2P_CUDA(cudaStreamSynchronize(stream));
+      bytes_down += static_cast<int64_t>(sizeof(CtaOut) * K);
+      // FP64 run from each LP's FP32 point (measured first), as from a
+      // restart: its primal weight, the iteration count carried on
+      std::vector<CtaLp> lps2 = cta_lps;
+      std::vector<int32_t> order2;
+      for (int b = 0; b < K; ++b) {
+        const CtaOut& o = out32[b];
+        if (o.status == B2P_STATUS_TIME_LIMIT) continue;
+        lps2[b].omega0 = o.omega;
+        lps2[b].it0 = o.status == B2P_STATUS_ITERATION_LIMIT ? o.iterations : o.iterations + 1;
+        ran32[b] = 1;
+      }
+      for (int b = 0; b < K; ++b) {
+        const int lp = host_order[b];
+        if (ran32[lp]) order2.push_back(lp);
+      }
+      launches = 1;
+      if (!order2.empty()) {
+        B2P_CUDA(cudaMemcpyAsync(d_lps2, lps2.data(), sizeof(CtaLp) * K, cudaMemcpyHostToDevice, stream));
+        B2P_CUDA(cudaMemcpyAsync(d_order2, order2.data(), sizeof(int32_t) * order2.size(), cudaMemcpyHostToDevice,
+                                 stream));
+        bytes_up += static_cast<int64_t>(sizeof(CtaLp) * K + sizeof(int32_t) * order2.size());
+        if (N) k_clamp_to_bounds<<<blocks(N), kBlock, 0, stream>>>(N, v[MXP], v[MLO], v[MUP], d_x2);
+        if (M) {
+          B2P_CUDA(cudaMemcpyAsync(d_y2, v[MYP], sizeof(double) * M, cudaMemcpyDeviceToDevice, stream));
+          k_spmv<<<blocks(M), kBlock, 0, stream>>>(M, 1, viewA(), d_x2, d_ax2);
+        }
+        B2P_CUDA(cudaGetLastError());
+        CtaArgs a2 = cta_args(opt.tolerance, opt.max_iterations);
+        a2.lps = d_lps2;
+        a2.order = d_order2;
+        a2.xinit = d_x2;
+        a2.yinit = d_y2;
+        a2.axinit = d_ax2;
+        a2.entry_check = 1;
+        launch_cta(cta_nt, cta_r, a2, static_cast<int>(order2.size()));
+        launches += 3;
+      }
+      B2P_CUDA(cudaEventRecord(ev_stop, stream));
+      wait_for(ev_stop);
     }
     float ms = 0;
     B2P_CUDA(cudaEventElapsedTime(&ms, ev_start, ev_stop));
     stats.kernel_seconds = ms / 1000.0;
-    std::vector<CtaOut> out(K);
     std::vector<double> xp(N), yp(M);
     B2P_CUDA(cudaMemcpyAsync(out.data(), d_out, sizeof(CtaOut) * K, cudaMemcpyDeviceToHost, stream));
     if (N) B2P_CUDA(cudaMemcpyAsync(xp.data(), v[MXP], sizeof(double) * N, cudaMemcpyDeviceToHost, stream));
     if (M) B2P_CUDA(cudaMemcpyAsync(yp.data(), v[MYP], sizeof(double) * M, cudaMemcpyDeviceToHost, stream));
     B2P_CUDA(cudaStreamSynchronize(stream));
     bytes_down += static_cast<int64_t>(sizeof(CtaOut) * K + sizeof(double) * (static_cast<int64_t>(N) + M));
-    int64_t its = 0;
+    int64_t its = 0, its32 = 0;
     stats.restarts = 0;
     for (int b = 0; b < K; ++b) {
-      const CtaOut& o = out[b];
+      CtaOut o = out[b];
+      if (mixed) {
+        // an LP without an FP64 run keeps its FP32 result; one with both
+        // counts the switch as a restart
+        if (!ran32[b]) o = out32[b];
+        else o.restarts += out32[b].restarts + 1;
+        its32 = std::max<int64_t>(its32, out32[b].iterations);
+        if (o.status == kCtaStalled) o.status = B2P_STATUS_ITERATION_LIMIT;
+      }
       store_result(b, o.status, o.rel_kkt, o.pobj, o.dobj, o.iterations, xp.data() + coff[b], yp.data() + roff[b]);
       its = std::max<int64_t>(its, o.iterations + (o.status == B2P_STATUS_OPTIMAL ? 1 : 0));
       stats.restarts += o.restarts;
     }
     stats.iterations = its;
+    stats.fp32_iterations = its32;
+    stats.precision_used = mixed ? B2P_PRECISION_MIXED : B2P_PRECISION_FP64;
     stats.primal_weight = K ? out[0].omega : 1.0;
     stats.solve_seconds = seconds_since(t_solve);
     stats.kernel_launches = launches;

@@ -93,21 +93,38 @@ class RefineryFamily:
 
 class PcaBasis:
     """Standardised PCA: z -> ((z - mean) / scale) V, V the leading right
-    singular vectors of the standardised training matrix."""
+    singular vectors of the standardised training matrix.
 
-    def fit(self, Z: np.ndarray, rank: int) -> "PcaBasis":
+    The leading singular subspace is found by a randomized range finder
+    (Halko, Martinsson and Tropp, SIAM Review 53 (2011), Algorithms 4.4 and
+    5.1): the standardised matrix S (members x (n + m)) is multiplied by a
+    Gaussian test matrix of rank + `oversample` columns, `power` subspace
+    iterations (re-orthonormalised every time) sharpen the spectrum, and the
+    SVD of the small projected matrix gives the basis.  Work and memory are
+    O(members x (n + m) x (rank + oversample)), never the members x (n + m)
+    SVD, so solution vectors of hundreds of thousands of entries are fine.
+    The share of the total energy the basis keeps is recorded (`explained`)."""
+
+    def fit(self, Z: np.ndarray, rank: int, oversample: int = 16, power: int = 3, seed: int = 0) -> "PcaBasis":
         Z = np.asarray(Z, dtype=np.float64)
         self.mean = Z.mean(axis=0)
         sd = Z.std(axis=0)
         self.scale = np.where(sd > 1e-12 * max(1.0, float(np.abs(Z).max())), sd, 1.0)
         S = (Z - self.mean) / self.scale
-        _, sv, vt = np.linalg.svd(S, full_matrices=False)
+        members, width = S.shape
+        k = min(rank + oversample, members, width)
+        rng = np.random.default_rng(seed)
+        Q, _ = np.linalg.qr(S @ rng.standard_normal((width, k)))
+        for _ in range(power):
+            W, _ = np.linalg.qr(S.T @ Q)
+            Q, _ = np.linalg.qr(S @ W)
+        _, sv, vt = np.linalg.svd(Q.T @ S, full_matrices=False)
         r = min(rank, vt.shape[0])
         self.V = vt[:r].T.copy()
         if r < rank:  # pad with zero directions so the coefficient count stays `rank`
             self.V = np.hstack([self.V, np.zeros((self.V.shape[0], rank - r))])
-        energy = sv ** 2
-        self.explained = float(energy[:r].sum() / max(energy.sum(), 1e-300))
+        total = float(np.einsum("ij,ij->", S, S))
+        self.explained = float((sv[:r] ** 2).sum() / max(total, 1e-300))
         return self
 
     def encode(self, Z) -> np.ndarray:

@@ -226,3 +226,56 @@ def test_cta_iterates_bit_identical_to_oracle(oracle_mod, iters, kernel):
     for lp, r in zip(lps, rs):
         o = oracle_mod.solve(lp, "oracle", tolerance=1e-30, max_iterations=iters)
         assert np.array_equal(r.x, o.x) and np.array_equal(r.rowDual, o.y)
+
+
+# ---- mixed precision in the CTA form -----------------------------------------
+
+MIXED = dict(multiForm=_lib.MULTI_CTA, precision=_lib.PRECISION_MIXED)
+# Objective error of a mixed-form answer against the FP64 oracle's answer at
+# the same tolerance: both are 1e-6 points of the same LP, so they agree to
+# the tolerance's order, not to rounding.
+MIXED_OBJ_TOL = 1e-5
+
+
+@pytest.mark.parametrize("limit", [0, 64 * 1024, 1])
+def test_cta_mixed_converged_vs_fp64_oracle(oracle_mod, limit):
+    """FP32 run, FP64 re-measure and FP64 continuation, in each storage tier
+    of the FP32 run: every LP ends Optimal with its KKT recomputed in FP64 on
+    the host <= tol, and its objective within MIXED_OBJ_TOL of the FP64
+    oracle's."""
+    lps = family()
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, maxIterations=200000, ctaSmemLimit=limit, **MIXED))
+    st = _stats()
+    assert st.multi_form == _lib.MULTI_CTA and st.precision_used == _lib.PRECISION_MIXED
+    assert st.fp32_iterations > 0
+    for lp, r in zip(lps, rs):
+        o = oracle_mod.solve(lp, "oracle", tolerance=1e-6, max_iterations=200000)
+        assert r.status == "Optimal" and o.status == 1
+        assert abs(r.objective - o.objective) <= MIXED_OBJ_TOL * (1 + abs(o.objective)), (r.objective, o.objective)
+        if lp.num_rows:
+            assert max(_host_kkt(lp, r.x, r.rowDual)) <= 1e-6 * (1 + 1e-6)
+        assert np.all(r.x >= lp.col_lower) and np.all(r.x <= lp.col_upper)
+
+
+def test_cta_mixed_refinery_family_vs_fp64():
+    """A refinery family: the mixed form's answers meet the tolerance in FP64
+    and match the plain FP64 CTA form's objectives."""
+    fam = W.RefineryFamily(seed=5, periods=2, regions=1, units=4, streams=4, properties=2, scale_exponent=0.0)
+    lps = [fam.instance(p) for p in fam.sample(24, 11)]
+    plain = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, maxIterations=400000, **CTA))
+    mixed = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, maxIterations=400000, **MIXED))
+    for lp, p, q in zip(lps, plain, mixed):
+        assert p.status == q.status == "Optimal"
+        assert max(_host_kkt(lp, q.x, q.rowDual)) <= 1e-6 * (1 + 1e-6)
+        assert abs(p.objective - q.objective) <= MIXED_OBJ_TOL * (1 + abs(p.objective))
+
+
+def test_cta_mixed_iteration_limit_and_time_limit():
+    lps = family()
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-12, maxIterations=640, **MIXED))
+    for r in rs:
+        assert r.status in ("Optimal", "IterationLimit") and r.iterations <= 640
+    # a time limit reaches the runs through the mapped stop flag
+    lps = [G.random_lp(300, 600, 4.0, 180, 50 + i) for i in range(4)]
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-30, maxIterations=100_000_000, timeLimit=0.2, **MIXED))
+    assert all(r.status == "TimeLimit" and 0 < r.iterations < 100_000_000 for r in rs)
