@@ -39,6 +39,7 @@ Other workloads (each prints its own line; see their functions):
   plan       the reference's headline refinery plan (plan_60x156) to 1e-4 / 1e-6
   families   the batched leg of the reference's published repeated-solve runs
   calibrate  the reference's six per-iteration calibration LPs
+  gemm       the warm-start network's tcgen05 BF16 GEMM at its shapes (TFLOP/s)
 ``--impl reference --reference-backend gpu`` times the reference's own GPU
 backend on this GPU (config-2, or --workload plan / families / calibrate).
 """
@@ -973,6 +974,60 @@ def run_multi(args, rank, world):
     return 0
 
 
+GEMM_SHAPES = ((1024, 512, 512), (1024, 128, 512), (512, 512, 1024), (1024, 512, 16), (4096, 512, 512),
+               (8192, 8192, 8192))
+
+
+def measured_bf16_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["bf16_tflops"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback"
+
+
+def run_gemm(args, rank, world):
+    """--workload gemm: the warm-start network's tcgen05 BF16 GEMM (k_gemm_bf16_tc)
+    timed with CUDA events (b2p_mlp_gemm_bf16_time) at the network's shapes --
+    batch 1,024 through 512-wide hidden layers, the output layer, a weight
+    gradient (K = batch), the input layer -- and two larger ones, as TFLOP/s
+    of 2 M N K against the bf16 tensor peak."""
+    import ctypes as C
+
+    import torch
+
+    from pramana_b200 import _lib
+    if world > 1 and rank != 0:
+        return 0
+    torch.cuda.set_device(0)
+    lib = _lib.load()
+    peak, kind = measured_bf16_peak()
+    g = torch.Generator(device="cuda").manual_seed(0)
+    rows = []
+    for m, n, k in GEMM_SHAPES:
+        a = torch.randn(m, k, device="cuda", generator=g).to(torch.bfloat16)
+        bt = torch.randn(n, k, device="cuda", generator=g).to(torch.bfloat16)  # B(k, n) = bt[n, k]
+        c = torch.empty(m, n, device="cuda", dtype=torch.float32)
+        ms = C.c_double(0)
+        reps = max(3, min(200, int(2e11 // (2 * m * n * k))))
+        _lib.check(lib.b2p_mlp_gemm_bf16_time(m, n, k, a.data_ptr(), k, 1, bt.data_ptr(), 1, k, c.data_ptr(), n,
+                                              reps, C.byref(ms)))
+        ref = a.float() @ bt.float().t()
+        err = float((c - ref).abs().max() / ref.abs().max())
+        tflops = 2.0 * m * n * k / (ms.value * 1e-3) / 1e12
+        rows.append({"M": m, "N": n, "K": k, "us_per_launch": ms.value * 1e3, "tflops": tflops,
+                     "frac_of_peak": tflops / peak, "ctas": -(-m // 128) * -(-n // 128), "reps": reps,
+                     "max_rel_err_vs_fp32_matmul": err})
+    line = {"metric": "tcgen05 BF16 GEMM TFLOP/s at the warm-start network's shapes", "workload": "gemm",
+            "unit": "TFLOP/s", "value": max(r["tflops"] for r in rows), "higher_is_better": True,
+            "peak": peak, "peak_source": kind, "kernel": "k_gemm_bf16_tc (128x128 tile, 2 cp.async stages)",
+            "shapes": rows}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -984,7 +1039,7 @@ def main():
     ap.add_argument("--cpu-sample-iters", type=int, default=CPU_SAMPLE_ITERS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["lp", "family", "multi", "sweep", "router", "plan", "families",
-                                           "calibrate"], default="lp")
+                                           "calibrate", "gemm"], default="lp")
     ap.add_argument("--plan", default="plan_60x156", help="plan: which refinery plan of the published runs")
     ap.add_argument("--plan-tol", type=float, default=1e-4, help="plan: relative KKT tolerance (1e-4 or 1e-6)")
     ap.add_argument("--router-limit", type=float, default=3.0, help="router: time limit per engine and LP (s)")
@@ -1036,6 +1091,8 @@ def main():
         return run_families(args, rank, world)
     if args.workload == "calibrate":
         return run_calibrate(args, rank, world)
+    if args.workload == "gemm":
+        return run_gemm(args, rank, world)
 
     import torch
     dist = None

@@ -83,6 +83,14 @@ int b2p_mlp_gemm_bf16(int32_t M, int32_t N, int32_t K, const uint16_t* A, int64_
                       const uint16_t* mask, int64_t ldm, float* cf, int64_t ldcf, uint16_t* cb, int64_t ldcb,
                       void* stream);
 
+/* Kernel timing: the tensor-core GEMM of b2p_mlp_gemm_bf16 (alpha 1, no
+ * epilogue options, FP32 output) launched `reps` times back to back on a
+ * private stream after one warm-up launch, bracketed by CUDA events;
+ * *ms_per_launch = the events' elapsed time / reps.  Device pointers. */
+int b2p_mlp_gemm_bf16_time(int32_t M, int32_t N, int32_t K, const uint16_t* A, int64_t sam, int64_t sak,
+                           const uint16_t* B, int64_t sbk, int64_t sbn, float* cf, int64_t ldcf, int32_t reps,
+                           double* ms_per_launch);
+
 #ifdef __cplusplus
 }
 #endif

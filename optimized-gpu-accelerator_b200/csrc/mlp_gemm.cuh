@@ -3,18 +3,21 @@
 // accumulation in tensor memory, plus a fused epilogue (bias, ReLU, a 0/1
 // mask from a BF16 array, FP32 and/or BF16 output).
 //
-// One CTA (128 threads) computes a 128 x kBN tile.  Per K chunk of 64 the
-// threads copy A (128 x 64) and B (kBN x 64) into shared memory in the
-// K-major, non-swizzled canonical layout of the UMMA descriptors -- core
-// matrices of 8 rows x 16 bytes, the two 8-element K halves of a 16-wide slab
-// LBO = 128 B apart, consecutive 8-row groups SBO = 256 B apart -- then one
-// elected thread issues four tcgen05.mma (K = 16 each) into the TMEM
-// accumulator and commits them to an mbarrier that every thread waits on
-// before the shared memory is refilled.  The epilogue reads the accumulator
-// with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = tile rows).
-// A and B are read from global memory through element strides, so either
-// operand may be used transposed.  Waits are bounded: on a timeout the kernel
-// records an error, frees its TMEM and returns.
+// One CTA (128 threads) computes a 128 x kBN tile.  The K dimension runs in
+// chunks of 64 through two shared-memory stages: while the tensor core works
+// on chunk c from one stage, the threads already fetch chunk c + 1 into the
+// other (16-byte cp.async copies from global memory when the operand is
+// K-contiguous, element loads otherwise).  Each stage holds A (128 x 64) and
+// B (kBN x 64) in the K-major, non-swizzled canonical layout of the UMMA
+// descriptors -- core matrices of 8 rows x 16 bytes, the two 8-element K
+// halves of a 16-wide slab LBO = 128 B apart, consecutive 8-row groups SBO =
+// 256 B apart.  One elected thread issues four tcgen05.mma (K = 16 each) per
+// chunk into the TMEM accumulator and commits them to the stage's mbarrier;
+// a stage is refilled only after its mbarrier reports the MMAs that read it
+// complete.  The epilogue reads the accumulator with tcgen05.ld (warp w owns
+// TMEM lanes 32w..32w+31 = tile rows).  A and B are read through element
+// strides, so either operand may be used transposed.  Waits are bounded: on
+// a timeout the kernel records an error, frees its TMEM and returns.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -28,9 +31,12 @@ constexpr int kGemmBN = 128;
 constexpr int kGemmBK = 64;
 constexpr int kGemmThreads = 128;
 constexpr unsigned kMbarSpinLimit = 1u << 24;
-// shared memory: A chunk 16 KB + B chunk 16 KB; padded to 96 KB so that at
-// most two CTAs share an SM (2 x 128 TMEM columns <= 512)
+constexpr int kGemmStages = 2;
+constexpr int kGemmStageBytes = (kGemmBM + kGemmBN) * kGemmBK * 2;  // A 16 KB + B 16 KB
+// two stages (64 KB), padded to 96 KB so that at most two CTAs share an SM
+// (2 x 128 TMEM columns <= 512)
 constexpr int kGemmSmemBytes = 96 * 1024;
+static_assert(kGemmStages * kGemmStageBytes <= kGemmSmemBytes, "stages exceed the shared-memory budget");
 
 struct GemmArgs {
   int32_t M, N, K;
@@ -83,17 +89,22 @@ __device__ __forceinline__ uint32_t chunk_offset(int r, int k, int rows) {
 // Copy the rows [r0, r0 + rows) x K columns [k0, k0 + 64) of an operand
 // X(r, k) = X[r * sr + k * sk] into the canonical layout, zero-filling past
 // R and K.  vec: sk == 1 and 16-byte aligned rows, so one thread moves one
-// 8-element core-matrix row (16 bytes) per step; otherwise single elements,
-// row index fastest when sr == 1 (a transposed operand) for coalescing.
+// 8-element core-matrix row (16 bytes) per step as an asynchronous cp.async
+// (source size 0 past the edge: the hardware writes zeros); the caller waits
+// for them with cp.async.wait_group.  Otherwise single elements, stored
+// directly, row index fastest when sr == 1 (a transposed operand) for
+// coalescing.
 __device__ __forceinline__ void stage_operand(unsigned char* dst, const __nv_bfloat16* X, int64_t sr, int64_t sk,
                                               int r0, int R, int k0, int K, int rows, bool vec, int tid) {
   if (vec) {
     for (int e = tid; e < rows * (kGemmBK / 8); e += kGemmThreads) {
       const int r = e / (kGemmBK / 8), k = (e % (kGemmBK / 8)) * 8;
       const int gr = r0 + r, gk = k0 + k;
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (gr < R && gk < K) v = *reinterpret_cast<const uint4*>(X + gr * sr + gk);
-      *reinterpret_cast<uint4*>(dst + chunk_offset(r, k, rows)) = v;
+      const bool in = gr < R && gk < K;
+      const __nv_bfloat16* src = in ? X + gr * sr + gk : X;
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst + chunk_offset(r, k, rows))),
+                   "l"(src), "r"(in ? 16 : 0)
+                   : "memory");
     }
     return;
   }
@@ -130,16 +141,16 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
 
 static __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tc(GemmArgs g) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ __align__(8) uint64_t mbar;
+  __shared__ __align__(8) uint64_t mbar[kGemmStages];
   __shared__ uint32_t tmem_base_sh;
   __shared__ int failed_sh;
-  unsigned char* sA = smem;
-  unsigned char* sB = smem + kGemmBM * kGemmBK * 2;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.x * kGemmBM, n0 = blockIdx.y * kGemmBN;
 
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)) : "memory");
+#pragma unroll
+    for (int st = 0; st < kGemmStages; ++st)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[st])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     failed_sh = 0;
   }
@@ -156,19 +167,41 @@ static __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tc(GemmArgs g
   const uint32_t idesc = umma_idesc_bf16(kGemmBN);
   const int nchunks = (g.K + kGemmBK - 1) / kGemmBK;
   const bool vec_a = stage_vec_ok(g.A, g.sam, g.sak, g.K), vec_b = stage_vec_ok(g.B, g.sbn, g.sbk, g.K);
-  uint32_t phase = 0;
+  uint32_t phase[kGemmStages] = {0u, 0u};  // parity of each stage's next completion
+  auto stage_a = [&](int st) { return smem + st * kGemmStageBytes; };
+  auto stage_b = [&](int st) { return smem + st * kGemmStageBytes + kGemmBM * kGemmBK * 2; };
+  auto fetch = [&](int ch) {  // chunk ch into stage ch % 2, as one cp.async group
+    const int st = ch % kGemmStages, k0 = ch * kGemmBK;
+    stage_operand(stage_a(st), g.A, g.sam, g.sak, m0, g.M, k0, g.K, kGemmBM, vec_a, tid);
+    stage_operand(stage_b(st), g.B, g.sbn, g.sbk, n0, g.N, k0, g.K, kGemmBN, vec_b, tid);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  if (nchunks > 0) fetch(0);
   for (int ch = 0; ch < nchunks; ++ch) {
-    const int k0 = ch * kGemmBK;
-    stage_operand(sA, g.A, g.sam, g.sak, m0, g.M, k0, g.K, kGemmBM, vec_a, tid);
-    stage_operand(sB, g.B, g.sbn, g.sbk, n0, g.N, k0, g.K, kGemmBN, vec_b, tid);
+    const int st = ch % kGemmStages;
+    if (ch + 1 < nchunks) {
+      // the other stage was read by chunk ch - 1's MMAs: refill it once they are done
+      const int nx = (ch + 1) % kGemmStages;
+      if (ch >= 1) {
+        if (!mbar_wait(smem_u32(&mbar[nx]), phase[nx])) failed_sh = 1;
+        phase[nx] ^= 1u;
+      }
+      __syncthreads();
+      if (failed_sh) break;
+      fetch(ch + 1);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");  // chunk ch has landed
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a_base = smem_u32(stage_a(st)), b_base = smem_u32(stage_b(st));
 #pragma unroll
       for (int s = 0; s < kGemmBK / 16; ++s) {
-        const uint64_t da = umma_desc(smem_u32(sA) + s * (kGemmBM / 8) * 256, 128, 256);
-        const uint64_t db = umma_desc(smem_u32(sB) + s * (kGemmBN / 8) * 256, 128, 256);
+        const uint64_t da = umma_desc(a_base + s * (kGemmBM / 8) * 256, 128, 256);
+        const uint64_t db = umma_desc(b_base + s * (kGemmBN / 8) * 256, 128, 256);
         const uint32_t acc = (ch > 0 || s > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -179,15 +212,17 @@ static __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tc(GemmArgs g
             : "memory");
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       smem_u32(&mbar))
+                       smem_u32(&mbar[st]))
                    : "memory");
     }
-    // every thread waits for the MMAs before the shared memory is reused
-    if (!mbar_wait(smem_u32(&mbar), phase)) failed_sh = 1;
-    phase ^= 1u;
-    __syncthreads();
-    if (failed_sh) break;
   }
+  // the last commit tracks every MMA issued before it
+  if (nchunks > 0 && !failed_sh) {
+    const int st = (nchunks - 1) % kGemmStages;
+    if (!mbar_wait(smem_u32(&mbar[st]), phase[st])) failed_sh = 1;
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (!failed_sh) {
     // epilogue: thread = tile row (TMEM lane), 8 columns per tcgen05.ld

@@ -151,6 +151,8 @@ SIGNATURES = {
     "b2p_mlp_gemm_bf16": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, u16ptr, C.c_int64, C.c_int64, u16ptr,
                                     C.c_int64, C.c_int64, C.c_float, C.c_void_p, C.c_int32, u16ptr, C.c_int64,
                                     C.c_void_p, C.c_int64, u16ptr, C.c_int64, C.c_void_p]),
+    "b2p_mlp_gemm_bf16_time": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, u16ptr, C.c_int64, C.c_int64, u16ptr,
+                                         C.c_int64, C.c_int64, C.c_void_p, C.c_int64, C.c_int32, dptr]),
 }
 
 _lock = threading.Lock()

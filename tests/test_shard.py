@@ -72,3 +72,55 @@ def test_gather_on_two_gloo_ranks():
     assert keys == list(range(7))
     assert owners == [0 if i in partition([5, 1, 1, 3, 2, 8, 1], 2)[0] else 1 for i in range(7)]
     assert t == [1.5, 2.0]
+
+
+def _solve_worker(rank, world, port, out):
+    """One rank: its nnz-balanced share of an uneven family, each LP solved
+    by the CPU oracle, then the gather on rank 0."""
+    import torch.distributed as dist
+
+    from oracle import oracle as O
+    from pramana_b200.shard import gather, partition
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        sizes = G.uneven_family_sizes(10, 2e3, 2e4, seed=12)
+        mine = partition(sizes, world)[rank]
+        lps = G.uneven_family(10, 2e3, 2e4, seed=12, only=mine)
+        local = {}
+        for i, lp in zip(mine, lps):
+            r = O.solve(lp, "oracle", tolerance=1e-5, max_iterations=100000)
+            local[i] = {"status": r.status, "iterations": r.iterations, "objective": r.objective,
+                        "x": r.x.tolist(), "y": r.y.tolist(), "rank": rank}
+        merged = gather(local)
+        if rank == 0:
+            out.put(merged)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(300)
+def test_sharded_solves_equal_one_process_solves(oracle_mod):
+    """Two gloo ranks split an uneven family by nonzeros, solve their shares
+    and gather: every instance's answer equals the one-process answer (the
+    same solver on the same LP), and every instance is solved exactly once."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_solve_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    merged = q.get(timeout=280)
+    for p in procs:
+        p.join(60)
+    assert all(p.exitcode == 0 for p in procs)
+    assert sorted(merged) == list(range(10))
+    assert {merged[i]["rank"] for i in merged} == {0, 1}
+    for i, lp in enumerate(G.uneven_family(10, 2e3, 2e4, seed=12)):
+        r = oracle_mod.solve(lp, "oracle", tolerance=1e-5, max_iterations=100000)
+        got = merged[i]
+        assert got["status"] == r.status and got["iterations"] == r.iterations
+        assert got["objective"] == r.objective
+        assert np.array_equal(np.array(got["x"]), r.x) and np.array_equal(np.array(got["y"]), r.y)
