@@ -40,6 +40,7 @@ Other workloads (each prints its own line; see their functions):
   families   the batched leg of the reference's published repeated-solve runs
   calibrate  the reference's six per-iteration calibration LPs
   gemm       the warm-start network's tcgen05 BF16 GEMM at its shapes (TFLOP/s)
+  sweep-tol  256-case crude-price sweep of the refinery LP to certified rel KKT 1e-6
 ``--impl reference --reference-backend gpu`` times the reference's own GPU
 backend on this GPU (config-2, or --workload plan / families / calibrate).
 """
@@ -844,6 +845,128 @@ def run_sweep(args, rank, world):
     return 0
 
 
+def sweep_family(K: int):
+    """The crude-price sweep of the large refinery family (5,064 x 11,376,
+    57,178 nonzeros, unit row and column scales): K cases whose 6 crude prices
+    are permutations of a seeded grid over 40-120 $/bbl, demands at their
+    mid scale.  Returns (family, K x 16 parameters)."""
+    import numpy as np
+
+    from pramana_b200 import warmstart as W
+    fam = W.RefineryFamily(seed=5, **FAMILY_SIZES["large"])
+    rng = np.random.default_rng(9)
+    levels = np.linspace(40.0, 120.0, K)
+    prices = np.stack([rng.permutation(levels) for _ in range(fam.crudes)], axis=1)
+    return fam, np.hstack([prices, np.ones((K, fam.num_params - fam.crudes))])
+
+
+SWEEP_TOL_METRIC = "time to certified rel KKT 1e-6 (s) of a 256-case crude-price sweep of the refinery LP"
+
+
+def run_sweep_tol(args, rank, world):
+    """--workload sweep-tol: the crude-price sweep of the refinery LP solved to
+    rel KKT 1e-6, every case certified (KKT recomputed in FP64 and the
+    reference's family rule on the outward-rounded bound over implied column
+    bounds).  Forms: the shared-A batch engine (k-interleaved vectors, per-case
+    restarts) and the multi-LP CTA form (one thread block per case, the one
+    operator in L2), each in plain FP64 and in the mixed form (FP32 iterates,
+    FP64 termination, re-measure and polish).  Baseline: plain FP64 single-LP
+    solves of a sample of the cases, one at a time, scaled to all cases.
+    Each form: one short untimed solve (module load), then --steps timed
+    batches; value = the fastest form's mean wall time per batch plus its
+    certification."""
+    import numpy as np
+    import torch
+
+    from pramana_b200 import _lib, pdhg
+    from pramana_b200 import warmstart as W
+
+    if world > 1 and rank != 0:
+        return 0
+    torch.cuda.set_device(0)
+    K = args.cases
+    fam, params = sweep_family(K)
+    base = fam.base
+    cases = [fam.case(p) for p in params]
+    lps = [fam.instance(p) for p in params]
+    with open(os.path.join(ROOT, "tests", "golden", "answers.json")) as f:
+        ans = json.load(f)["sweep"]
+    sample = ans["sample"] if ans["cases"] == K else []
+    exact = dict(zip(sample, ans["exact"]))
+    forms = {}
+    with ClockSampler(0) as clk:
+        for name, prec, engine in (("batch_fp64", 0, "batch"), ("batch_mixed", 1, "batch"),
+                                   ("cta_fp64", 0, "cta"), ("cta_mixed", 1, "cta")):
+            if args.sweep_forms and name not in args.sweep_forms.split(","):
+                continue
+            kw = dict(tolerance=TOL, maxIterations=args.family_max_iters, precision=prec)
+            if engine == "cta":
+                kw["multiForm"] = _lib.MULTI_CTA
+            opts = pdhg.PdhgOptions(**kw)
+            short = pdhg.PdhgOptions(**{**kw, "maxIterations": 128})
+            walls, loops = [], []
+            for step in range(args.steps + 1):
+                o = short if step == 0 else opts
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                if engine == "batch":
+                    rs = pdhg.solvePdhgBatch(base, cases, o)
+                else:
+                    rs = pdhg.solvePdhgMulti(lps, o)
+                wall = time.perf_counter() - t0
+                if step > 0:
+                    walls.append(wall)
+                    loops.append(rs[0].stats.kernelSeconds)
+            X = np.array([r.x for r in rs])
+            Y = np.array([r.rowDual for r in rs])
+            t1 = time.perf_counter()
+            cert = W.certify_family(fam, params, X, Y, kkt_tol=TOL)
+            cert_s = time.perf_counter() - t1
+            obj = np.array([r.objective for r in rs])
+            err = [abs(obj[i] - e) / (1 + abs(e)) for i, e in exact.items()]
+            its = np.array([r.iterations for r in rs])
+            forms[name] = {"seconds_per_batch": statistics.mean(walls), "loop_seconds": statistics.mean(loops),
+                           "certify_seconds": cert_s, "optimal": int(sum(r.status == "Optimal" for r in rs)),
+                           "certified": int(cert["certified"].sum()),
+                           "certification_failures": int((~cert["certified"]).sum()),
+                           "max_relative_kkt_fp64": float(cert["kkt"][:, 3].max()),
+                           "iterations_mean": float(its.mean()), "iterations_max": int(its.max()),
+                           "fp32_iterations": int(rs[0].stats.fp32Iterations),
+                           "max_objective_rel_err_vs_exact_sample": float(max(err)) if err else None}
+    # baseline: plain FP64 single-LP solves, one case at a time
+    plain = pdhg.PdhgOptions(tolerance=TOL, maxIterations=args.family_max_iters, precision=0)
+    pick = [int(i) for i in np.linspace(0, K - 1, args.per_instance_sample).round()]
+    per, its1 = [], []
+    pdhg.solvePdhg(lps[0], pdhg.PdhgOptions(tolerance=TOL, maxIterations=128))
+    for i in pick:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = pdhg.solvePdhg(lps[i], plain)
+        per.append(time.perf_counter() - t0)
+        its1.append(r.iterations)
+    seq = statistics.mean(per) * K
+    best = min(forms, key=lambda k: forms[k]["seconds_per_batch"] + forms[k]["certify_seconds"])
+    value = forms[best]["seconds_per_batch"] + forms[best]["certify_seconds"]
+    line = {"metric": SWEEP_TOL_METRIC, "value": value, "unit": "s", "n_gpus": 1, "steps": args.steps,
+            "warmup": 1, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": f"{best}: " + ("f32 iterates, f64 checks and polish" if "mixed" in best
+                                                        else "f64"),
+            "data": "synthetic (seeded)", "workload": "sweep-tol",
+            "config": {"workload": f"refinery LP {base.num_rows} rows x {base.num_cols} cols, {base.nnz} nnz "
+                                   f"(12 periods, 6 crudes, 8 units, 12 pools, 2 regions, unit scales), {K} cases "
+                                   f"with the 6 crude prices on a seeded grid over 40-120, to rel KKT {TOL:g}, "
+                                   "every case certified",
+                       "step": "one batch call from host arrays plus certify_family on its answers"},
+            "chosen_form": best, "forms": forms,
+            "sequential_fp64": {"cases_timed": len(pick), "seconds_per_case": statistics.mean(per),
+                                "iterations_mean": float(np.mean(its1)), "seconds_all_cases_scaled": seq},
+            "speedup_vs_sequential_fp64": seq / value,
+            "exact_sample": {"cases": sample, "source": "the reference's dual simplex (tests/golden/answers.json)"},
+            "clocks": clk.summary()}
+    print(json.dumps(line))
+    return 0
+
+
 MULTI_METRIC = "time-to-1e-6 rel KKT (s) of a batch of uneven LPs in one multi-LP run & its HBM GB/s"
 
 
@@ -1039,7 +1162,7 @@ def main():
     ap.add_argument("--cpu-sample-iters", type=int, default=CPU_SAMPLE_ITERS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["lp", "family", "multi", "sweep", "router", "plan", "families",
-                                           "calibrate", "gemm"], default="lp")
+                                           "calibrate", "gemm", "sweep-tol"], default="lp")
     ap.add_argument("--plan", default="plan_60x156", help="plan: which refinery plan of the published runs")
     ap.add_argument("--plan-tol", type=float, default=1e-4, help="plan: relative KKT tolerance (1e-4 or 1e-6)")
     ap.add_argument("--router-limit", type=float, default=3.0, help="router: time limit per engine and LP (s)")
@@ -1057,6 +1180,7 @@ def main():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed",
                     help="family: arithmetic of the batched solves (the per-instance baseline is plain FP64)")
     ap.add_argument("--family-max-iters", type=int, default=400000, help="family: iteration limit per member")
+    ap.add_argument("--sweep-forms", default="", help="sweep-tol: comma-separated subset of the forms to run")
     ap.add_argument("--batch", type=int, default=1024, help="family: members per batched solve")
     ap.add_argument("--engine", choices=["multi", "batch"], default="multi",
                     help="family: multi-LP engine (one block per member) or the shared-A batch engine")
@@ -1093,6 +1217,8 @@ def main():
         return run_calibrate(args, rank, world)
     if args.workload == "gemm":
         return run_gemm(args, rank, world)
+    if args.workload == "sweep-tol":
+        return run_sweep_tol(args, rank, world)
 
     import torch
     dist = None

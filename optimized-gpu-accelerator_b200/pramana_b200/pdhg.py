@@ -105,6 +105,7 @@ class PdhgStats:
     spectralNorm: float = 0.0
     backend: str = "gpu"
     device: str = ""
+    fp32Iterations: int = 0  # mixed form: iterations run in FP32 (no counterpart in the reference)
 
     @classmethod
     def from_c(cls, s: _lib.B2pStats, device: str = "") -> "PdhgStats":
@@ -113,7 +114,7 @@ class PdhgStats:
                    setupSeconds=s.setup_seconds, solveSeconds=s.solve_seconds, kernelSeconds=s.kernel_seconds,
                    transferSeconds=s.transfer_seconds, bytesUploaded=s.bytes_uploaded,
                    bytesDownloaded=s.bytes_downloaded, kernelLaunches=s.kernel_launches,
-                   spectralNorm=s.spectral_norm, device=device)
+                   spectralNorm=s.spectral_norm, device=device, fp32Iterations=s.fp32_iterations)
 
     def toJson(self) -> dict:
         """Keys of PdhgStats::toJson (src/pdhg/pdhg.cpp:691-710)."""
