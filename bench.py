@@ -75,6 +75,20 @@ def workload_config(lp, world=1):
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
 
 
+def answer_errors(objective):
+    """Relative objective error of a config-2 answer against the reference's
+    FP64 CPU PDHG answer at TOL and against the exact optimum (its dual
+    simplex), both stored by tests/golden/make_answers_golden.py."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "answers.json")) as f:
+            a = json.load(f)["config2"]
+    except (OSError, KeyError, ValueError):
+        return {}
+    ref, exact = a[f"{TOL:g}"]["objective"], a["exact"]["objective"]
+    return {"objective_rel_err_vs_fp64_oracle": abs(objective - ref) / (1 + abs(ref)),
+            "objective_rel_err_vs_exact": abs(objective - exact) / (1 + abs(exact))}
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -1359,7 +1373,8 @@ def main():
                     "mixed": {"value": t_dev, "iterations": iters, "fp32_iterations": fp32_iters,
                               "relative_kkt_fp64": r_mixed.relativeKkt,
                               "objective_rel_diff_vs_fp64": abs(r_mixed.objective - r_plain.objective)
-                              / (1 + abs(r_plain.objective))},
+                              / (1 + abs(r_plain.objective)),
+                              **answer_errors(r_mixed.objective)},
                     "plain_fp64": {"value": t_plain, "iterations": r_plain.iterations,
                                    "relative_kkt": r_plain.relativeKkt,
                                    "e2e": {"value": t_e2e_plain, "unit": "s", "h2d_bytes_per_step": h2d,

@@ -107,9 +107,10 @@ inline PdhgStats stats(const b2p_stats& s) {
   return t;
 }
 
-// One solve (cases == nullptr) or a batch over a shared A.
-inline std::vector<PdhgResult> solve(const Model& lp, const std::vector<LpCase>* cases, const PdhgOptions& o,
-                                     const Deadline* dl, PdhgStats* batchStats) {
+// One solve (cases == nullptr) or a batch over a shared A; external linkage,
+// so that the routing may sit in src/pdhg/pdhg.cpp.
+std::vector<PdhgResult> solve(const Model& lp, const std::vector<LpCase>* cases, const PdhgOptions& o,
+                              const Deadline* dl, PdhgStats* batchStats) {
   const int n = lp.numCols(), m = lp.numRows();
   const int k = cases ? static_cast<int>(cases->size()) : 1;
   CancelRelay cancel(dl);
