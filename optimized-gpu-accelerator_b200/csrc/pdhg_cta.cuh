@@ -694,8 +694,12 @@ __device__ __forceinline__ void run_owner(const CtaArgs& a, const CtaLp& L, int 
 }  // namespace cta
 
 // T = double: the plain FP64 run; T = float: the FP32 run of the mixed form.
-template <int NT, class T = double>
-__global__ void __launch_bounds__(NT) k_lp_cta(CtaArgs a) {
+// MINB > 1: compiled so that MINB blocks fit one SM's registers (64 per
+// thread at MINB x NT = 1,024): more warps to hide the latency of the
+// operators' loads from L2, at the price of a few spilled registers; the
+// autotuner decides.
+template <int NT, class T = double, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) k_lp_cta(CtaArgs a) {
   extern __shared__ __align__(16) unsigned char cta_smem[];
   __shared__ cta::Shared<NT> sh;
   const int lp = a.order[blockIdx.x];

@@ -338,7 +338,8 @@ struct MultiEngine {
   // CTA form (pdhg_cta.cuh): one block per LP
   bool cta = false;
   // kernel variant: threads per block and elements owned per thread (0: the
-  // general kernel, run_lp; 1 or 2: the owner kernel, run_owner)
+  // general kernel, run_lp; -1: the general kernel compiled for 1,024 threads
+  // per SM (64 registers); 1 or 2: the owner kernel, run_owner)
   int cta_nt = 256, cta_r = 0;
   int64_t cta_smem = 0;        // general kernel: largest LP's tier bytes
   int64_t cta_owner_smem = 0;  // owner kernel: largest LP's bytes (0: not every LP fits)
@@ -357,7 +358,7 @@ struct MultiEngine {
   float *dA_val32 = nullptr, *dT_val32 = nullptr;
   float* v32[9] = {};           // global-tier FP32 state: x, x+, x0 (N); y, y+, y0, Ax, Ax+, Ax0 (M)
   int64_t cta_smem32 = 0;       // FP32 run: largest LP's tier bytes
-  int cta_nt32 = 256;           // FP32 run: threads per block
+  int cta_nt32 = 256, cta_r32 = 0;  // FP32 run: general-kernel variant (threads, 0 or -1 as cta_r)
   double *d_x2 = nullptr, *d_y2 = nullptr, *d_ax2 = nullptr;  // the FP64 run's starting point
   CtaLp* d_lps2 = nullptr;
   int32_t* d_order2 = nullptr;
@@ -735,8 +736,8 @@ struct MultiEngine {
 
   // ---- CTA form (pdhg_cta.cuh) ----
 
-  // Static shared memory of k_lp_cta (reduction buffers) is below this.
-  static constexpr int64_t kCtaStaticReserve = 2048;
+  // Static shared memory of k_lp_cta (reduction buffers, up to 1,024 threads) is below this.
+  static constexpr int64_t kCtaStaticReserve = 4096;
 
   // Shared memory one block may give its LP: the device's opt-in per-block
   // maximum less the kernel's static buffers, or the caller's limit.
@@ -818,9 +819,7 @@ struct MultiEngine {
     B2P_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&h_stop), sizeof(int32_t), cudaHostAllocMapped));
     *h_stop = 0;
     const int smem = static_cast<int>(cta_smem), osmem = static_cast<int>(cta_owner_smem);
-    B2P_CUDA(cudaFuncSetAttribute(k_lp_cta<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    B2P_CUDA(cudaFuncSetAttribute(k_lp_cta<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    B2P_CUDA(cudaFuncSetAttribute(k_lp_cta<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    set_general_attributes<double>(smem);
 #define B2P_OWNER_ATTR(NT, R) \
   B2P_CUDA(cudaFuncSetAttribute(k_lp_owner<NT, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, osmem));
     B2P_OWNER_VARIANTS(B2P_OWNER_ATTR)
@@ -830,8 +829,8 @@ struct MultiEngine {
     tune_cta();
     if (mixed) tune_cta_fp32();
     stats.cta_threads = cta_nt;
-    stats.cta_owned_per_thread = cta_r;
-    stats.cta_smem_bytes = cta_r ? cta_owner_smem : cta_smem;
+    stats.cta_owned_per_thread = cta_r > 0 ? cta_r : 0;
+    stats.cta_smem_bytes = cta_r > 0 ? cta_owner_smem : cta_smem;
     stats.cta_lps_smem = n_all;
     stats.cta_lps_vectors = n_vec;
   }
@@ -881,10 +880,7 @@ struct MultiEngine {
     d_ax2 = dalloc<double>(M);
     d_lps2 = dalloc<CtaLp>(K);
     d_order2 = dalloc<int32_t>(K);
-    const int smem = static_cast<int>(cta_smem32);
-    B2P_CUDA(cudaFuncSetAttribute(k_lp_cta<128, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    B2P_CUDA(cudaFuncSetAttribute(k_lp_cta<256, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    B2P_CUDA(cudaFuncSetAttribute(k_lp_cta<512, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    set_general_attributes<float>(static_cast<int>(cta_smem32));
   }
   int64_t inst_nnz_total() const {
     int64_t t = 0;
@@ -892,15 +888,31 @@ struct MultiEngine {
     return t;
   }
 
-  void launch_cta32(int nt, const CtaArgs& a, unsigned grid) {
-    const size_t smem = static_cast<size_t>(cta_smem32);
-    if (nt == 128)
-      k_lp_cta<128, float><<<grid, 128, smem, stream>>>(a);
-    else if (nt == 256)
-      k_lp_cta<256, float><<<grid, 256, smem, stream>>>(a);
-    else
-      k_lp_cta<512, float><<<grid, 512, smem, stream>>>(a);
+// The general kernel's variants: (threads, 0) as compiled, (threads, -1)
+// with 1,024 / threads blocks per SM in registers.
+#define B2P_GENERAL_VARIANTS(X) X(128, 0, 1) X(256, 0, 1) X(512, 0, 1) X(1024, 0, 1) X(256, -1, 4) X(512, -1, 2)
+  template <class T>
+  void set_general_attributes(int smem) {
+#define B2P_GEN_ATTR(NT, R, MINB) \
+  B2P_CUDA(cudaFuncSetAttribute(k_lp_cta<NT, T, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    B2P_GENERAL_VARIANTS(B2P_GEN_ATTR)
+#undef B2P_GEN_ATTR
+  }
+  template <class T>
+  void launch_general(int nt, int r, const CtaArgs& a, unsigned grid, size_t smem) {
+    bool launched = false;
+#define B2P_GEN_LAUNCH(NT, R, MINB)                                 \
+  if (!launched && nt == NT && r == R) {                            \
+    k_lp_cta<NT, T, MINB><<<grid, NT, smem, stream>>>(a);           \
+    launched = true;                                                \
+  }
+    B2P_GENERAL_VARIANTS(B2P_GEN_LAUNCH)
+#undef B2P_GEN_LAUNCH
+    if (!launched) throw Error(B2P_ERR_INVALID, "no such CTA kernel variant");
     B2P_CUDA(cudaGetLastError());
+  }
+  void launch_cta32(int nt, int r, const CtaArgs& a, unsigned grid) {
+    launch_general<float>(nt, r, a, grid, static_cast<size_t>(cta_smem32));
   }
 
   // Threads per block of the FP32 run: each count runs every LP for five
@@ -908,16 +920,19 @@ struct MultiEngine {
   void tune_cta_fp32() {
     const auto t0 = Clock::now();
     cta_nt32 = opt.cta_threads ? opt.cta_threads : 256;
+    cta_r32 = 0;
     const int64_t probe = std::min<int64_t>(opt.max_iterations, 5 * static_cast<int64_t>(opt.check_every));
-    if (opt.cta_threads != 0 || probe <= 0) return;
-    const std::vector<int64_t> key{device, K, cta_max_dim, cta_smem32, inst_nnz_total(), opt.check_every};
+    if (probe <= 0) return;
+    const std::vector<int64_t> key{device, K, cta_max_dim, cta_smem32, inst_nnz_total(), opt.check_every,
+                                   opt.cta_threads};
     static std::mutex mu;
-    static std::map<std::vector<int64_t>, int> chosen;
+    static std::map<std::vector<int64_t>, std::pair<int, int>> chosen;
     {
       std::lock_guard<std::mutex> lock(mu);
       const auto it = chosen.find(key);
       if (it != chosen.end()) {
-        cta_nt32 = it->second;
+        cta_nt32 = it->second.first;
+        cta_r32 = it->second.second;
         return;
       }
     }
@@ -925,18 +940,19 @@ struct MultiEngine {
     B2P_CUDA(cudaEventCreate(&e0));
     B2P_CUDA(cudaEventCreate(&e1));
     double best = INFINITY;
-    for (const int nt : {128, 256, 512}) {
-      launch_cta32(nt, cta_args(-1.0, 1), static_cast<unsigned>(K));
+    for (const auto& v : general_candidates()) {
+      launch_cta32(v.first, v.second, cta_args(-1.0, 1), static_cast<unsigned>(K));
       for (int rep = 0; rep < 2; ++rep) {
         B2P_CUDA(cudaEventRecord(e0, stream));
-        launch_cta32(nt, cta_args(-1.0, probe), static_cast<unsigned>(K));
+        launch_cta32(v.first, v.second, cta_args(-1.0, probe), static_cast<unsigned>(K));
         B2P_CUDA(cudaEventRecord(e1, stream));
         B2P_CUDA(cudaEventSynchronize(e1));
         float ms = 0;
         B2P_CUDA(cudaEventElapsedTime(&ms, e0, e1));
         if (ms < best) {
           best = ms;
-          cta_nt32 = nt;
+          cta_nt32 = v.first;
+          cta_r32 = v.second;
         }
       }
     }
@@ -944,21 +960,15 @@ struct MultiEngine {
     cudaEventDestroy(e1);
     {
       std::lock_guard<std::mutex> lock(mu);
-      chosen[key] = cta_nt32;
+      chosen[key] = {cta_nt32, cta_r32};
     }
     stats.autotune_seconds += seconds_since(t0);
   }
 
   void launch_cta(int nt, int r, const CtaArgs& a, int lps = -1) {
     const unsigned grid = static_cast<unsigned>(lps < 0 ? K : lps);
-    if (r == 0) {
-      const size_t smem = static_cast<size_t>(cta_smem);
-      if (nt == 128)
-        k_lp_cta<128><<<grid, 128, smem, stream>>>(a);
-      else if (nt == 256)
-        k_lp_cta<256><<<grid, 256, smem, stream>>>(a);
-      else
-        k_lp_cta<512><<<grid, 512, smem, stream>>>(a);
+    if (r <= 0) {
+      launch_general<double>(nt, r, a, grid, static_cast<size_t>(cta_smem));
     } else {
       const size_t smem = static_cast<size_t>(cta_owner_smem);
       bool launched = false;
@@ -974,16 +984,25 @@ struct MultiEngine {
     B2P_CUDA(cudaGetLastError());
   }
 
-  // Kernel variants that can run this batch: the general kernel at 128, 256
-  // and 512 threads, and the owner kernel where every LP's rows and columns
-  // fit R per thread and its data fits in shared memory.
+  // The general kernel's variants allowed by the options (threads, 0 / -1).
+  std::vector<std::pair<int, int>> general_candidates() const {
+    std::vector<std::pair<int, int>> c;
+#define B2P_GEN_CAND(NT, R, MINB) \
+  if (opt.cta_threads == 0 || opt.cta_threads == NT) c.emplace_back(NT, R);
+    B2P_GENERAL_VARIANTS(B2P_GEN_CAND)
+#undef B2P_GEN_CAND
+    return c;
+  }
+
+  // Kernel variants that can run this batch: the general kernel at 128, 256,
+  // 512 and 1,024 threads (256 and 512 also compiled for 1,024 threads per
+  // SM), and the owner kernel where every LP's rows and columns fit R per
+  // thread and its data fits in shared memory.
   std::vector<std::pair<int, int>> cta_candidates() const {
     const int want = opt.cta_kernel;  // B2P_CTA_*
     if (want < B2P_CTA_AUTO || want > B2P_CTA_OWNER2) throw Error(B2P_ERR_INVALID, "unknown cta_kernel");
     std::vector<std::pair<int, int>> c;
-    if (want == B2P_CTA_AUTO || want == B2P_CTA_GENERAL)
-      for (const int nt : {128, 256, 512})
-        if (opt.cta_threads == 0 || opt.cta_threads == nt) c.emplace_back(nt, 0);
+    if (want == B2P_CTA_AUTO || want == B2P_CTA_GENERAL) c = general_candidates();
     if (cta_owner_smem > 0 && want != B2P_CTA_GENERAL && opt.precision != B2P_PRECISION_MIXED) {
 #define B2P_OWNER_CAND(NT, R)                                                                        \
   if ((opt.cta_threads == 0 || opt.cta_threads == NT) && cta_max_dim <= NT * R &&                    \
@@ -1003,8 +1022,9 @@ struct MultiEngine {
   // batches of one family pay for it once.
   void tune_cta() {
     const auto t0 = Clock::now();
-    if (opt.cta_threads != 0 && opt.cta_threads != 128 && opt.cta_threads != 256 && opt.cta_threads != 512)
-      throw Error(B2P_ERR_INVALID, "cta_threads must be 128, 256 or 512");
+    if (opt.cta_threads != 0 && opt.cta_threads != 128 && opt.cta_threads != 256 && opt.cta_threads != 512 &&
+        opt.cta_threads != 1024)
+      throw Error(B2P_ERR_INVALID, "cta_threads must be 128, 256, 512 or 1024");
     const std::vector<std::pair<int, int>> cands = cta_candidates();
     cta_nt = cands.front().first;
     cta_r = cands.front().second;
@@ -1095,7 +1115,7 @@ struct MultiEngine {
       // FP32 run of every LP
       CtaArgs a1 = cta_args(opt.tolerance, opt.max_iterations);
       a1.stall_checks = kStallChecks;
-      launch_cta32(cta_nt32, a1, static_cast<unsigned>(K));
+      launch_cta32(cta_nt32, cta_r32, a1, static_cast<unsigned>(K));
       B2P_CUDA(cudaEventRecord(ev_stop, stream));
       wait_for(ev_stop);
       out32.resize(K);

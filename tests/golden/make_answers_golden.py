@@ -3,7 +3,9 @@ judged against at sizes too slow for the oracle inside a test.
 
 * config-2 (the bench LP, seed 2): the reference's own CPU PDHG
   (oracle/_ref, all host threads) to rel KKT 1e-6 and 1e-8 -- objective,
-  iterations -- and the exact optimum by the reference's dual simplex;
+  iterations; its 1e-8 objective stands for the optimum (the reference's
+  dual simplex does not finish this 40,000 x 80,000 LP within 20 minutes
+  here);
 * the crude-price sweep of the large refinery family (bench.py
   --workload sweep-tol): for a sample of its cases, the exact optimum by the
   reference's dual simplex.
@@ -39,9 +41,8 @@ def main():
         out["config2"][f"{tol:g}"] = {"objective": r.objective, "iterations": r.iterations,
                                       "relative_kkt": r.relative_kkt, "status": r.status}
         print("config2", tol, r.status, r.iterations, r.objective, flush=True)
-    ex = O.simplex(lp)
-    out["config2"]["exact"] = {"objective": ex["objective"], "status": ex["status"]}
-    print("config2 exact", ex, flush=True)
+    out["config2"]["exact"] = {"objective": out["config2"]["1e-08"]["objective"],
+                               "source": "the reference's CPU PDHG to rel KKT 1e-8"}
     fam, params = bench.sweep_family(256)
     sample = [int(i) for i in np.linspace(0, 255, 8).round()]
     out["sweep"] = {"cases": 256, "sample": sample, "exact": []}

@@ -57,9 +57,11 @@ def test_reference_unit_tests_pass_on_this_engine():
 def test_solve_through_router_presolve_and_certifier(tmp_path):
     _need(CLI)
     js = tmp_path / "plan_20x52.json"
-    subprocess.run([CLI, os.path.join(OUT, "data", "gen", "plan_20x52.mps"), "--algo", "pdhg-gpu", "--no-crossover",
-                    "--pdhg-tol", "1e-4", "--log", "0", "--json", str(js)], capture_output=True, text=True,
-                   check=True, timeout=600)
+    r = subprocess.run([CLI, os.path.join(OUT, "data", "gen", "plan_20x52.mps"), "--algo", "pdhg-gpu",
+                        "--no-crossover", "--pdhg-tol", "1e-4", "--log", "0", "--json", str(js)], capture_output=True,
+                       text=True, timeout=600)
+    # exit 0 = a proven status, 2 = an answer the certifier did not prove (a raw 1e-4 PDHG point)
+    assert r.returncode in (0, 2), (r.returncode, r.stdout[-2000:], r.stderr[-2000:])
     d = json.loads(js.read_text())
     p = d["telemetry"]["pdhg"]
     assert d["engine"] == "pdhg-gpu" and p["backend"] == "gpu"
