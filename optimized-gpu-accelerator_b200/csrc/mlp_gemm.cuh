@@ -225,9 +225,14 @@ static __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tc(GemmArgs g
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (!failed_sh) {
-    // epilogue: thread = tile row (TMEM lane), 8 columns per tcgen05.ld
+    // epilogue: thread = tile row (TMEM lane), 8 columns per tcgen05.ld; a
+    // thread's 8 consecutive outputs go out as 16- or 32-byte vector stores
+    // when the row stride and base allow it (one sector per store instead of
+    // eight scattered ones)
     const int row = warp * 32 + lane;
     const int gm = m0 + row;
+    const bool vec_f = g.cf && g.ldcf % 4 == 0 && (reinterpret_cast<uintptr_t>(g.cf) & 15) == 0;
+    const bool vec_b = g.cb && g.ldcb % 8 == 0 && (reinterpret_cast<uintptr_t>(g.cb) & 15) == 0;
     for (int c = 0; c < kGemmBN; c += 8) {
       uint32_t r[8];
       const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c);
@@ -236,17 +241,42 @@ static __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tc(GemmArgs g
           : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (gm < g.M) {
+      if (gm >= g.M || n0 + c >= g.N) continue;
+      float v[8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int gn = n0 + c + q;
-          if (gn >= g.N) continue;
-          float v = __uint_as_float(r[q]) * g.alpha;
-          if (g.bias) v += g.bias[gn];
-          if (g.relu) v = v > 0.0f ? v : 0.0f;
-          if (g.mask && !(__bfloat162float(g.mask[gm * g.ldm + gn]) > 0.0f)) v = 0.0f;
-          if (g.cf) g.cf[gm * g.ldcf + gn] = v;
-          if (g.cb) g.cb[gm * g.ldcb + gn] = __float2bfloat16(v);
+      for (int q = 0; q < 8; ++q) {
+        const int gn = n0 + c + q;
+        float t = __uint_as_float(r[q]) * g.alpha;
+        if (gn < g.N) {
+          if (g.bias) t += g.bias[gn];
+          if (g.relu) t = t > 0.0f ? t : 0.0f;
+          if (g.mask && !(__bfloat162float(g.mask[gm * g.ldm + gn]) > 0.0f)) t = 0.0f;
+        }
+        v[q] = t;
+      }
+      const bool full = n0 + c + 8 <= g.N;
+      if (g.cf) {
+        float* dst = g.cf + gm * g.ldcf + n0 + c;
+        if (vec_f && full) {
+          reinterpret_cast<float4*>(dst)[0] = make_float4(v[0], v[1], v[2], v[3]);
+          reinterpret_cast<float4*>(dst)[1] = make_float4(v[4], v[5], v[6], v[7]);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            if (n0 + c + q < g.N) dst[q] = v[q];
+        }
+      }
+      if (g.cb) {
+        __nv_bfloat16* dst = g.cb + gm * g.ldcb + n0 + c;
+        if (vec_b && full) {
+          __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) h[q] = __float2bfloat16(v[q]);
+          *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(h);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            if (n0 + c + q < g.N) dst[q] = __float2bfloat16(v[q]);
         }
       }
     }

@@ -11,6 +11,9 @@
 //                 operators (CSR of A and A^T) in shared memory;
 //   kCtaVectors : the nine iterate / anchor vectors in shared memory, the
 //                 operators and constants read from global memory (L1/L2);
+//   kCtaVectorsPtr : as kCtaVectors, plus both operators' row pointers in
+//                 shared memory (one L2 round trip less at the head of every
+//                 row sum's chain of dependent loads);
 //   kCtaGlobal  : everything in global memory (the engine's state arrays).
 // The iteration is the engine's arithmetic element by element: every row sum
 // runs left to right with separately rounded products and sums (the
@@ -44,7 +47,7 @@
 
 namespace b2p {
 
-enum CtaTier : int32_t { kCtaAll = 0, kCtaVectors = 1, kCtaGlobal = 2 };
+enum CtaTier : int32_t { kCtaAll = 0, kCtaVectors = 1, kCtaGlobal = 2, kCtaVectorsPtr = 3 };
 
 // Per LP: where it sits in the concatenated operators and vectors, and the
 // scalars its decisions need (src/pdhg/pdhg.cpp:506-545).
@@ -129,6 +132,7 @@ __host__ __device__ inline int64_t cta_tier_bytes(int tier, int64_t m, int64_t n
   if (tier == kCtaGlobal) return 0;
   const int64_t vec = esize * cta_vector_elems(m, n, esize);
   if (tier == kCtaVectors) return vec;
+  if (tier == kCtaVectorsPtr) return vec + (4 * ((m + 1) + (n + 1)) + 7) / 8 * 8;
   const int64_t vals = (esize * 2 * nnz + 7) / 8 * 8;
   return vec + 8 * (4 * n + 3 * m) + vals + 4 * ((m + 1) + (n + 1) + 2 * nnz);
 }
@@ -432,6 +436,12 @@ __device__ __forceinline__ void run_lp(const CtaArgs& a, const CtaLp& L, int lp,
     rl = a.rl + L.roff, ru = a.ru + L.roff, rfac = a.rfac + L.roff;
     Ap = a.A.ptr + L.aptr_off, Ai = a.A.idx, Av = g.Av;
     Tp = a.AT.ptr + L.tptr_off, Ti = a.AT.idx, Tv = g.Tv;
+    if (TIER == kCtaVectorsPtr) {
+      int32_t* sp = reinterpret_cast<int32_t*>(smem + sizeof(T) * cta_vector_elems(m, n, sizeof(T)));
+      copy_in(sp, Ap, m + 1);
+      copy_in(sp + m + 1, Tp, n + 1);
+      Ap = sp, Tp = sp + m + 1;
+    }
   }
   // starting point (x0 = x = x_init, y0 = y = y_init, A x0)
   for (int j = tid; j < n; j += NT) x[j] = x0[j] = static_cast<T>(a.xinit[L.coff + j]);
@@ -707,6 +717,8 @@ __global__ void __launch_bounds__(NT, MINB) k_lp_cta(CtaArgs a) {
   const int tier = sizeof(T) == sizeof(double) ? L.tier : L.tier32;
   if (tier == kCtaAll)
     cta::run_lp<NT, kCtaAll, T>(a, L, lp, cta_smem, sh);
+  else if (tier == kCtaVectorsPtr)
+    cta::run_lp<NT, kCtaVectorsPtr, T>(a, L, lp, cta_smem, sh);
   else if (tier == kCtaVectors)
     cta::run_lp<NT, kCtaVectors, T>(a, L, lp, cta_smem, sh);
   else

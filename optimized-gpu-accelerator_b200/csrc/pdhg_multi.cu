@@ -752,6 +752,7 @@ struct MultiEngine {
     const Prepared& p = P[b];
     const int64_t nnz = static_cast<int64_t>(p.A.val.size());
     if (cta_tier_bytes(kCtaAll, p.m, p.n, nnz, esize) <= budget) return kCtaAll;
+    if (cta_tier_bytes(kCtaVectorsPtr, p.m, p.n, nnz, esize) <= budget) return kCtaVectorsPtr;
     if (cta_tier_bytes(kCtaVectors, p.m, p.n, nnz, esize) <= budget) return kCtaVectors;
     return kCtaGlobal;
   }
@@ -805,7 +806,7 @@ struct MultiEngine {
       cta_owner_smem = std::max(cta_owner_smem, cta_owner_bytes(p.m, p.n, c.nnz));
       cta_max_dim = std::max(cta_max_dim, std::max(p.m, p.n));
       n_all += c.tier == kCtaAll;
-      n_vec += c.tier == kCtaVectors;
+      n_vec += c.tier == kCtaVectors || c.tier == kCtaVectorsPtr;
     }
     if (cta_owner_smem > budget) cta_owner_smem = 0;
     // largest LPs first, so that the small ones fill in behind them

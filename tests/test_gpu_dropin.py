@@ -69,8 +69,10 @@ def test_solve_through_router_presolve_and_certifier(tmp_path):
     assert p["relative_kkt"] <= 1e-4
     assert abs(p["objective"] - (-524258.98167169833)) <= 1e-8 * 524258.98167169833
     c = d["certificate"]
-    # the certifier ran on the postsolved answer; its safe bound is a valid lower bound of the optimum
-    assert c["claimed_status"] == "OPTIMAL" and c["safe_dual_bound"] <= c["primal_objective"] + 1e-6 * 524258.98
+    # the certifier ran on the postsolved answer of this maximisation model: its safe bound lies above
+    # the objective, 7.8e-4 relative away at this 1e-4 point (as on the reference's CPU engine)
+    assert c["claimed_status"] == "OPTIMAL"
+    assert c["primal_objective"] <= c["safe_dual_bound"] <= c["primal_objective"] * (1 + 1e-3)
 
 
 def test_reference_family_strategy_on_this_engine(tmp_path):
