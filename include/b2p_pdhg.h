@@ -70,7 +70,11 @@ enum {
    * point (the FP64 polish).  A batch (num_cases > 1) runs in FP32 until
    * every case has met the tolerance there or stalled, then re-measures all
    * cases in FP64: those that pass terminate, the rest continue in FP64.  A
-   * single LP too large for the resident form runs in FP64. */
+   * single LP too large for the resident form runs in FP64.  Many LPs
+   * (b2p_solve_pdhg_multi) in the CTA form: every LP runs in FP32 until its
+   * FP32 point meets the tolerance or stalls, then in FP64 from that point,
+   * measured first; the block-diagonal form runs FP64 (stats.precision_used
+   * says which ran). */
   B2P_PRECISION_MIXED = 1
 };
 
@@ -145,8 +149,8 @@ typedef struct b2p_options {
    * per-block maximum); an LP that does not fit keeps its operators, or all
    * of its data, in global memory. */
   int32_t cta_smem_limit;
-  /* CTA form: threads per block (128, 256 or 512; 0 = autotuned with the
-   * kernel variant). */
+  /* CTA form: threads per block (128, 256, 512 or 1024; 0 = autotuned with
+   * the kernel variant). */
   int32_t cta_threads;
   /* CTA form: kernel variant (B2P_CTA_*; 0 = autotuned): the general kernel
    * (any LP size, three storage tiers) or the owner kernel, whose threads
