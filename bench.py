@@ -859,15 +859,15 @@ def run_sweep(args, rank, world):
     return 0
 
 
-def sweep_family(K: int):
-    """The crude-price sweep of the large refinery family (5,064 x 11,376,
-    57,178 nonzeros, unit row and column scales): K cases whose 6 crude prices
-    are permutations of a seeded grid over 40-120 $/bbl, demands at their
-    mid scale.  Returns (family, K x 16 parameters)."""
+def sweep_family(K: int, size: str = "large"):
+    """The crude-price sweep of a refinery family (by default the large one:
+    5,064 x 11,376, 57,178 nonzeros, unit row and column scales): K cases whose
+    6 crude prices are permutations of a seeded grid over 40-120 $/bbl,
+    demands at their mid scale.  Returns (family, K x 16 parameters)."""
     import numpy as np
 
     from pramana_b200 import warmstart as W
-    fam = W.RefineryFamily(seed=5, **FAMILY_SIZES["large"])
+    fam = W.RefineryFamily(seed=5, **FAMILY_SIZES[size])
     rng = np.random.default_rng(9)
     levels = np.linspace(40.0, 120.0, K)
     prices = np.stack([rng.permutation(levels) for _ in range(fam.crudes)], axis=1)
@@ -899,13 +899,13 @@ def run_sweep_tol(args, rank, world):
         return 0
     torch.cuda.set_device(0)
     K = args.cases
-    fam, params = sweep_family(K)
+    fam, params = sweep_family(K, args.family_size)
     base = fam.base
     cases = [fam.case(p) for p in params]
     lps = [fam.instance(p) for p in params]
     with open(os.path.join(ROOT, "tests", "golden", "answers.json")) as f:
         ans = json.load(f)["sweep"]
-    sample = ans["sample"] if ans["cases"] == K else []
+    sample = ans["sample"] if ans["cases"] == K and args.family_size == "large" else []
     exact = dict(zip(sample, ans["exact"]))
     forms = {}
     with ClockSampler(0) as clk:
@@ -966,8 +966,8 @@ def run_sweep_tol(args, rank, world):
             "vs_baseline": None, "dtype": f"{best}: " + ("f32 iterates, f64 checks and polish" if "mixed" in best
                                                         else "f64"),
             "data": "synthetic (seeded)", "workload": "sweep-tol",
-            "config": {"workload": f"refinery LP {base.num_rows} rows x {base.num_cols} cols, {base.nnz} nnz "
-                                   f"(12 periods, 6 crudes, 8 units, 12 pools, 2 regions, unit scales), {K} cases "
+            "config": {"workload": f"refinery LP ({args.family_size}) {base.num_rows} rows x {base.num_cols} cols, "
+                                   f"{base.nnz} nnz ({FAMILY_SIZES[args.family_size]}), {K} cases "
                                    f"with the 6 crude prices on a seeded grid over 40-120, to rel KKT {TOL:g}, "
                                    "every case certified",
                        "step": "one batch call from host arrays plus certify_family on its answers"},
@@ -1189,8 +1189,9 @@ def main():
     ap.add_argument("--schedule", choices=["auto", "binned", "tiled", "tuned"], default="auto",
                     help="multi: SpMV schedule of the multi-LP kernels")
     ap.add_argument("--train", type=int, default=32768, help="family: training members")
-    ap.add_argument("--family-size", choices=sorted(FAMILY_SIZES), default="small",
-                    help="family: refinery LP size (small 164 x 324, medium 1,692 x 3,528, large 5,064 x 11,376)")
+    ap.add_argument("--family-size", choices=sorted(FAMILY_SIZES), default=None,
+                    help="family / sweep-tol: refinery LP size (small 164 x 324, medium 1,692 x 3,528, large "
+                         "5,064 x 11,376; default medium for family, large for sweep-tol)")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed",
                     help="family: arithmetic of the batched solves (the per-instance baseline is plain FP64)")
     ap.add_argument("--family-max-iters", type=int, default=400000, help="family: iteration limit per member")
@@ -1205,6 +1206,8 @@ def main():
                     help="small case for ncu: stop every solve after this many iterations, skip e2e and the CPU "
                          "baseline; the printed line is not a benchmark result")
     args = ap.parse_args()
+    if args.family_size is None:
+        args.family_size = "large" if args.workload == "sweep-tol" else "medium"
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.steps < 1:
