@@ -50,7 +50,7 @@ class PdhgOptions:
     spmvSchedule: int = _lib.SCHEDULE_AUTO  # multi-LP SpMV schedule (SCHEDULE_BINNED / _TILED / _TUNED)
     multiForm: int = _lib.MULTI_AUTO  # multi-LP engine form (MULTI_GRID / MULTI_CTA)
     ctaSmemLimit: int = 0  # CTA form: shared-memory bytes one LP may use (0 = device maximum)
-    ctaThreads: int = 0  # CTA form: threads per block (128 / 256 / 512; 0 = autotuned)
+    ctaThreads: int = 0  # CTA form: threads per block (128 / 256 / 512 / 1024; 0 = autotuned)
     ctaKernel: int = _lib.CTA_AUTO  # CTA form: CTA_GENERAL / CTA_OWNER1 / CTA_OWNER2 (0 = autotuned)
     batchVariant: int = 0  # FP64 batches: 0 = tuned; 1..4 = (cases per thread, streamed) (1,no) (2,no) (1,yes) (2,yes)
 
