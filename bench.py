@@ -806,6 +806,21 @@ def run_sweep(args, rank, world):
         prof[name] = {"launches": n_l, "avg_us": ms / n_l * 1e3, "bytes_per_launch": eng.kernel_bytes(cls),
                       "gbs": eng.kernel_bytes(cls) / (ms / n_l / 1e3) / 1e9}
     eng.close()
+    # the same batch in the mixed form: the FP32 k-interleaved kernels (classes 3 and 4)
+    eng32 = pdhg.Engine(base, pdhg.PdhgOptions(tolerance=1e-4, maxIterations=iters, precision=1), cases)
+    eng32.solve()
+    eng32.set_profiling(True)
+    flush.zero_()
+    torch.cuda.synchronize()
+    eng32.solve()
+    eng32.set_profiling(False)
+    prof32 = {}
+    for cls, name in ((3, "k_primal32"), (4, "k_dual32")):
+        n_l, ms = eng32.kernel_times(cls)
+        if n_l:
+            prof32[name] = {"launches": n_l, "avg_us": ms / n_l * 1e3, "bytes_per_launch": eng32.kernel_bytes(cls),
+                            "gbs": eng32.kernel_bytes(cls) / (ms / n_l / 1e3) / 1e9}
+    eng32.close()
     nnz, m, n = base.nnz, base.num_rows, base.num_cols
     ref_model = 24.0 * nnz + 80.0 * (m + n) * K  # the reference's effective-bandwidth model, per iteration
     fused_bytes = sum(p["bytes_per_launch"] for p in prof.values())
@@ -842,6 +857,7 @@ def run_sweep(args, rank, world):
             "status": {"optimal": int(sum(r.status == "Optimal" for r in rs)),
                        "max_relative_kkt": float(max(r.relativeKkt for r in rs))},
             "kernels": prof,
+            "kernels_fp32": prof32,
             "reference_model_gbs": ref_model / (t_dev / iters) / 1e9,
             "tuned": {"streamed_vectors_primal": bool(st.streaming_at), "streamed_vectors_dual": bool(st.streaming_a),
                       "cases_per_thread_primal": int(st.cases_per_thread_at),

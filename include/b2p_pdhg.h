@@ -284,13 +284,15 @@ int b2p_engine_set_start(b2p_engine* e, const double* x, const double* row_dual,
 /* When on, every fused SpMV kernel launch (and, in resident form, every
  * interval launch) of the next solve is bracketed by CUDA events;
  * b2p_engine_kernel_times then returns, per kernel class (0 = A^T y + primal
- * step, 1 = A x+ + dual step, 2 = resident interval kernel), the count and the
- * summed device milliseconds; for class 2 the count is in iterations. */
+ * step, 1 = A x+ + dual step, 2 = resident interval kernel, 3 / 4 = the FP32
+ * primal / dual kernels of a mixed-precision batch), the count and the summed
+ * device milliseconds; for class 2 the count is in iterations. */
 int b2p_engine_set_profiling(b2p_engine* e, int32_t on);
 int b2p_engine_kernel_times(b2p_engine* e, int32_t kernel_class, int64_t* launches, double* total_ms);
 /* Algorithmic bytes of one launch of a kernel class (CSR values, indices and
  * row pointers read once, gathered vector read once, every streamed vector
- * read or written once); class 2: bytes of one iteration (classes 0 + 1). */
+ * read or written once; classes 3 and 4 with 4-byte values and vectors);
+ * class 2: bytes of one iteration (classes 0 + 1). */
 int b2p_engine_kernel_bytes(b2p_engine* e, int32_t kernel_class, double* bytes);
 
 /* ---- KKT evaluation ---------------------------------------------------------

@@ -162,8 +162,8 @@ struct Engine {
   bool batch_wr_p = false, batch_wr_d = false;  // whole warps per row, entries passed by shuffle (tuned)
   bool profiling = false;
   std::vector<cudaEvent_t> prof_ev;  // 4 per iteration of the longest interval
-  int64_t prof_launches[3] = {0, 0, 0};
-  double prof_ms[3] = {0, 0, 0};
+  int64_t prof_launches[5] = {0, 0, 0, 0, 0};
+  double prof_ms[5] = {0, 0, 0, 0, 0};
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
 
   // ---- last solve ----
@@ -901,6 +901,7 @@ struct Engine {
     for (int l = 0; l < L; ++l) {
       const bool last = l == L - 1;
       const IterClock ck{d_it_base, d_restart_at, l};
+      if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 0], stream));
       if (nk) {
         if (last)
           launch(k_primal32<false>, gp, stream, true, n, k, AT, w[Y32], w[C32], w[LO32], w[UP32], w[X32], w[XP32],
@@ -909,6 +910,8 @@ struct Engine {
           launch(k_primal32<true>, gp, stream, true, n, k, AT, w[Y32], w[C32], w[LO32], w[UP32], w[X32], w[XP32],
                  w[X032], d_tau, ck, rho);
       }
+      if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 1], stream));
+      if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 2], stream));
       if (mk) {
         if (last)
           launch(k_dual32<false>, gd, stream, true, m, k, A, w[XP32], w[RL32], w[RU32], w[Y32], w[YP32], w[Y032],
@@ -917,6 +920,7 @@ struct Engine {
           launch(k_dual32<true>, gd, stream, true, m, k, A, w[XP32], w[RL32], w[RU32], w[Y32], w[YP32], w[Y032],
                  w[AX32], w[AXP32], w[AX032], d_sigma, ck, rho);
       }
+      if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 3], stream));
       B2P_CUDA(cudaGetLastError());
     }
     const IterClock ck{d_it_base, d_restart_at, L - 1};
@@ -982,7 +986,22 @@ struct Engine {
 
   void collect_profile(int L) {
     if (!profiling) return;
-    if (phase32 && mixed_batch) return;  // the FP32 batch kernels are not profiled per class
+    if (phase32 && mixed_batch) {  // the FP32 batch kernels: classes 3 and 4
+      for (int l = 0; l < L; ++l) {
+        float ms = 0;
+        if (n) {
+          B2P_CUDA(cudaEventElapsedTime(&ms, prof_ev[4 * l], prof_ev[4 * l + 1]));
+          prof_ms[3] += ms;
+          prof_launches[3]++;
+        }
+        if (m) {
+          B2P_CUDA(cudaEventElapsedTime(&ms, prof_ev[4 * l + 2], prof_ev[4 * l + 3]));
+          prof_ms[4] += ms;
+          prof_launches[4]++;
+        }
+      }
+      return;
+    }
     if (phase32 || resident) {
       float ms = 0;
       B2P_CUDA(cudaEventElapsedTime(&ms, prof_ev[0], prof_ev[1]));
@@ -1024,8 +1043,10 @@ struct Engine {
     const auto t_solve = Clock::now();
     std::vector<double> omega;
     launches = 0;
-    prof_launches[0] = prof_launches[1] = prof_launches[2] = 0;
-    prof_ms[0] = prof_ms[1] = prof_ms[2] = 0;
+    for (int c = 0; c < 5; ++c) {
+      prof_launches[c] = 0;
+      prof_ms[c] = 0;
+    }
     reset_state(omega);
     phase32 = mixed || mixed_batch;
     if (phase32) state_to_fp32();
@@ -1293,7 +1314,11 @@ struct Engine {
     // dual: y, ax, rl, ru, y0, ax0 read + y, y+, ax, ax+ written = 10).
     const double nnz = static_cast<double>(P.A.val.size());
     if (cls == 0) return 12.0 * nnz + 4.0 * (n + 1) + 8.0 * m * k + 8.0 * 7 * n * k;
-    return 12.0 * nnz + 4.0 * (m + 1) + 8.0 * n * k + 8.0 * 10 * m * k;
+    if (cls == 1) return 12.0 * nnz + 4.0 * (m + 1) + 8.0 * n * k + 8.0 * 10 * m * k;
+    // FP32 batch kernels: 4-byte values and vectors (the streamed costs and
+    // bounds are FP32 copies too)
+    if (cls == 3) return 8.0 * nnz + 4.0 * (n + 1) + 4.0 * m * k + 4.0 * 7 * n * k;
+    return 8.0 * nnz + 4.0 * (m + 1) + 4.0 * n * k + 4.0 * 10 * m * k;
   }
 };
 
@@ -1386,7 +1411,7 @@ int b2p_engine_set_profiling(b2p_engine* h, int32_t on) {
 
 int b2p_engine_kernel_times(b2p_engine* h, int32_t cls, int64_t* launches, double* total_ms) {
   return guarded([&] {
-    if (!h || cls < 0 || cls > 2) throw Error(B2P_ERR_INVALID, "bad engine or kernel class");
+    if (!h || cls < 0 || cls > 4) throw Error(B2P_ERR_INVALID, "bad engine or kernel class");
     Engine& e = *reinterpret_cast<Engine*>(h);
     if (launches) *launches = e.prof_launches[cls];
     if (total_ms) *total_ms = e.prof_ms[cls];
@@ -1395,7 +1420,7 @@ int b2p_engine_kernel_times(b2p_engine* h, int32_t cls, int64_t* launches, doubl
 
 int b2p_engine_kernel_bytes(b2p_engine* h, int32_t cls, double* bytes) {
   return guarded([&] {
-    if (!h || cls < 0 || cls > 2 || !bytes) throw Error(B2P_ERR_INVALID, "bad engine, class or output");
+    if (!h || cls < 0 || cls > 4 || !bytes) throw Error(B2P_ERR_INVALID, "bad engine, class or output");
     *bytes = reinterpret_cast<Engine*>(h)->kernel_bytes(cls);
   });
 }
