@@ -343,25 +343,6 @@ __device__ __forceinline__ double row_sum(int p, const int e, const int32_t* __r
   return s;
 }
 
-// Two rows' left-to-right sums advanced in lockstep (their loads
-// independent), then the longer row's tail; each sum's order is row_sum's.
-template <class T>
-__device__ __forceinline__ void row_sum2(int p0, const int e0, int p1, const int e1, const int32_t* __restrict__ idx,
-                                         const T* __restrict__ val, const T* __restrict__ v, int shift, double& s0,
-                                         double& s1) {
-  double a = 0.0, b = 0.0;
-  for (; p0 < e0 && p1 < e1; ++p0, ++p1) {
-    const double x0 = static_cast<double>(val[p0]), g0 = static_cast<double>(v[idx[p0] - shift]);
-    const double x1 = static_cast<double>(val[p1]), g1 = static_cast<double>(v[idx[p1] - shift]);
-    a = __dadd_rn(a, __dmul_rn(x0, g0));
-    b = __dadd_rn(b, __dmul_rn(x1, g1));
-  }
-  for (; p0 < e0; ++p0) a = __dadd_rn(a, __dmul_rn(static_cast<double>(val[p0]), static_cast<double>(v[idx[p0] - shift])));
-  for (; p1 < e1; ++p1) b = __dadd_rn(b, __dmul_rn(static_cast<double>(val[p1]), static_cast<double>(v[idx[p1] - shift])));
-  s0 = a;
-  s1 = b;
-}
-
 __device__ __forceinline__ double lambda_at(int64_t j) {
   const double jj = static_cast<double>(j);
   return __ddiv_rn(__dadd_rn(jj, 1.0), __dadd_rn(jj, 2.0));
@@ -497,10 +478,9 @@ __device__ __forceinline__ void run_lp(const CtaArgs& a, const CtaLp& L, int lp,
     for (int l = 0; l < Lint; ++l) {
       const bool halpern = l != Lint - 1;
       const double lam = lambda_at(it + l - restartAt);
-      // x+ = proj(x - tau (c - A^T y)), Halpern step of x; a thread takes its
-      // columns j and j + NT together, so that two chains of dependent loads
-      // are in flight (each column's sum keeps its own order)
-      auto primal = [&](int j, double aty) {
+      // x+ = proj(x - tau (c - A^T y)), Halpern step of x
+      for (int j = tid; j < n; j += NT) {
+        const double aty = row_sum(Tp[j], Tp[j + 1], Ti, Tv, y, L.tshift);
         const double xv = static_cast<double>(x[j]);
         double v = __dsub_rn(xv, __dmul_rn(tau, __dsub_rn(c[j], aty)));
         const double lj = lo[j], uj = up[j];
@@ -508,20 +488,11 @@ __device__ __forceinline__ void run_lp(const CtaArgs& a, const CtaLp& L, int lp,
         v = (uj < v) ? uj : v;
         xp[j] = static_cast<T>(v);
         if (halpern) x[j] = static_cast<T>(halpern_step(xv, v, static_cast<double>(x0[j]), lam, rho));
-      };
-      for (int j = tid; j < n; j += 2 * NT) {
-        if (j + NT < n) {
-          double a0, a1;
-          row_sum2(Tp[j], Tp[j + 1], Tp[j + NT], Tp[j + NT + 1], Ti, Tv, y, L.tshift, a0, a1);
-          primal(j, a0);
-          primal(j + NT, a1);
-        } else {
-          primal(j, row_sum(Tp[j], Tp[j + 1], Ti, Tv, y, L.tshift));
-        }
       }
       __syncthreads();
       // A x+, y+ = v + sigma proj(-v / sigma), Halpern steps of y and A x
-      auto dual = [&](int i, double axpv) {
+      for (int i = tid; i < m; i += NT) {
+        const double axpv = row_sum(Ap[i], Ap[i + 1], Ai, Av, xp, L.ashift);
         const double axv = static_cast<double>(ax[i]), yv = static_cast<double>(y[i]);
         const double v = __dsub_rn(yv, __dmul_rn(sigma, __dsub_rn(__dmul_rn(2.0, axpv), axv)));
         double w = __ddiv_rn(-v, sigma);
@@ -534,16 +505,6 @@ __device__ __forceinline__ void run_lp(const CtaArgs& a, const CtaLp& L, int lp,
         if (halpern) {
           y[i] = static_cast<T>(halpern_step(yv, ypv, static_cast<double>(y0[i]), lam, rho));
           ax[i] = static_cast<T>(halpern_step(axv, axpv, static_cast<double>(ax0[i]), lam, rho));
-        }
-      };
-      for (int i = tid; i < m; i += 2 * NT) {
-        if (i + NT < m) {
-          double a0, a1;
-          row_sum2(Ap[i], Ap[i + 1], Ap[i + NT], Ap[i + NT + 1], Ai, Av, xp, L.ashift, a0, a1);
-          dual(i, a0);
-          dual(i + NT, a1);
-        } else {
-          dual(i, row_sum(Ap[i], Ap[i + 1], Ai, Av, xp, L.ashift));
         }
       }
       __syncthreads();
