@@ -1210,7 +1210,9 @@ def main():
                          "5,064 x 11,376; default medium for family, large for sweep-tol)")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed",
                     help="family: arithmetic of the batched solves (the per-instance baseline is plain FP64)")
-    ap.add_argument("--family-max-iters", type=int, default=400000, help="family: iteration limit per member")
+    ap.add_argument("--family-max-iters", type=int, default=None,
+                    help="family / sweep-tol: iteration limit per member (default 400,000 for family; the "
+                         "reference's 1,000,000 for sweep-tol)")
     ap.add_argument("--sweep-forms", default="", help="sweep-tol: comma-separated subset of the forms to run")
     ap.add_argument("--batch", type=int, default=1024, help="family: members per batched solve")
     ap.add_argument("--engine", choices=["multi", "batch"], default="multi",
@@ -1224,6 +1226,8 @@ def main():
     args = ap.parse_args()
     if args.family_size is None:
         args.family_size = "large" if args.workload == "sweep-tol" else "medium"
+    if args.family_max_iters is None:
+        args.family_max_iters = 1000000 if args.workload == "sweep-tol" else 400000
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.steps < 1:

@@ -920,10 +920,11 @@ struct MultiEngine {
   // check intervals, twice; the fastest is kept (remembered per batch shape).
   void tune_cta_fp32() {
     const auto t0 = Clock::now();
-    cta_nt32 = opt.cta_threads ? opt.cta_threads : 256;
-    cta_r32 = 0;
+    const std::vector<std::pair<int, int>> cands = general_candidates();
+    cta_nt32 = cands.front().first;
+    cta_r32 = cands.front().second;
     const int64_t probe = std::min<int64_t>(opt.max_iterations, 5 * static_cast<int64_t>(opt.check_every));
-    if (probe <= 0) return;
+    if (probe <= 0 || cands.size() == 1) return;
     const std::vector<int64_t> key{device, K, cta_max_dim, cta_smem32, inst_nnz_total(), opt.check_every,
                                    opt.cta_threads};
     static std::mutex mu;
@@ -941,7 +942,7 @@ struct MultiEngine {
     B2P_CUDA(cudaEventCreate(&e0));
     B2P_CUDA(cudaEventCreate(&e1));
     double best = INFINITY;
-    for (const auto& v : general_candidates()) {
+    for (const auto& v : cands) {
       launch_cta32(v.first, v.second, cta_args(-1.0, 1), static_cast<unsigned>(K));
       for (int rep = 0; rep < 2; ++rep) {
         B2P_CUDA(cudaEventRecord(e0, stream));
