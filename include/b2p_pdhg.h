@@ -164,7 +164,11 @@ typedef struct b2p_options {
    * warps per row (row entries loaded once per warp and shared by shuffle)
    * where k / cases per thread is a multiple of 32. */
   int32_t batch_variant;
-  int32_t pad_options;
+  /* Batches (k > 1 cases sharing A), FP64 phase: 0 = whenever half of the
+   * live cases have terminated, pack the others into a narrower interleave
+   * (each case's state moves unchanged, so its iterates do not change; the
+   * kernels stop streaming the finished cases' vectors); 1 = never. */
+  int32_t batch_no_compaction;
 } b2p_options;
 enum { B2P_MULTI_AUTO = 0, B2P_MULTI_GRID = 1, B2P_MULTI_CTA = 2 };
 enum { B2P_CTA_AUTO = 0, B2P_CTA_GENERAL = 1, B2P_CTA_OWNER1 = 2, B2P_CTA_OWNER2 = 3 };
@@ -194,7 +198,7 @@ typedef struct b2p_stats {
   int32_t resident_blocks;                    /* cooperative grid size in resident form */
   int64_t resident_smem_bytes;                /* largest block's shared memory in resident form */
   int32_t precision_used;                     /* B2P_PRECISION_* actually run */
-  int32_t pad1;
+  int32_t batch_compactions;                  /* batches: times the live cases were packed narrower */
   int64_t fp32_iterations;                    /* mixed form: iterations run in FP32 */
   int32_t schedule_a, schedule_at;            /* multi-LP: B2P_SCHEDULE_BINNED or _TILED per operator */
   double autotune_seconds;                    /* multi-LP: time the autotuner took (part of setup) */

@@ -107,6 +107,17 @@ int resident_lanes(const HostCsr& M, const std::vector<int32_t>& bounds) {
 
 }  // namespace
 
+// dst[r * k2 + q] = src[r * k + map[q]]: the k-interleaved rows of a vector
+// with only the cases map[0..k2) kept (case compaction of a batch).
+__global__ void __launch_bounds__(kBlock) k_pack_cases(int64_t rows, int32_t k, int32_t k2,
+                                                       const int32_t* __restrict__ map, const double* __restrict__ src,
+                                                       double* __restrict__ dst) {
+  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= rows * k2) return;
+  const int64_t r = t / k2;
+  dst[t] = src[r * k + map[t - r * k2]];
+}
+
 struct Engine {
   // ---- problem ----
   int device = 0;
@@ -125,6 +136,16 @@ struct Engine {
   int32_t *dA_ptr = nullptr, *dA_idx = nullptr, *dT_ptr = nullptr, *dT_idx = nullptr;
   double *dA_val = nullptr, *dT_val = nullptr, *d_rfac = nullptr, *d_cfac = nullptr;
   double* v[NSLOT] = {};
+  // Case compaction of a batch (FP64 phase): when half the live cases have
+  // terminated, the rest are packed into a narrower interleave, so that the
+  // kernels stop streaming the finished cases' vectors.  k is the current
+  // width, case_of maps a packed case to the engine's case; v_full and k_full
+  // are the engine's own buffers and width, restored when the solve ends.
+  int k_full = 1;
+  double* v_full[NSLOT] = {};
+  std::vector<int32_t> case_of;
+  int32_t* d_case_map = nullptr;
+  int compactions = 0;
   double *d_tau = nullptr, *d_sigma = nullptr, *d_prow = nullptr, *d_pcol = nullptr, *d_sums = nullptr;
   int64_t *d_it_base = nullptr, *d_restart_at = nullptr;
   int32_t* d_mask = nullptr;
@@ -160,6 +181,7 @@ struct Engine {
   bool batch_stream_p = false, batch_stream_d = false;  // evict-first streamed vectors (tuned per kernel)
   int batch_cpt_p = 1, batch_cpt_d = 1;  // cases per thread of the primal / dual batch kernels (tuned)
   bool batch_wr_p = false, batch_wr_d = false;  // whole warps per row, entries passed by shuffle (tuned)
+  bool batch_wr_p_full = false, batch_wr_d_full = false;  // the tuned choice, restored after a compaction
   bool profiling = false;
   std::vector<cudaEvent_t> prof_ev;  // 4 per iteration of the longest interval
   int64_t prof_launches[5] = {0, 0, 0, 0, 0};
@@ -322,6 +344,11 @@ struct Engine {
     stats.kernel_mode = (resident || mixed) ? B2P_KERNELS_RESIDENT : B2P_KERNELS_FUSED;
     stats.precision_used = (mixed || mixed_batch) ? B2P_PRECISION_MIXED : B2P_PRECISION_FP64;
     for (int s = 0; s < NSLOT; ++s) v[s] = dalloc<double>(row_slot(s) ? mk : nk);
+    k_full = k;
+    for (int s = 0; s < NSLOT; ++s) v_full[s] = v[s];
+    case_of.resize(k);
+    for (int b = 0; b < k; ++b) case_of[b] = b;
+    d_case_map = dalloc<int32_t>(k);
     auto put = [&](int s, const std::vector<double>& h) {
       if (!h.empty())
         B2P_CUDA(cudaMemcpyAsync(v[s], h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
@@ -1037,9 +1064,75 @@ struct Engine {
     transfer_seconds += seconds_since(t0);
   }
 
+  void drop_graphs() {
+    for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+    for (auto& g : graph_defs) cudaGraphDestroy(g.second);
+    graphs.clear();
+    graph_defs.clear();
+  }
+
+  // Keeps the packed cases keep[0..k2) (ascending, k2 >= 2): every vector slot
+  // re-interleaved k -> k2 into new buffers, the restart clocks re-indexed;
+  // each kept case's state is moved unchanged, so its iterates are those it
+  // would have had.  Graphs are recaptured for the new width.
+  void compact_cases(const std::vector<int32_t>& keep) {
+    const int k2 = static_cast<int>(keep.size());
+    B2P_CUDA(cudaMemcpyAsync(d_case_map, keep.data(), sizeof(int32_t) * k2, cudaMemcpyHostToDevice, stream));
+    double* nv[NSLOT];
+    for (int q = 0; q < NSLOT; ++q) {
+      const int64_t rows = row_slot(q) ? m : n;
+      void* p = nullptr;
+      B2P_CUDA(cudaMallocFromPoolAsync(&p, std::max<int64_t>(rows * k2, 1) * sizeof(double), device_pool(device),
+                                       stream));
+      nv[q] = static_cast<double*>(p);
+      if (rows) k_pack_cases<<<blocks(rows * k2), kBlock, 0, stream>>>(rows, k, k2, d_case_map, v[q], nv[q]);
+    }
+    B2P_CUDA(cudaGetLastError());
+    std::vector<int64_t> ra(k), rb(k2);
+    B2P_CUDA(cudaMemcpyAsync(ra.data(), d_restart_at, sizeof(int64_t) * k, cudaMemcpyDeviceToHost, stream));
+    B2P_CUDA(cudaStreamSynchronize(stream));
+    for (int q = 0; q < k2; ++q) rb[q] = ra[keep[q]];
+    B2P_CUDA(cudaMemcpyAsync(d_restart_at, rb.data(), sizeof(int64_t) * k2, cudaMemcpyHostToDevice, stream));
+    if (v[0] != v_full[0])
+      for (int q = 0; q < NSLOT; ++q) B2P_CUDA(cudaFreeAsync(v[q], stream));
+    for (int q = 0; q < NSLOT; ++q) v[q] = nv[q];
+    std::vector<int32_t> co(k2);
+    for (int q = 0; q < k2; ++q) co[q] = case_of[keep[q]];
+    case_of = co;
+    k = k2;
+    // whole-warp rows need k / (cases per thread) to be a multiple of 32
+    if (batch_wr_p && ((k + batch_cpt_p - 1) / batch_cpt_p) % 32 != 0) batch_wr_p = false;
+    if (batch_wr_d && ((k + batch_cpt_d - 1) / batch_cpt_d) % 32 != 0) batch_wr_d = false;
+    drop_graphs();
+    ++compactions;
+    B2P_CUDA(cudaStreamSynchronize(stream));
+  }
+
+  // Back to the engine's own buffers and width (after a solve that compacted).
+  void restore_cases() {
+    if (k == k_full && v[0] == v_full[0]) return;
+    B2P_CUDA(cudaStreamSynchronize(stream));
+    for (int q = 0; q < NSLOT; ++q) {
+      if (v[q] != v_full[q]) B2P_CUDA(cudaFreeAsync(v[q], stream));
+      v[q] = v_full[q];
+    }
+    k = k_full;
+    case_of.resize(k);
+    for (int b = 0; b < k; ++b) case_of[b] = b;
+    batch_wr_p = batch_wr_p_full;
+    batch_wr_d = batch_wr_d_full;
+    drop_graphs();
+    B2P_CUDA(cudaStreamSynchronize(stream));
+  }
+
   // runPdhg's loop (src/pdhg/pdhg.cpp:560-687).
   void solve(Clock::time_point deadline_start) {
     B2P_CUDA(cudaSetDevice(device));
+    restore_cases();
+    batch_wr_p_full = batch_wr_p;
+    batch_wr_d_full = batch_wr_d;
+    compactions = 0;
+    std::vector<double> cn(cNorm), rn(rhsNorm);  // per packed case
     const auto t_solve = Clock::now();
     std::vector<double> omega;
     launches = 0;
@@ -1074,11 +1167,10 @@ struct Engine {
       return opt.time_limit > 0 && seconds_since(deadline_start) >= opt.time_limit;
     };
     auto extract = [&](int b, int status, double relKkt, double pobj, double dobj, int64_t it) {
-      for (int j = 0; j < n; ++j)
-        x_out[static_cast<size_t>(b) * n + j] = xs[static_cast<size_t>(j) * k + b] * P.Cs[j] * P.beta;
-      for (int i = 0; i < m; ++i)
-        y_out[static_cast<size_t>(b) * m + i] = ys[static_cast<size_t>(i) * k + b] * P.R[i] * P.gamma;
-      b2p_result& r = results[b];
+      const size_t cb = static_cast<size_t>(case_of[b]);
+      for (int j = 0; j < n; ++j) x_out[cb * n + j] = xs[static_cast<size_t>(j) * k + b] * P.Cs[j] * P.beta;
+      for (int i = 0; i < m; ++i) y_out[cb * m + i] = ys[static_cast<size_t>(i) * k + b] * P.R[i] * P.gamma;
+      b2p_result& r = results[cb];
       r.status = status;
       r.iterations = it;
       r.relative_kkt = relKkt;
@@ -1113,8 +1205,8 @@ struct Engine {
           if (done[b]) continue;
           const double* s = h_sums + static_cast<size_t>(b) * kNumSums;
           const double pobj = s[CS_POBJ] * scaleObj, dobj = (s[CS_ROW_DOBJ] + s[CS_COL_DOBJ]) * scaleObj;
-          const double relP = std::sqrt(s[CS_ROW_RES2]) / (1.0 + rhsNorm[b]);
-          const double relD = std::sqrt(s[CS_COL_RES2]) / (1.0 + cNorm[b]);
+          const double relP = std::sqrt(s[CS_ROW_RES2]) / (1.0 + rn[b]);
+          const double relD = std::sqrt(s[CS_COL_RES2]) / (1.0 + cn[b]);
           const double gap = std::fabs(pobj - dobj) / (1.0 + std::fabs(pobj) + std::fabs(dobj));
           const double kkt32 = smax(relP, smax(relD, gap));
           if (relP <= opt.tolerance && relD <= opt.tolerance && gap <= opt.tolerance) {
@@ -1135,8 +1227,8 @@ struct Engine {
             if (done[b]) continue;
             const double* s = h_sums + static_cast<size_t>(b) * kNumSums;
             const double pobj = s[CS_POBJ] * scaleObj, dobj = (s[CS_ROW_DOBJ] + s[CS_COL_DOBJ]) * scaleObj;
-            const double relP = std::sqrt(s[CS_ROW_RES2]) / (1.0 + rhsNorm[b]);
-            const double relD = std::sqrt(s[CS_COL_RES2]) / (1.0 + cNorm[b]);
+            const double relP = std::sqrt(s[CS_ROW_RES2]) / (1.0 + rn[b]);
+            const double relD = std::sqrt(s[CS_COL_RES2]) / (1.0 + cn[b]);
             const double gap = std::fabs(pobj - dobj) / (1.0 + std::fabs(pobj) + std::fabs(dobj));
             if (relP <= opt.tolerance && relD <= opt.tolerance && gap <= opt.tolerance) {
               if (!fetched64) {
@@ -1166,8 +1258,8 @@ struct Engine {
         // without a 10% gain, the solve continues in FP64 from this point.
         const double* s = h_sums;
         const double pobj = s[CS_POBJ] * scaleObj, dobj = (s[CS_ROW_DOBJ] + s[CS_COL_DOBJ]) * scaleObj;
-        const double relP = std::sqrt(s[CS_ROW_RES2]) / (1.0 + rhsNorm[0]);
-        const double relD = std::sqrt(s[CS_COL_RES2]) / (1.0 + cNorm[0]);
+        const double relP = std::sqrt(s[CS_ROW_RES2]) / (1.0 + rn[0]);
+        const double relD = std::sqrt(s[CS_COL_RES2]) / (1.0 + cn[0]);
         const double gap = std::fabs(pobj - dobj) / (1.0 + std::fabs(pobj) + std::fabs(dobj));
         const double kkt32 = smax(relP, smax(relD, gap));
         bool to_fp64 = false;
@@ -1176,8 +1268,8 @@ struct Engine {
           verify_fp64();
           const double vpobj = h_sums[CS_POBJ] * scaleObj;
           const double vdobj = (h_sums[CS_ROW_DOBJ] + h_sums[CS_COL_DOBJ]) * scaleObj;
-          const double vrelP = std::sqrt(h_sums[CS_ROW_RES2]) / (1.0 + rhsNorm[0]);
-          const double vrelD = std::sqrt(h_sums[CS_COL_RES2]) / (1.0 + cNorm[0]);
+          const double vrelP = std::sqrt(h_sums[CS_ROW_RES2]) / (1.0 + rn[0]);
+          const double vrelD = std::sqrt(h_sums[CS_COL_RES2]) / (1.0 + cn[0]);
           const double vgap = std::fabs(vpobj - vdobj) / (1.0 + std::fabs(vpobj) + std::fabs(vdobj));
           stats.primal_residual = vrelP;
           stats.dual_residual = vrelD;
@@ -1213,8 +1305,8 @@ struct Engine {
         const double* s = h_sums + static_cast<size_t>(b) * kNumSums;
         const double pobj = s[CS_POBJ] * scaleObj;
         const double dobj = (s[CS_ROW_DOBJ] + s[CS_COL_DOBJ]) * scaleObj;
-        const double relP = std::sqrt(s[CS_ROW_RES2]) / (1.0 + rhsNorm[b]);
-        const double relD = std::sqrt(s[CS_COL_RES2]) / (1.0 + cNorm[b]);
+        const double relP = std::sqrt(s[CS_ROW_RES2]) / (1.0 + rn[b]);
+        const double relD = std::sqrt(s[CS_COL_RES2]) / (1.0 + cn[b]);
         const double gap = std::fabs(pobj - dobj) / (1.0 + std::fabs(pobj) + std::fabs(dobj));
         const double kktErr = smax(relP, smax(relD, gap));
         if (k == 1) {
@@ -1270,6 +1362,30 @@ struct Engine {
         B2P_CUDA(cudaGetLastError());
         ++launches;
       }
+      if (!phase32 && !opt.batch_no_compaction && k > 2 && remaining * 2 <= k) {
+        // half the packed cases have terminated: keep the live ones (and, if
+        // only one is live, one finished case beside it, so that the width
+        // stays >= 2 for the batch kernels)
+        std::vector<int32_t> keep;
+        for (int b = 0; b < k; ++b)
+          if (!done[b] || (remaining == 1 && b == (done[0] ? 0 : 1))) keep.push_back(b);
+        compact_cases(keep);
+        auto remap = [&](auto& vec) {
+          auto old = vec;
+          vec.resize(keep.size());
+          for (size_t q = 0; q < keep.size(); ++q) vec[q] = old[keep[q]];
+        };
+        remap(done);
+        remap(restarts);
+        remap(omega);
+        remap(rn);
+        remap(cn);
+        remap(conv32);
+        remap(stall32);
+        remap(best32v);
+        remap(stale32v);
+        upload_steps(omega);
+      }
       ++it;
     }
     B2P_CUDA(cudaEventRecord(ev_stop, stream));
@@ -1293,8 +1409,8 @@ struct Engine {
         if (done[b]) continue;
         const double* s = h_sums + static_cast<size_t>(b) * kNumSums;
         const double pobj = s[CS_POBJ] * scaleObj, dobj = (s[CS_ROW_DOBJ] + s[CS_COL_DOBJ]) * scaleObj;
-        const double relP = std::sqrt(s[CS_ROW_RES2]) / (1 + rhsNorm[b]);
-        const double relD = std::sqrt(s[CS_COL_RES2]) / (1 + cNorm[b]);
+        const double relP = std::sqrt(s[CS_ROW_RES2]) / (1 + rn[b]);
+        const double relD = std::sqrt(s[CS_COL_RES2]) / (1 + cn[b]);
         const double gap = std::fabs(pobj - dobj) / (1 + std::fabs(pobj) + std::fabs(dobj));
         extract(b, (expiredStop || expired()) ? B2P_STATUS_TIME_LIMIT : B2P_STATUS_ITERATION_LIMIT,
                 smax(relP, smax(relD, gap)), pobj, dobj, it);
@@ -1304,6 +1420,8 @@ struct Engine {
     stats.bytes_uploaded = bytes_up;
     stats.bytes_downloaded = bytes_down;
     stats.transfer_seconds = transfer_seconds;
+    stats.batch_compactions = compactions;
+    restore_cases();
   }
 
   double kernel_bytes(int cls) const {

@@ -48,7 +48,7 @@ class B2pOptions(C.Structure):
                 ("lanes_per_row_a", C.c_int32), ("lanes_per_row_at", C.c_int32), ("short_row_rounds", C.c_int32),
                 ("kernel_mode", C.c_int32), ("spmv_schedule", C.c_int32), ("multi_form", C.c_int32),
                 ("cta_smem_limit", C.c_int32), ("cta_threads", C.c_int32), ("cta_kernel", C.c_int32),
-                ("batch_variant", C.c_int32), ("pad_options", C.c_int32)]
+                ("batch_variant", C.c_int32), ("batch_no_compaction", C.c_int32)]
 
 
 class B2pStats(C.Structure):
@@ -60,7 +60,7 @@ class B2pStats(C.Structure):
                 ("prepare_seconds", C.c_double), ("upload_seconds", C.c_double), ("graph_seconds", C.c_double),
                 ("lanes_per_row_a", C.c_int32), ("lanes_per_row_at", C.c_int32), ("kernel_mode", C.c_int32),
                 ("resident_blocks", C.c_int32), ("resident_smem_bytes", C.c_int64), ("precision_used", C.c_int32),
-                ("pad1", C.c_int32), ("fp32_iterations", C.c_int64), ("schedule_a", C.c_int32),
+                ("batch_compactions", C.c_int32), ("fp32_iterations", C.c_int64), ("schedule_a", C.c_int32),
                 ("schedule_at", C.c_int32), ("autotune_seconds", C.c_double), ("streaming_a", C.c_int32),
                 ("streaming_at", C.c_int32), ("multi_form", C.c_int32), ("cta_threads", C.c_int32),
                 ("cta_smem_bytes", C.c_int64), ("cta_lps_smem", C.c_int32), ("cta_lps_vectors", C.c_int32),

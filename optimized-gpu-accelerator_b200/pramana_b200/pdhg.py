@@ -53,6 +53,7 @@ class PdhgOptions:
     ctaThreads: int = 0  # CTA form: threads per block (128 / 256 / 512 / 1024; 0 = autotuned)
     ctaKernel: int = _lib.CTA_AUTO  # CTA form: CTA_GENERAL / CTA_OWNER1 / CTA_OWNER2 (0 = autotuned)
     batchVariant: int = 0  # FP64 batches: 0 = tuned; 1..4 = (cases per thread, streamed) (1,no) (2,no) (1,yes) (2,yes)
+    batchNoCompaction: bool = False  # batches: keep finished cases in the interleave (no packing)
 
     def to_c(self, cancel_flag=None) -> _lib.B2pOptions:
         if not self.useGpu:
@@ -81,6 +82,7 @@ class PdhgOptions:
         o.cta_threads = int(self.ctaThreads)
         o.cta_kernel = int(self.ctaKernel)
         o.batch_variant = int(self.batchVariant)
+        o.batch_no_compaction = int(bool(self.batchNoCompaction))
         if cancel_flag is not None:
             o.cancel_flag = C.cast(cancel_flag, C.POINTER(C.c_int32))
         return o

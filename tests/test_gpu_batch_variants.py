@@ -60,3 +60,38 @@ def test_batch_variants_agree_bitwise_and_tuner_runs():
         for a, b in zip(rs, base):
             assert a.iterations == b.iterations
             assert np.array_equal(a.x, b.x) and np.array_equal(a.rowDual, b.rowDual), variant
+
+
+@pytest.mark.parametrize("variant", [0, 1, 4, 5])
+def test_case_compaction_changes_no_iterate(variant):
+    """Cases of uneven difficulty: as they terminate, the live ones are packed
+    into narrower interleaves (more than once).  Every case's iterations,
+    status and point are bit for bit those of the same batch run without
+    packing -- with the warp-row variant too, whose choice falls back when the
+    packed width is no multiple of 32."""
+    lp = G.random_lp(150, 300, 4.0, 90, 13)
+    cases = lp_cases.mixed_cases(lp, 64)
+    out = {}
+    for off in (False, True):
+        with pdhg.Engine(lp, opts(tolerance=1e-6, maxIterations=100000, batchVariant=variant,
+                                  batchNoCompaction=off), cases) as e:
+            out[off] = (e.solve(), e.last_stats.batch_compactions)
+    (packed, n_packed), (plain, n_plain) = out[False], out[True]
+    assert n_plain == 0 and n_packed >= 2
+    for a, b in zip(packed, plain):
+        assert a.status == b.status and a.iterations == b.iterations
+        assert np.array_equal(a.x, b.x) and np.array_equal(a.rowDual, b.rowDual)
+        assert a.objective == b.objective and a.relativeKkt == b.relativeKkt
+
+
+def test_compacted_engine_repeats_its_solve():
+    """The engine's own buffers come back after a solve that packed its cases:
+    a second solve from the same start is identical to the first."""
+    lp = G.random_lp(150, 300, 4.0, 90, 13)
+    cases = lp_cases.mixed_cases(lp, 16)
+    with pdhg.Engine(lp, opts(tolerance=1e-6, maxIterations=100000), cases) as e:
+        first = e.solve()
+        assert e.last_stats.batch_compactions >= 1
+        second = e.solve()
+    for a, b in zip(first, second):
+        assert a.iterations == b.iterations and np.array_equal(a.x, b.x) and np.array_equal(a.rowDual, b.rowDual)
