@@ -378,8 +378,11 @@ def run_family(args, rank, world):
                     TrainOptions(epochs=args.epochs, batch=512, lr=1e-3, lr_final=1e-5, seed=2))
     nn = W.NearestWarmStart(fam).fit(P_train[ok], tr.X[ok], tr.Y[ok])
     strategies = {"cold": None, "nearest": nn, "learned": lw}
-    for w in range(args.warmup):  # untimed warm-up batches
-        W.solve_warm(fam, fam.sample(args.batch, 900 + w), lw, opts, batch=args.batch, engine=args.engine)
+    # untimed warm-up batches (module loads, variant tuning, pools): the first at full size, the
+    # others of 128 members
+    for w in range(args.warmup):
+        size_w = args.batch if w == 0 else min(args.batch, 128)
+        W.solve_warm(fam, fam.sample(size_w, 900 + w), lw, opts, batch=args.batch, engine=args.engine)
     acc = {k: {"seconds": [], "solve_seconds": [], "iterations": [], "certified": [], "fallback": [], "kkt": []}
            for k in strategies}
     with ClockSampler(0) as clk:
