@@ -377,12 +377,14 @@ def run_family(args, rank, world):
     losses = lw.fit(P_train[ok], tr.X[ok], tr.Y[ok],
                     TrainOptions(epochs=args.epochs, batch=512, lr=1e-3, lr_final=1e-5, seed=2))
     nn = W.NearestWarmStart(fam).fit(P_train[ok], tr.X[ok], tr.Y[ok])
+    est = W.WorkEstimate(fam).fit(P_train[ok], tr.iterations[ok])
     strategies = {"cold": None, "nearest": nn, "learned": lw}
     # untimed warm-up batches (module loads, variant tuning, pools): the first at full size, the
     # others of 128 members
     for w in range(args.warmup):
         size_w = args.batch if w == 0 else min(args.batch, 128)
-        W.solve_warm(fam, fam.sample(size_w, 900 + w), lw, opts, batch=args.batch, engine=args.engine)
+        Pw = fam.sample(size_w, 900 + w)
+        W.solve_warm(fam, Pw, lw, opts, batch=args.batch, engine=args.engine, work=est.predict(Pw))
     acc = {k: {"seconds": [], "solve_seconds": [], "iterations": [], "certified": [], "fallback": [], "kkt": []}
            for k in strategies}
     with ClockSampler(0) as clk:
@@ -391,7 +393,8 @@ def run_family(args, rank, world):
             for name, pred in strategies.items():
                 torch.cuda.synchronize()
                 t1 = time.perf_counter()
-                r, cert, redo = W.solve_warm(fam, P, pred, opts, batch=args.batch, engine=args.engine)
+                r, cert, redo = W.solve_warm(fam, P, pred, opts, batch=args.batch, engine=args.engine,
+                                             work=est.predict(P))
                 wall = time.perf_counter() - t1
                 a = acc[name]
                 a["seconds"].append(wall)
@@ -436,6 +439,8 @@ def run_family(args, rank, world):
                                    f"members, {args.steps} x {args.batch} held-out members, to rel KKT {TOL:g}",
                        "precision": args.precision,
                        "step": "one held-out batch solved and certified per strategy",
+                       "launch_order": "members in decreasing predicted work (mean cold iterations of the 4 nearest "
+                                       "training members), every strategy",
                        "engine": {"multi": "multi-LP engine (AUTO form: one thread block per member)",
                                   "batch": "shared-A batch engine (k-interleaved cases)"}[args.engine],
                        "network": lw.widths, "pca_rank": lw.rank, "pca_explained": lw.basis.explained,

@@ -4,9 +4,9 @@
 // mask from a BF16 array, FP32 and/or BF16 output).
 //
 // One CTA (128 threads) computes a 128 x kBN tile.  The K dimension runs in
-// chunks of 64 through two shared-memory stages: while the tensor core works
-// on chunk c from one stage, the threads already fetch chunk c + 1 into the
-// other (16-byte cp.async copies from global memory when the operand is
+// chunks of 64 through three shared-memory stages: while the tensor core
+// works on chunk c, the threads already fetch chunk c + 2 into the stage
+// chunk c - 1 used (16-byte cp.async copies from global memory when the operand is
 // K-contiguous, element loads otherwise).  Each stage holds A (128 x 64) and
 // B (kBN x 64) in the K-major, non-swizzled canonical layout of the UMMA
 // descriptors -- core matrices of 8 rows x 16 bytes, the two 8-element K
@@ -31,10 +31,10 @@ constexpr int kGemmBN = 128;
 constexpr int kGemmBK = 64;
 constexpr int kGemmThreads = 128;
 constexpr unsigned kMbarSpinLimit = 1u << 24;
-constexpr int kGemmStages = 2;
+constexpr int kGemmStages = 3;
 constexpr int kGemmStageBytes = (kGemmBM + kGemmBN) * kGemmBK * 2;  // A 16 KB + B 16 KB
-// two stages (64 KB), padded to 96 KB so that at most two CTAs share an SM
-// (2 x 128 TMEM columns <= 512)
+// three stages (96 KB): at most two CTAs share an SM (2 x 128 TMEM columns
+// <= 512)
 constexpr int kGemmSmemBytes = 96 * 1024;
 static_assert(kGemmStages * kGemmStageBytes <= kGemmSmemBytes, "stages exceed the shared-memory budget");
 
@@ -167,29 +167,32 @@ static __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tc(GemmArgs g
   const uint32_t idesc = umma_idesc_bf16(kGemmBN);
   const int nchunks = (g.K + kGemmBK - 1) / kGemmBK;
   const bool vec_a = stage_vec_ok(g.A, g.sam, g.sak, g.K), vec_b = stage_vec_ok(g.B, g.sbn, g.sbk, g.K);
-  uint32_t phase[kGemmStages] = {0u, 0u};  // parity of each stage's next completion
+  uint32_t phase[kGemmStages] = {};  // parity of each stage's next completion
   auto stage_a = [&](int st) { return smem + st * kGemmStageBytes; };
   auto stage_b = [&](int st) { return smem + st * kGemmStageBytes + kGemmBM * kGemmBK * 2; };
-  auto fetch = [&](int ch) {  // chunk ch into stage ch % 2, as one cp.async group
+  auto fetch = [&](int ch) {  // chunk ch into stage ch % kGemmStages, as one cp.async group
     const int st = ch % kGemmStages, k0 = ch * kGemmBK;
     stage_operand(stage_a(st), g.A, g.sam, g.sak, m0, g.M, k0, g.K, kGemmBM, vec_a, tid);
     stage_operand(stage_b(st), g.B, g.sbn, g.sbk, n0, g.N, k0, g.K, kGemmBN, vec_b, tid);
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
-  if (nchunks > 0) fetch(0);
+  // prologue: the first kGemmStages - 1 chunks in flight
+  for (int c = 0; c < kGemmStages - 1; ++c)
+    if (c < nchunks) fetch(c);
   for (int ch = 0; ch < nchunks; ++ch) {
     const int st = ch % kGemmStages;
-    if (ch + 1 < nchunks) {
-      // the other stage was read by chunk ch - 1's MMAs: refill it once they are done
-      const int nx = (ch + 1) % kGemmStages;
+    const int ahead = ch + kGemmStages - 1;  // the chunk fetched in this step
+    if (ahead < nchunks) {
+      // its stage was read by chunk ch - 1's MMAs: refill it once they are done
+      const int nx = ahead % kGemmStages;
       if (ch >= 1) {
         if (!mbar_wait(smem_u32(&mbar[nx]), phase[nx])) failed_sh = 1;
         phase[nx] ^= 1u;
       }
       __syncthreads();
       if (failed_sh) break;
-      fetch(ch + 1);
-      asm volatile("cp.async.wait_group 1;" ::: "memory");  // chunk ch has landed
+      fetch(ahead);
+      asm volatile("cp.async.wait_group %0;" ::"n"(kGemmStages - 1) : "memory");  // chunk ch has landed
     } else {
       asm volatile("cp.async.wait_group 0;" ::: "memory");
     }

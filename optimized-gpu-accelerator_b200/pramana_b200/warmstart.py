@@ -196,6 +196,29 @@ class NearestWarmStart:
         return self.X[j], self.Y[j]
 
 
+class WorkEstimate:
+    """Predicted work of a member: the mean cold iteration count of its four
+    nearest training members (normalised parameters).  Used to launch the
+    members of a batch in decreasing predicted work, so that the hardest ones
+    do not start last (longest-processing-time order)."""
+
+    def __init__(self, family: RefineryFamily, neighbours: int = 4):
+        self.family = family
+        self.k = neighbours
+
+    def fit(self, params, iterations):
+        self.P = self.family.normalize(params).astype(np.float64)
+        self.it = np.asarray(iterations, dtype=np.float64)
+        return self
+
+    def predict(self, params) -> np.ndarray:
+        Q = self.family.normalize(params).astype(np.float64)
+        d = (Q ** 2).sum(1)[:, None] - 2.0 * Q @ self.P.T + (self.P ** 2).sum(1)[None, :]
+        k = min(self.k, d.shape[1])
+        j = np.argpartition(d, k - 1, axis=1)[:, :k]
+        return self.it[j].mean(axis=1)
+
+
 @dataclass
 class FamilySolve:
     status: np.ndarray          # per instance (1 = Optimal)
@@ -210,12 +233,15 @@ class FamilySolve:
 
 
 def solve_family(family: RefineryFamily, params, opts: PdhgOptions | None = None, starts=None,
-                 batch: int = 1024, engine: str = "batch") -> FamilySolve:
+                 batch: int = 1024, engine: str = "batch", work=None) -> FamilySolve:
     """Batched PDHG over the family members `params`, in batches of `batch`
     members; `starts` = (X, Y) in the original space, or None (cold start).
-    engine "batch": one shared-A k-case solve per chunk (every case advances
-    until the last one stops); "multi": the multi-LP engine, whose schedule
-    shrinks to the members still running."""
+    engine "batch": one shared-A k-case solve per chunk (the live cases are
+    packed narrower as others finish); "multi": the multi-LP engine (one
+    thread block per member in its CTA form).  `work` (per member, optional):
+    predicted work; within each chunk the multi-LP engine gets the members in
+    decreasing predicted work, which is the order its blocks start in.
+    Results come back in the members' order."""
     opts = opts or PdhgOptions()
     params = np.asarray(params, dtype=np.float64).reshape(-1, family.num_params)
     n, m = family.base.num_cols, family.base.num_rows
@@ -225,12 +251,18 @@ def solve_family(family: RefineryFamily, params, opts: PdhgOptions | None = None
         sl = slice(b0, min(b0 + batch, len(params)))
         t0 = time.perf_counter()
         if engine == "multi":
-            lps = [family.instance(p) for p in params[sl]]
-            st = None if starts is None else list(zip(np.asarray(starts[0])[sl], np.asarray(starts[1])[sl]))
+            idx = np.arange(sl.start, sl.stop)
+            if work is not None:
+                idx = idx[np.argsort(-np.asarray(work, dtype=np.float64)[idx], kind="stable")]
+            lps = [family.instance(p) for p in params[idx]]
+            st = None if starts is None else list(zip(np.asarray(starts[0])[idx], np.asarray(starts[1])[idx]))
             t1 = time.perf_counter()
             res = solvePdhgMulti(lps, opts, starts=st)
             t2 = time.perf_counter()
             t1 = t2 - res[0].stats.solveSeconds if res else t1
+            back = np.empty(len(idx), dtype=np.int64)
+            back[idx - sl.start] = np.arange(len(idx))
+            res = [res[q] for q in back]
         else:
             cases = [family.case(p) for p in params[sl]]
             eng = Engine(family.base, opts, cases)
@@ -299,19 +331,20 @@ def certify_family(family: RefineryFamily, params, X, Y, kkt_tol: float = 1e-6, 
 
 
 def solve_warm(family: RefineryFamily, params, predictor=None, opts: PdhgOptions | None = None, batch: int = 1024,
-               engine: str = "batch", kkt_tol: float | None = None):
+               engine: str = "batch", kkt_tol: float | None = None, work=None):
     """Solve from the predictor's starts, judge every answer with
     certify_family, and re-solve the members that fail from a cold start
     (the fallback).  Returns (FamilySolve, certification, fallback mask)."""
     opts = opts or PdhgOptions()
     kkt_tol = opts.tolerance if kkt_tol is None else kkt_tol
     starts = predictor.predict(params) if predictor is not None else None
-    res = solve_family(family, params, opts, starts=starts, batch=batch, engine=engine)
+    res = solve_family(family, params, opts, starts=starts, batch=batch, engine=engine, work=work)
     cert = certify_family(family, params, res.X, res.Y, kkt_tol=kkt_tol)
     redo = ~cert["certified"]
     if predictor is not None and redo.any():
         idx = np.flatnonzero(redo)
-        again = solve_family(family, np.asarray(params)[idx], opts, batch=batch, engine=engine)
+        again = solve_family(family, np.asarray(params)[idx], opts, batch=batch, engine=engine,
+                             work=None if work is None else np.asarray(work)[idx])
         c2 = certify_family(family, np.asarray(params)[idx], again.X, again.Y, kkt_tol=kkt_tol)
         warm_its = res.iterations[idx].copy()
         for f in ("status", "iterations", "relative_kkt", "objective"):

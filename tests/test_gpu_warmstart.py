@@ -71,3 +71,21 @@ def test_nonfinite_prediction_falls_back_to_cold(trained):
     got, cert, _ = W.solve_warm(fam, P, Broken(), opts)
     assert got.iterations[0] == cold.iterations[0]  # member 0 ran exactly the cold start
     assert cert["certified"].all()
+
+
+def test_launch_order_by_predicted_work_changes_no_answer():
+    """Members handed to the multi-LP engine in decreasing predicted work come
+    back in their own order with exactly the answers of the plain order (each
+    block runs its member alone)."""
+    fam = W.RefineryFamily(seed=5, periods=2, regions=1, units=4, streams=4, properties=2, scale_exponent=0.0)
+    train = fam.sample(64, 3)
+    tr = W.solve_family(fam, train, PdhgOptions(tolerance=1e-6, maxIterations=200000), engine="multi")
+    est = W.WorkEstimate(fam).fit(train, tr.iterations)
+    P = fam.sample(48, 4)
+    work = est.predict(P)
+    assert work.shape == (48,) and np.all(work > 0)
+    opts = PdhgOptions(tolerance=1e-6, maxIterations=200000)
+    plain = W.solve_family(fam, P, opts, engine="multi")
+    ordered = W.solve_family(fam, P, opts, engine="multi", work=work)
+    assert np.array_equal(plain.iterations, ordered.iterations)
+    assert np.array_equal(plain.X, ordered.X) and np.array_equal(plain.Y, ordered.Y)
