@@ -377,14 +377,21 @@ def run_family(args, rank, world):
     losses = lw.fit(P_train[ok], tr.X[ok], tr.Y[ok],
                     TrainOptions(epochs=args.epochs, batch=512, lr=1e-3, lr_final=1e-5, seed=2))
     nn = W.NearestWarmStart(fam).fit(P_train[ok], tr.X[ok], tr.Y[ok])
-    est = W.WorkEstimate(fam).fit(P_train[ok], tr.iterations[ok])
+    use_w = args.family_weights == "nearest" and args.engine == "multi"
+    est = W.WorkEstimate(fam).fit(P_train[ok], tr.iterations[ok], tr.weights[ok] if use_w else None)
     strategies = {"cold": None, "nearest": nn, "learned": lw}
+
+    def start_weights(name, params):
+        # warm-started strategies also start from the nearest members' primal weights
+        return est.predict_weight(params) if use_w and name != "cold" else None
+
     # untimed warm-up batches (module loads, variant tuning, pools): the first at full size, the
     # others of 128 members
     for w in range(args.warmup):
         size_w = args.batch if w == 0 else min(args.batch, 128)
         Pw = fam.sample(size_w, 900 + w)
-        W.solve_warm(fam, Pw, lw, opts, batch=args.batch, engine=args.engine, work=est.predict(Pw))
+        W.solve_warm(fam, Pw, lw, opts, batch=args.batch, engine=args.engine, work=est.predict(Pw),
+                     weights=start_weights("learned", Pw))
     acc = {k: {"seconds": [], "solve_seconds": [], "iterations": [], "certified": [], "fallback": [], "kkt": []}
            for k in strategies}
     with ClockSampler(0) as clk:
@@ -394,7 +401,7 @@ def run_family(args, rank, world):
                 torch.cuda.synchronize()
                 t1 = time.perf_counter()
                 r, cert, redo = W.solve_warm(fam, P, pred, opts, batch=args.batch, engine=args.engine,
-                                             work=est.predict(P))
+                                             work=est.predict(P), weights=start_weights(name, P))
                 wall = time.perf_counter() - t1
                 a = acc[name]
                 a["seconds"].append(wall)
@@ -441,6 +448,8 @@ def run_family(args, rank, world):
                        "step": "one held-out batch solved and certified per strategy",
                        "launch_order": "members in decreasing predicted work (mean cold iterations of the 4 nearest "
                                        "training members), every strategy",
+                       "primal_weights": ("warm strategies start from the geometric mean of the 4 nearest training "
+                                          "members' final primal weights" if use_w else "default (||c|| / ||b||)"),
                        "engine": {"multi": "multi-LP engine (AUTO form: one thread block per member)",
                                   "batch": "shared-A batch engine (k-interleaved cases)"}[args.engine],
                        "network": lw.widths, "pca_rank": lw.rank, "pca_explained": lw.basis.explained,
@@ -870,7 +879,8 @@ def run_sweep(args, rank, world):
             "tuned": {"streamed_vectors_primal": bool(st.streaming_at), "streamed_vectors_dual": bool(st.streaming_a),
                       "cases_per_thread_primal": int(st.cases_per_thread_at),
                       "cases_per_thread_dual": int(st.cases_per_thread_a),
-                      "warp_rows_primal": bool(st.warp_rows_at), "warp_rows_dual": bool(st.warp_rows_a)},
+                      "warp_rows_primal": bool(st.warp_rows_at), "warp_rows_dual": bool(st.warp_rows_a),
+                      "tile_rows_primal": int(st.tile_rows_at), "tile_rows_dual": int(st.tile_rows_a)},
             "e2e": {"value": t_e2e, "unit": "s per batch call (host arrays)", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "single_case_ms_per_iteration": t_single * 1e3,
@@ -1221,6 +1231,9 @@ def main():
     ap.add_argument("--family-max-iters", type=int, default=None,
                     help="family / sweep-tol: iteration limit per member (default 400,000 for family; the "
                          "reference's 1,000,000 for sweep-tol)")
+    ap.add_argument("--family-weights", choices=["default", "nearest"], default="default",
+                    help="family (engine multi): starting primal weight of the warm strategies -- the default "
+                         "||c|| / ||b||, or the geometric mean of the 4 nearest training members' final weights")
     ap.add_argument("--sweep-forms", default="", help="sweep-tol: comma-separated subset of the forms to run")
     ap.add_argument("--batch", type=int, default=1024, help="family: members per batched solve")
     ap.add_argument("--engine", choices=["multi", "batch"], default="multi",

@@ -162,7 +162,10 @@ typedef struct b2p_options {
    * (plain otherwise); 1..4 force (cases per thread, evict-first streamed
    * vectors) = (1, no), (2, no), (1, yes), (2, yes); 5..8 the same with whole
    * warps per row (row entries loaded once per warp and shared by shuffle)
-   * where k / cases per thread is a multiple of 32. */
+   * where k / cases per thread is a multiple of 32; 9..16, 17..24 and 25..32
+   * are 1..8 in the row-tiled layouts of 4, 8 and 16 rows per block (each
+   * warp one row, the warps of a block on consecutive rows of one chunk of 32
+   * cases, the blocks chunk by chunk). */
   int32_t batch_variant;
   /* Batches (k > 1 cases sharing A), FP64 phase: 0 = whenever half of the
    * live cases have terminated, pack the others into a narrower interleave
@@ -209,9 +212,11 @@ typedef struct b2p_stats {
   int32_t cta_lps_smem;                       /* CTA form: LPs held wholly in shared memory */
   int32_t cta_lps_vectors;                    /* CTA form: LPs with only their iterates in shared memory */
   int32_t cta_owned_per_thread;               /* CTA form: rows and columns each thread owns (0 = general kernel) */
-  int32_t pad2;
+  int32_t tile_rows_at;                       /* FP64 batches: rows per block of the A^T kernel's row-tiled layout (0 = none) */
   int32_t cases_per_thread_at, cases_per_thread_a; /* FP64 batches: cases per thread of the A^T / A kernels */
   int32_t warp_rows_at, warp_rows_a;          /* FP64 batches: whole warps per row, entries shared by shuffle */
+  int32_t tile_rows_a;                        /* FP64 batches: the same for the A kernel */
+  int32_t pad3;
 } b2p_stats;
 
 /* Replaces pramana::PdhgResult (src/pdhg/pdhg.h:58-65) minus the vectors,
@@ -252,6 +257,20 @@ int b2p_solve_pdhg_batch(const b2p_lp* base, const b2p_case* cases, int32_t num_
 int b2p_solve_pdhg_multi(const b2p_lp* lps, int32_t num_lps, const b2p_options* opts, const double* const* x_start,
                          const double* const* row_dual_start, double* const* x, double* const* row_dual,
                          b2p_result* results, b2p_stats* stats);
+
+/* b2p_solve_pdhg_multi with primal weights in and out (no counterpart in the
+ * reference, whose primal weight starts at ||c|| / ||b|| of the scaled LP,
+ * src/pdhg/pdhg.cpp:497-500).  Weights are in the original space's units:
+ * w = omega gamma / beta, omega the scaled LP's primal weight and beta /
+ * gamma its bound and objective rescalings, so that LPs of one family with
+ * different rescalings exchange them.  primal_weight_start[b] (the array may
+ * be NULL; entries that are not finite and positive keep the default) sets
+ * LP b's initial weight; primal_weight[b] (may be NULL) receives its weight
+ * at termination.  b2p_solve_pdhg_multi is this call with both NULL. */
+int b2p_solve_pdhg_multi_warm(const b2p_lp* lps, int32_t num_lps, const b2p_options* opts,
+                              const double* const* x_start, const double* const* row_dual_start,
+                              const double* primal_weight_start, double* const* x, double* const* row_dual,
+                              double* primal_weight, b2p_result* results, b2p_stats* stats);
 
 /* gpuAvailable (src/pdhg/pdhg.cpp:730): 1 if an sm_100 device is usable. */
 int b2p_gpu_available(void);

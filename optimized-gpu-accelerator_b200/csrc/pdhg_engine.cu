@@ -182,6 +182,7 @@ struct Engine {
   int batch_cpt_p = 1, batch_cpt_d = 1;  // cases per thread of the primal / dual batch kernels (tuned)
   bool batch_wr_p = false, batch_wr_d = false;  // whole warps per row, entries passed by shuffle (tuned)
   bool batch_wr_p_full = false, batch_wr_d_full = false;  // the tuned choice, restored after a compaction
+  int batch_tr_p = 0, batch_tr_d = 0;  // rows per block of the row-tiled layout (0 = one row's cases per block; tuned)
   bool profiling = false;
   std::vector<cudaEvent_t> prof_ev;  // 4 per iteration of the longest interval
   int64_t prof_launches[5] = {0, 0, 0, 0, 0};
@@ -780,68 +781,85 @@ struct Engine {
     B2P_CUDA(cudaMemcpyAsync(h_sums, d_sums, sizeof(double) * k * kNumSums, cudaMemcpyDeviceToHost, stream));
   }
 
+  // Calls f with the compile-time form of a batch kernel variant: Halpern
+  // step, streamed vectors, cases per thread, whole warps per row, tile rows.
+  template <class F>
+  static void batch_dispatch(bool h, bool st, int cpt, bool wr, int tr, F&& f) {
+    using std::false_type;
+    using std::integral_constant;
+    using std::true_type;
+    auto d4 = [&](auto H, auto ST, auto CP, auto WR) {
+      if (tr == 16) f(H, ST, CP, WR, integral_constant<int, 16>{});
+      else if (tr == 8) f(H, ST, CP, WR, integral_constant<int, 8>{});
+      else if (tr == 4) f(H, ST, CP, WR, integral_constant<int, 4>{});
+      else f(H, ST, CP, WR, integral_constant<int, 0>{});
+    };
+    auto d3 = [&](auto H, auto ST, auto CP) {
+      if (wr) d4(H, ST, CP, true_type{});
+      else d4(H, ST, CP, false_type{});
+    };
+    auto d2 = [&](auto H, auto ST) {
+      if (cpt == 2) d3(H, ST, integral_constant<int, 2>{});
+      else d3(H, ST, integral_constant<int, 1>{});
+    };
+    auto d1 = [&](auto H) {
+      if (st) d2(H, true_type{});
+      else d2(H, false_type{});
+    };
+    if (h) d1(true_type{});
+    else d1(false_type{});
+  }
+
+  // Grid of a batch kernel over `rows` rows (layouts in pdhg_kernels.cuh).
+  unsigned batch_grid(int64_t rows, int cpt, int tr) const {
+    const int64_t kh = (k + cpt - 1) / cpt;
+    if (tr == 0) return blocks(rows * kh);
+    return static_cast<unsigned>(std::max<int64_t>(1, ((rows + tr - 1) / tr) * ((kh + 31) / 32)));
+  }
+
   // FP64 batch kernels (k > 1) of one iteration.
-  void enqueue_batch_primal(bool halpern, bool streamed, const IterClock& ck, int cpt, bool wr) {
+  void enqueue_batch_primal(bool halpern, bool streamed, const IterClock& ck, int cpt, bool wr, int tr) {
     const double rho = opt.reflection;
-    const unsigned gp = blocks(static_cast<int64_t>(n) * ((k + cpt - 1) / cpt));
+    const unsigned grid = batch_grid(n, cpt, tr), block = batch_block(tr);
     const CsrView AT = viewAT();
-#define B2P_BP(H, ST, CP, WR)                                                                                   \
-  launch(k_primal<H, ST, CP, WR>, gp, stream, true, n, k, AT, v[Y], v[C], v[LO], v[UP], v[X], v[XP], v[X0], d_tau, \
-         ck, rho)
-#define B2P_BP2(H, ST)                \
-  if (cpt == 2) {                     \
-    if (wr) B2P_BP(H, ST, 2, true);   \
-    else B2P_BP(H, ST, 2, false);     \
-  } else {                            \
-    if (wr) B2P_BP(H, ST, 1, true);   \
-    else B2P_BP(H, ST, 1, false);     \
+    batch_dispatch(halpern, streamed, cpt, wr, tr, [&](auto H, auto ST, auto CP, auto WR, auto TR) {
+      launch_nt(k_primal<decltype(H)::value, decltype(ST)::value, decltype(CP)::value, decltype(WR)::value,
+                         decltype(TR)::value>,
+                grid, block, stream, true, n, k, AT, v[Y], v[C], v[LO], v[UP], v[X], v[XP], v[X0], d_tau, ck, rho);
+    });
   }
-    if (halpern) {
-      if (streamed) { B2P_BP2(true, true) } else { B2P_BP2(true, false) }
-    } else {
-      if (streamed) { B2P_BP2(false, true) } else { B2P_BP2(false, false) }
-    }
-#undef B2P_BP2
-#undef B2P_BP
-  }
-  void enqueue_batch_dual(bool halpern, bool streamed, const IterClock& ck, int cpt, bool wr) {
+  void enqueue_batch_dual(bool halpern, bool streamed, const IterClock& ck, int cpt, bool wr, int tr) {
     const double rho = opt.reflection;
-    const unsigned gd = blocks(static_cast<int64_t>(m) * ((k + cpt - 1) / cpt));
+    const unsigned grid = batch_grid(m, cpt, tr), block = batch_block(tr);
     const CsrView A = viewA();
-#define B2P_BD(H, ST, CP, WR)                                                                                        \
-  launch(k_dual<H, ST, CP, WR>, gd, stream, true, m, k, A, v[XP], v[RL], v[RU], v[Y], v[YP], v[Y0], v[AX], v[AXP], \
-         v[AX0], d_sigma, ck, rho)
-#define B2P_BD2(H, ST)                \
-  if (cpt == 2) {                     \
-    if (wr) B2P_BD(H, ST, 2, true);   \
-    else B2P_BD(H, ST, 2, false);     \
-  } else {                            \
-    if (wr) B2P_BD(H, ST, 1, true);   \
-    else B2P_BD(H, ST, 1, false);     \
+    batch_dispatch(halpern, streamed, cpt, wr, tr, [&](auto H, auto ST, auto CP, auto WR, auto TR) {
+      launch_nt(k_dual<decltype(H)::value, decltype(ST)::value, decltype(CP)::value, decltype(WR)::value,
+                       decltype(TR)::value>,
+                grid, block, stream, true, m, k, A, v[XP], v[RL], v[RU], v[Y], v[YP], v[Y0], v[AX], v[AXP], v[AX0],
+                d_sigma, ck, rho);
+    });
   }
-    if (halpern) {
-      if (streamed) { B2P_BD2(true, true) } else { B2P_BD2(true, false) }
-    } else {
-      if (streamed) { B2P_BD2(false, true) } else { B2P_BD2(false, false) }
-    }
-#undef B2P_BD2
-#undef B2P_BD
-  }
+
+  // Row tiles of the batch kernels' layouts (0 = one row's cases per block).
+  static constexpr int kTileRows[4] = {0, 4, 8, 16};
 
   // FP64 batch kernel variants: forced by the options, or, for batches whose
   // vectors far exceed L2 (k (m + n) >= 2^22 elements), each kernel is timed
   // with one and with two cases per thread, with and (when k / cases per
   // thread is a multiple of 32) without per-lane index loads, with cached and
-  // with evict-first streamed vectors (one warm-up, three timed launches
+  // with evict-first streamed vectors, in the row-per-block layout and the
+  // row-tiled ones of 4, 8 and 16 rows (one warm-up, three timed launches
   // each, from the starting state), and the fastest is kept per kernel.
   void tune_batch() {
-    if (opt.batch_variant < 0 || opt.batch_variant > 8) throw Error(B2P_ERR_INVALID, "batch_variant must be 0..8");
+    if (opt.batch_variant < 0 || opt.batch_variant > 32) throw Error(B2P_ERR_INVALID, "batch_variant must be 0..32");
     if (k <= 1 || mixed_batch) return;
     if (opt.batch_variant > 0) {
-      const int v0 = (opt.batch_variant - 1) % 4 + 1;
+      const int w = (opt.batch_variant - 1) % 8 + 1;  // the layout-free part, 1..8
+      const int v0 = (w - 1) % 4 + 1;
       batch_cpt_p = batch_cpt_d = (v0 == 2 || v0 == 4) ? 2 : 1;
       batch_stream_p = batch_stream_d = v0 >= 3;
-      batch_wr_p = batch_wr_d = opt.batch_variant > 4 && warp_rows(batch_cpt_p);
+      batch_wr_p = batch_wr_d = w > 4 && warp_rows(batch_cpt_p);
+      batch_tr_p = batch_tr_d = kTileRows[(opt.batch_variant - 1) / 8];
     } else if (static_cast<int64_t>(n + m) * k >= (int64_t(1) << 22)) {
       time_batch_variants();
     }
@@ -851,6 +869,8 @@ struct Engine {
     stats.cases_per_thread_a = batch_cpt_d;
     stats.warp_rows_at = batch_wr_p;
     stats.warp_rows_a = batch_wr_d;
+    stats.tile_rows_at = batch_tr_p;
+    stats.tile_rows_a = batch_tr_d;
   }
 
   // Whole warps per row: k / cpt (rounded up) a multiple of 32.
@@ -875,20 +895,23 @@ struct Engine {
       return static_cast<double>(ms);
     };
     double best_p = INFINITY, best_d = INFINITY;
-    for (const int cpt : {1, 2})
-      for (int wr = 0; wr < 2; ++wr) {
-        if (wr && !warp_rows(cpt)) continue;
-        for (int st = 0; st < 2; ++st) {
-          if (n) {
-            const double t = timed([&] { enqueue_batch_primal(true, st != 0, ck, cpt, wr != 0); });
-            if (t < best_p) best_p = t, batch_stream_p = st != 0, batch_cpt_p = cpt, batch_wr_p = wr != 0;
-          }
-          if (m) {
-            const double t = timed([&] { enqueue_batch_dual(true, st != 0, ck, cpt, wr != 0); });
-            if (t < best_d) best_d = t, batch_stream_d = st != 0, batch_cpt_d = cpt, batch_wr_d = wr != 0;
+    for (const int tr : kTileRows)
+      for (const int cpt : {1, 2})
+        for (int wr = 0; wr < 2; ++wr) {
+          if (wr && !warp_rows(cpt)) continue;
+          for (int st = 0; st < 2; ++st) {
+            if (n) {
+              const double t = timed([&] { enqueue_batch_primal(true, st != 0, ck, cpt, wr != 0, tr); });
+              if (t < best_p)
+                best_p = t, batch_stream_p = st != 0, batch_cpt_p = cpt, batch_wr_p = wr != 0, batch_tr_p = tr;
+            }
+            if (m) {
+              const double t = timed([&] { enqueue_batch_dual(true, st != 0, ck, cpt, wr != 0, tr); });
+              if (t < best_d)
+                best_d = t, batch_stream_d = st != 0, batch_cpt_d = cpt, batch_wr_d = wr != 0, batch_tr_d = tr;
+            }
           }
         }
-      }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     stats.autotune_seconds = seconds_since(t0);
@@ -905,10 +928,10 @@ struct Engine {
       const bool last = l == L - 1;
       const IterClock ck{d_it_base, d_restart_at, l};
       if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 0], stream));
-      if (nk) enqueue_batch_primal(!last, batch_stream_p, ck, batch_cpt_p, batch_wr_p);
+      if (nk) enqueue_batch_primal(!last, batch_stream_p, ck, batch_cpt_p, batch_wr_p, batch_tr_p);
       if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 1], stream));
       if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 2], stream));
-      if (mk) enqueue_batch_dual(!last, batch_stream_d, ck, batch_cpt_d, batch_wr_d);
+      if (mk) enqueue_batch_dual(!last, batch_stream_d, ck, batch_cpt_d, batch_wr_d, batch_tr_d);
       if (profiling) B2P_CUDA(cudaEventRecord(prof_ev[4 * l + 3], stream));
       B2P_CUDA(cudaGetLastError());
     }

@@ -162,8 +162,41 @@ __device__ __forceinline__ void row_dot_cases(const CsrView& M, const double* __
   }
 }
 
-// Batch kernels (k > 1 cases sharing A, k-interleaved vectors): thread t takes
-// row t / kh and the cases t % kh + q kh, q < CPT (kh = ceil(k / CPT));
+// Row and first case of this thread in a batch kernel (the layouts TR are
+// described with the kernels below); false for a thread past the last row or
+// past kh.
+template <int TR>
+__device__ __forceinline__ bool batch_thread(int32_t rows, int kh, int64_t& row, int& b0) {
+  if constexpr (TR == 0) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= static_cast<int64_t>(rows) * kh) return false;
+    row = t / kh;
+    b0 = static_cast<int>(t - row * kh);
+    return true;
+  } else {
+    const int64_t row_blocks = (static_cast<int64_t>(rows) + TR - 1) / TR;
+    const int64_t chunk = blockIdx.x / row_blocks;
+    row = (blockIdx.x - chunk * row_blocks) * TR + (threadIdx.x >> 5);
+    b0 = static_cast<int>(chunk * 32) + static_cast<int>(threadIdx.x & 31);
+    return row < rows && b0 < kh;
+  }
+}
+
+// Threads per block and the register cap (blocks per SM) of a batch kernel.
+constexpr int batch_block(int tr) { return tr ? 32 * tr : kBlock; }
+constexpr int batch_min_blocks(int tr, int cpt) { return (2048 / batch_block(tr)) / cpt; }
+
+// Batch kernels (k > 1 cases sharing A, k-interleaved vectors).  A thread
+// takes one row and the cases b0 + q kh, q < CPT (kh = ceil(k / CPT)):
+//   TR = 0: thread t of the grid takes row t / kh and b0 = t % kh (a row's
+//           cases are spread over consecutive threads: the warps of a block
+//           share the row's entries);
+//   TR > 0: a block of TR warps takes TR consecutive rows, one per warp, for
+//           one chunk of 32 consecutive b0 (blocks run chunk by chunk): where
+//           nearby rows share columns, the warps of a block gather the same
+//           256-byte slices of the k-interleaved vector, and the later ones
+//           find them in L1; the slice of the gathered vector that one chunk
+//           reads (rows x 32 x 8 bytes) stays in L2 while the chunk runs.
 // WARPROW requires kh to be a multiple of 32 (whole warps per row).
 // k_primal : aty = A^T y (row j of A^T), x+ = proj(x - tau (c - aty)),
 //            Halpern step of x                    (spmvT + primalStep + halpern x)
@@ -175,19 +208,19 @@ __device__ __forceinline__ void row_dot_cases(const CsrView& M, const double* __
 // gathers.  (k_restart and k_halpern_all, which write x, x0, y, y0, Ax and
 // A x0, do not trigger early: a kernel that follows them starts only when
 // they have completed.)
-template <bool HALPERN, bool STREAM = false, int CPT = 1, bool WARPROW = false>
-static __global__ void __launch_bounds__(kBlock, 8 / CPT)
+template <bool HALPERN, bool STREAM = false, int CPT = 1, bool WARPROW = false, int TR = 0>
+static __global__ void __launch_bounds__(batch_block(TR), batch_min_blocks(TR, CPT))
     k_primal(int32_t n, int32_t k, CsrView AT, const double* __restrict__ y, const double* __restrict__ c,
              const double* __restrict__ lo, const double* __restrict__ up, double* __restrict__ x,
              double* __restrict__ xp, const double* __restrict__ x0, const double* __restrict__ tau, IterClock ck,
              double rho) {
   const int kh = (k + CPT - 1) / CPT;
-  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= static_cast<int64_t>(n) * kh) return;
-  const int64_t j = t / kh;
+  int64_t j;
+  int b0;
+  if (!batch_thread<TR>(n, kh, j, b0)) return;
   int b[CPT];
 #pragma unroll
-  for (int q = 0; q < CPT; ++q) b[q] = static_cast<int>(t - j * kh) + q * kh;
+  for (int q = 0; q < CPT; ++q) b[q] = b0 + q * kh;
   double xv[CPT], cv[CPT], l[CPT], u[CPT], x0v[CPT];
 #pragma unroll
   for (int q = 0; q < CPT; ++q)
@@ -216,19 +249,19 @@ static __global__ void __launch_bounds__(kBlock, 8 / CPT)
   pdl_launch_dependents();
 }
 
-template <bool HALPERN, bool STREAM = false, int CPT = 1, bool WARPROW = false>
-static __global__ void __launch_bounds__(kBlock, 8 / CPT)
+template <bool HALPERN, bool STREAM = false, int CPT = 1, bool WARPROW = false, int TR = 0>
+static __global__ void __launch_bounds__(batch_block(TR), batch_min_blocks(TR, CPT))
     k_dual(int32_t m, int32_t k, CsrView A, const double* __restrict__ xp, const double* __restrict__ rl,
            const double* __restrict__ ru, double* __restrict__ y, double* __restrict__ yp,
            const double* __restrict__ y0, double* __restrict__ ax, double* __restrict__ axp,
            const double* __restrict__ ax0, const double* __restrict__ sigma, IterClock ck, double rho) {
   const int kh = (k + CPT - 1) / CPT;
-  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= static_cast<int64_t>(m) * kh) return;
-  const int64_t i = t / kh;
+  int64_t i;
+  int b0;
+  if (!batch_thread<TR>(m, kh, i, b0)) return;
   int b[CPT];
 #pragma unroll
-  for (int q = 0; q < CPT; ++q) b[q] = static_cast<int>(t - i * kh) + q * kh;
+  for (int q = 0; q < CPT; ++q) b[q] = b0 + q * kh;
   double axv[CPT], yv[CPT], l[CPT], u[CPT], y0v[CPT], ax0v[CPT];
 #pragma unroll
   for (int q = 0; q < CPT; ++q)

@@ -332,6 +332,7 @@ struct MultiEngine {
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
   b2p_stats stats{};
   std::vector<b2p_result> results;
+  std::vector<double> weights;  // per LP: final primal weight, original-space units (omega gamma / beta)
   std::vector<std::vector<double>> xs, ys;  // per instance, original space
   int64_t launches = 0, bytes_up = 0, bytes_down = 0;
   int compactions = 0;
@@ -1083,6 +1084,7 @@ struct MultiEngine {
   void solve_cta(Clock::time_point deadline_start) {
     const auto t_solve = Clock::now();
     results.assign(K, b2p_result{});
+    weights.assign(K, 1.0);
     xs.assign(K, {});
     ys.assign(K, {});
     *reinterpret_cast<volatile int32_t*>(h_stop) = 0;
@@ -1186,6 +1188,7 @@ struct MultiEngine {
         if (o.status == kCtaStalled) o.status = B2P_STATUS_ITERATION_LIMIT;
       }
       store_result(b, o.status, o.rel_kkt, o.pobj, o.dobj, o.iterations, xp.data() + coff[b], yp.data() + roff[b]);
+      weights[b] = o.omega * P[b].gamma / P[b].beta;
       its = std::max<int64_t>(its, o.iterations + (o.status == B2P_STATUS_OPTIMAL ? 1 : 0));
       stats.restarts += o.restarts;
     }
@@ -1200,7 +1203,20 @@ struct MultiEngine {
   }
 
   // Warm starts of some instances (original space); others keep the cold start.
-  void set_start(const double* const* xst, const double* const* yst) {
+  // Warm start of the next solve: points in the original space (x projected
+  // onto the bounds) and primal weights in the original space's units
+  // (w = omega gamma / beta of the scaled problem); NULL arrays, NULL entries
+  // and weights that are not finite and positive leave that part cold.
+  void set_start(const double* const* xst, const double* const* yst, const double* wst = nullptr) {
+    if (wst) {
+      for (int b = 0; b < K; ++b)
+        if (std::isfinite(wst[b]) && wst[b] > 0) omega0[b] = wst[b] * P[b].beta / P[b].gamma;
+      if (cta) {
+        for (int b = 0; b < K; ++b) cta_lps[b].omega0 = omega0[b];
+        B2P_CUDA(cudaMemcpyAsync(d_lps, cta_lps.data(), sizeof(CtaLp) * K, cudaMemcpyHostToDevice, stream));
+        B2P_CUDA(cudaStreamSynchronize(stream));
+      }
+    }
     if (M) B2P_CUDA(cudaMemsetAsync(v[MYINIT], 0, sizeof(double) * M, stream));
     if (!xst && !yst) return;
     std::vector<double> lo(N), up(N), x0(N), y0(M, 0.0);
@@ -1663,6 +1679,7 @@ struct MultiEngine {
     reset_state();
     std::vector<double> omega = omega0;
     results.assign(K, b2p_result{});
+    weights.assign(K, 1.0);
     xs.assign(K, {});
     ys.assign(K, {});
     stats.restarts = 0;
@@ -1695,6 +1712,7 @@ struct MultiEngine {
         const double gap = std::fabs(pobj - dobj) / (1.0 + std::fabs(pobj) + std::fabs(dobj));
         if (relP <= opt.tolerance && relD <= opt.tolerance && gap <= opt.tolerance) {
           extract(b, B2P_STATUS_OPTIMAL, smax(relP, smax(relD, gap)), pobj, dobj, it);
+          weights[b] = omega[b] * P[b].gamma / P[b].beta;
           done[b] = 1;
           anyDone = true;
           --remaining;
@@ -1746,6 +1764,7 @@ struct MultiEngine {
       const double gap = std::fabs(pobj - dobj) / (1 + std::fabs(pobj) + std::fabs(dobj));
       extract(b, (expiredStop || expired()) ? B2P_STATUS_TIME_LIMIT : B2P_STATUS_ITERATION_LIMIT,
               smax(relP, smax(relD, gap)), pobj, dobj, it);
+      weights[b] = omega[b] * P[b].gamma / P[b].beta;
     }
     stats.kernel_launches = launches;
     stats.bytes_uploaded = bytes_up;
@@ -1756,22 +1775,32 @@ struct MultiEngine {
 }  // namespace
 }  // namespace b2p
 
-extern "C" int b2p_solve_pdhg_multi(const b2p_lp* lps, int32_t num_lps, const b2p_options* opts,
-                                    const double* const* x_start, const double* const* row_dual_start,
-                                    double* const* x, double* const* row_dual, b2p_result* results, b2p_stats* stats) {
+extern "C" int b2p_solve_pdhg_multi_warm(const b2p_lp* lps, int32_t num_lps, const b2p_options* opts,
+                                         const double* const* x_start, const double* const* row_dual_start,
+                                         const double* primal_weight_start, double* const* x,
+                                         double* const* row_dual, double* primal_weight, b2p_result* results,
+                                         b2p_stats* stats) {
   using namespace b2p;
   return guarded([&] {
     const auto t0 = Clock::now();
     MultiEngine e;
     e.create(lps, num_lps, opts);
-    e.set_start(x_start, row_dual_start);
+    e.set_start(x_start, row_dual_start, primal_weight_start);
     e.solve(t0);
     for (int b = 0; b < e.K; ++b) {
       if (x && x[b] && !e.xs[b].empty()) std::memcpy(x[b], e.xs[b].data(), sizeof(double) * e.xs[b].size());
       if (row_dual && row_dual[b] && !e.ys[b].empty())
         std::memcpy(row_dual[b], e.ys[b].data(), sizeof(double) * e.ys[b].size());
+      if (primal_weight) primal_weight[b] = e.weights[b];
       if (results) results[b] = e.results[b];
     }
     if (stats) *stats = e.stats;
   });
+}
+
+extern "C" int b2p_solve_pdhg_multi(const b2p_lp* lps, int32_t num_lps, const b2p_options* opts,
+                                    const double* const* x_start, const double* const* row_dual_start,
+                                    double* const* x, double* const* row_dual, b2p_result* results, b2p_stats* stats) {
+  return b2p_solve_pdhg_multi_warm(lps, num_lps, opts, x_start, row_dual_start, nullptr, x, row_dual, nullptr,
+                                   results, stats);
 }

@@ -109,10 +109,11 @@ inline HostTiles make_tiles(const std::vector<int32_t>& ptr, const std::vector<i
 }
 
 template <typename... KArgs, typename... Args>
-inline void launch(void (*kern)(KArgs...), unsigned grid, cudaStream_t stream, bool pdl, Args... args) {
+inline void launch_nt(void (*kern)(KArgs...), unsigned grid, unsigned block, cudaStream_t stream, bool pdl,
+                      Args... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(kBlock);
+  cfg.blockDim = dim3(block);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = stream;
   cudaLaunchAttribute attr[1];
@@ -121,6 +122,11 @@ inline void launch(void (*kern)(KArgs...), unsigned grid, cudaStream_t stream, b
   cfg.attrs = pdl ? attr : nullptr;
   cfg.numAttrs = pdl ? 1 : 0;
   B2P_CUDA(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
+}
+
+template <typename... KArgs, typename... Args>
+inline void launch(void (*kern)(KArgs...), unsigned grid, cudaStream_t stream, bool pdl, Args... args) {
+  launch_nt(kern, grid, kBlock, stream, pdl, args...);
 }
 
 #define B2P_G_SWITCH(g, F)                           \

@@ -64,9 +64,10 @@ class B2pStats(C.Structure):
                 ("schedule_at", C.c_int32), ("autotune_seconds", C.c_double), ("streaming_a", C.c_int32),
                 ("streaming_at", C.c_int32), ("multi_form", C.c_int32), ("cta_threads", C.c_int32),
                 ("cta_smem_bytes", C.c_int64), ("cta_lps_smem", C.c_int32), ("cta_lps_vectors", C.c_int32),
-                ("cta_owned_per_thread", C.c_int32), ("pad2", C.c_int32),
+                ("cta_owned_per_thread", C.c_int32), ("tile_rows_at", C.c_int32),
                 ("cases_per_thread_at", C.c_int32), ("cases_per_thread_a", C.c_int32),
-                ("warp_rows_at", C.c_int32), ("warp_rows_a", C.c_int32)]
+                ("warp_rows_at", C.c_int32), ("warp_rows_a", C.c_int32),
+                ("tile_rows_a", C.c_int32), ("pad3", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_ if not f.startswith("pad")}
@@ -114,6 +115,9 @@ SIGNATURES = {
     "b2p_solve_pdhg_multi": (C.c_int, [C.POINTER(B2pLp), C.c_int32, C.POINTER(B2pOptions), C.POINTER(dptr),
                                        C.POINTER(dptr), C.POINTER(dptr), C.POINTER(dptr), C.POINTER(B2pResult),
                                        C.POINTER(B2pStats)]),
+    "b2p_solve_pdhg_multi_warm": (C.c_int, [C.POINTER(B2pLp), C.c_int32, C.POINTER(B2pOptions), C.POINTER(dptr),
+                                            C.POINTER(dptr), dptr, C.POINTER(dptr), C.POINTER(dptr), dptr,
+                                            C.POINTER(B2pResult), C.POINTER(B2pStats)]),
     "b2p_engine_set_start": (C.c_int, [C.c_void_p, dptr, dptr, C.c_double]),
     "b2p_gpu_available": (C.c_int, []),
     "b2p_gpu_info_json": (C.c_int, [C.c_char_p, C.c_size_t]),

@@ -141,6 +141,9 @@ class PdhgResult:
     iterations: int
     relativeKkt: float
     stats: PdhgStats = field(default_factory=PdhgStats)
+    # solvePdhgMulti: this LP's primal weight at termination in original-space
+    # units (scaled weight x gamma / beta); no counterpart in the reference
+    primalWeight: float = 0.0
 
 
 def _lp_struct(lp: Model):
@@ -243,11 +246,14 @@ def solvePdhgBatch(base: Model, cases: list[LpCase], opts: PdhgOptions | None = 
 
 
 def solvePdhgMulti(lps: list[Model], opts: PdhgOptions | None = None, batchStats: PdhgStats | None = None,
-                   starts: list | None = None, cancel_flag=None) -> list[PdhgResult]:
+                   starts: list | None = None, cancel_flag=None, primalWeights=None) -> list[PdhgResult]:
     """Independent LPs of different sizes solved together on the GPU, each with
     the reference's algorithm (no counterpart in the reference).  starts[b] =
-    (x, y) warm-starts LP b (None entries: cold start); cancel_flag: a ctypes
-    int32 array whose element 0 stops the solve when set."""
+    (x, y) warm-starts LP b (None entries: cold start); primalWeights[b]
+    (original-space units, as the results' primalWeight; entries that are not
+    finite and positive keep the default) sets LP b's initial primal weight;
+    cancel_flag: a ctypes int32 array whose element 0 stops the solve when
+    set."""
     if not lps:
         return []
     opts = opts or PdhgOptions()
@@ -273,7 +279,14 @@ def solvePdhgMulti(lps: list[Model], opts: PdhgOptions | None = None, batchStats
         keep.append((sx, sy))
         xst = (_lib.dptr * k)(*[a.ctypes.data_as(_lib.dptr) if a is not None else None for a in sx])
         yst = (_lib.dptr * k)(*[a.ctypes.data_as(_lib.dptr) if a is not None else None for a in sy])
-    _lib.check(lib.b2p_solve_pdhg_multi(arr, k, C.byref(o), xst, yst, xp, yp, res, C.byref(st)))
+    w_in = None
+    if primalWeights is not None:
+        w_in = np.ascontiguousarray(np.asarray(primalWeights, dtype=np.float64).reshape(k))
+        keep.append(w_in)
+    w_out = np.zeros(k)
+    _lib.check(lib.b2p_solve_pdhg_multi_warm(arr, k, C.byref(o), xst, yst,
+                                              None if w_in is None else w_in.ctypes.data_as(_lib.dptr), xp, yp,
+                                              w_out.ctypes.data_as(_lib.dptr), res, C.byref(st)))
     del keep, structs
     stats = PdhgStats.from_c(st, _device_name())
     if batchStats is not None:
@@ -281,7 +294,8 @@ def solvePdhgMulti(lps: list[Model], opts: PdhgOptions | None = None, batchStats
     solvePdhgMulti.last_stats = st
     return [PdhgResult(status=Status.get(res[b].status, str(res[b].status)), objective=res[b].objective,
                        dualObjective=res[b].dual_objective, x=xs[b], rowDual=ys[b], iterations=res[b].iterations,
-                       relativeKkt=res[b].relative_kkt, stats=stats) for b in range(k)]
+                       relativeKkt=res[b].relative_kkt, stats=stats, primalWeight=float(w_out[b]))
+            for b in range(k)]
 
 
 def gpuAvailable() -> bool:

@@ -200,23 +200,42 @@ class WorkEstimate:
     """Predicted work of a member: the mean cold iteration count of its four
     nearest training members (normalised parameters).  Used to launch the
     members of a batch in decreasing predicted work, so that the hardest ones
-    do not start last (longest-processing-time order)."""
+    do not start last (longest-processing-time order).  Fitted with the
+    training members' final primal weights too, it predicts a member's
+    starting primal weight: their geometric mean."""
 
     def __init__(self, family: RefineryFamily, neighbours: int = 4):
         self.family = family
         self.k = neighbours
+        self.w = None
 
-    def fit(self, params, iterations):
+    def fit(self, params, iterations, weights=None):
         self.P = self.family.normalize(params).astype(np.float64)
         self.it = np.asarray(iterations, dtype=np.float64)
+        if weights is not None:
+            w = np.asarray(weights, dtype=np.float64)
+            self.w = np.where(np.isfinite(w) & (w > 0), w, np.nan)
         return self
 
-    def predict(self, params) -> np.ndarray:
+    def _nearest(self, params) -> np.ndarray:
         Q = self.family.normalize(params).astype(np.float64)
         d = (Q ** 2).sum(1)[:, None] - 2.0 * Q @ self.P.T + (self.P ** 2).sum(1)[None, :]
         k = min(self.k, d.shape[1])
-        j = np.argpartition(d, k - 1, axis=1)[:, :k]
-        return self.it[j].mean(axis=1)
+        return np.argpartition(d, k - 1, axis=1)[:, :k]
+
+    def predict(self, params) -> np.ndarray:
+        return self.it[self._nearest(params)].mean(axis=1)
+
+    def predict_weight(self, params) -> np.ndarray:
+        """Starting primal weights (original-space units, as
+        solvePdhgMulti's primalWeights); 0 (the default weight) where no
+        neighbour has one."""
+        if self.w is None:
+            raise ValueError("WorkEstimate was fitted without weights")
+        lw = np.log(self.w[self._nearest(params)])
+        have = np.isfinite(lw)
+        mean = np.where(have, lw, 0.0).sum(axis=1) / np.maximum(have.sum(axis=1), 1)
+        return np.where(have.any(axis=1), np.exp(mean), 0.0)
 
 
 @dataclass
@@ -230,10 +249,11 @@ class FamilySolve:
     seconds: float = 0.0        # wall time: engine setup + start + solve + fetch
     solve_seconds: float = 0.0  # the PDHG loop alone
     batches: list = field(default_factory=list)
+    weights: np.ndarray = field(default_factory=lambda: np.zeros(0))  # final primal weights (engine "multi")
 
 
 def solve_family(family: RefineryFamily, params, opts: PdhgOptions | None = None, starts=None,
-                 batch: int = 1024, engine: str = "batch", work=None) -> FamilySolve:
+                 batch: int = 1024, engine: str = "batch", work=None, weights=None) -> FamilySolve:
     """Batched PDHG over the family members `params`, in batches of `batch`
     members; `starts` = (X, Y) in the original space, or None (cold start).
     engine "batch": one shared-A k-case solve per chunk (the live cases are
@@ -241,7 +261,9 @@ def solve_family(family: RefineryFamily, params, opts: PdhgOptions | None = None
     thread block per member in its CTA form).  `work` (per member, optional):
     predicted work; within each chunk the multi-LP engine gets the members in
     decreasing predicted work, which is the order its blocks start in.
-    Results come back in the members' order."""
+    `weights` (per member, optional; engine "multi"): starting primal weights.
+    Results come back in the members' order; with engine "multi" the result's
+    `weights` holds each member's final primal weight."""
     opts = opts or PdhgOptions()
     params = np.asarray(params, dtype=np.float64).reshape(-1, family.num_params)
     n, m = family.base.num_cols, family.base.num_rows
@@ -256,8 +278,9 @@ def solve_family(family: RefineryFamily, params, opts: PdhgOptions | None = None
                 idx = idx[np.argsort(-np.asarray(work, dtype=np.float64)[idx], kind="stable")]
             lps = [family.instance(p) for p in params[idx]]
             st = None if starts is None else list(zip(np.asarray(starts[0])[idx], np.asarray(starts[1])[idx]))
+            pw = None if weights is None else np.asarray(weights, dtype=np.float64)[idx]
             t1 = time.perf_counter()
-            res = solvePdhgMulti(lps, opts, starts=st)
+            res = solvePdhgMulti(lps, opts, starts=st, primalWeights=pw)
             t2 = time.perf_counter()
             t1 = t2 - res[0].stats.solveSeconds if res else t1
             back = np.empty(len(idx), dtype=np.int64)
@@ -287,6 +310,7 @@ def solve_family(family: RefineryFamily, params, opts: PdhgOptions | None = None
     out.objective = np.array([r.objective for r in res])
     out.X = np.array([r.x for r in res]).reshape(-1, n)
     out.Y = np.array([r.rowDual for r in res]).reshape(-1, m)
+    out.weights = np.array([r.primalWeight for r in res])
     return out
 
 
@@ -331,14 +355,15 @@ def certify_family(family: RefineryFamily, params, X, Y, kkt_tol: float = 1e-6, 
 
 
 def solve_warm(family: RefineryFamily, params, predictor=None, opts: PdhgOptions | None = None, batch: int = 1024,
-               engine: str = "batch", kkt_tol: float | None = None, work=None):
-    """Solve from the predictor's starts, judge every answer with
+               engine: str = "batch", kkt_tol: float | None = None, work=None, weights=None):
+    """Solve from the predictor's starts (and, with engine "multi", the
+    starting primal weights `weights`), judge every answer with
     certify_family, and re-solve the members that fail from a cold start
     (the fallback).  Returns (FamilySolve, certification, fallback mask)."""
     opts = opts or PdhgOptions()
     kkt_tol = opts.tolerance if kkt_tol is None else kkt_tol
     starts = predictor.predict(params) if predictor is not None else None
-    res = solve_family(family, params, opts, starts=starts, batch=batch, engine=engine, work=work)
+    res = solve_family(family, params, opts, starts=starts, batch=batch, engine=engine, work=work, weights=weights)
     cert = certify_family(family, params, res.X, res.Y, kkt_tol=kkt_tol)
     redo = ~cert["certified"]
     if predictor is not None and redo.any():
@@ -351,6 +376,7 @@ def solve_warm(family: RefineryFamily, params, predictor=None, opts: PdhgOptions
             getattr(res, f)[idx] = getattr(again, f)
         res.iterations[idx] += warm_its  # the work of both attempts
         res.X[idx], res.Y[idx] = again.X, again.Y
+        res.weights[idx] = again.weights
         res.seconds += again.seconds
         res.solve_seconds += again.solve_seconds
         for k in cert:

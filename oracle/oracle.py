@@ -31,7 +31,7 @@ STATUS_NAMES = {0: "NotSolved", 1: "Optimal", 5: "TimeLimit", 6: "IterationLimit
 class Options(C.Structure):
     _fields_ = [("tolerance", C.c_double), ("max_iterations", C.c_int64), ("check_every", C.c_int32),
                 ("ruiz_iterations", C.c_int32), ("pock_chambolle", C.c_int32), ("rescale", C.c_int32),
-                ("reflection", C.c_double), ("time_limit", C.c_double)]
+                ("reflection", C.c_double), ("time_limit", C.c_double), ("primal_weight_start", C.c_double)]
 
 
 class CaseResult(C.Structure):
@@ -110,7 +110,7 @@ def _ip(a):
 
 def default_options(**kw) -> Options:
     o = Options(tolerance=1e-6, max_iterations=1000000, check_every=64, ruiz_iterations=10, pock_chambolle=1,
-                rescale=1, reflection=1.0, time_limit=0.0)
+                rescale=1, reflection=1.0, time_limit=0.0, primal_weight_start=0.0)
     for k, v in kw.items():
         setattr(o, k, v)
     return o

@@ -45,6 +45,11 @@ typedef struct {
   int32_t rescale;
   double reflection;
   double time_limit; /* ignored by the oracle (no clock); kept for layout parity */
+  /* > 0 and finite: every case's initial primal weight, in original-space
+   * units (scaled weight = w beta / gamma).  No counterpart in the reference
+   * (its weight starts at ||c|| / ||b||); it checks the engine's primal-weight
+   * warm start.  The reference shim ignores it. */
+  double primal_weight_start;
 } oracle_options;
 
 typedef struct {
@@ -435,6 +440,7 @@ int oracle_pdhg_solve(int m, int n, const int* start, const int* index, const do
       if (fin(be.v[RU][t]) && be.v[RU][t] != be.v[RL][t]) bn += be.v[RU][t] * be.v[RU][t];
     }
     if (cn > 1e-20 && bn > 1e-20) omega[b] = sqrt(cn) / sqrt(bn);
+    if (isfinite(o->primal_weight_start) && o->primal_weight_start > 0) omega[b] = o->primal_weight_start * beta / gamma;
   }
   memcpy(be.v[X0], be.v[X], sizeof(double) * (size_t)n * k);
   oracle_csr_mult(m, k, be.A.ptr, be.A.idx, be.A.val, be.v[X], be.v[AX]);

@@ -1,8 +1,11 @@
 """Variants of the FP64 batch kernels (k cases sharing A, k-interleaved
 vectors): one or two cases per thread, cached or evict-first streamed
-vectors, row entries loaded per lane or once per warp and shared by shuffle.  Every variant does each case's arithmetic in the same order, so all
-of them follow the oracle's batch run exactly and agree with one another bit
-for bit; the tuner's choice on a batch larger than L2 is one of them."""
+vectors, row entries loaded per lane or once per warp and shared by shuffle,
+and the thread layouts: one row's cases per block, or row tiles of 4, 8 or
+16 rows per block (one warp per row, 32 cases per chunk).  Every variant does
+each case's arithmetic in the same order, so all of them follow the oracle's
+batch run exactly and agree with one another bit for bit; the tuner's choice
+on a batch larger than L2 is one of them."""
 import numpy as np
 import pytest
 
@@ -13,14 +16,16 @@ from test_gpu_parity import assert_close, opts
 
 pytestmark = pytest.mark.gpu
 
-VARIANTS = [1, 2, 3, 4]  # (cases per thread, streamed) = (1, no), (2, no), (1, yes), (2, yes)
+# (cases per thread, streamed) = (1, no), (2, no), (1, yes), (2, yes); + 8, + 16, + 24: row tiles of 4, 8, 16
+VARIANTS = [1, 2, 3, 4, 9, 10, 11, 12, 17, 18, 19, 20, 25, 26, 27, 28]
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("which", ["sweep", "mixed"])
 def test_batch_variant_vs_oracle(oracle_mod, variant, which):
     lp = G.random_lp(150, 300, 4.0, 90, 13)
-    # odd k: with two cases per thread, the last thread of each row has one case
+    # odd k: with two cases per thread, the last thread of each row has one case;
+    # in the row-tiled layouts most lanes of each chunk have no case
     cases = lp_cases.cost_sweep_cases(lp, 5) if which == "sweep" else lp_cases.mixed_cases(lp, 7)
     gs = pdhg.solvePdhgBatch(lp, cases, opts(tolerance=1e-6, maxIterations=100000, batchVariant=variant))
     os_ = oracle_mod.solve(lp, "oracle", cases=cases, tolerance=1e-6, max_iterations=100000)
@@ -28,7 +33,7 @@ def test_batch_variant_vs_oracle(oracle_mod, variant, which):
         assert_close(g, o)
 
 
-@pytest.mark.parametrize("variant", [5, 6, 7, 8])
+@pytest.mark.parametrize("variant", [5, 6, 7, 8, 13, 14, 15, 16, 21, 22, 23, 24, 29, 30, 31, 32])
 @pytest.mark.parametrize("iters", [1, 64, 500])
 def test_warp_row_variant_vs_oracle(oracle_mod, variant, iters):
     """k = 64: k / cases per thread is a multiple of 32, so whole warps share
@@ -50,7 +55,7 @@ def test_batch_variants_agree_bitwise_and_tuner_runs():
     rng = np.random.default_rng(4)
     cases = [lp_cases.LpCase(cost=lp.col_cost * (1.0 + 0.05 * rng.standard_normal(lp.num_cols))) for _ in range(k)]
     runs = {}
-    for variant in [0, 1, 2, 3, 4, 5, 6, 7, 8]:
+    for variant in range(33):
         stats = pdhg.PdhgStats()
         rs = pdhg.solvePdhgBatch(lp, cases, opts(tolerance=1e-30, maxIterations=300, batchVariant=variant),
                                  batchStats=stats)
@@ -62,7 +67,7 @@ def test_batch_variants_agree_bitwise_and_tuner_runs():
             assert np.array_equal(a.x, b.x) and np.array_equal(a.rowDual, b.rowDual), variant
 
 
-@pytest.mark.parametrize("variant", [0, 1, 4, 5])
+@pytest.mark.parametrize("variant", [0, 1, 4, 5, 13, 24])
 def test_case_compaction_changes_no_iterate(variant):
     """Cases of uneven difficulty: as they terminate, the live ones are packed
     into narrower interleaves (more than once).  Every case's iterations,

@@ -281,3 +281,34 @@ def test_cta_mixed_iteration_limit_and_time_limit():
     lps = [G.random_lp(300, 600, 4.0, 180, 50 + i) for i in range(4)]
     rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-30, maxIterations=100_000_000, timeLimit=0.2, **MIXED))
     assert all(r.status == "TimeLimit" and 0 < r.iterations < 100_000_000 for r in rs)
+
+
+@pytest.mark.parametrize("form", [_lib.MULTI_CTA, _lib.MULTI_GRID])
+@pytest.mark.parametrize("iters", [1, 64, 1000])
+def test_primal_weight_start_vs_oracle(oracle_mod, form, iters):
+    """Starting primal weights (original-space units): every LP given one
+    follows the oracle started from the same weight, iterate for iterate, in
+    both forms; the others (weights 0, -1, nan) keep the default start."""
+    lps = family()
+    w = [0.37, 0.0, 2.5, -1.0, 11.0, np.nan, 0.05, 1.0]
+    rs = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-30, maxIterations=iters, multiForm=form), primalWeights=w)
+    for lp, r, wb in zip(lps, rs, w):
+        start = wb if np.isfinite(wb) and wb > 0 else 0.0
+        assert_close(r, oracle_mod.solve(lp, "oracle", tolerance=1e-30, max_iterations=iters,
+                                         primal_weight_start=start))
+        assert np.isfinite(r.primalWeight) and r.primalWeight > 0
+
+
+def test_primal_weight_round_trip():
+    """Each LP's final weight comes back finite and positive, and a solve
+    restarted from the cold solve's point and final weight converges to the
+    same objective."""
+    lps = family()[:6]
+    cold = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, **CTA))
+    w = [r.primalWeight for r in cold]
+    assert all(np.isfinite(x) and x > 0 for x in w)
+    warm = pdhg.solvePdhgMulti(lps, opts(tolerance=1e-6, **CTA), starts=[(r.x, r.rowDual) for r in cold],
+                               primalWeights=w)
+    for c, r in zip(cold, warm):
+        assert r.status == "Optimal"
+        assert abs(r.objective - c.objective) <= 1e-5 * (1 + abs(c.objective))
