@@ -643,6 +643,79 @@ def run_plan(args, rank, world):
     return 0
 
 
+C3_METRIC = "time to rel KKT 1e-6 (s), full-size config-3 refinery LP, mixed precision"
+
+
+def run_c3(args, rank, world):
+    """--workload c3: the config-3 refinery planning LP at full size (the
+    generator's 12 periods x 6 crudes x 10 units x 15 pools x 10 regions,
+    48,072 x 99,144, 756,660 nonzeros), with unit row and column scales and
+    with the 10^U(-3,3) rescaling, each solved once per (tolerance 1e-4 /
+    1e-6, plain FP64 / mixed) under --c3-max-iters: status, iterations,
+    device time, the KKT recomputed on the device from the returned point,
+    the mixed answer's distance to the FP64 one, and the outward-rounded
+    dual bound over the constraint-implied column bounds.  One solve per
+    form: a 1e-6 solve is ~2,000,000 iterations (~20 s)."""
+    import numpy as np
+    import torch
+
+    from pramana_b200 import _lib, pdhg
+    from pramana_b200 import generators as G
+    from pramana_b200.model import LpCase
+
+    if world > 1 and rank != 0:
+        return 0
+    torch.cuda.set_device(0)
+    results = {}
+    launches = 0
+    with ClockSampler(0) as clk:
+        for scaling, expo in (("unit", 0.0), ("rescaled", 3.0)):
+            lp = G.refinery_lp(seed=5, scale_exponent=expo)
+            lo, up = pdhg.impliedBounds(lp)
+            box = [LpCase(col_lower=lo[0], col_upper=up[0])]
+            for tol in (1e-4, 1e-6):
+                ref = None
+                for form, prec in (("fp64", _lib.PRECISION_FP64), ("mixed", _lib.PRECISION_MIXED)):
+                    r = pdhg.solvePdhg(lp, pdhg.PdhgOptions(tolerance=tol, maxIterations=args.c3_max_iters,
+                                                            precision=prec))
+                    launches += r.stats.kernelLaunches
+                    kkt = pdhg.kktResidual(lp, r.x, r.rowDual)[0]
+                    lb = pdhg.safeDualBound(lp, r.rowDual, box)[0]["bound"] + lp.obj_offset
+                    rec = {"status": r.status, "iterations": r.iterations, "fp32_iterations": r.stats.fp32Iterations,
+                           "seconds": r.stats.kernelSeconds, "objective": r.objective,
+                           "relative_kkt": float(kkt[3]), "kkt_parts": [float(v) for v in kkt[:3]],
+                           "certified_bound": lb,
+                           "bound_gap": (abs(r.objective - lb) / (1 + abs(r.objective))) if np.isfinite(lb) else None}
+                    if ref is None:
+                        ref = r
+                    else:
+                        rec["objective_vs_fp64"] = abs(r.objective - ref.objective) / (1 + abs(ref.objective))
+                        rec["x_vs_fp64"] = float(np.linalg.norm(r.x - ref.x) / (1 + np.linalg.norm(ref.x)))
+                    results[f"{scaling}_{tol:g}_{form}"] = rec
+    head = results["unit_1e-06_mixed"]
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        if O.available("ref"):
+            lp = G.refinery_lp(seed=5, scale_exponent=0.0)
+            threads = os.cpu_count() or 1
+            spi, wall, _ = cpu_reference_sample(lp, args.cpu_sample_iters, threads)
+            cpu = {"value": spi * head["iterations"], "unit": "s", "cores": threads, "kind": "reference",
+                   "sample": f"first {args.cpu_sample_iters} iterations of the unit-scale LP ({wall:.1f} s), "
+                             f"scaled to the mixed 1e-6 solve's {head['iterations']} iterations"}
+    line = {"metric": C3_METRIC, "value": head["seconds"], "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 0,
+            "ms_per_step": head["seconds"] * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 iterates, f64 checks and polish (the fp64 forms: f64)",
+            "data": "synthetic (seeded generator)", "workload": "c3",
+            "config": {"workload": "refinery LP 48072 rows x 99144 cols, 756660 nnz (12 periods, 6 crudes, 10 units, "
+                                   "15 pools, 10 regions), unit scales and 10^U(-3,3)-rescaled, to rel KKT 1e-4 and "
+                                   f"1e-6, at most {args.c3_max_iters} iterations per solve",
+                       "steps": "one solve per form (about 20 s each at 1e-6)"},
+            "results": results, "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu}
+    print(json.dumps(line))
+    return 0
+
+
 def run_families(args, rank, world):
     """--workload families: the batched-PDHG leg of the reference's published
     repeated-solve experiment (compareFamilyStrategies; tests/golden/families/,
@@ -1210,9 +1283,10 @@ def main():
     ap.add_argument("--cpu-sample-iters", type=int, default=CPU_SAMPLE_ITERS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["lp", "family", "multi", "sweep", "router", "plan", "families",
-                                           "calibrate", "gemm", "sweep-tol"], default="lp")
+                                           "calibrate", "gemm", "sweep-tol", "c3"], default="lp")
     ap.add_argument("--plan", default="plan_60x156", help="plan: which refinery plan of the published runs")
     ap.add_argument("--plan-tol", type=float, default=1e-4, help="plan: relative KKT tolerance (1e-4 or 1e-6)")
+    ap.add_argument("--c3-max-iters", type=int, default=3000000, help="c3: iteration limit per solve")
     ap.add_argument("--router-limit", type=float, default=3.0, help="router: time limit per engine and LP (s)")
     ap.add_argument("--router-out", default="router_calibration",
                     help="router: folder for the fitted model and the per-LP timings")
@@ -1275,6 +1349,8 @@ def main():
         return run_calibrate(args, rank, world)
     if args.workload == "gemm":
         return run_gemm(args, rank, world)
+    if args.workload == "c3":
+        return run_c3(args, rank, world)
     if args.workload == "sweep-tol":
         return run_sweep_tol(args, rank, world)
 
