@@ -172,7 +172,15 @@ typedef struct b2p_options {
    * (each case's state moves unchanged, so its iterates do not change; the
    * kernels stop streaming the finished cases' vectors); 1 = never. */
   int32_t batch_no_compaction;
+  /* CTA form: layout of the operators its general kernel reads from global
+   * memory -- B2P_CTA_LAYOUT_AUTO (sliced ELL: the entries of 32 consecutive
+   * rows interleaved so that a warp's loads are coalesced) or
+   * B2P_CTA_LAYOUT_CSR (the CSR arrays as they are).  The row sums are the
+   * same in both (left to right per row), so are the iterates. */
+  int32_t cta_layout;
+  int32_t pad_options;
 } b2p_options;
+enum { B2P_CTA_LAYOUT_AUTO = 0, B2P_CTA_LAYOUT_CSR = 1 };
 enum { B2P_MULTI_AUTO = 0, B2P_MULTI_GRID = 1, B2P_MULTI_CTA = 2 };
 enum { B2P_CTA_AUTO = 0, B2P_CTA_GENERAL = 1, B2P_CTA_OWNER1 = 2, B2P_CTA_OWNER2 = 3 };
 
@@ -216,7 +224,7 @@ typedef struct b2p_stats {
   int32_t cases_per_thread_at, cases_per_thread_a; /* FP64 batches: cases per thread of the A^T / A kernels */
   int32_t warp_rows_at, warp_rows_a;          /* FP64 batches: whole warps per row, entries shared by shuffle */
   int32_t tile_rows_a;                        /* FP64 batches: the same for the A kernel */
-  int32_t pad3;
+  int32_t cta_sliced;                         /* CTA form: 1 if the sliced-ELL operators were built and used */
 } b2p_stats;
 
 /* Replaces pramana::PdhgResult (src/pdhg/pdhg.h:58-65) minus the vectors,

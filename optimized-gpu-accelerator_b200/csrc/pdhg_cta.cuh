@@ -98,6 +98,14 @@ struct CtaArgs {
   // x+ and y+ still go to xp and yp above, converted)
   const float *A32, *AT32;
   float *x32, *xp32, *x032, *y32, *yp32, *y032, *ax32, *axp32, *ax032;
+  // sliced-ELL copies of the operators (NULL sbase: none): the entries of
+  // rows 32 s .. 32 s + 31 of an LP interleaved, entry q of the row at
+  // sbase[row] + 32 q (sbase indexed like the row pointers; the row's length
+  // from them), so that the 32 lanes of a warp -- 32 consecutive rows -- load
+  // one entry each from consecutive addresses
+  const int32_t *sa_base, *sa_idx, *st_base, *st_idx;
+  const double *sa_val, *st_val;
+  const float *sa_val32, *st_val32;
   double tol, rho;
   int64_t max_it;
   int32_t check_every;
@@ -111,12 +119,15 @@ template <class T>
 struct CtaState {
   T *x, *xp, *x0, *y, *yp, *y0, *ax, *axp, *ax0;
   const T *Av, *Tv;
+  const T *SAv, *STv;  // sliced-ELL values
 };
 __device__ __forceinline__ CtaState<double> cta_state(const CtaArgs& a, double*) {
-  return CtaState<double>{a.x, a.xp, a.x0, a.y, a.yp, a.y0, a.ax, a.axp, a.ax0, a.A.val, a.AT.val};
+  return CtaState<double>{a.x,  a.xp,  a.x0,    a.y,      a.yp,     a.y0,    a.ax,
+                          a.axp, a.ax0, a.A.val, a.AT.val, a.sa_val, a.st_val};
 }
 __device__ __forceinline__ CtaState<float> cta_state(const CtaArgs& a, float*) {
-  return CtaState<float>{a.x32, a.xp32, a.x032, a.y32, a.yp32, a.y032, a.ax32, a.axp32, a.ax032, a.A32, a.AT32};
+  return CtaState<float>{a.x32, a.xp32, a.x032, a.y32, a.yp32, a.y032, a.ax32,
+                         a.axp32, a.ax032, a.A32, a.AT32, a.sa_val32, a.st_val32};
 }
 
 // Iterate / anchor vector elements of an LP in shared memory, rounded up so
@@ -343,6 +354,36 @@ __device__ __forceinline__ double row_sum(int p, const int e, const int32_t* __r
   return s;
 }
 
+// The same left-to-right sum over a row of length len stored sliced-ELL from
+// position b (entry q at b + 32 q).
+template <class T>
+__device__ __forceinline__ double row_sum_sliced(int b, const int len, const int32_t* __restrict__ idx,
+                                                 const T* __restrict__ val, const T* __restrict__ v, int shift) {
+  double s = 0.0;
+#pragma unroll 4
+  for (int q = 0; q < len; ++q, b += 32)
+    s = __dadd_rn(s, __dmul_rn(static_cast<double>(val[b]), static_cast<double>(v[idx[b] - shift])));
+  return s;
+}
+
+// Row sums of one operator of an LP: its CSR (row pointers local to the LP,
+// in shared memory or global), or, when sbase is set, its sliced-ELL copy.
+template <class T>
+struct RowOp {
+  const int32_t* ptr;
+  const int32_t* idx;
+  const T* val;
+  const int32_t* sbase;  // NULL: CSR
+  const int32_t* sidx;
+  const T* sval;
+  int shift;
+  __device__ __forceinline__ double sum(int r, const T* __restrict__ v) const {
+    const int p = ptr[r], e = ptr[r + 1];
+    if (sbase) return row_sum_sliced(sbase[r], e - p, sidx, sval, v, shift);
+    return row_sum(p, e, idx, val, v, shift);
+  }
+};
+
 __device__ __forceinline__ double lambda_at(int64_t j) {
   const double jj = static_cast<double>(j);
   return __ddiv_rn(__dadd_rn(jj, 1.0), __dadd_rn(jj, 2.0));
@@ -443,6 +484,14 @@ __device__ __forceinline__ void run_lp(const CtaArgs& a, const CtaLp& L, int lp,
       Ap = sp, Tp = sp + m + 1;
     }
   }
+  // the operators' row sums: sliced-ELL where the engine built that copy and
+  // the LP reads its operators from global memory but gathers from shared
+  // memory (the vectors tiers: operator loads, scattered per lane in CSR,
+  // are what the block waits on there; with the vectors in global memory
+  // too, the CSR arrays' fewer bytes measured faster)
+  const bool sliced = (TIER == kCtaVectors || TIER == kCtaVectorsPtr) && a.sa_base != nullptr;
+  const RowOp<T> opA{Ap, Ai, Av, sliced ? a.sa_base + L.aptr_off : nullptr, a.sa_idx, g.SAv, L.ashift};
+  const RowOp<T> opT{Tp, Ti, Tv, sliced ? a.st_base + L.tptr_off : nullptr, a.st_idx, g.STv, L.tshift};
   // starting point (x0 = x = x_init, y0 = y = y_init, A x0)
   for (int j = tid; j < n; j += NT) x[j] = x0[j] = static_cast<T>(a.xinit[L.coff + j]);
   for (int i = tid; i < m; i += NT) {
@@ -467,7 +516,7 @@ __device__ __forceinline__ void run_lp(const CtaArgs& a, const CtaLp& L, int lp,
     }
     for (int j = tid; j < n; j += NT) {
       const double xv = static_cast<double>(x[j]);
-      col_check(s, row_sum(Tp[j], Tp[j + 1], Ti, Tv, y, L.tshift), c[j], lo[j], up[j], cfac[j], xv, xv, xv);
+      col_check(s, opT.sum(j, y), c[j], lo[j], up[j], cfac[j], xv, xv, xv);
       xp[j] = x[j];
     }
     entry_decide<NT>(s, sh, a, L);
@@ -480,7 +529,7 @@ __device__ __forceinline__ void run_lp(const CtaArgs& a, const CtaLp& L, int lp,
       const double lam = lambda_at(it + l - restartAt);
       // x+ = proj(x - tau (c - A^T y)), Halpern step of x
       for (int j = tid; j < n; j += NT) {
-        const double aty = row_sum(Tp[j], Tp[j + 1], Ti, Tv, y, L.tshift);
+        const double aty = opT.sum(j, y);
         const double xv = static_cast<double>(x[j]);
         double v = __dsub_rn(xv, __dmul_rn(tau, __dsub_rn(c[j], aty)));
         const double lj = lo[j], uj = up[j];
@@ -492,7 +541,7 @@ __device__ __forceinline__ void run_lp(const CtaArgs& a, const CtaLp& L, int lp,
       __syncthreads();
       // A x+, y+ = v + sigma proj(-v / sigma), Halpern steps of y and A x
       for (int i = tid; i < m; i += NT) {
-        const double axpv = row_sum(Ap[i], Ap[i + 1], Ai, Av, xp, L.ashift);
+        const double axpv = opA.sum(i, xp);
         const double axv = static_cast<double>(ax[i]), yv = static_cast<double>(y[i]);
         const double v = __dsub_rn(yv, __dmul_rn(sigma, __dsub_rn(__dmul_rn(2.0, axpv), axv)));
         double w = __ddiv_rn(-v, sigma);
@@ -521,7 +570,7 @@ __device__ __forceinline__ void run_lp(const CtaArgs& a, const CtaLp& L, int lp,
       ax[i] = static_cast<T>(halpern_step(static_cast<double>(ax[i]), axpv, static_cast<double>(ax0[i]), lam, rho));
     }
     for (int j = tid; j < n; j += NT) {
-      const double atyp = row_sum(Tp[j], Tp[j + 1], Ti, Tv, yp, L.tshift);
+      const double atyp = opT.sum(j, yp);
       const double xc = static_cast<double>(x[j]), xpv = static_cast<double>(xp[j]), x0v = static_cast<double>(x0[j]);
       col_check(s, atyp, c[j], lo[j], up[j], cfac[j], xpv, xc, x0v);
       x[j] = static_cast<T>(halpern_step(xc, xpv, x0v, lam, rho));

@@ -224,6 +224,20 @@ __global__ void __launch_bounds__(kBlock) k_restart_multi(int32_t n, int32_t m, 
 
 // idx[q] += off[b] for the entries q of LP b (block b): LP-local indices of
 // the concatenated operator become global ones.
+// Sliced-ELL copy of CSR rows: row r's entries to base[r] + 32 q.
+__global__ void __launch_bounds__(kBlock) k_to_sliced(int32_t rows, const int32_t* __restrict__ ptr,
+                                                      const int32_t* __restrict__ idx, const double* __restrict__ val,
+                                                      const int32_t* __restrict__ base, int32_t* __restrict__ sidx,
+                                                      double* __restrict__ sval) {
+  const int32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  int64_t b = base[r];
+  for (int32_t p = ptr[r]; p < ptr[r + 1]; ++p, b += 32) {
+    sidx[b] = idx[p];
+    sval[b] = val[p];
+  }
+}
+
 __global__ void k_offset_segments(const int64_t* __restrict__ seg, const int32_t* __restrict__ off,
                                   int32_t* __restrict__ idx) {
   const int b = blockIdx.x;
@@ -297,6 +311,11 @@ struct MultiEngine {
   cudaStream_t stream = nullptr;
   std::vector<void*> allocs;
   int32_t *dA_ptr = nullptr, *dA_idx = nullptr, *dT_ptr = nullptr, *dT_idx = nullptr;
+  // CTA form: sliced-ELL copies of the operators (see CtaArgs), NULL when not built
+  int32_t *d_sa_base = nullptr, *d_sa_idx = nullptr, *d_st_base = nullptr, *d_st_idx = nullptr;
+  double *d_sa_val = nullptr, *d_st_val = nullptr;
+  float *d_sa_val32 = nullptr, *d_st_val32 = nullptr;
+  int64_t sa_len = 0, st_len = 0;
   double *dA_val = nullptr, *dT_val = nullptr, *d_rfac = nullptr, *d_cfac = nullptr;
   double* v[MNSLOT] = {};
   int32_t *d_rinst = nullptr, *d_cinst = nullptr, *d_done = nullptr, *d_mask = nullptr;
@@ -827,6 +846,12 @@ struct MultiEngine {
     B2P_OWNER_VARIANTS(B2P_OWNER_ATTR)
 #undef B2P_OWNER_ATTR
     mixed = opt.precision == B2P_PRECISION_MIXED;
+    bool vec_tier = false;  // an LP that reads its operators from global memory and gathers from shared
+    for (const CtaLp& c : cta_lps) {
+      vec_tier = vec_tier || c.tier == kCtaVectors || c.tier == kCtaVectorsPtr;
+      if (mixed) vec_tier = vec_tier || c.tier32 == kCtaVectors || c.tier32 == kCtaVectorsPtr;
+    }
+    if (opt.cta_layout != B2P_CTA_LAYOUT_CSR && vec_tier) build_sliced(A, AT);
     if (mixed) setup_cta_fp32();
     tune_cta();
     if (mixed) tune_cta_fp32();
@@ -835,6 +860,53 @@ struct MultiEngine {
     stats.cta_smem_bytes = cta_r > 0 ? cta_owner_smem : cta_smem;
     stats.cta_lps_smem = n_all;
     stats.cta_lps_vectors = n_vec;
+    stats.cta_sliced = d_sa_base != nullptr && cta_r <= 0;
+  }
+
+  // Sliced-ELL copies of A and A^T for the CTA form: per LP (LP 0 alone when
+  // all LPs share one operator), the rows in slices of 32 consecutive local
+  // rows -- the rows one warp of the CTA kernel takes together -- each slice
+  // as wide as its longest row, entry q of the slice's lane l at
+  // slice + 32 q + l.  Not built when the padded copy would exceed 2^31
+  // entries.
+  void build_sliced(const HostCsr& A, const HostCsr& AT) {
+    const int nlp = shared_operator ? std::min(K, 1) : K;
+    auto bases = [&](const HostCsr& H, const std::vector<int64_t>& off, bool cols, std::vector<int32_t>& base,
+                     int64_t& total) {
+      base.assign(H.ptr.size() > 0 ? H.ptr.size() - 1 : 0, 0);
+      total = 0;
+      for (int b = 0; b < nlp; ++b) {
+        const int64_t r0 = off[b], rows = cols ? P[b].n : P[b].m;
+        for (int64_t s0 = 0; s0 < rows; s0 += 32) {
+          const int64_t s1 = std::min<int64_t>(rows, s0 + 32);
+          int32_t w = 0;
+          for (int64_t r = s0; r < s1; ++r) w = std::max(w, H.ptr[r0 + r + 1] - H.ptr[r0 + r]);
+          if (total + 32 * static_cast<int64_t>(w) >= (int64_t(1) << 31)) return false;
+          for (int64_t r = s0; r < s1; ++r) base[r0 + r] = static_cast<int32_t>(total + (r - s0));
+          total += 32 * static_cast<int64_t>(w);
+        }
+      }
+      return true;
+    };
+    std::vector<int32_t> ba, bt;
+    if (!bases(A, roff, false, ba, sa_len) || !bases(AT, coff, true, bt, st_len)) {
+      sa_len = st_len = 0;
+      return;
+    }
+    d_sa_base = upload(ba);
+    d_st_base = upload(bt);
+    d_sa_idx = dalloc<int32_t>(std::max<int64_t>(sa_len, 1));
+    d_sa_val = dalloc<double>(std::max<int64_t>(sa_len, 1));
+    d_st_idx = dalloc<int32_t>(std::max<int64_t>(st_len, 1));
+    d_st_val = dalloc<double>(std::max<int64_t>(st_len, 1));
+    B2P_CUDA(cudaMemsetAsync(d_sa_idx, 0, sizeof(int32_t) * std::max<int64_t>(sa_len, 1), stream));
+    B2P_CUDA(cudaMemsetAsync(d_sa_val, 0, sizeof(double) * std::max<int64_t>(sa_len, 1), stream));
+    B2P_CUDA(cudaMemsetAsync(d_st_idx, 0, sizeof(int32_t) * std::max<int64_t>(st_len, 1), stream));
+    B2P_CUDA(cudaMemsetAsync(d_st_val, 0, sizeof(double) * std::max<int64_t>(st_len, 1), stream));
+    const int32_t ra = nlp == K ? M : P[0].m, rt = nlp == K ? N : P[0].n;
+    if (ra) k_to_sliced<<<blocks(ra), kBlock, 0, stream>>>(ra, dA_ptr, dA_idx, dA_val, d_sa_base, d_sa_idx, d_sa_val);
+    if (rt) k_to_sliced<<<blocks(rt), kBlock, 0, stream>>>(rt, dT_ptr, dT_idx, dT_val, d_st_base, d_st_idx, d_st_val);
+    B2P_CUDA(cudaGetLastError());
   }
 
   CtaArgs cta_args(double tol, int64_t max_it) const {
@@ -851,6 +923,8 @@ struct MultiEngine {
     a.y = v[MY], a.yp = v[MYP], a.y0 = v[MY0];
     a.ax = v[MAX], a.axp = v[MAXP], a.ax0 = v[MAX0];
     a.A32 = dA_val32, a.AT32 = dT_val32;
+    a.sa_base = d_sa_base, a.sa_idx = d_sa_idx, a.st_base = d_st_base, a.st_idx = d_st_idx;
+    a.sa_val = d_sa_val, a.st_val = d_st_val, a.sa_val32 = d_sa_val32, a.st_val32 = d_st_val32;
     a.x32 = v32[0], a.xp32 = v32[1], a.x032 = v32[2];
     a.y32 = v32[3], a.yp32 = v32[4], a.y032 = v32[5];
     a.ax32 = v32[6], a.axp32 = v32[7], a.ax032 = v32[8];
@@ -874,6 +948,13 @@ struct MultiEngine {
     if (annz) {
       k_convert<double, float><<<blocks(static_cast<int64_t>(annz)), kBlock, 0, stream>>>(annz, dA_val, dA_val32);
       k_convert<double, float><<<blocks(static_cast<int64_t>(annz)), kBlock, 0, stream>>>(annz, dT_val, dT_val32);
+      B2P_CUDA(cudaGetLastError());
+    }
+    if (d_sa_base) {
+      d_sa_val32 = dalloc<float>(std::max<int64_t>(sa_len, 1));
+      d_st_val32 = dalloc<float>(std::max<int64_t>(st_len, 1));
+      if (sa_len) k_convert<double, float><<<blocks(sa_len), kBlock, 0, stream>>>(sa_len, d_sa_val, d_sa_val32);
+      if (st_len) k_convert<double, float><<<blocks(st_len), kBlock, 0, stream>>>(st_len, d_st_val, d_st_val32);
       B2P_CUDA(cudaGetLastError());
     }
     for (int q = 0; q < 9; ++q) v32[q] = dalloc<float>(q < 3 ? N : M);

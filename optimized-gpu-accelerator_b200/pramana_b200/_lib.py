@@ -22,6 +22,7 @@ PRECISION_MIXED = 1
 KERNELS_AUTO, KERNELS_FUSED, KERNELS_RESIDENT = 0, 1, 2
 SCHEDULE_AUTO, SCHEDULE_BINNED, SCHEDULE_TILED, SCHEDULE_TUNED = 0, 1, 2, 3
 MULTI_AUTO, MULTI_GRID, MULTI_CTA = 0, 1, 2
+CTA_LAYOUT_AUTO, CTA_LAYOUT_CSR = 0, 1
 CTA_AUTO, CTA_GENERAL, CTA_OWNER1, CTA_OWNER2 = 0, 1, 2, 3
 
 dptr = C.POINTER(C.c_double)
@@ -48,7 +49,8 @@ class B2pOptions(C.Structure):
                 ("lanes_per_row_a", C.c_int32), ("lanes_per_row_at", C.c_int32), ("short_row_rounds", C.c_int32),
                 ("kernel_mode", C.c_int32), ("spmv_schedule", C.c_int32), ("multi_form", C.c_int32),
                 ("cta_smem_limit", C.c_int32), ("cta_threads", C.c_int32), ("cta_kernel", C.c_int32),
-                ("batch_variant", C.c_int32), ("batch_no_compaction", C.c_int32)]
+                ("batch_variant", C.c_int32), ("batch_no_compaction", C.c_int32),
+                ("cta_layout", C.c_int32), ("pad_options", C.c_int32)]
 
 
 class B2pStats(C.Structure):
@@ -67,7 +69,7 @@ class B2pStats(C.Structure):
                 ("cta_owned_per_thread", C.c_int32), ("tile_rows_at", C.c_int32),
                 ("cases_per_thread_at", C.c_int32), ("cases_per_thread_a", C.c_int32),
                 ("warp_rows_at", C.c_int32), ("warp_rows_a", C.c_int32),
-                ("tile_rows_a", C.c_int32), ("pad3", C.c_int32)]
+                ("tile_rows_a", C.c_int32), ("cta_sliced", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_ if not f.startswith("pad")}

@@ -54,6 +54,7 @@ class PdhgOptions:
     ctaKernel: int = _lib.CTA_AUTO  # CTA form: CTA_GENERAL / CTA_OWNER1 / CTA_OWNER2 (0 = autotuned)
     batchVariant: int = 0  # FP64 batches: 0 = tuned; 1..4 = (cases per thread, streamed) (1,no) (2,no) (1,yes) (2,yes)
     batchNoCompaction: bool = False  # batches: keep finished cases in the interleave (no packing)
+    ctaLayout: int = 0  # CTA form: 0 = sliced-ELL operators where read from global memory, 1 = CSR
 
     def to_c(self, cancel_flag=None) -> _lib.B2pOptions:
         if not self.useGpu:
@@ -83,6 +84,7 @@ class PdhgOptions:
         o.cta_kernel = int(self.ctaKernel)
         o.batch_variant = int(self.batchVariant)
         o.batch_no_compaction = int(bool(self.batchNoCompaction))
+        o.cta_layout = int(self.ctaLayout)
         if cancel_flag is not None:
             o.cancel_flag = C.cast(cancel_flag, C.POINTER(C.c_int32))
         return o

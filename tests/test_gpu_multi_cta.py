@@ -312,3 +312,43 @@ def test_primal_weight_round_trip():
     for c, r in zip(cold, warm):
         assert r.status == "Optimal"
         assert abs(r.objective - c.objective) <= 1e-5 * (1 + abs(c.objective))
+
+
+def _vectors_ptr_bytes(lp):
+    """Shared memory of an LP whose iterates and row pointers are in shared
+    memory and whose operators are not (FP64)."""
+    m, n = lp.num_rows, lp.num_cols
+    return 8 * (3 * n + 6 * m) + (4 * ((m + 1) + (n + 1)) + 7) // 8 * 8
+
+
+@pytest.mark.parametrize("precision", [_lib.PRECISION_FP64, _lib.PRECISION_MIXED])
+@pytest.mark.parametrize("shared", [True, False])
+@pytest.mark.parametrize("limit", ["vectors", "auto"])
+def test_sliced_operators_change_no_iterate(precision, shared, limit):
+    """The CTA form's sliced-ELL operators (read from global memory by LPs
+    whose vectors fit shared memory but whose operators do not) sum every
+    row in the CSR's order: iterates, statuses and iteration counts bit for
+    bit those of the CSR layout -- for a family sharing one operator and for
+    LPs with their own, in FP64 and in the mixed form."""
+    if shared:
+        fam = W.RefineryFamily(seed=5, periods=3, regions=2, units=5, streams=5, properties=3, pools=12,
+                               scale_exponent=0.0)
+        lps = [fam.instance(p) for p in fam.sample(12, 4)]
+    else:
+        lps = [G.random_lp(m, 2 * m, 5.0, int(0.6 * m), 300 + i) for i, m in enumerate([40, 333, 700, 1500, 65])]
+    # "vectors": a limit that leaves the largest LP's iterates and row
+    # pointers in shared memory and its operators in global memory; "auto":
+    # each LP in the tier its size gets
+    smem = max(_vectors_ptr_bytes(lp) for lp in lps) if limit == "vectors" else 0
+    out = {}
+    for layout in (_lib.CTA_LAYOUT_CSR, _lib.CTA_LAYOUT_AUTO):
+        o = opts(tolerance=1e-6, maxIterations=20000, precision=precision, ctaSmemLimit=smem, ctaLayout=layout,
+                 **CTA)
+        out[layout] = pdhg.solvePdhgMulti(lps, o)
+        assert _stats().multi_form == _lib.MULTI_CTA
+        if smem:
+            assert _stats().cta_lps_vectors > 0
+            assert _stats().cta_sliced == (layout == _lib.CTA_LAYOUT_AUTO)
+    for a, b in zip(out[_lib.CTA_LAYOUT_CSR], out[_lib.CTA_LAYOUT_AUTO]):
+        assert a.status == b.status and a.iterations == b.iterations
+        assert np.array_equal(a.x, b.x) and np.array_equal(a.rowDual, b.rowDual)
