@@ -27,14 +27,14 @@ fallback (``solve_family`` with ``starts=None``).
 from __future__ import annotations
 
 import time
-from dataclasses import dataclass, field
+from dataclasses import dataclass, field, replace
 
 import numpy as np
 
 from . import generators as G
 from .mlp import MlpNetwork, TrainOptions
 from .model import LpCase, Model
-from .pdhg import (Engine, PdhgOptions, certifyLp, impliedBounds, kktResidual, safeDualBound,
+from .pdhg import (Engine, PdhgOptions, PdhgResult, certifyLp, impliedBounds, kktResidual, safeDualBound,
                    solvePdhgMulti)
 
 N_DEMAND = 10
@@ -258,7 +258,9 @@ def solve_family(family: RefineryFamily, params, opts: PdhgOptions | None = None
     members; `starts` = (X, Y) in the original space, or None (cold start).
     engine "batch": one shared-A k-case solve per chunk (the live cases are
     packed narrower as others finish); "multi": the multi-LP engine (one
-    thread block per member in its CTA form).  `work` (per member, optional):
+    thread block per member in its CTA form); "single": the single-LP engine
+    per member, one after another (every SM on one member: for a handful of
+    members).  `work` (per member, optional):
     predicted work; within each chunk the multi-LP engine gets the members in
     decreasing predicted work, which is the order its blocks start in.
     `weights` (per member, optional; engine "multi"): starting primal weights.
@@ -286,6 +288,16 @@ def solve_family(family: RefineryFamily, params, opts: PdhgOptions | None = None
             back = np.empty(len(idx), dtype=np.int64)
             back[idx - sl.start] = np.arange(len(idx))
             res = [res[q] for q in back]
+        elif engine == "single":
+            res = []
+            t1 = time.perf_counter()
+            for q in range(sl.start, sl.stop):
+                with Engine(family.instance(params[q]), opts) as eng:
+                    if starts is not None:
+                        eng.set_start(np.asarray(starts[0])[q], np.asarray(starts[1])[q])
+                    r = eng.solve()[0]
+                res.append(PdhgResult(**{**r.__dict__, "primalWeight": 0.0}))
+            t2 = time.perf_counter()
         else:
             cases = [family.case(p) for p in params[sl]]
             eng = Engine(family.base, opts, cases)
@@ -355,20 +367,31 @@ def certify_family(family: RefineryFamily, params, X, Y, kkt_tol: float = 1e-6, 
 
 
 def solve_warm(family: RefineryFamily, params, predictor=None, opts: PdhgOptions | None = None, batch: int = 1024,
-               engine: str = "batch", kkt_tol: float | None = None, work=None, weights=None):
+               engine: str = "batch", kkt_tol: float | None = None, work=None, weights=None,
+               warm_max_iterations: int | None = None, single_fallback: int = 0):
     """Solve from the predictor's starts (and, with engine "multi", the
     starting primal weights `weights`), judge every answer with
     certify_family, and re-solve the members that fail from a cold start
-    (the fallback).  Returns (FamilySolve, certification, fallback mask)."""
+    (the fallback).  `warm_max_iterations` (optional) caps the warm attempt
+    below opts.maxIterations, so that a start that leads nowhere falls back
+    sooner; the fallback keeps opts.maxIterations.  A fallback of at most
+    `single_fallback` members (default none) runs on the single-LP engine,
+    one member at a time with every SM, instead of on `engine`.  Returns
+    (FamilySolve, certification, fallback mask)."""
     opts = opts or PdhgOptions()
     kkt_tol = opts.tolerance if kkt_tol is None else kkt_tol
     starts = predictor.predict(params) if predictor is not None else None
-    res = solve_family(family, params, opts, starts=starts, batch=batch, engine=engine, work=work, weights=weights)
+    warm_opts = opts
+    if predictor is not None and warm_max_iterations is not None:
+        warm_opts = replace(opts, maxIterations=min(opts.maxIterations, int(warm_max_iterations)))
+    res = solve_family(family, params, warm_opts, starts=starts, batch=batch, engine=engine, work=work,
+                       weights=weights)
     cert = certify_family(family, params, res.X, res.Y, kkt_tol=kkt_tol)
     redo = ~cert["certified"]
     if predictor is not None and redo.any():
         idx = np.flatnonzero(redo)
-        again = solve_family(family, np.asarray(params)[idx], opts, batch=batch, engine=engine,
+        again = solve_family(family, np.asarray(params)[idx], opts, batch=batch,
+                             engine="single" if len(idx) <= single_fallback else engine,
                              work=None if work is None else np.asarray(work)[idx])
         c2 = certify_family(family, np.asarray(params)[idx], again.X, again.Y, kkt_tol=kkt_tol)
         warm_its = res.iterations[idx].copy()

@@ -89,3 +89,21 @@ def test_launch_order_by_predicted_work_changes_no_answer():
     ordered = W.solve_family(fam, P, opts, engine="multi", work=work)
     assert np.array_equal(plain.iterations, ordered.iterations)
     assert np.array_equal(plain.X, ordered.X) and np.array_equal(plain.Y, ordered.Y)
+
+
+def test_warm_cap_and_single_engine_fallback(trained):
+    """Warm attempts capped at one iteration fail certification, and those
+    members re-solve cold: a fallback of at most 8 members on the single-LP
+    engine, each answer exactly that member's cold single-LP solve; a larger
+    one on the batched engine.  Every answer certified."""
+    fam, opts, lw, _, _ = trained
+    P = fam.sample(12, 400)
+    got, cert, redo = W.solve_warm(fam, P[:6], lw, opts, engine="multi", warm_max_iterations=1, single_fallback=8)
+    assert redo.sum() >= 3 and cert["certified"].all()
+    single = W.solve_family(fam, P[:6][redo], opts, engine="single")
+    assert np.array_equal(got.X[redo], single.X) and np.array_equal(got.Y[redo], single.Y)
+    extra = got.iterations[redo] - single.iterations  # the warm attempt's work, counted too
+    assert np.all((extra >= 1) & (extra <= 2))
+    got12, cert12, redo12 = W.solve_warm(fam, P, lw, opts, engine="multi", warm_max_iterations=1,
+                                         single_fallback=2)
+    assert redo12.sum() > 2 and cert12["certified"].all()
