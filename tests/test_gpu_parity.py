@@ -2,7 +2,7 @@
 bit-identical to the reference's CpuBackend) and with the golden fixtures
 produced by the reference itself.
 
-Bar (north_star): iterates within 1e-9 relative after a fixed number of
+Bar: iterates within 1e-9 relative after a fixed number of
 iterations, the same termination status, and on converged solves the
 reference's own GPU-vs-CPU window of 4 * checkEvery iterations
 (tests/cpp/test_solvers.cpp:128).  SpMV is bit-exact."""
