@@ -391,7 +391,8 @@ def run_family(args, rank, world):
         size_w = args.batch if w == 0 else min(args.batch, 128)
         Pw = fam.sample(size_w, 900 + w)
         W.solve_warm(fam, Pw, lw, opts, batch=args.batch, engine=args.engine, work=est.predict(Pw),
-                     weights=start_weights("learned", Pw), warm_max_iterations=args.warm_max_iters)
+                     weights=start_weights("learned", Pw), warm_max_iterations=args.warm_max_iters,
+                     continue_failed=args.continue_failed)
     acc = {k: {"seconds": [], "solve_seconds": [], "iterations": [], "certified": [], "fallback": [], "kkt": []}
            for k in strategies}
     with ClockSampler(0) as clk:
@@ -402,7 +403,8 @@ def run_family(args, rank, world):
                 t1 = time.perf_counter()
                 r, cert, redo = W.solve_warm(fam, P, pred, opts, batch=args.batch, engine=args.engine,
                                              work=est.predict(P), weights=start_weights(name, P),
-                                             warm_max_iterations=args.warm_max_iters)
+                                             warm_max_iterations=args.warm_max_iters,
+                                             continue_failed=args.continue_failed)
                 wall = time.perf_counter() - t1
                 a = acc[name]
                 a["seconds"].append(wall)
@@ -450,7 +452,9 @@ def run_family(args, rank, world):
                        "launch_order": "members in decreasing predicted work (mean cold iterations of the 4 nearest "
                                        "training members), every strategy",
                        "warm_max_iterations": args.warm_max_iters or args.family_max_iters,
-                       "fallback": "members that fail certification re-solved cold by the same engine",
+                       "fallback": ("members that fail certification continue from their final point and "
+                                    "primal weight, then what still fails re-solves cold" if args.continue_failed else
+                                    "members that fail certification re-solved cold by the same engine"),
                        "primal_weights": ("warm strategies start from the geometric mean of the 4 nearest training "
                                           "members' final primal weights" if use_w else "default (||c|| / ||b||)"),
                        "engine": {"multi": "multi-LP engine (AUTO form: one thread block per member)",
@@ -1311,6 +1315,9 @@ def main():
     ap.add_argument("--warm-max-iters", type=int, default=None,
                     help="family: iteration limit of the warm attempts (default: --family-max-iters); a member "
                          "past it falls back to a cold solve")
+    ap.add_argument("--cold-fallback-only", dest="continue_failed", action="store_false",
+                    help="family: a warm-started member that fails re-solves cold at once (default: it continues "
+                         "from its final point and primal weight first, then cold)")
     ap.add_argument("--family-weights", choices=["default", "nearest"], default="default",
                     help="family (engine multi): starting primal weight of the warm strategies -- the default "
                          "||c|| / ||b||, or the geometric mean of the 4 nearest training members' final weights")

@@ -368,7 +368,7 @@ def certify_family(family: RefineryFamily, params, X, Y, kkt_tol: float = 1e-6, 
 
 def solve_warm(family: RefineryFamily, params, predictor=None, opts: PdhgOptions | None = None, batch: int = 1024,
                engine: str = "batch", kkt_tol: float | None = None, work=None, weights=None,
-               warm_max_iterations: int | None = None, single_fallback: int = 0):
+               warm_max_iterations: int | None = None, single_fallback: int = 0, continue_failed: bool = True):
     """Solve from the predictor's starts (and, with engine "multi", the
     starting primal weights `weights`), judge every answer with
     certify_family, and re-solve the members that fail from a cold start
@@ -376,8 +376,11 @@ def solve_warm(family: RefineryFamily, params, predictor=None, opts: PdhgOptions
     below opts.maxIterations, so that a start that leads nowhere falls back
     sooner; the fallback keeps opts.maxIterations.  A fallback of at most
     `single_fallback` members (default none) runs on the single-LP engine,
-    one member at a time with every SM, instead of on `engine`.  Returns
-    (FamilySolve, certification, fallback mask)."""
+    one member at a time with every SM, instead of on `engine`.  With
+    `continue_failed` (the default; engine "multi"), a member that fails
+    first continues from its own final point and primal weight, and only
+    what still fails then starts cold.  Returns (FamilySolve, certification,
+    fallback mask)."""
     opts = opts or PdhgOptions()
     kkt_tol = opts.tolerance if kkt_tol is None else kkt_tol
     starts = predictor.predict(params) if predictor is not None else None
@@ -388,8 +391,24 @@ def solve_warm(family: RefineryFamily, params, predictor=None, opts: PdhgOptions
                        weights=weights)
     cert = certify_family(family, params, res.X, res.Y, kkt_tol=kkt_tol)
     redo = ~cert["certified"]
-    if predictor is not None and redo.any():
-        idx = np.flatnonzero(redo)
+    if predictor is not None and continue_failed and engine == "multi" and redo.any():
+        idx = np.flatnonzero(redo & np.all(np.isfinite(res.X), axis=1) & np.all(np.isfinite(res.Y), axis=1))
+        if len(idx):
+            w = res.weights[idx] if len(res.weights) == len(res.X) else None
+            more = solve_family(family, np.asarray(params)[idx], opts, starts=(res.X[idx], res.Y[idx]), batch=batch,
+                                engine=engine, work=None if work is None else np.asarray(work)[idx], weights=w)
+            c3 = certify_family(family, np.asarray(params)[idx], more.X, more.Y, kkt_tol=kkt_tol)
+            for f in ("status", "relative_kkt", "objective"):
+                getattr(res, f)[idx] = getattr(more, f)
+            res.iterations[idx] += more.iterations
+            res.X[idx], res.Y[idx] = more.X, more.Y
+            res.weights[idx] = more.weights
+            res.seconds += more.seconds
+            res.solve_seconds += more.solve_seconds
+            for k in cert:
+                cert[k][idx] = c3[k]
+    if predictor is not None and (~cert["certified"]).any():
+        idx = np.flatnonzero(~cert["certified"])
         again = solve_family(family, np.asarray(params)[idx], opts, batch=batch,
                              engine="single" if len(idx) <= single_fallback else engine,
                              work=None if work is None else np.asarray(work)[idx])

@@ -98,12 +98,30 @@ def test_warm_cap_and_single_engine_fallback(trained):
     one on the batched engine.  Every answer certified."""
     fam, opts, lw, _, _ = trained
     P = fam.sample(12, 400)
-    got, cert, redo = W.solve_warm(fam, P[:6], lw, opts, engine="multi", warm_max_iterations=1, single_fallback=8)
+    got, cert, redo = W.solve_warm(fam, P[:6], lw, opts, engine="multi", warm_max_iterations=1, single_fallback=8,
+                                   continue_failed=False)
     assert redo.sum() >= 3 and cert["certified"].all()
     single = W.solve_family(fam, P[:6][redo], opts, engine="single")
     assert np.array_equal(got.X[redo], single.X) and np.array_equal(got.Y[redo], single.Y)
     extra = got.iterations[redo] - single.iterations  # the warm attempt's work, counted too
     assert np.all((extra >= 1) & (extra <= 2))
     got12, cert12, redo12 = W.solve_warm(fam, P, lw, opts, engine="multi", warm_max_iterations=1,
-                                         single_fallback=2)
+                                         single_fallback=2, continue_failed=False)
     assert redo12.sum() > 2 and cert12["certified"].all()
+
+
+def test_failed_members_continue_from_their_point(trained):
+    """With continue_failed, members whose one-iteration warm attempt fails
+    continue from that attempt's point and primal weight on the multi-LP
+    engine; every answer certified, and the iterations count both attempts."""
+    fam, opts, lw, _, _ = trained
+    P = fam.sample(6, 500)
+    got, cert, redo = W.solve_warm(fam, P, lw, opts, engine="multi", warm_max_iterations=1, continue_failed=True)
+    assert redo.sum() >= 3 and cert["certified"].all()
+    X0, Y0 = lw.predict(P)
+    first = W.solve_family(fam, P, PdhgOptions(tolerance=opts.tolerance, maxIterations=1), starts=(X0, Y0),
+                           engine="multi")
+    more = W.solve_family(fam, P[redo], opts, starts=(first.X[redo], first.Y[redo]), engine="multi",
+                          weights=first.weights[redo])
+    assert np.array_equal(got.X[redo], more.X) and np.array_equal(got.iterations[redo], first.iterations[redo]
+                                                                    + more.iterations)
