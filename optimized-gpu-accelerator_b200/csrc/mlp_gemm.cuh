@@ -3,12 +3,17 @@
 // accumulation in tensor memory, plus a fused epilogue (bias, ReLU, a 0/1
 // mask from a BF16 array, FP32 and/or BF16 output).
 //
-// One CTA (128 threads) computes a 128 x kBN tile.  The K dimension runs in
-// chunks of 64 through three shared-memory stages: while the tensor core
-// works on chunk c, the threads already fetch chunk c + 2 into the stage
-// chunk c - 1 used (16-byte cp.async copies from global memory when the operand is
-// K-contiguous, element loads otherwise).  Each stage holds A (128 x 64) and
-// B (kBN x 64) in the K-major, non-swizzled canonical layout of the UMMA
+// One CTA (128 threads) computes a 128 x BN tile, BN = 128 or 256 (the wide
+// tile reads each A chunk once for twice the output and is chosen when the
+// grid of wide tiles still fills every SM).  The K dimension runs in chunks
+// of 64 through S shared-memory stages, refilled LAG chunks after the MMAs
+// that read them were issued (BN = 128: S = 3, LAG = 1, two CTAs per SM;
+// BN = 256: S = 4, LAG = 2, one CTA per SM, so that chunk c's MMAs are
+// issued while chunk c - 1's still run): at chunk c the threads fetch chunk
+// c + S - LAG into the stage chunk c - LAG used (16-byte cp.async copies from
+// global memory when the operand is K-contiguous, element loads otherwise).
+// Each stage holds A (128 x 64) and
+// B (BN x 64) in the K-major, non-swizzled canonical layout of the UMMA
 // descriptors -- core matrices of 8 rows x 16 bytes, the two 8-element K
 // halves of a 16-wide slab LBO = 128 B apart, consecutive 8-row groups SBO =
 // 256 B apart.  One elected thread issues four tcgen05.mma (K = 16 each) per
@@ -27,16 +32,24 @@
 namespace b2p {
 
 constexpr int kGemmBM = 128;
-constexpr int kGemmBN = 128;
 constexpr int kGemmBK = 64;
 constexpr int kGemmThreads = 128;
 constexpr unsigned kMbarSpinLimit = 1u << 24;
-constexpr int kGemmStages = 3;
-constexpr int kGemmStageBytes = (kGemmBM + kGemmBN) * kGemmBK * 2;  // A 16 KB + B 16 KB
-// three stages (96 KB): at most two CTAs share an SM (2 x 128 TMEM columns
-// <= 512)
-constexpr int kGemmSmemBytes = 96 * 1024;
-static_assert(kGemmStages * kGemmStageBytes <= kGemmSmemBytes, "stages exceed the shared-memory budget");
+
+// Tile shape: BN output columns (= TMEM columns), S stages of A 16 KB + B
+// BN x 64 x 2 bytes.  BN = 128: three stages (96 KB), at most two CTAs per
+// SM (2 x 128 TMEM columns <= 512).  BN = 256: four stages (192 KB), one CTA
+// per SM.
+template <int BN>
+struct GemmTile {
+  static constexpr int kStages = BN == 256 ? 4 : 3;
+  static constexpr int kLag = BN == 256 ? 2 : 1;  // stage refill lag, in chunks
+  static constexpr int kAhead = kStages - kLag;   // chunks in flight ahead of the MMAs
+  static constexpr int kStageBytes = (kGemmBM + BN) * kGemmBK * 2;
+  static constexpr int kSmemBytes = kStages * kStageBytes;
+  static_assert(BN == 128 || BN == 256, "tile width");
+  static_assert(kSmemBytes <= 200 * 1024, "stages exceed the shared-memory budget");
+};
 
 struct GemmArgs {
   int32_t M, N, K;
@@ -71,7 +84,8 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo_bytes,
   return d;
 }
 
-// Instruction descriptor: kind::f16, BF16 x BF16 -> F32, both K-major, M = 128.
+// Instruction descriptor: kind::f16, BF16 x BF16 -> F32, both K-major, M = 128,
+// N = n (a multiple of 16 up to 256).
 __host__ __device__ constexpr uint32_t umma_idesc_bf16(int n) {
   return (1u << 4)                                   // D format F32
          | (1u << 7)                                 // A format BF16
@@ -139,7 +153,12 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
   return false;
 }
 
-static __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tc(GemmArgs g) {
+template <int BN>
+__global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tc(GemmArgs g) {
+  constexpr int kGemmBN = BN;
+  constexpr int kGemmStages = GemmTile<BN>::kStages;
+  constexpr int kGemmStageBytes = GemmTile<BN>::kStageBytes;
+  constexpr int kLag = GemmTile<BN>::kLag, kAhead = GemmTile<BN>::kAhead;
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t mbar[kGemmStages];
   __shared__ uint32_t tmem_base_sh;
@@ -176,23 +195,24 @@ static __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tc(GemmArgs g
     stage_operand(stage_b(st), g.B, g.sbn, g.sbk, n0, g.N, k0, g.K, kGemmBN, vec_b, tid);
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
-  // prologue: the first kGemmStages - 1 chunks in flight
-  for (int c = 0; c < kGemmStages - 1; ++c)
+  // prologue: the first kAhead chunks in flight
+  for (int c = 0; c < kAhead; ++c)
     if (c < nchunks) fetch(c);
   for (int ch = 0; ch < nchunks; ++ch) {
     const int st = ch % kGemmStages;
-    const int ahead = ch + kGemmStages - 1;  // the chunk fetched in this step
+    const int ahead = ch + kAhead;  // the chunk fetched in this step
     if (ahead < nchunks) {
-      // its stage was read by chunk ch - 1's MMAs: refill it once they are done
+      // its stage was last read by chunk ch - kLag's MMAs: refill it once
+      // they are done (a stage not used yet needs no wait)
       const int nx = ahead % kGemmStages;
-      if (ch >= 1) {
+      if (ch >= kLag) {
         if (!mbar_wait(smem_u32(&mbar[nx]), phase[nx])) failed_sh = 1;
         phase[nx] ^= 1u;
       }
       __syncthreads();
       if (failed_sh) break;
       fetch(ahead);
-      asm volatile("cp.async.wait_group %0;" ::"n"(kGemmStages - 1) : "memory");  // chunk ch has landed
+      asm volatile("cp.async.wait_group %0;" ::"n"(kAhead) : "memory");  // chunk ch has landed
     } else {
       asm volatile("cp.async.wait_group 0;" ::: "memory");
     }

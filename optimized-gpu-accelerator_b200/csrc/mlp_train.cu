@@ -114,21 +114,39 @@ __global__ void k_to_bf16(int64_t n, const float* __restrict__ src, __nv_bfloat1
     dst[i] = __float2bfloat16(src[i]);
 }
 
+int gemm_sms[64] = {};  // SM count per device, set with the attributes
+
 void set_gemm_attributes() {
   static std::once_flag once[64];
   int dev = 0;
   B2P_CUDA(cudaGetDevice(&dev));
   cudaError_t err = cudaSuccess;
   std::call_once(once[dev & 63], [&] {
-    err = cudaFuncSetAttribute(k_gemm_bf16_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmemBytes);
+    err = cudaFuncSetAttribute(k_gemm_bf16_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               GemmTile<128>::kSmemBytes);
+    if (err == cudaSuccess)
+      err = cudaFuncSetAttribute(k_gemm_bf16_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 GemmTile<256>::kSmemBytes);
+    if (err == cudaSuccess) err = cudaDeviceGetAttribute(&gemm_sms[dev & 63], cudaDevAttrMultiProcessorCount, dev);
   });
   B2P_CUDA(err);
 }
 
+// 128 x 256 tiles when they still give every SM a CTA, else 128 x 128
+// (the network's small GEMMs need the wider grid).
 void launch_gemm(const GemmArgs& g, cudaStream_t stream) {
   if (g.M <= 0 || g.N <= 0) return;
-  const dim3 grid((g.M + kGemmBM - 1) / kGemmBM, (g.N + kGemmBN - 1) / kGemmBN);
-  k_gemm_bf16_tc<<<grid, kGemmThreads, kGemmSmemBytes, stream>>>(g);
+  int dev = 0;
+  B2P_CUDA(cudaGetDevice(&dev));
+  const int64_t mt = (g.M + kGemmBM - 1) / kGemmBM;
+  const int sms = gemm_sms[dev & 63];
+  if (sms > 0 && mt * ((g.N + 255) / 256) >= sms) {
+    const dim3 grid(static_cast<unsigned>(mt), (g.N + 255) / 256);
+    k_gemm_bf16_tc<256><<<grid, kGemmThreads, GemmTile<256>::kSmemBytes, stream>>>(g);
+  } else {
+    const dim3 grid(static_cast<unsigned>(mt), (g.N + 127) / 128);
+    k_gemm_bf16_tc<128><<<grid, kGemmThreads, GemmTile<128>::kSmemBytes, stream>>>(g);
+  }
   B2P_CUDA(cudaGetLastError());
 }
 

@@ -24,8 +24,10 @@ def _rand_bf16(shape, seed):
     return torch.randn(shape, generator=g).to(torch.bfloat16).to(DEV)
 
 
+# (2048, 2600, 200) and (2100, 2600, 96) give 176 and 187 tiles of 128 x 256,
+# enough for every SM of a B200, so they run the wide-tile kernel (ragged N and K)
 @pytest.mark.parametrize("m,n,k", [(128, 128, 64), (200, 72, 40), (300, 136, 1000), (1, 8, 16), (513, 257, 200),
-                                   (1024, 512, 512)])
+                                   (1024, 512, 512), (2048, 2600, 200)])
 def test_gemm_matches_fp32_matmul(m, n, k):
     a = _rand_bf16((m, k), 1)
     b = _rand_bf16((k, n), 2)
@@ -37,8 +39,8 @@ def test_gemm_matches_fp32_matmul(m, n, k):
     assert torch.all((c - want).abs() <= 1e-5 * scale + 1e-30), (c - want).abs().max().item()
 
 
-def test_gemm_transposed_operands_and_epilogue():
-    m, n, k = 260, 136, 96
+@pytest.mark.parametrize("m,n,k", [(260, 136, 96), (2100, 2600, 96)])
+def test_gemm_transposed_operands_and_epilogue(m, n, k):
     at = _rand_bf16((k, m), 3)  # A stored k-major: A(m, k) = at[k, m]
     bt = _rand_bf16((n, k), 4)  # B stored n-major: B(k, n) = bt[n, k]
     bias = torch.randn(n, generator=torch.Generator().manual_seed(5)).float().to(DEV)
