@@ -25,6 +25,7 @@
 // a timeout the kernel records an error, frees its TMEM and returns.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (the type only; maps are encoded through the runtime's driver entry point)
 #include <cuda_bf16.h>
 
 #include <cstdint>
@@ -153,6 +154,67 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
   return false;
 }
 
+// Epilogue of one 128 x BN tile: thread = tile row (TMEM lane), 8 columns
+// per tcgen05.ld; alpha, bias, ReLU and the 0/1 mask applied in FP32; a
+// thread's 8 consecutive outputs go out as 16- or 32-byte vector stores when
+// the row stride and base allow it (one sector per store instead of eight
+// scattered ones).
+template <int BN>
+__device__ __forceinline__ void gemm_epilogue(const GemmArgs& g, uint32_t tmem, int m0, int n0, int warp, int lane) {
+  constexpr int kGemmBN = BN;
+  const int row = warp * 32 + lane;
+  const int gm = m0 + row;
+  const bool vec_f = g.cf && g.ldcf % 4 == 0 && (reinterpret_cast<uintptr_t>(g.cf) & 15) == 0;
+  const bool vec_b = g.cb && g.ldcb % 8 == 0 && (reinterpret_cast<uintptr_t>(g.cb) & 15) == 0;
+  for (int c = 0; c < kGemmBN; c += 8) {
+    uint32_t r[8];
+    const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c);
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    if (gm >= g.M || n0 + c >= g.N) continue;
+    float v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int gn = n0 + c + q;
+      float t = __uint_as_float(r[q]) * g.alpha;
+      if (gn < g.N) {
+        if (g.bias) t += g.bias[gn];
+        if (g.relu) t = t > 0.0f ? t : 0.0f;
+        if (g.mask && !(__bfloat162float(g.mask[gm * g.ldm + gn]) > 0.0f)) t = 0.0f;
+      }
+      v[q] = t;
+    }
+    const bool full = n0 + c + 8 <= g.N;
+    if (g.cf) {
+      float* dst = g.cf + gm * g.ldcf + n0 + c;
+      if (vec_f && full) {
+        reinterpret_cast<float4*>(dst)[0] = make_float4(v[0], v[1], v[2], v[3]);
+        reinterpret_cast<float4*>(dst)[1] = make_float4(v[4], v[5], v[6], v[7]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (n0 + c + q < g.N) dst[q] = v[q];
+      }
+    }
+    if (g.cb) {
+      __nv_bfloat16* dst = g.cb + gm * g.ldcb + n0 + c;
+      if (vec_b && full) {
+        __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) h[q] = __float2bfloat16(v[q]);
+        *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(h);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (n0 + c + q < g.N) dst[q] = __float2bfloat16(v[q]);
+      }
+    }
+  }
+}
+
 template <int BN>
 __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tc(GemmArgs g) {
   constexpr int kGemmBN = BN;
@@ -248,61 +310,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tc(GemmArgs g) {
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (!failed_sh) {
-    // epilogue: thread = tile row (TMEM lane), 8 columns per tcgen05.ld; a
-    // thread's 8 consecutive outputs go out as 16- or 32-byte vector stores
-    // when the row stride and base allow it (one sector per store instead of
-    // eight scattered ones)
-    const int row = warp * 32 + lane;
-    const int gm = m0 + row;
-    const bool vec_f = g.cf && g.ldcf % 4 == 0 && (reinterpret_cast<uintptr_t>(g.cf) & 15) == 0;
-    const bool vec_b = g.cb && g.ldcb % 8 == 0 && (reinterpret_cast<uintptr_t>(g.cb) & 15) == 0;
-    for (int c = 0; c < kGemmBN; c += 8) {
-      uint32_t r[8];
-      const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c);
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-          : "r"(taddr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (gm >= g.M || n0 + c >= g.N) continue;
-      float v[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const int gn = n0 + c + q;
-        float t = __uint_as_float(r[q]) * g.alpha;
-        if (gn < g.N) {
-          if (g.bias) t += g.bias[gn];
-          if (g.relu) t = t > 0.0f ? t : 0.0f;
-          if (g.mask && !(__bfloat162float(g.mask[gm * g.ldm + gn]) > 0.0f)) t = 0.0f;
-        }
-        v[q] = t;
-      }
-      const bool full = n0 + c + 8 <= g.N;
-      if (g.cf) {
-        float* dst = g.cf + gm * g.ldcf + n0 + c;
-        if (vec_f && full) {
-          reinterpret_cast<float4*>(dst)[0] = make_float4(v[0], v[1], v[2], v[3]);
-          reinterpret_cast<float4*>(dst)[1] = make_float4(v[4], v[5], v[6], v[7]);
-        } else {
-#pragma unroll
-          for (int q = 0; q < 8; ++q)
-            if (n0 + c + q < g.N) dst[q] = v[q];
-        }
-      }
-      if (g.cb) {
-        __nv_bfloat16* dst = g.cb + gm * g.ldcb + n0 + c;
-        if (vec_b && full) {
-          __align__(16) __nv_bfloat16 h[8];
-#pragma unroll
-          for (int q = 0; q < 8; ++q) h[q] = __float2bfloat16(v[q]);
-          *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(h);
-        } else {
-#pragma unroll
-          for (int q = 0; q < 8; ++q)
-            if (n0 + c + q < g.N) dst[q] = __float2bfloat16(v[q]);
-        }
-      }
-    }
+    gemm_epilogue<kGemmBN>(g, tmem, m0, n0, warp, lane);
   } else if (tid == 0) {
     atomicExch(g.error, 1);
   }
@@ -310,6 +318,180 @@ __global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tc(GemmArgs g) {
   __syncthreads();
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kGemmBN) : "memory");
+}
+
+
+// ---------------------------------------------------------------------------
+// TMA form, for operands whose K dimension is contiguous (A row-major M x K,
+// B stored N x K) with 16-byte aligned rows.  The same 128 x BN tiles and
+// stage counts, but the operands are brought in by the tensor memory
+// accelerator (cp.async.bulk.tensor.2d, one 64 x rows box per operand and
+// chunk, zero-filled past the edges) into the 128-byte-swizzled K-major
+// layout, and the CTA's roles are split: warp 0 issues the copies, warp 1
+// the MMAs (one lane each, the other lanes following in step so that no lane
+// spins beside them), and all four warps run the epilogue.  Each stage
+// has a "full" mbarrier (the copies' bytes arrived) and an "empty" one (the
+// MMAs that read it completed); the producer refills a stage once it is
+// empty, so up to S chunks are in flight while the tensor core works.  Every
+// wait is bounded: on a timeout the kernel records an error, waits (bounded)
+// for the copies it issued, frees its TMEM and returns.
+
+template <int BN>
+struct GemmTmaTile {
+  static constexpr int kStages = BN == 256 ? 4 : 3;
+  static constexpr int kABytes = kGemmBM * kGemmBK * 2;  // 16 KB
+  static constexpr int kBBytes = BN * kGemmBK * 2;
+  static constexpr int kStageBytes = kABytes + kBBytes;
+  // + 1 KB so that the stages can start on a 1,024-byte boundary (the
+  // period of the 128-byte swizzle)
+  static constexpr int kSmemBytes = kStages * kStageBytes + 1024;
+};
+
+// UMMA shared-memory descriptor, K-major, 128-byte swizzle: rows of 64 BF16
+// (128 bytes) as the copies wrote them, 8-row groups SBO = 1,024 bytes apart,
+// LBO unused (1).  addr advances by 32 bytes per K = 16 step inside the
+// 128-byte row; the swizzle is applied to the absolute address bits.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t addr) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((addr >> 4) & 0x3FFF);
+  d |= static_cast<uint64_t>(1) << 16;            // LBO (unused for swizzled K-major)
+  d |= static_cast<uint64_t>(1024 >> 4) << 32;    // SBO
+  d |= static_cast<uint64_t>(1) << 46;            // descriptor version (Blackwell)
+  d |= static_cast<uint64_t>(2) << 61;            // layout type SWIZZLE_128B
+  return d;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+template <int BN>
+__global__ void __launch_bounds__(kGemmThreads) k_gemm_bf16_tma(const __grid_constant__ CUtensorMap map_a,
+                                                                 const __grid_constant__ CUtensorMap map_b,
+                                                                 GemmArgs g) {
+  using Tile = GemmTmaTile<BN>;
+  constexpr int S = Tile::kStages;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t full[S], empty[S], done;
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ int failed_sh, issued_sh, consumed_sh;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * kGemmBM, n0 = blockIdx.y * BN;
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;  // stage 0, 1,024-byte aligned
+  const int nchunks = (g.K + kGemmBK - 1) / kGemmBK;
+
+  if (tid == 0) {
+    for (int st = 0; st < S; ++st) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[st])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[st])) : "memory");
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&done)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    failed_sh = 0;
+    issued_sh = 0;
+    consumed_sh = 0;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                 "r"(BN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_base_sh;
+
+  if (warp == 0) {
+    // producer warp (lane 0 issues): chunk ch into stage ch % S once the MMAs
+    // of chunk ch - S are done
+    if (lane == 0) {
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_a)) : "memory");
+      asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&map_b)) : "memory");
+    }
+    int ch = 0;
+    for (; ch < nchunks; ++ch) {
+      const int st = ch % S;
+      bool ok = true;
+      if (ch >= S) ok = mbar_wait(smem_u32(&empty[st]), static_cast<uint32_t>((ch / S - 1) & 1));
+      if (!__all_sync(0xffffffffu, ok) || *reinterpret_cast<volatile int*>(&failed_sh)) {
+        if (lane == 0) failed_sh = 1;
+        break;
+      }
+      if (lane == 0) {
+        const uint32_t sa = base + st * Tile::kStageBytes, sb = sa + Tile::kABytes;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&full[st])),
+                     "r"(Tile::kStageBytes)
+                     : "memory");
+        tma_load_2d(sa, &map_a, ch * kGemmBK, m0, smem_u32(&full[st]));
+        tma_load_2d(sb, &map_b, ch * kGemmBK, n0, smem_u32(&full[st]));
+      }
+      __syncwarp();
+    }
+    if (lane == 0) issued_sh = ch;
+  } else if (warp == 1) {
+    // MMA warp (lane 0 issues): four K = 16 steps per chunk, then commit the
+    // stage back
+    const uint32_t idesc = umma_idesc_bf16(BN);
+    int ch = 0;
+    for (; ch < nchunks; ++ch) {
+      const int st = ch % S;
+      const bool ok = mbar_wait(smem_u32(&full[st]), static_cast<uint32_t>((ch / S) & 1));
+      if (!__all_sync(0xffffffffu, ok)) {
+        if (lane == 0) failed_sh = 1;
+        break;
+      }
+      if (lane == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t sa = base + st * Tile::kStageBytes, sb = sa + Tile::kABytes;
+#pragma unroll
+        for (int s = 0; s < kGemmBK / 16; ++s) {
+          const uint64_t da = umma_desc_sw128(sa + s * 32), db = umma_desc_sw128(sb + s * 32);
+          const uint32_t acc = (ch > 0 || s > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n\t.reg .pred p;\n\t"
+              "setp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+              :
+              : "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+              : "memory");
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(&empty[st]))
+                     : "memory");
+      }
+      __syncwarp();
+    }
+    if (lane == 0) {
+      consumed_sh = ch;
+      // tracks every MMA issued before it
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&done))
+                   : "memory");
+    }
+    __syncwarp();
+  }
+  if (!mbar_wait(smem_u32(&done), 0u)) failed_sh = 1;
+  __syncthreads();
+  __syncwarp();  // the producer and MMA lanes rejoin their warps before tcgen05.ld
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (!failed_sh) {
+    gemm_epilogue<BN>(g, tmem, m0, n0, warp, lane);
+  } else if (tid == 0) {
+    atomicExch(g.error, 1);
+    // copies issued but not consumed still write into shared memory: wait for them
+    for (int ch = consumed_sh; ch < issued_sh; ++ch)
+      mbar_wait(smem_u32(&full[ch % S]), static_cast<uint32_t>((ch / S) & 1));
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
 }
 
 }  // namespace b2p

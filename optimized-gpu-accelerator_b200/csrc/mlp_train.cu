@@ -4,6 +4,7 @@
 // deterministic for a given seed.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
 
 #include <algorithm>
 #include <cmath>
@@ -116,6 +117,45 @@ __global__ void k_to_bf16(int64_t n, const float* __restrict__ src, __nv_bfloat1
 
 int gemm_sms[64] = {};  // SM count per device, set with the attributes
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library); NULL if the driver does not offer it.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// Tensor map of a K-contiguous operand X(r, k) = X[r * sr + k], r < R,
+// k < K: 64 x box_rows boxes, 128-byte swizzle, zeros past the edges.
+bool encode_operand(CUtensorMap* map, const __nv_bfloat16* X, int64_t sr, int R, int K, int box_rows) {
+  const auto fn = tensor_map_encoder();
+  if (!fn) return false;
+  const cuuint64_t dims[2] = {static_cast<cuuint64_t>(K), static_cast<cuuint64_t>(R)};
+  const cuuint64_t strides[1] = {static_cast<cuuint64_t>(sr) * 2};
+  const cuuint32_t box[2] = {static_cast<cuuint32_t>(kGemmBK), static_cast<cuuint32_t>(box_rows)};
+  const cuuint32_t elem[2] = {1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16*>(X), dims, strides, box, elem,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The TMA form applies when both operands are K-contiguous with rows of a
+// multiple of 16 bytes on a 16-byte aligned base (the tensor map's rules).
+bool gemm_tma_ok(const GemmArgs& g) {
+  auto ok = [&](const void* X, int64_t sr, int64_t sk) {
+    return sk == 1 && sr >= g.K && sr % 8 == 0 && sr < (int64_t{1} << 38) &&
+           (reinterpret_cast<uintptr_t>(X) & 15) == 0;
+  };
+  return g.K > 0 && ok(g.A, g.sam, g.sak) && ok(g.B, g.sbn, g.sbk);
+}
+
 void set_gemm_attributes() {
   static std::once_flag once[64];
   int dev = 0;
@@ -127,20 +167,42 @@ void set_gemm_attributes() {
     if (err == cudaSuccess)
       err = cudaFuncSetAttribute(k_gemm_bf16_tc<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  GemmTile<256>::kSmemBytes);
+    if (err == cudaSuccess)
+      err = cudaFuncSetAttribute(k_gemm_bf16_tma<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 GemmTmaTile<128>::kSmemBytes);
+    if (err == cudaSuccess)
+      err = cudaFuncSetAttribute(k_gemm_bf16_tma<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 GemmTmaTile<256>::kSmemBytes);
     if (err == cudaSuccess) err = cudaDeviceGetAttribute(&gemm_sms[dev & 63], cudaDevAttrMultiProcessorCount, dev);
   });
   B2P_CUDA(err);
 }
 
 // 128 x 256 tiles when they still give every SM a CTA, else 128 x 128
-// (the network's small GEMMs need the wider grid).
+// (the network's small GEMMs need the wider grid); the TMA form when both
+// operands are K-contiguous, the cp.async form otherwise.
 void launch_gemm(const GemmArgs& g, cudaStream_t stream) {
   if (g.M <= 0 || g.N <= 0) return;
   int dev = 0;
   B2P_CUDA(cudaGetDevice(&dev));
   const int64_t mt = (g.M + kGemmBM - 1) / kGemmBM;
   const int sms = gemm_sms[dev & 63];
-  if (sms > 0 && mt * ((g.N + 255) / 256) >= sms) {
+  const bool wide = sms > 0 && mt * ((g.N + 255) / 256) >= sms;
+  if (sms > 0 && gemm_tma_ok(g)) {
+    CUtensorMap ma, mb;
+    if (encode_operand(&ma, g.A, g.sam, g.M, g.K, kGemmBM) && encode_operand(&mb, g.B, g.sbn, g.N, g.K, wide ? 256 : 128)) {
+      if (wide) {
+        const dim3 grid(static_cast<unsigned>(mt), (g.N + 255) / 256);
+        k_gemm_bf16_tma<256><<<grid, kGemmThreads, GemmTmaTile<256>::kSmemBytes, stream>>>(ma, mb, g);
+      } else {
+        const dim3 grid(static_cast<unsigned>(mt), (g.N + 127) / 128);
+        k_gemm_bf16_tma<128><<<grid, kGemmThreads, GemmTmaTile<128>::kSmemBytes, stream>>>(ma, mb, g);
+      }
+      B2P_CUDA(cudaGetLastError());
+      return;
+    }
+  }
+  if (wide) {
     const dim3 grid(static_cast<unsigned>(mt), (g.N + 255) / 256);
     k_gemm_bf16_tc<256><<<grid, kGemmThreads, GemmTile<256>::kSmemBytes, stream>>>(g);
   } else {

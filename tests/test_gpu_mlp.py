@@ -58,6 +58,29 @@ def test_gemm_transposed_operands_and_epilogue(m, n, k):
     assert (cf[mask.float() <= 0] == 0).all()
 
 
+# A row-major and B stored n x k: both operands K-contiguous with 16-byte
+# rows, so the kernel's TMA form runs (128-byte-swizzled tiles brought in by
+# the tensor memory accelerator, zero-filled past ragged edges); the last
+# shape gives enough 128 x 256 tiles for every SM (the wide-tile TMA form)
+@pytest.mark.parametrize("m,n,k", [(128, 128, 64), (200, 72, 40), (513, 257, 200), (1, 8, 16), (300, 136, 1000),
+                                   (1024, 512, 512), (2048, 2600, 200)])
+def test_gemm_tma_form_k_contiguous(m, n, k):
+    a = _rand_bf16((m, k), 7)
+    bt = _rand_bf16((n, k), 8)  # B(k, n) = bt[n, k]
+    bias = torch.randn(n, generator=torch.Generator().manual_seed(9)).float().to(DEV)
+    mask = _rand_bf16((m, n), 10)
+    cf = torch.empty((m, n), dtype=torch.float32, device=DEV)
+    cb = torch.empty((m, n), dtype=torch.bfloat16, device=DEV)
+    gemm_bf16(a, bt, alpha=0.5, bias=bias, relu=True, mask=mask, out_f32=cf, out_bf16=cb, b_strides=(1, k), m=m, n=n,
+              k=k)
+    torch.cuda.synchronize()
+    want = torch.relu(0.5 * (a.float() @ bt.float().t()) + bias)
+    want = torch.where(mask.float() > 0, want, torch.zeros_like(want))
+    scale = 0.5 * (a.float().abs() @ bt.float().t().abs()) + bias.abs()
+    assert torch.all((cf - want).abs() <= 1e-5 * scale + 1e-30), (cf - want).abs().max().item()
+    assert torch.equal(cb, cf.to(torch.bfloat16))
+
+
 def test_gemm_rejects_bad_arguments():
     lib = _lib.load()
     assert lib.b2p_mlp_gemm_bf16(-1, 8, 8, None, 0, 0, None, 0, 0, 1.0, None, 0, None, 0, None, 0, None, 0,
