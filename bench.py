@@ -1240,8 +1240,8 @@ def measured_bf16_peak():
 
 
 def run_gemm(args, rank, world):
-    """--workload gemm: the warm-start network's tcgen05 BF16 GEMM (k_gemm_bf16_tc)
-    timed with CUDA events (b2p_mlp_gemm_bf16_time) at the network's shapes --
+    """--workload gemm: the warm-start network's tcgen05 BF16 GEMM (its TMA form,
+    k_gemm_bf16_tma: both operands here are K-contiguous) timed with CUDA events (b2p_mlp_gemm_bf16_time) at the network's shapes --
     batch 1,024 through 512-wide hidden layers, the output layer, a weight
     gradient (K = batch), the input layer -- and two larger ones, as TFLOP/s
     of 2 M N K against the bf16 tensor peak."""
@@ -1273,7 +1273,7 @@ def run_gemm(args, rank, world):
                      "max_rel_err_vs_fp32_matmul": err})
     line = {"metric": "tcgen05 BF16 GEMM TFLOP/s at the warm-start network's shapes", "workload": "gemm",
             "unit": "TFLOP/s", "value": max(r["tflops"] for r in rows), "higher_is_better": True,
-            "peak": peak, "peak_source": kind, "kernel": "k_gemm_bf16_tc (128x128 tile, 2 cp.async stages)",
+            "peak": peak, "peak_source": kind, "kernel": "k_gemm_bf16_tma (TMA copies into 128B-swizzled stages, producer and MMA warps; 128x128, or 128x256 tiles when they fill every SM)",
             "shapes": rows}
     print(json.dumps(line))
     return 0
