@@ -77,7 +77,11 @@ int b2p_mlp_train(b2p_mlp* net, const float* x, const float* target, int64_t cou
  * A[m * sam + k * sak], B(k, n) = B[k * sbk + n * sbn]; the epilogue adds
  * bias[n] (NULL = none), applies ReLU when relu != 0, zeroes C(m, n) where
  * mask[m * ldm + n] <= 0 (NULL = none), and stores FP32 to cf (ldcf) and/or
- * BF16 to cb (ldcb).  Synchronous on the given stream (NULL = default). */
+ * BF16 to cb (ldcb).  Synchronous on the given stream (NULL = default).
+ * When both operands are K-contiguous (sak == 1, sbk == 1) with row strides
+ * that are multiples of 8 elements and 16-byte aligned bases, the tiles are
+ * brought in by TMA; otherwise by the threads' cp.async copies.  Both forms
+ * issue the same tensor-core instructions in the same K order. */
 int b2p_mlp_gemm_bf16(int32_t M, int32_t N, int32_t K, const uint16_t* A, int64_t sam, int64_t sak,
                       const uint16_t* B, int64_t sbk, int64_t sbn, float alpha, const float* bias, int32_t relu,
                       const uint16_t* mask, int64_t ldm, float* cf, int64_t ldcf, uint16_t* cb, int64_t ldcb,
