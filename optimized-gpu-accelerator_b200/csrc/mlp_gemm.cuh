@@ -12,8 +12,8 @@
 // issued while chunk c - 1's still run): at chunk c the threads fetch chunk
 // c + S - LAG into the stage chunk c - LAG used (16-byte cp.async copies from
 // global memory when the operand is K-contiguous, element loads otherwise).
-// Each stage holds A (128 x 64) and
-// B (BN x 64) in the K-major, non-swizzled canonical layout of the UMMA
+// Each stage holds A (128 x 64) and B (BN x 64) in the K-major, non-swizzled
+// canonical layout of the UMMA
 // descriptors -- core matrices of 8 rows x 16 bytes, the two 8-element K
 // halves of a 16-wide slab LBO = 128 B apart, consecutive 8-row groups SBO =
 // 256 B apart.  One elected thread issues four tcgen05.mma (K = 16 each) per
@@ -23,6 +23,10 @@
 // TMEM lanes 32w..32w+31 = tile rows).  A and B are read through element
 // strides, so either operand may be used transposed.  Waits are bounded: on
 // a timeout the kernel records an error, frees its TMEM and returns.
+//
+// When both operands are K-contiguous, the TMA form at the end of this file
+// (k_gemm_bf16_tma) replaces the threads' copies with tensor-map copies into
+// 128-byte-swizzled stages and splits the CTA into producer and MMA warps.
 #pragma once
 
 #include <cuda.h>  // CUtensorMap (the type only; maps are encoded through the runtime's driver entry point)
